@@ -1,0 +1,370 @@
+"""Benchmark: path-samples/s of the spectral transport path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+                    [--workload c2|c1|c3]
+
+A step is one full frame of the workload: every pixel's `spp` path-samples traced,
+folded in sample order and added into the film.  Step i renders the absolute sample
+range [i*spp, (i+1)*spp) (progressive accumulation, as the reference does), so no
+step repeats another's work.  Default workload (c2): the 57-facet round brilliant
+(table 57%, crown 34.5 deg, pavilion 40.75 deg, 16 girdle planes), diamond
+Sellmeier, max depth 32, camera Camera::new(0.35, 0.28, 5.0, 18.0), 1920x1080,
+256 spp, a seeded 2048x1024 lat-long map of 12 Gaussian light blobs on black.
+
+Prints ONE JSON line (rank 0):
+  value   whole-job path-samples/s with the scene resident in HBM (device-event timed,
+          max over ranks, L2 flushed by a 256 MiB write between steps);
+  e2e     the same metric through the reference-facing C-ABI call gr_accumulate with
+          host buffers (host->device upload of scene + film and the film readback
+          inside the timed region);
+  roofline  FP32 bound of the dominant kernel (k_trace_persistent): algorithmic
+          flops from the event-tallied FLOP model / its event-timed duration, against
+          the FP32 FMA throughput measured on this device;
+  cpu_baseline  the C++ restatement of the reference CPU tracer on this host's cores.
+With --impl reference the same metric is measured for the reference CPU tracer
+(restated in C++: the reference is Rust and no Rust toolchain exists here).
+For N > 1 (torchrun) ranks render disjoint absolute sample ranges of the same frame
+(weak scaling: each rank does one full frame per step; no data-path collective).
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+import numpy as np  # noqa: E402
+
+WORKLOADS = {
+    "c1": dict(width=256, height=256, spp=64, max_bounces=32, env="uniform", stone="rb57"),
+    "c2": dict(width=1920, height=1080, spp=256, max_bounces=32, env="latlong", stone="rb57"),
+    "c3": dict(width=1024, height=1024, spp=1024, max_bounces=64, env="studio", stone="em49"),
+}
+
+
+def make_scene(name: str):
+    from gemray_studio_b200 import abi, scene as S
+    w = WORKLOADS[name]
+    planes = S.round_brilliant_57() if w["stone"] == "rb57" else S.emerald_cut_49()
+    env_mode = {"uniform": abi.GR_ENV_UNIFORM, "latlong": abi.GR_ENV_LATLONG, "studio": abi.GR_ENV_STUDIO}[w["env"]]
+    latlong = S.gaussian_blob_latlong(2048, 1024, 12, seed=0) if w["env"] == "latlong" else None
+    mat = S.builtin_material("Diamond") if w["stone"] == "rb57" else S.builtin_material("Emerald")
+    sc = S.Scene(width=w["width"], height=w["height"], planes=planes, material=mat, cam=S.camera(0.35, 0.28, 5.0, 18.0),
+                 max_bounces=w["max_bounces"], env_mode=env_mode, latlong=latlong, uniform_rgb=(1.0, 1.0, 1.0))
+    return sc, w
+
+
+def workload_config(name: str, w: dict, parallelism: str) -> dict:
+    stone = {"rb57": "round brilliant, 57 facets + 16 girdle planes (table 57%, crown 34.5 deg, pavilion 40.75 deg)",
+             "em49": "step-cut emerald, 49 planes"}[w["stone"]]
+    return {"workload": f"{name}: {stone}, {w['width']}x{w['height']}, {w['spp']} spp, max depth {w['max_bounces']}, "
+                        f"{w['env']} environment",
+            "width": w["width"], "height": w["height"], "spp": w["spp"], "max_bounces": w["max_bounces"],
+            "environment": w["env"], "material": "Diamond" if w["stone"] == "rb57" else "Emerald",
+            "path_samples_per_step": w["width"] * w["height"] * w["spp"], "parallelism": parallelism,
+            "l2": "flushed between steps (256 MiB device write)"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while running."""
+
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
+             "clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.gpu), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_baseline(sc, w: dict, seconds_target: float = 15.0) -> dict:
+    """The oracle (C++ restatement of the reference CPU tracer) on this host's cores,
+    over a bounded row subset of the same frame and sample budget."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_lib
+    oracle_lib.build_oracle()
+    L = oracle_lib.lib()
+    threads = os.cpu_count() or 1
+    n = sc.width * sc.height
+    acc = np.zeros((n, 3), np.float32)
+    cs = sc.c_scene()
+    up = C.POINTER(C.c_uint32)
+    # calibrate on 2 rows, then size the sample to ~seconds_target
+    rows = np.array([sc.height // 2, sc.height // 2 + 1], np.uint32)
+    t0 = time.perf_counter()
+    L.gro_accumulate_rows(C.byref(cs), rows.ctypes.data_as(up), rows.size, 0, w["spp"],
+                          acc.ctypes.data_as(C.POINTER(C.c_float)), threads)
+    t_probe = time.perf_counter() - t0
+    per_row = max(t_probe / 2, 1e-4)
+    n_rows = int(max(2, min(sc.height, seconds_target / per_row)))
+    rows = np.linspace(0, sc.height - 1, n_rows).astype(np.uint32)
+    t0 = time.perf_counter()
+    L.gro_accumulate_rows(C.byref(cs), rows.ctypes.data_as(up), rows.size, 0, w["spp"],
+                          acc.ctypes.data_as(C.POINTER(C.c_float)), threads)
+    dt = time.perf_counter() - t0
+    samples = rows.size * sc.width * w["spp"]
+    return {"value": samples / dt, "unit": "path-samples/s", "cores": threads, "kind": "port",
+            "sample": f"{rows.size} evenly spaced rows of the frame x {sc.width} px x {w['spp']} spp "
+                      f"({samples} path-samples, {dt:.1f} s)"}
+
+
+def run_reference(args):
+    world, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return
+    sc, w = make_scene(args.workload)
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_lib
+    oracle_lib.build_oracle()
+    L = oracle_lib.lib()
+    threads = os.cpu_count() or 1
+    cs = sc.c_scene()
+    up = C.POINTER(C.c_uint32)
+    acc = np.zeros((sc.width * sc.height, 3), np.float32)
+    # a bounded sample per step: evenly spaced rows, sized to ~6 s of CPU work
+    rows = np.array([sc.height // 2], np.uint32)
+    t0 = time.perf_counter()
+    L.gro_accumulate_rows(C.byref(cs), rows.ctypes.data_as(up), 1, 0, w["spp"], acc.ctypes.data_as(C.POINTER(C.c_float)),
+                          threads)
+    per_row = max(time.perf_counter() - t0, 1e-4)
+    n_rows = int(max(1, min(sc.height, 6.0 / per_row)))
+    rows = np.linspace(0, sc.height - 1, n_rows).astype(np.uint32)
+    for i in range(args.warmup):
+        L.gro_accumulate_rows(C.byref(cs), rows.ctypes.data_as(up), rows.size, i * w["spp"], w["spp"],
+                              acc.ctypes.data_as(C.POINTER(C.c_float)), threads)
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        L.gro_accumulate_rows(C.byref(cs), rows.ctypes.data_as(up), rows.size, (args.warmup + i) * w["spp"], w["spp"],
+                              acc.ctypes.data_as(C.POINTER(C.c_float)), threads)
+    dt = time.perf_counter() - t0
+    samples = args.steps * rows.size * sc.width * w["spp"]
+    value = samples / dt
+    sample = f"{rows.size} evenly spaced rows x {sc.width} px x {w['spp']} spp per step"
+    print(json.dumps({
+        "impl": "reference", "metric": "path-samples/s", "value": value, "unit": "path-samples/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(args.workload, w, f"cpu x{threads} threads"),
+        "cpu_baseline": {"value": value, "unit": "path-samples/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "path-samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "reference CPU tracer restated in C++ (oracle/): the reference is Rust and no Rust toolchain is "
+                "available; its own GPU path runs through wgpu/Vulkan, unavailable on this box",
+    }), flush=True)
+
+
+def run_engine(args):
+    world, rank, local = dist_setup()
+    import torch
+
+    from gemray_studio_b200 import GpuFrameRenderer, abi, build, flop_model
+    build.build()
+    torch.cuda.set_device(local)
+    sc, w = make_scene(args.workload)
+    r = GpuFrameRenderer(device=local)
+    lib, ctx = r.lib, r.ctx
+    stream_ptr = lib.gr_stream(ctx)
+    stream = torch.cuda.ExternalStream(stream_ptr)
+    spp = w["spp"]
+    n_px = sc.width * sc.height
+    samples_per_step = n_px * spp
+
+    peak = C.c_double()
+    assert lib.gr_probe_fp32_peak(ctx, C.byref(peak)) == abi.GR_OK
+    fp32_peak = peak.value
+
+    # event tallies of one full frame (instrumented variant, untimed) -> algorithmic flops
+    counts = (C.c_uint64 * abi.GR_EVENT_COUNT)()
+    assert lib.gr_event_counts(ctx, C.byref(sc.c_scene()), 0, n_px, 0, spp, counts, abi.GR_EVENT_COUNT) == abi.GR_OK
+    tallies = {n: int(counts[i]) for i, n in enumerate(abi.EVENT_NAMES)}
+    n_bands = int(sc.material.o_ray_band_count) if tallies["absorb"] else 0
+    model = flop_model.evaluate(tallies, sc.planes.shape[0], sc.env_mode, n_bands)
+
+    sid = C.c_uint64()
+    assert lib.gr_scene_upload(ctx, C.byref(sc.c_scene()), C.byref(sid)) == abi.GR_OK
+    with torch.cuda.stream(stream):
+        film = torch.zeros((n_px, 3), dtype=torch.float32, device="cuda")
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    base = rank * (args.warmup + args.steps) * spp  # disjoint absolute sample ranges per rank
+
+    def step(i):
+        st = lib.gr_render_resident(ctx, sid.value, base + i * spp, spp, C.c_void_p(film.data_ptr()),
+                                    C.c_void_p(stream_ptr))
+        assert st == abi.GR_OK, lib.gr_last_error_string()
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    barrier(world)
+    lib.gr_timing_enable(ctx, 1)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        barrier(world)
+        for i in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(i & 0xFF)
+                evs[i][0].record(stream)
+            step(args.warmup + i)
+            with torch.cuda.stream(stream):
+                evs[i][1].record(stream)
+        torch.cuda.synchronize()
+        barrier(world)
+    step_ms = sum(a.elapsed_time(b) for a, b in evs)
+    tr, fo, ntr, nfo = C.c_double(), C.c_double(), C.c_uint64(), C.c_uint64()
+    lib.gr_timing_read(ctx, C.byref(tr), C.byref(fo), C.byref(ntr), C.byref(nfo))
+    lib.gr_timing_enable(ctx, 0)
+    step_ms_max = max_over_ranks(step_ms, world)
+    value = world * args.steps * samples_per_step / (step_ms_max * 1e-3)
+
+    # e2e through the C-ABI call with host buffers (upload + readback in the timed region)
+    host_acc = np.zeros((n_px, 3), np.float32)
+    r.accumulate(sc, base, spp, host_acc)  # warm
+    barrier(world)
+    e_evs = []
+    for i in range(args.steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        r.accumulate(sc, base + (args.warmup + i) * spp, spp, host_acc)
+        b.record(stream)
+        e_evs.append((a, b))
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in e_evs), world)
+    e2e_value = world * args.steps * samples_per_step / (e2e_ms * 1e-3)
+    map_bytes = 0 if sc.latlong is None else sc.latlong.nbytes
+    h2d = n_px * 12 + sc.planes.nbytes + C.sizeof(abi.gr_material) + map_bytes
+    d2h = n_px * 12
+
+    trace_ms_per_launch = tr.value / max(1, ntr.value)
+    frames = args.steps
+    flops_per_frame = model.flops_per_sample * samples_per_step
+    achieved = flops_per_frame * frames / (tr.value * 1e-3) / 1e12
+    clk = clocks.summary()
+
+    lib.gr_scene_release(ctx, sid.value)
+    if rank == 0:
+        out = {
+            "metric": "path-samples/s", "value": value, "unit": "path-samples/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms_max / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": workload_config(args.workload, w, f"sample-range shards x{world}" if world > 1 else "single GPU"),
+            "e2e": {"value": e2e_value, "unit": "path-samples/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "roofline": {"bound": "fp32", "kernel": "k_trace_persistent", "achieved": achieved, "peak": fp32_peak,
+                         "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
+                         "peak_source": "measured on this device by gr_probe_fp32_peak (8 independent FFMA chains)",
+                         "flops_per_sample": model.flops_per_sample,
+                         "sfu_ops_per_sample": model.sfu / max(1, model.paths),
+                         "kernel_ms_per_step": tr.value / frames, "fold_ms_per_step": fo.value / frames,
+                         "launches_per_step": (ntr.value + nfo.value) / frames},
+            "events_per_sample": {k: v / max(1, tallies["paths"]) for k, v in tallies.items() if k != "paths"},
+            "gpu_launches": int(ntr.value + nfo.value + args.steps),  # + the L2 flush fills
+            "clocks": clk,
+            "device": r.adapter_label(),
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            out["cpu_baseline"] = cpu_baseline(sc, w)
+        print(json.dumps(out), flush=True)
+    r.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_engine(args)
+
+
+if __name__ == "__main__":
+    main()

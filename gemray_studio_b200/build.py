@@ -1,0 +1,69 @@
+"""Build the CUDA engine in-tree: gemray_studio_b200/libgemray_cuda.so (sm_100a).
+
+The library is compiled with nvcc directly (no JIT cache): the .so sits next to this
+file so it travels with the repository snapshot.  Floating-point flags are part of the
+engine's contract with the reference arithmetic: no FMA contraction (--fmad=false on
+the device, -ffp-contract=off on the host), IEEE division and square root, no fast
+math.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+OUT = PKG / "libgemray_cuda.so"
+SOURCES = ["gr_host.cu", "gr_tonemap.cu", "gr_scene_builders.cpp"]
+HEADERS = ["gr_device.cuh", "gr_trace.cuh", "gr_kernels.cuh", "gr_host.h"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and Path(cand).exists():
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def flags(extra_ptxas: bool = False) -> list[str]:
+    f = [
+        *ARCH, "-O3", "-lineinfo", "-std=c++17", "--fmad=false", "-prec-div=true", "-prec-sqrt=true",
+        "-ftz=false", "-Xcompiler", "-fPIC,-ffp-contract=off,-fno-fast-math", "-I", str(ROOT / "include"),
+        "-I", str(CSRC),
+    ]
+    if extra_ptxas:
+        f += ["-Xptxas", "-v"]
+    return f
+
+
+def needs_build() -> bool:
+    if not OUT.exists():
+        return True
+    newest = max((CSRC / n).stat().st_mtime for n in SOURCES + HEADERS)
+    newest = max(newest, (ROOT / "include" / "gemray_cuda.h").stat().st_mtime, Path(__file__).stat().st_mtime)
+    return OUT.stat().st_mtime < newest
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    if not force and not needs_build():
+        return OUT
+    tmp = OUT.with_suffix(".so.tmp")
+    cmd = [nvcc(), *flags(verbose), "-shared", "-o", str(tmp), *[str(CSRC / s) for s in SOURCES]]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("nvcc failed building libgemray_cuda.so")
+    if verbose:
+        sys.stderr.write(r.stdout + r.stderr)
+    os.replace(tmp, OUT)
+    return OUT
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose="-v" in sys.argv)
+    print(OUT)

@@ -1,0 +1,916 @@
+// gr_host.cu -- the C ABI (include/gemray_cuda.h): context lifecycle, scene
+// validation and encoding, chunked launches, film accumulation.
+//
+// Host-side physics that the reference evaluates once per scene or per ray from
+// scene constants alone is evaluated here once per call with the same f32
+// arithmetic (this file is compiled without FMA contraction):
+//   * compute_illuminant_white_balance (optics/raytracer/color.rs:281-315),
+//   * StudioRig::new (optics/studio_rig.rs:50-81),
+//   * blackbody_spectrum's 560 nm normaliser (optics/raytracer/environment.rs:16-18),
+//   * AbsorptionTensor3::uniaxial's axis frame (optics/birefringence.rs:202-209).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "gemray_cuda.h"
+#include "gr_host.h"
+#include "gr_kernels.cuh"
+
+using grd::SceneConst;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+gr_status fail(gr_status st, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return st;
+}
+
+#define GR_CUDA(call)                                                                                 \
+    do {                                                                                              \
+        cudaError_t e_ = (call);                                                                      \
+        if (e_ != cudaSuccess) return fail(GR_ECUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------
+// Host-side f32 helpers (glam scalar semantics).
+// ---------------------------------------------------------------------------------
+namespace grh {
+
+struct H3 {
+    float x, y, z;
+};
+static inline H3 h3(float x, float y, float z) { return H3{x, y, z}; }
+static inline float hdot(H3 a, H3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+static inline H3 hmul(H3 a, float s) { return h3(a.x * s, a.y * s, a.z * s); }
+static inline H3 hsub(H3 a, H3 b) { return h3(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline H3 hcross(H3 a, H3 b) { return h3(a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y); }
+static inline H3 hnormalize(H3 a) { return hmul(a, 1.0f / sqrtf(hdot(a, a))); }
+static inline H3 hnormalize_or_zero(H3 a) {
+    float r = 1.0f / sqrtf(hdot(a, a));
+    if (std::isfinite(r) && r > 0.0f) return hmul(a, r);
+    return h3(0.f, 0.f, 0.f);
+}
+static inline float hclamp(float x, float lo, float hi) {
+    if (x < lo) x = lo;
+    if (x > hi) x = hi;
+    return x;
+}
+static inline float hpowi(float x, int n) {
+    float r = 1.0f, sq = x;
+    bool have = false;
+    while (n) {
+        if (n & 1) {
+            r = have ? r * sq : sq;
+            have = true;
+        }
+        n >>= 1;
+        if (n) sq = sq * sq;
+    }
+    return r;
+}
+static inline float hgauss(float x, float mu, float slo, float shi) {
+    float sigma = x < mu ? slo : shi;
+    float t = (x - mu) / sigma;
+    return expf(-0.5f * t * t);
+}
+// color/cie1931.rs:29-42 (scalar libm form used by the white-balance integral)
+static inline H3 cmf_scalar(float l) {
+    float x = fmaf(0.065f, -hgauss(l, 501.1f, 20.4f, 26.2f),
+                   fmaf(1.056f, hgauss(l, 599.8f, 37.9f, 31.0f), 0.362f * hgauss(l, 442.0f, 16.0f, 26.7f)));
+    float y = fmaf(0.286f, hgauss(l, 530.9f, 16.3f, 31.1f), 0.821f * hgauss(l, 568.8f, 46.9f, 40.5f));
+    float z = fmaf(0.681f, hgauss(l, 459.0f, 26.0f, 13.8f), 1.217f * hgauss(l, 437.0f, 11.8f, 36.0f));
+    return h3(fmaxf(x, 0.0f), fmaxf(y, 0.0f), fmaxf(z, 0.0f));
+}
+// optics/raytracer/environment.rs:12-21
+static inline float blackbody(float lambda_nm, float temp_k) {
+    float t_k = fmaxf(temp_k, 1000.0f);
+    const float hck = 14388000.0f;
+    float e = expf(fminf(hck / (lambda_nm * t_k), 80.0f));
+    float e5 = expf(fminf(hck / (560.0f * t_k), 80.0f));
+    float d = fmaxf(e - 1.0f, 1e-6f), d5 = fmaxf(e5 - 1.0f, 1e-6f);
+    return hclamp(hpowi(560.0f / lambda_nm, 5) * (d5 / d), 0.01f, 20.0f);
+}
+static inline H3 bradford(const float m[3][3], H3 v) {
+    return h3(fmaf(m[0][0], v.x, fmaf(m[0][1], v.y, m[0][2] * v.z)),
+              fmaf(m[1][0], v.x, fmaf(m[1][1], v.y, m[1][2] * v.z)),
+              fmaf(m[2][0], v.x, fmaf(m[2][1], v.y, m[2][2] * v.z)));
+}
+static const float XYZ_TO_LMS[3][3] = {{0.8951f, 0.2664f, -0.1614f}, {-0.7502f, 1.7135f, 0.0367f}, {0.0389f, -0.0685f, 1.0296f}};
+
+// optics/raytracer/color.rs:281-315
+H3 white_balance(float temp_k) {
+    H3 w = h3(0.f, 0.f, 0.f);
+    for (int step = 0; step <= 400; ++step) {
+        float lambda = 380.0f + (float)step;
+        H3 c = cmf_scalar(lambda);
+        float b = blackbody(lambda, temp_k);
+        w = h3(w.x + c.x * b, w.y + c.y * b, w.z + c.z * b);
+    }
+    float ty = fmaxf(w.y, 1e-6f);
+    const float wx = 0.3127f, wy = 0.3290f;
+    H3 target = h3((wx / wy) * ty, ty, ((1.0f - wx - wy) / wy) * ty);
+    H3 ls = bradford(XYZ_TO_LMS, w), lt = bradford(XYZ_TO_LMS, target);
+    return h3(ls.x > 1e-6f ? lt.x / ls.x : 1.0f, ls.y > 1e-6f ? lt.y / ls.y : 1.0f, ls.z > 1e-6f ? lt.z / ls.z : 1.0f);
+}
+
+// optics/studio_rig.rs:50-81
+void studio_rig(float yaw, float pitch, float key[3], float fill[3], float ring[16][3]) {
+    float cos_lp = cosf(pitch), sin_lp = sinf(pitch), cos_ly = cosf(yaw), sin_ly = sinf(yaw);
+    H3 k = hnormalize(h3(cos_lp * sin_ly, sin_lp, cos_lp * cos_ly));
+    key[0] = k.x; key[1] = k.y; key[2] = k.z;
+    const float PI = 3.14159265358979323846f;
+    float fill_yaw = fmaf(PI, 0.78f, yaw);
+    float fill_pitch = hclamp(pitch * 0.65f, 0.15f, 1.2f);
+    H3 f = hnormalize(h3(cosf(fill_pitch) * sinf(fill_yaw), sinf(fill_pitch), cosf(fill_pitch) * cosf(fill_yaw)));
+    fill[0] = f.x; fill[1] = f.y; fill[2] = f.z;
+    const float step = PI * 2.0f / 16.0f;
+    for (int i = 0; i < 16; ++i) {
+        float angle = fmaf((float)i, step, yaw);
+        H3 r = hnormalize(h3(cosf(angle) * 0.75f, sin_lp * 0.8f, sinf(angle) * 0.75f));
+        ring[i][0] = r.x; ring[i][1] = r.y; ring[i][2] = r.z;
+    }
+}
+
+// optics/birefringence.rs:126-131,202-209
+void tensor_frame(const float c_axis[3], float ax0[3], float ax1[3], float ax2[3]) {
+    H3 c = hnormalize_or_zero(h3(c_axis[0], c_axis[1], c_axis[2]));
+    H3 a = fabsf(c.x) > 0.9f ? h3(0.f, 1.f, 0.f) : h3(1.f, 0.f, 0.f);
+    H3 t = hnormalize_or_zero(hsub(a, hmul(c, hdot(c, a))));
+    H3 b = hcross(c, t);
+    ax0[0] = t.x; ax0[1] = t.y; ax0[2] = t.z;
+    ax1[0] = b.x; ax1[1] = b.y; ax1[2] = b.z;
+    ax2[0] = c.x; ax2[1] = c.y; ax2[2] = c.z;
+}
+
+}  // namespace grh
+
+// ---------------------------------------------------------------------------------
+// Scene encoding
+// ---------------------------------------------------------------------------------
+namespace grh {
+
+gr_status validate_scene(const gr_scene *sc) {
+    if (!sc) return fail(GR_EINVAL, "scene is NULL");
+    if (!sc->material) return fail(GR_EINVAL, "scene.material is NULL");
+    if (sc->n_planes > GR_MAX_PLANES) return fail(GR_EINVAL, "n_planes %u exceeds GR_MAX_PLANES", sc->n_planes);
+    if (sc->n_planes > 0 && !sc->planes) return fail(GR_EINVAL, "scene.planes is NULL");
+    if (sc->max_bounces > GR_MAX_BOUNCES) return fail(GR_EINVAL, "max_bounces %u exceeds GR_MAX_BOUNCES", sc->max_bounces);
+    if ((uint64_t)sc->width * (uint64_t)sc->height > 0xFFFFFFFFull)
+        return fail(GR_EINVAL, "width*height exceeds the u32 pixel index");
+    const gr_material *m = sc->material;
+    if (m->o_ray_band_count > GR_MAX_BANDS || m->e_ray_band_count > GR_MAX_BANDS || m->beta_ray_band_count > GR_MAX_BANDS)
+        return fail(GR_EINVAL, "absorption band count exceeds GR_MAX_BANDS");
+    if (m->dispersion.model_type > GR_DISP_CAUCHY) return fail(GR_EINVAL, "unknown dispersion model %u", m->dispersion.model_type);
+    if (sc->env.mode > GR_ENV_LATLONG) return fail(GR_EINVAL, "unknown environment mode %u", sc->env.mode);
+    if (sc->env.mode == GR_ENV_LATLONG) {
+        if (!sc->env.latlong_rgb || sc->env.latlong_w == 0 || sc->env.latlong_h == 0)
+            return fail(GR_EINVAL, "lat-long environment needs a non-empty map");
+        if ((uint64_t)sc->env.latlong_w * sc->env.latlong_h > (1ull << 28)) return fail(GR_EINVAL, "lat-long map too large");
+    }
+    if (sc->material_ext) {
+        const gr_material_ext *e = sc->material_ext;
+        if (e->n_absorption > 0 && (!e->alpha_o_table || !e->alpha_e_table || !(e->absorption_nm_step > 0.0f)))
+            return fail(GR_EINVAL, "material_ext absorption table is incomplete");
+        if (e->n_absorption > (1u << 20)) return fail(GR_EINVAL, "material_ext absorption table too long");
+    }
+    return GR_OK;
+}
+
+// v1 device coverage: polished facets of isotropic / uniaxial, non-scattering
+// materials.  Anything else is declined (GpuFrameError::UnsupportedMaterial
+// semantics: the caller renders it on the CPU tracer).
+gr_status check_supported(const gr_scene *sc) {
+    const gr_material *m = sc->material;
+    if (m->dispersion.has_biaxial_delta) return fail(GR_DECLINED_MATERIAL, "biaxial materials are not handled on the device");
+    if (m->has_beta_ray) return fail(GR_DECLINED_MATERIAL, "trichroic (beta-ray) absorption is not handled on the device");
+    if (m->scattering_sigma_s > 0.0f) return fail(GR_DECLINED_MATERIAL, "volumetric scattering is not handled on the device");
+    if (sc->finishes)
+        for (uint32_t i = 0; i < sc->n_planes; ++i)
+            if (sc->finishes[i] != 0) return fail(GR_DECLINED_MATERIAL, "frosted facets are not handled on the device");
+    return GR_OK;
+}
+
+void encode_scene(const gr_scene *sc, SceneConst &S) {
+    std::memset(&S, 0, sizeof(S));
+    for (int i = 0; i < 3; ++i) {
+        S.cam_o[i] = sc->camera.origin[i];
+        S.cam_f[i] = sc->camera.forward[i];
+        S.cam_r[i] = sc->camera.right[i];
+        S.cam_u[i] = sc->camera.up[i];
+    }
+    S.fov_tan = sc->camera.fov_tan;
+    S.width = sc->width;
+    S.height = sc->height;
+    S.width_f = (float)sc->width;
+    S.height_f = (float)sc->height;
+    S.max_bounces = sc->max_bounces;
+    S.n_planes = sc->n_planes;
+    const gr_material *m = sc->material;
+    S.disp_model = m->dispersion.model_type;
+    for (int i = 0; i < 3; ++i) {
+        S.disp_a[i] = m->dispersion.param_a[i];
+        S.disp_b[i] = m->dispersion.param_b[i];
+        S.c_axis[i] = m->dispersion.c_axis_and_birefringence[i];
+    }
+    S.bire = m->dispersion.c_axis_and_birefringence[3];
+    // transport.rs:620-621
+    S.anisotropic = (m->crystal_system != GR_CRYSTAL_CUBIC && fabsf(S.bire) > 1e-4f) ? 1u : 0u;
+    S.n_o_bands = m->o_ray_band_count;
+    S.n_e_bands = m->e_ray_band_count;
+    for (uint32_t i = 0; i < GR_MAX_BANDS; ++i) {
+        S.o_bands[i][0] = m->o_ray_bands[i].center_nm;
+        S.o_bands[i][1] = m->o_ray_bands[i].width_nm;
+        S.o_bands[i][2] = m->o_ray_bands[i].peak;
+        S.e_bands[i][0] = m->e_ray_bands[i].center_nm;
+        S.e_bands[i][1] = m->e_ray_bands[i].width_nm;
+        S.e_bands[i][2] = m->e_ray_bands[i].peak;
+    }
+    S.path_scale = m->absorption_path_scale;
+    S.edge_radius = m->edge_rounding_radius;
+    tensor_frame(S.c_axis, S.ax0, S.ax1, S.ax2);
+    const gr_material_ext *ext = sc->material_ext;
+    if (ext) {
+        S.ext_n = ext->n_absorption;
+        S.ext_first = ext->absorption_nm_first;
+        S.ext_step = ext->absorption_nm_step;
+        S.has_cauchy_e = ext->has_cauchy_e ? 1u : 0u;
+        for (int i = 0; i < 3; ++i) S.cauchy_e[i] = ext->cauchy_e[i];
+    }
+    S.absorbing = (S.ext_n > 0 || S.n_o_bands > 0 || S.n_e_bands > 0) ? 1u : 0u;
+    S.env_mode = sc->env.mode;
+    for (int i = 0; i < 3; ++i) S.uni_rgb[i] = sc->env.uniform_rgb[i];
+    S.temp_k = sc->env.temp_k;
+    S.spot_mult = sc->env.spot_mult;
+    S.exposure = sc->env.exposure;
+    S.wb[0] = S.wb[1] = S.wb[2] = 1.0f;  // environment.rs:238-243: maps -> Vec3::ONE
+    if (sc->env.mode == GR_ENV_STUDIO) {
+        H3 w = white_balance(sc->env.temp_k);
+        S.wb[0] = w.x; S.wb[1] = w.y; S.wb[2] = w.z;
+        studio_rig(sc->env.light_yaw, sc->env.light_pitch, S.key, S.fill, S.ring);
+        float t_k = fmaxf(sc->env.temp_k, 1000.0f);
+        float e5 = expf(fminf(14388000.0f / (560.0f * t_k), 80.0f));
+        S.denom560 = fmaxf(e5 - 1.0f, 1e-6f);
+    }
+    S.map_w = sc->env.latlong_w;
+    S.map_h = sc->env.latlong_h;
+    S.flags = sc->flags;
+}
+
+}  // namespace grh
+
+// ---------------------------------------------------------------------------------
+// Context
+// ---------------------------------------------------------------------------------
+// A scene kept on the device between calls (serving / benchmark): encoded
+// constants plus its own copies of the planes, map and extension tables.
+struct ResidentScene {
+    SceneConst S;
+    grh::DeviceBuffer planes, map, ext;
+    uint64_t bytes = 0;
+};
+
+struct gr_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    std::string label;
+    size_t chunk_budget = 256ull << 20;
+    uint64_t serve_budget = 60ull << 30;
+    int sm_count = 0;
+    int persistent_blocks = 0;
+    grh::DeviceBuffer xyz, film, planes, map, ext, counter, rgba;
+    int kernel_mode = GR_KERNEL_PERSISTENT;
+    // Optional per-launch timing of the trace and fold kernels (CUDA events on the
+    // launch stream); read back by gr_timing_read.
+    bool timing = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> trace_ev, fold_ev;
+    size_t trace_used = 0, fold_used = 0;
+    uint64_t trace_launches = 0, fold_launches = 0;
+    std::map<uint64_t, ResidentScene *> scenes;
+    uint64_t next_scene_id = 1;
+    uint64_t resident_bytes = 0;
+};
+
+namespace grd {
+__global__ void k_rng_records(const uint32_t *__restrict__ pixels, const uint32_t *__restrict__ samples, uint32_t n,
+                              gr_rng_record *__restrict__ out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Draws d = sample_draws(pixels[i], samples[i]);
+    gr_rng_record r;
+    r.seed = d.seed;
+    r.jitter_x = d.jx;
+    r.jitter_y = d.jy;
+    r.hero_rand = d.hero;
+    for (uint32_t b = 0; b < 4; ++b) {
+        r.draws[b][0] = rng_draw(d.seed, b, FRESNEL_BRANCH_STREAM);
+        r.draws[b][1] = rng_draw(d.seed, b, RUSSIAN_ROULETTE_STREAM);
+        r.draws[b][2] = rng_draw(d.seed, b, BIREFRINGENT_SPLIT_STREAM);
+        r.draws[b][3] = rng_draw(d.seed, b, MODE_COUPLING_STREAM);
+    }
+    out[i] = r;
+}
+}  // namespace grd
+
+namespace grh {
+
+gr_status DeviceBuffer::reserve(size_t bytes) {
+    if (bytes <= cap) return GR_OK;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+    cudaError_t e = cudaMalloc(&ptr, bytes);
+    if (e != cudaSuccess) {
+        ptr = nullptr;
+        return fail(GR_ENOMEM, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+    }
+    cap = bytes;
+    return GR_OK;
+}
+void DeviceBuffer::release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+}
+
+// Upload the scene's device-side arrays into the context's buffers.
+gr_status upload_scene(gr_ctx *ctx, const gr_scene *sc, const SceneConst &S, grd::SceneBuffers &B) {
+    std::memset(&B, 0, sizeof(B));
+    size_t pbytes = (size_t)(sc->n_planes ? sc->n_planes : 1) * sizeof(float4);
+    gr_status st = ctx->planes.reserve(pbytes);
+    if (st != GR_OK) return st;
+    if (sc->n_planes) {
+        static_assert(sizeof(gr_plane) == sizeof(float4), "plane layout");
+        GR_CUDA(cudaMemcpyAsync(ctx->planes.ptr, sc->planes, sc->n_planes * sizeof(gr_plane), cudaMemcpyHostToDevice,
+                                ctx->stream));
+    }
+    B.planes = (const float4 *)ctx->planes.ptr;
+    if (S.env_mode == GR_ENV_LATLONG) {
+        size_t mbytes = (size_t)S.map_w * S.map_h * 3 * sizeof(float);
+        st = ctx->map.reserve(mbytes);
+        if (st != GR_OK) return st;
+        GR_CUDA(cudaMemcpyAsync(ctx->map.ptr, sc->env.latlong_rgb, mbytes, cudaMemcpyHostToDevice, ctx->stream));
+        B.map = (const float *)ctx->map.ptr;
+    }
+    if (S.ext_n > 0) {
+        size_t ebytes = (size_t)S.ext_n * 2 * sizeof(float);
+        st = ctx->ext.reserve(ebytes);
+        if (st != GR_OK) return st;
+        float *d = (float *)ctx->ext.ptr;
+        GR_CUDA(cudaMemcpyAsync(d, sc->material_ext->alpha_o_table, S.ext_n * sizeof(float), cudaMemcpyHostToDevice, ctx->stream));
+        GR_CUDA(cudaMemcpyAsync(d + S.ext_n, sc->material_ext->alpha_e_table, S.ext_n * sizeof(float), cudaMemcpyHostToDevice,
+                                ctx->stream));
+        B.ext_alpha_o = d;
+        B.ext_alpha_e = d + S.ext_n;
+    }
+    return GR_OK;
+}
+
+// Trace tuples [0, R.n_tuples) of one chunk into xyz (device).
+gr_status launch_trace(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuffers &B, const grd::LaunchRange &R,
+                       float *xyz, cudaStream_t stream, int mode) {
+    if (R.n_tuples == 0) return GR_OK;
+    size_t smem = (size_t)S.n_planes * sizeof(float4);
+    if (mode == GR_KERNEL_PLAIN || S.max_bounces == 0) {
+        uint64_t blocks = (R.n_tuples + grd::TRACE_THREADS - 1) / grd::TRACE_THREADS;
+        grd::k_trace_plain<<<(unsigned)blocks, grd::TRACE_THREADS, smem, stream>>>(S, B, R, xyz);
+    } else {
+        gr_status st = ctx->counter.reserve(sizeof(unsigned long long));
+        if (st != GR_OK) return st;
+        GR_CUDA(cudaMemsetAsync(ctx->counter.ptr, 0, sizeof(unsigned long long), stream));
+        uint64_t want = (R.n_tuples + grd::TRACE_THREADS - 1) / grd::TRACE_THREADS;
+        uint64_t blocks = (uint64_t)ctx->persistent_blocks;
+        if (want < blocks) blocks = want;
+        grd::k_trace_persistent<grd::NoCounters><<<(unsigned)blocks, grd::TRACE_THREADS, smem, stream>>>(
+            S, B, R, xyz, (unsigned long long *)ctx->counter.ptr, nullptr);
+    }
+    GR_CUDA(cudaGetLastError());
+    return GR_OK;
+}
+
+gr_status launch_fold(const float *xyz, uint32_t n_pixels, uint32_t spp, uint32_t first_pixel, float *film,
+                      uint32_t kahan, cudaStream_t stream) {
+    if (n_pixels == 0) return GR_OK;
+    const unsigned threads = 256;
+    uint64_t blocks = ((uint64_t)n_pixels * 32 + threads - 1) / threads;
+    grd::k_film_fold<<<(unsigned)blocks, threads, 0, stream>>>(xyz, n_pixels, spp, first_pixel, film, kahan);
+    GR_CUDA(cudaGetLastError());
+    return GR_OK;
+}
+
+// Next free (start, stop) event pair for a timed launch, or NULL when timing is off.
+cudaEvent_t *timing_slot(gr_ctx *ctx, std::vector<std::pair<cudaEvent_t, cudaEvent_t>> &pool, size_t &used) {
+    if (!ctx->timing) return nullptr;
+    if (used == pool.size()) {
+        cudaEvent_t a, b;
+        if (cudaEventCreate(&a) != cudaSuccess) return nullptr;
+        if (cudaEventCreate(&b) != cudaSuccess) {
+            cudaEventDestroy(a);
+            return nullptr;
+        }
+        pool.emplace_back(a, b);
+    }
+    return &pool[used++].first;
+}
+
+// The shared body of gr_accumulate / gr_accumulate_device: trace every pixel's
+// [sample_offset, sample_offset + spp) samples chunk by chunk and add each pixel's
+// folded sum into film_dev.
+gr_status render_into(gr_ctx *ctx, const gr_scene *sc, const SceneConst &S, const grd::SceneBuffers &B,
+                      uint32_t sample_offset, uint32_t spp, float *film_dev, cudaStream_t stream) {
+    const uint64_t n_pixels = (uint64_t)sc->width * sc->height;
+    uint64_t budget_tuples = ctx->chunk_budget / (3 * sizeof(float));
+    uint64_t chunk_pixels = budget_tuples / spp;
+    if (chunk_pixels < 1) chunk_pixels = 1;
+    if (chunk_pixels > n_pixels) chunk_pixels = n_pixels;
+    gr_status st = ctx->xyz.reserve((size_t)chunk_pixels * spp * 3 * sizeof(float));
+    if (st != GR_OK) return st;
+    for (uint64_t first = 0; first < n_pixels; first += chunk_pixels) {
+        uint64_t np = n_pixels - first < chunk_pixels ? n_pixels - first : chunk_pixels;
+        grd::LaunchRange R;
+        R.first_pixel = (uint32_t)first;
+        R.n_pixels = (uint32_t)np;
+        R.sample_offset = sample_offset;
+        R.spp = spp;
+        R.n_tuples = np * spp;
+        cudaEvent_t *tev = timing_slot(ctx, ctx->trace_ev, ctx->trace_used);
+        if (tev) cudaEventRecord(tev[0], stream);
+        st = launch_trace(ctx, S, B, R, (float *)ctx->xyz.ptr, stream, ctx->kernel_mode);
+        if (st != GR_OK) return st;
+        if (tev) cudaEventRecord(tev[1], stream);
+        ctx->trace_launches++;
+        cudaEvent_t *fev = timing_slot(ctx, ctx->fold_ev, ctx->fold_used);
+        if (fev) cudaEventRecord(fev[0], stream);
+        st = launch_fold((const float *)ctx->xyz.ptr, (uint32_t)np, spp, (uint32_t)first, film_dev,
+                         (S.flags & GR_FLAG_KAHAN_FILM) ? 1u : 0u, stream);
+        if (st != GR_OK) return st;
+        if (fev) cudaEventRecord(fev[1], stream);
+        ctx->fold_launches++;
+    }
+    return GR_OK;
+}
+
+gr_status prepare(gr_ctx *ctx, const gr_scene *sc, SceneConst &S, grd::SceneBuffers &B) {
+    gr_status st = validate_scene(sc);
+    if (st != GR_OK) return st;
+    st = check_supported(sc);
+    if (st != GR_OK) return st;
+    encode_scene(sc, S);
+    return upload_scene(ctx, sc, S, B);
+}
+
+}  // namespace grh
+
+// ---------------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------------
+extern "C" {
+
+uint32_t gr_abi_version(void) { return GR_ABI_VERSION; }
+
+const char *gr_last_error_string(void) { return g_last_error.c_str(); }
+
+gr_status gr_create(gr_ctx **out, const gr_create_opts *opts) {
+    if (!out) return fail(GR_EINVAL, "out is NULL");
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return fail(GR_NO_DEVICE, "no CUDA device: %s", e == cudaSuccess ? "device count is 0" : cudaGetErrorString(e));
+    }
+    int dev = 0;
+    if (opts && opts->device >= 0) dev = opts->device;
+    if (dev >= count) return fail(GR_NO_DEVICE, "device %d out of range (%d devices)", dev, count);
+    cudaDeviceProp prop;
+    GR_CUDA(cudaGetDeviceProperties(&prop, dev));
+    if (prop.major < 10) return fail(GR_NO_DEVICE, "device %d (%s, sm_%d%d) is not sm_100", dev, prop.name, prop.major, prop.minor);
+    GR_CUDA(cudaSetDevice(dev));
+    gr_ctx *ctx = new gr_ctx();
+    ctx->device = dev;
+    if (opts && opts->chunk_budget_bytes) ctx->chunk_budget = opts->chunk_budget_bytes;
+    if (opts && opts->serve_budget_bytes) ctx->serve_budget = opts->serve_budget_bytes;
+    e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete ctx;
+        return fail(GR_ECUDA, "cudaStreamCreate failed: %s", cudaGetErrorString(e));
+    }
+    ctx->sm_count = prop.multiProcessorCount;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grd::k_trace_persistent<grd::NoCounters>, grd::TRACE_THREADS,
+                                                      GR_MAX_PLANES * sizeof(float4));
+    if (e != cudaSuccess || per_sm < 1) per_sm = 1;
+    ctx->persistent_blocks = per_sm * ctx->sm_count;
+    char buf[256];
+    snprintf(buf, sizeof(buf), "%s (CUDA, sm_%d%d, %d SMs)", prop.name, prop.major, prop.minor, prop.multiProcessorCount);
+    ctx->label = buf;
+    *out = ctx;
+    return GR_OK;
+}
+
+gr_status gr_destroy(gr_ctx *ctx) {
+    if (!ctx) return GR_OK;
+    {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        cudaSetDevice(ctx->device);
+        cudaStreamSynchronize(ctx->stream);
+        ctx->xyz.release();
+        ctx->film.release();
+        ctx->planes.release();
+        ctx->map.release();
+        ctx->ext.release();
+        ctx->counter.release();
+        ctx->rgba.release();
+        for (auto &p : ctx->trace_ev) { cudaEventDestroy(p.first); cudaEventDestroy(p.second); }
+        for (auto &p : ctx->fold_ev) { cudaEventDestroy(p.first); cudaEventDestroy(p.second); }
+        for (auto &kv : ctx->scenes) {
+            kv.second->planes.release();
+            kv.second->map.release();
+            kv.second->ext.release();
+            delete kv.second;
+        }
+        ctx->scenes.clear();
+        cudaStreamDestroy(ctx->stream);
+    }
+    delete ctx;
+    return GR_OK;
+}
+
+const char *gr_device_label(gr_ctx *ctx) { return ctx ? ctx->label.c_str() : ""; }
+
+gr_status gr_accumulate(gr_ctx *ctx, const gr_scene *sc, uint32_t sample_offset, uint32_t spp, float *accum) {
+    if (!ctx) return fail(GR_EINVAL, "ctx is NULL");
+    if (!sc) return fail(GR_EINVAL, "scene is NULL");
+    const uint64_t n_pixels = (uint64_t)sc->width * sc->height;
+    if (spp == 0 || n_pixels == 0) return GR_OK;  // frame.rs:678-680
+    if (!accum) return fail(GR_EINVAL, "accum is NULL");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    GR_CUDA(cudaSetDevice(ctx->device));
+    SceneConst S;
+    grd::SceneBuffers B;
+    gr_status st = grh::prepare(ctx, sc, S, B);
+    if (st != GR_OK) return st;
+    const size_t fbytes = (size_t)n_pixels * 3 * sizeof(float);
+    st = ctx->film.reserve(fbytes);
+    if (st != GR_OK) return st;
+    GR_CUDA(cudaMemcpyAsync(ctx->film.ptr, accum, fbytes, cudaMemcpyHostToDevice, ctx->stream));
+    st = grh::render_into(ctx, sc, S, B, sample_offset, spp, (float *)ctx->film.ptr, ctx->stream);
+    if (st != GR_OK) {
+        cudaStreamSynchronize(ctx->stream);
+        return st;
+    }
+    // Copy into a staging vector first so a failure leaves accum untouched.
+    std::vector<float> tmp(n_pixels * 3);
+    GR_CUDA(cudaMemcpyAsync(tmp.data(), ctx->film.ptr, fbytes, cudaMemcpyDeviceToHost, ctx->stream));
+    GR_CUDA(cudaStreamSynchronize(ctx->stream));
+    std::memcpy(accum, tmp.data(), fbytes);
+    return GR_OK;
+}
+
+gr_status gr_accumulate_device(gr_ctx *ctx, const gr_scene *sc, uint32_t sample_offset, uint32_t spp,
+                               float *accum_dev, void *stream) {
+    if (!ctx) return fail(GR_EINVAL, "ctx is NULL");
+    if (!sc) return fail(GR_EINVAL, "scene is NULL");
+    const uint64_t n_pixels = (uint64_t)sc->width * sc->height;
+    if (spp == 0 || n_pixels == 0) return GR_OK;
+    if (!accum_dev) return fail(GR_EINVAL, "accum_xyz_device is NULL");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    GR_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    SceneConst S;
+    grd::SceneBuffers B;
+    gr_status st = grh::prepare(ctx, sc, S, B);
+    if (st != GR_OK) return st;
+    if (s != ctx->stream) {
+        // Order the caller's stream after the scene upload on the context stream.
+        cudaEvent_t ev;
+        GR_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        cudaEventRecord(ev, ctx->stream);
+        cudaStreamWaitEvent(s, ev, 0);
+        cudaEventDestroy(ev);
+    }
+    st = grh::render_into(ctx, sc, S, B, sample_offset, spp, accum_dev, s);
+    if (st != GR_OK) return st;
+    if (s != ctx->stream) {
+        // Later uploads on the context stream must wait for this work.
+        cudaEvent_t ev;
+        GR_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        cudaEventRecord(ev, s);
+        cudaStreamWaitEvent(ctx->stream, ev, 0);
+        cudaEventDestroy(ev);
+    }
+    return GR_OK;
+}
+
+gr_status gr_trace_samples(gr_ctx *ctx, const gr_scene *sc, uint32_t first_pixel, uint32_t n_pixels,
+                           uint32_t sample_offset, uint32_t spp, float *xyz_out) {
+    if (!ctx || !sc) return fail(GR_EINVAL, "ctx or scene is NULL");
+    if (n_pixels == 0 || spp == 0) return GR_OK;
+    if (!xyz_out) return fail(GR_EINVAL, "xyz_out is NULL");
+    if ((uint64_t)first_pixel + n_pixels > (uint64_t)sc->width * sc->height)
+        return fail(GR_EINVAL, "pixel range exceeds the frame");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    GR_CUDA(cudaSetDevice(ctx->device));
+    SceneConst S;
+    grd::SceneBuffers B;
+    gr_status st = grh::prepare(ctx, sc, S, B);
+    if (st != GR_OK) return st;
+    uint64_t n_tuples = (uint64_t)n_pixels * spp;
+    size_t bytes = (size_t)n_tuples * 3 * sizeof(float);
+    st = ctx->xyz.reserve(bytes);
+    if (st != GR_OK) return st;
+    grd::LaunchRange R;
+    R.first_pixel = first_pixel;
+    R.n_pixels = n_pixels;
+    R.sample_offset = sample_offset;
+    R.spp = spp;
+    R.n_tuples = n_tuples;
+    st = grh::launch_trace(ctx, S, B, R, (float *)ctx->xyz.ptr, ctx->stream, ctx->kernel_mode);
+    if (st != GR_OK) return st;
+    GR_CUDA(cudaMemcpyAsync(xyz_out, ctx->xyz.ptr, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    GR_CUDA(cudaStreamSynchronize(ctx->stream));
+    return GR_OK;
+}
+
+gr_status gr_tonemap(gr_ctx *ctx, const float *xyz, float scale, uint32_t n_px, uint8_t *rgba) {
+    if (!ctx) return fail(GR_EINVAL, "ctx is NULL");
+    if (n_px == 0) return GR_OK;
+    if (!xyz || !rgba) return fail(GR_EINVAL, "xyz or rgba is NULL");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    GR_CUDA(cudaSetDevice(ctx->device));
+    size_t in_bytes = (size_t)n_px * 3 * sizeof(float), out_bytes = (size_t)n_px * 4;
+    gr_status st = ctx->film.reserve(in_bytes);
+    if (st != GR_OK) return st;
+    st = ctx->rgba.reserve(out_bytes);
+    if (st != GR_OK) return st;
+    GR_CUDA(cudaMemcpyAsync(ctx->film.ptr, xyz, in_bytes, cudaMemcpyHostToDevice, ctx->stream));
+    st = grh::tonemap_device((const float *)ctx->film.ptr, scale, n_px, ctx->rgba.ptr, ctx->stream);
+    if (st != GR_OK) return fail(st, "tone-map launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    GR_CUDA(cudaMemcpyAsync(rgba, ctx->rgba.ptr, out_bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    GR_CUDA(cudaStreamSynchronize(ctx->stream));
+    return GR_OK;
+}
+
+gr_status gr_rng_records(gr_ctx *ctx, const uint32_t *pixels, const uint32_t *samples, uint32_t n,
+                         gr_rng_record *out) {
+    if (!ctx) return fail(GR_EINVAL, "ctx is NULL");
+    if (n == 0) return GR_OK;
+    if (!pixels || !samples || !out) return fail(GR_EINVAL, "NULL array");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    GR_CUDA(cudaSetDevice(ctx->device));
+    size_t in_bytes = (size_t)n * sizeof(uint32_t), out_bytes = (size_t)n * sizeof(gr_rng_record);
+    gr_status st = ctx->xyz.reserve(2 * in_bytes + out_bytes + 16);
+    if (st != GR_OK) return st;
+    char *base = (char *)ctx->xyz.ptr;
+    uint32_t *dp = (uint32_t *)base, *ds = (uint32_t *)(base + in_bytes);
+    gr_rng_record *dout = (gr_rng_record *)(base + ((2 * in_bytes + 15) & ~(size_t)15));
+    GR_CUDA(cudaMemcpyAsync(dp, pixels, in_bytes, cudaMemcpyHostToDevice, ctx->stream));
+    GR_CUDA(cudaMemcpyAsync(ds, samples, in_bytes, cudaMemcpyHostToDevice, ctx->stream));
+    grd::k_rng_records<<<(n + 127) / 128, 128, 0, ctx->stream>>>(dp, ds, n, dout);
+    GR_CUDA(cudaGetLastError());
+    GR_CUDA(cudaMemcpyAsync(out, dout, out_bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    GR_CUDA(cudaStreamSynchronize(ctx->stream));
+    return GR_OK;
+}
+
+gr_status gr_scene_upload(gr_ctx *ctx, const gr_scene *sc, uint64_t *out_id) {
+    if (!ctx || !out_id) return fail(GR_EINVAL, "ctx or out_id is NULL");
+    gr_status st = grh::validate_scene(sc);
+    if (st != GR_OK) return st;
+    st = grh::check_supported(sc);
+    if (st != GR_OK) return st;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    GR_CUDA(cudaSetDevice(ctx->device));
+    ResidentScene *rs = new ResidentScene();
+    grh::encode_scene(sc, rs->S);
+    size_t pbytes = (size_t)(sc->n_planes ? sc->n_planes : 1) * sizeof(float4);
+    size_t mbytes = rs->S.env_mode == GR_ENV_LATLONG ? (size_t)rs->S.map_w * rs->S.map_h * 3 * sizeof(float) : 0;
+    size_t ebytes = (size_t)rs->S.ext_n * 2 * sizeof(float);
+    uint64_t total = pbytes + mbytes + ebytes;
+    if (ctx->resident_bytes + total > ctx->serve_budget) {
+        delete rs;
+        return fail(GR_EBUSY, "resident scene (%llu B) exceeds the device-memory budget", (unsigned long long)total);
+    }
+    if ((st = rs->planes.reserve(pbytes)) != GR_OK || (mbytes && (st = rs->map.reserve(mbytes)) != GR_OK) ||
+        (ebytes && (st = rs->ext.reserve(ebytes)) != GR_OK)) {
+        rs->planes.release();
+        rs->map.release();
+        rs->ext.release();
+        delete rs;
+        return st;
+    }
+    cudaError_t e = cudaSuccess;
+    if (sc->n_planes) e = cudaMemcpy(rs->planes.ptr, sc->planes, sc->n_planes * sizeof(gr_plane), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && mbytes) e = cudaMemcpy(rs->map.ptr, sc->env.latlong_rgb, mbytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && ebytes) {
+        e = cudaMemcpy(rs->ext.ptr, sc->material_ext->alpha_o_table, rs->S.ext_n * sizeof(float), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = cudaMemcpy((float *)rs->ext.ptr + rs->S.ext_n, sc->material_ext->alpha_e_table,
+                           rs->S.ext_n * sizeof(float), cudaMemcpyHostToDevice);
+    }
+    if (e != cudaSuccess) {
+        rs->planes.release();
+        rs->map.release();
+        rs->ext.release();
+        delete rs;
+        return fail(GR_ECUDA, "scene upload failed: %s", cudaGetErrorString(e));
+    }
+    rs->bytes = total;
+    ctx->resident_bytes += total;
+    uint64_t id = ctx->next_scene_id++;
+    ctx->scenes[id] = rs;
+    *out_id = id;
+    return GR_OK;
+}
+
+gr_status gr_scene_release(gr_ctx *ctx, uint64_t id) {
+    if (!ctx) return fail(GR_EINVAL, "ctx is NULL");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    auto it = ctx->scenes.find(id);
+    if (it == ctx->scenes.end()) return fail(GR_ENOTFOUND, "unknown scene id %llu", (unsigned long long)id);
+    GR_CUDA(cudaSetDevice(ctx->device));
+    GR_CUDA(cudaStreamSynchronize(ctx->stream));
+    ResidentScene *rs = it->second;
+    ctx->resident_bytes -= rs->bytes;
+    rs->planes.release();
+    rs->map.release();
+    rs->ext.release();
+    delete rs;
+    ctx->scenes.erase(it);
+    return GR_OK;
+}
+
+static grd::SceneBuffers resident_buffers(ResidentScene *rs) {
+    grd::SceneBuffers B;
+    std::memset(&B, 0, sizeof(B));
+    B.planes = (const float4 *)rs->planes.ptr;
+    B.map = (const float *)rs->map.ptr;
+    if (rs->S.ext_n) {
+        B.ext_alpha_o = (const float *)rs->ext.ptr;
+        B.ext_alpha_e = (const float *)rs->ext.ptr + rs->S.ext_n;
+    }
+    return B;
+}
+
+gr_status gr_render_resident(gr_ctx *ctx, uint64_t id, uint32_t sample_offset, uint32_t spp, float *film_dev,
+                             void *stream) {
+    if (!ctx) return fail(GR_EINVAL, "ctx is NULL");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    auto it = ctx->scenes.find(id);
+    if (it == ctx->scenes.end()) return fail(GR_ENOTFOUND, "unknown scene id %llu", (unsigned long long)id);
+    ResidentScene *rs = it->second;
+    const uint64_t n_pixels = (uint64_t)rs->S.width * rs->S.height;
+    if (spp == 0 || n_pixels == 0) return GR_OK;
+    if (!film_dev) return fail(GR_EINVAL, "film is NULL");
+    GR_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    gr_scene shape;
+    std::memset(&shape, 0, sizeof(shape));
+    shape.width = rs->S.width;
+    shape.height = rs->S.height;
+    return grh::render_into(ctx, &shape, rs->S, resident_buffers(rs), sample_offset, spp, film_dev, s);
+}
+
+gr_status gr_event_counts(gr_ctx *ctx, const gr_scene *sc, uint32_t first_pixel, uint32_t n_pixels,
+                          uint32_t sample_offset, uint32_t spp, uint64_t *counts, uint32_t n_counts) {
+    if (!ctx || !sc || !counts) return fail(GR_EINVAL, "NULL argument");
+    if (n_counts < GR_EVENT_COUNT) return fail(GR_EINVAL, "counts needs %u entries", GR_EVENT_COUNT);
+    if ((uint64_t)first_pixel + n_pixels > (uint64_t)sc->width * sc->height)
+        return fail(GR_EINVAL, "pixel range exceeds the frame");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    GR_CUDA(cudaSetDevice(ctx->device));
+    SceneConst S;
+    grd::SceneBuffers B;
+    gr_status st = grh::prepare(ctx, sc, S, B);
+    if (st != GR_OK) return st;
+    uint64_t n_tuples = (uint64_t)n_pixels * spp;
+    if (n_tuples == 0 || S.max_bounces == 0) {
+        for (uint32_t i = 0; i < GR_EVENT_COUNT; ++i) counts[i] = 0;
+        return GR_OK;
+    }
+    st = ctx->xyz.reserve((size_t)n_tuples * 3 * sizeof(float));
+    if (st != GR_OK) return st;
+    st = ctx->counter.reserve(sizeof(unsigned long long) * (1 + GR_EVENT_COUNT));
+    if (st != GR_OK) return st;
+    GR_CUDA(cudaMemsetAsync(ctx->counter.ptr, 0, sizeof(unsigned long long) * (1 + GR_EVENT_COUNT), ctx->stream));
+    grd::LaunchRange R;
+    R.first_pixel = first_pixel;
+    R.n_pixels = n_pixels;
+    R.sample_offset = sample_offset;
+    R.spp = spp;
+    R.n_tuples = n_tuples;
+    unsigned long long *dc = (unsigned long long *)ctx->counter.ptr;
+    size_t smem = (size_t)S.n_planes * sizeof(float4);
+    uint64_t want = (n_tuples + grd::TRACE_THREADS - 1) / grd::TRACE_THREADS;
+    uint64_t blocks = want < (uint64_t)ctx->persistent_blocks ? want : (uint64_t)ctx->persistent_blocks;
+    grd::k_trace_persistent<grd::Counters><<<(unsigned)blocks, grd::TRACE_THREADS, smem, ctx->stream>>>(
+        S, B, R, (float *)ctx->xyz.ptr, dc, dc + 1);
+    GR_CUDA(cudaGetLastError());
+    unsigned long long host[1 + GR_EVENT_COUNT];
+    GR_CUDA(cudaMemcpyAsync(host, dc, sizeof(host), cudaMemcpyDeviceToHost, ctx->stream));
+    GR_CUDA(cudaStreamSynchronize(ctx->stream));
+    for (uint32_t i = 0; i < GR_EVENT_COUNT; ++i) counts[i] = host[1 + i];
+    return GR_OK;
+}
+
+gr_status gr_probe_fp32_peak(gr_ctx *ctx, double *tflops) {
+    if (!ctx || !tflops) return fail(GR_EINVAL, "NULL argument");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    GR_CUDA(cudaSetDevice(ctx->device));
+    gr_status st = ctx->counter.reserve(64);
+    if (st != GR_OK) return st;
+    const unsigned threads = 256, blocks = (unsigned)ctx->sm_count * 8;
+    const uint32_t iters = 4096;
+    cudaEvent_t a, b;
+    GR_CUDA(cudaEventCreate(&a));
+    GR_CUDA(cudaEventCreate(&b));
+    grd::k_fp32_probe<<<blocks, threads, 0, ctx->stream>>>((float *)ctx->counter.ptr, 64, 1.0f);  // warm-up
+    float best = 1e30f;
+    for (int rep = 0; rep < 5; ++rep) {
+        cudaEventRecord(a, ctx->stream);
+        grd::k_fp32_probe<<<blocks, threads, 0, ctx->stream>>>((float *)ctx->counter.ptr, iters, 1.0f);
+        cudaEventRecord(b, ctx->stream);
+        GR_CUDA(cudaEventSynchronize(b));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        if (ms < best) best = ms;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    GR_CUDA(cudaGetLastError());
+    double flops = (double)blocks * threads * iters * 16.0 * 8.0 * 2.0;
+    *tflops = flops / (best * 1e-3) / 1e12;
+    return GR_OK;
+}
+
+gr_status gr_timing_enable(gr_ctx *ctx, uint32_t on) {
+    if (!ctx) return fail(GR_EINVAL, "ctx is NULL");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->timing = on != 0;
+    ctx->trace_used = ctx->fold_used = 0;
+    ctx->trace_launches = ctx->fold_launches = 0;
+    return GR_OK;
+}
+
+gr_status gr_timing_read(gr_ctx *ctx, double *trace_ms, double *fold_ms, uint64_t *trace_launches,
+                         uint64_t *fold_launches) {
+    if (!ctx) return fail(GR_EINVAL, "ctx is NULL");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    GR_CUDA(cudaSetDevice(ctx->device));
+    GR_CUDA(cudaStreamSynchronize(ctx->stream));
+    double t = 0.0, f = 0.0;
+    for (size_t i = 0; i < ctx->trace_used; ++i) {
+        GR_CUDA(cudaEventSynchronize(ctx->trace_ev[i].second));
+        float ms = 0.f;
+        GR_CUDA(cudaEventElapsedTime(&ms, ctx->trace_ev[i].first, ctx->trace_ev[i].second));
+        t += ms;
+    }
+    for (size_t i = 0; i < ctx->fold_used; ++i) {
+        GR_CUDA(cudaEventSynchronize(ctx->fold_ev[i].second));
+        float ms = 0.f;
+        GR_CUDA(cudaEventElapsedTime(&ms, ctx->fold_ev[i].first, ctx->fold_ev[i].second));
+        f += ms;
+    }
+    if (trace_ms) *trace_ms = t;
+    if (fold_ms) *fold_ms = f;
+    if (trace_launches) *trace_launches = ctx->trace_launches;
+    if (fold_launches) *fold_launches = ctx->fold_launches;
+    ctx->trace_used = ctx->fold_used = 0;
+    ctx->trace_launches = ctx->fold_launches = 0;
+    return GR_OK;
+}
+
+gr_status gr_set_kernel(gr_ctx *ctx, uint32_t kernel) {
+    if (!ctx) return fail(GR_EINVAL, "ctx is NULL");
+    if (kernel != GR_KERNEL_PLAIN && kernel != GR_KERNEL_PERSISTENT) return fail(GR_EINVAL, "unknown kernel %u", kernel);
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->kernel_mode = (int)kernel;
+    return GR_OK;
+}
+
+gr_status gr_synchronize(gr_ctx *ctx) {
+    if (!ctx) return fail(GR_EINVAL, "ctx is NULL");
+    GR_CUDA(cudaSetDevice(ctx->device));
+    GR_CUDA(cudaStreamSynchronize(ctx->stream));
+    return GR_OK;
+}
+
+void *gr_stream(gr_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+}  // extern "C"

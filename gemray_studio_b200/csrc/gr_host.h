@@ -1,0 +1,23 @@
+// gr_host.h -- internal host-side declarations shared by the C-ABI translation units.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include "gemray_cuda.h"
+
+namespace grh {
+
+// A lazily grown device allocation owned by a context (the reference's
+// `ensure_capacity`, renderer/gpu/frame.rs:868-879).
+struct DeviceBuffer {
+    void *ptr = nullptr;
+    size_t cap = 0;
+    gr_status reserve(size_t bytes);
+    void release();
+};
+
+// Device tone map (gr_tonemap.cu): rgba_dev[i] = sRGB ACES encode of xyz_dev[i] * scale.
+gr_status tonemap_device(const float *xyz_dev, float scale, uint32_t n, void *rgba_dev, struct CUstream_st *s);
+
+}  // namespace grh

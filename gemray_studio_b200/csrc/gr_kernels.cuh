@@ -1,0 +1,196 @@
+// gr_kernels.cuh -- transport and film kernels (sm_100a).
+//
+// Work unit: a tuple t in [0, n_pixels * spp) of one launch maps to
+//   pixel = first_pixel + t / spp, absolute sample = sample_offset + t % spp,
+// the reference kernel's `idx = pixel * spp + s` numbering
+// (renderer/shaders/spectral_transport.wgsl:672-691), and its XYZ lands in
+// xyz[3 * t .. 3 * t + 3).  A film kernel then folds each pixel's spp samples in
+// sample order and adds the sum once to the film -- the reference's per-pixel
+// `sum += sample; accum[p] += sum` (renderer/gpu/frame.rs:799-814).
+#pragma once
+
+#include "gr_trace.cuh"
+
+namespace grd {
+
+constexpr int TRACE_THREADS = 128;
+
+struct LaunchRange {
+    uint32_t first_pixel;
+    uint32_t n_pixels;
+    uint32_t sample_offset;
+    uint32_t spp;
+    uint64_t n_tuples;  // n_pixels * spp
+};
+
+__device__ __forceinline__ void stage_planes(float4 *sp, const float4 *__restrict__ gp, uint32_t n) {
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) sp[i] = gp[i];
+    __syncthreads();
+}
+
+__device__ __forceinline__ void tuple_coords(const LaunchRange &R, uint64_t t, uint32_t &pixel, uint32_t &sample) {
+    uint32_t local_pixel = (uint32_t)(t / R.spp);
+    uint32_t s = (uint32_t)(t - (uint64_t)local_pixel * R.spp);
+    pixel = R.first_pixel + local_pixel;
+    sample = R.sample_offset + s;  // u32 wrapping add, as the reference's wrapping_add
+}
+
+// Plain kernel: one thread traces one tuple start to finish.
+__global__ void __launch_bounds__(TRACE_THREADS) k_trace_plain(SceneConst S, SceneBuffers B, LaunchRange R,
+                                                               float *__restrict__ xyz) {
+    extern __shared__ float4 s_planes[];
+    stage_planes(s_planes, B.planes, S.n_planes);
+    uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= R.n_tuples) return;
+    uint32_t pixel, sample;
+    tuple_coords(R, t, pixel, sample);
+    Path P;
+    path_init(P, S, B, pixel, sample, (uint32_t)t);
+    P.alive = S.max_bounces > 0;
+    NoCounters nc;
+    while (P.alive) path_step(P, S, s_planes, nc);
+    V3 c = path_finish(P, S, B);
+    xyz[3 * t + 0] = c.x;
+    xyz[3 * t + 1] = c.y;
+    xyz[3 * t + 2] = c.z;
+}
+
+// Persistent kernel with path regeneration: each warp claims up to 32 consecutive
+// tuples at a time from a global counter; a lane whose path ends writes its XYZ and
+// takes the next unassigned tuple of the claim, so every bounce step runs with
+// (nearly) all 32 lanes busy instead of idling behind the warp's longest path.
+// Requires max_bounces >= 1 (the host routes max_bounces == 0 to k_trace_plain).
+template <class CT>
+__global__ void __launch_bounds__(TRACE_THREADS) k_trace_persistent(SceneConst S, SceneBuffers B, LaunchRange R,
+                                                                    float *__restrict__ xyz,
+                                                                    unsigned long long *__restrict__ counter,
+                                                                    unsigned long long *__restrict__ tallies) {
+    extern __shared__ float4 s_planes[];
+    stage_planes(s_planes, B.planes, S.n_planes);
+    const uint32_t lane = threadIdx.x & 31u;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    uint64_t next = 0;     // next unassigned tuple of the warp's claim (warp-uniform)
+    uint32_t avail = 0;    // unassigned tuples left in the claim (warp-uniform)
+    bool exhausted = false;
+    bool have = false;
+    Path P;
+    CT ct;
+    if constexpr (sizeof(CT) == sizeof(Counters)) {
+        for (int i = 0; i < C_COUNT; ++i) ((Counters &)ct).c[i] = 0;
+    }
+    for (;;) {
+        unsigned need = __ballot_sync(0xffffffffu, !have);
+        while (need && !exhausted) {
+            if (avail == 0) {
+                unsigned long long b = 0;
+                if (lane == 0) b = atomicAdd(counter, 32ull);
+                b = __shfl_sync(0xffffffffu, b, 0);
+                if (b >= R.n_tuples) {
+                    exhausted = true;
+                    break;
+                }
+                next = b;
+                uint64_t left = R.n_tuples - b;
+                avail = left < 32ull ? (uint32_t)left : 32u;
+            }
+            const uint32_t cnt = (uint32_t)__popc(need);
+            const uint32_t take = cnt < avail ? cnt : avail;
+            const uint32_t rank = (uint32_t)__popc(need & lt_mask);
+            const bool mine = ((need >> lane) & 1u) && rank < take;
+            if (mine) {
+                uint64_t t = next + rank;
+                uint32_t pixel, sample;
+                tuple_coords(R, t, pixel, sample);
+                path_init(P, S, B, pixel, sample, (uint32_t)t);
+                tally(ct, C_PATHS);
+                have = true;
+            }
+            next += take;
+            avail -= take;
+            need &= ~__ballot_sync(0xffffffffu, mine);
+        }
+        if (__ballot_sync(0xffffffffu, have) == 0) break;
+        if (have) {
+            path_step(P, S, s_planes, ct);
+            if (!P.alive) {
+                V3 c = path_finish(P, S, B);
+                const uint64_t t = P.tuple;
+                xyz[3 * t + 0] = c.x;
+                xyz[3 * t + 1] = c.y;
+                xyz[3 * t + 2] = c.z;
+                have = false;
+            }
+        }
+    }
+    if constexpr (sizeof(CT) == sizeof(Counters)) {
+        for (int i = 0; i < C_COUNT; ++i) {
+            unsigned long long v = ((Counters &)ct).c[i];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+            if (lane == 0 && v) atomicAdd(tallies + i, v);
+        }
+    }
+}
+
+// Film kernel: one warp per pixel.  Lanes load 32 samples at a time (coalesced);
+// every lane then folds them in sample order with shuffles, so the sum is the exact
+// sequential f32 sum the reference forms on the host.  Kahan mode keeps a
+// compensation term instead (flags & GR_FLAG_KAHAN_FILM).
+__global__ void k_film_fold(const float *__restrict__ xyz, uint32_t n_pixels, uint32_t spp, uint32_t first_pixel,
+                            float *__restrict__ film, uint32_t kahan) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (warp >= n_pixels) return;
+    const float *src = xyz + (size_t)warp * spp * 3;
+    float sx = 0.0f, sy = 0.0f, sz = 0.0f;
+    float cx = 0.0f, cy = 0.0f, cz = 0.0f;
+    for (uint32_t s0 = 0; s0 < spp; s0 += 32) {
+        uint32_t s = s0 + lane;
+        float x = 0.f, y = 0.f, z = 0.f;
+        if (s < spp) {
+            x = src[3 * s + 0];
+            y = src[3 * s + 1];
+            z = src[3 * s + 2];
+        }
+        uint32_t cnt = spp - s0 < 32u ? spp - s0 : 32u;
+        for (uint32_t j = 0; j < cnt; ++j) {
+            float vx = __shfl_sync(0xffffffffu, x, j);
+            float vy = __shfl_sync(0xffffffffu, y, j);
+            float vz = __shfl_sync(0xffffffffu, z, j);
+            if (kahan) {
+                float yx = vx - cx, tx = sx + yx; cx = (tx - sx) - yx; sx = tx;
+                float yy = vy - cy, ty = sy + yy; cy = (ty - sy) - yy; sy = ty;
+                float yz = vz - cz, tz = sz + yz; cz = (tz - sz) - yz; sz = tz;
+            } else {
+                sx = sx + vx;
+                sy = sy + vy;
+                sz = sz + vz;
+            }
+        }
+    }
+    if (lane == 0) {
+        size_t p = (size_t)(first_pixel + (uint32_t)warp) * 3;
+        film[p + 0] = film[p + 0] + sx;
+        film[p + 1] = film[p + 1] + sy;
+        film[p + 2] = film[p + 2] + sz;
+    }
+}
+
+static_assert(C_COUNT == GR_EVENT_COUNT, "counter layout");
+
+// FP32 throughput probe: 8 independent FMA chains per thread (2 flops per FMA).
+__global__ void k_fp32_probe(float *__restrict__ out, uint32_t iters, float seed) {
+    float a0 = seed + threadIdx.x, a1 = a0 + 1.f, a2 = a0 + 2.f, a3 = a0 + 3.f;
+    float a4 = a0 + 4.f, a5 = a0 + 5.f, a6 = a0 + 6.f, a7 = a0 + 7.f;
+    const float m = 0.9999999f, c = 1e-7f;
+    for (uint32_t i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            a0 = fmaf(a0, m, c); a1 = fmaf(a1, m, c); a2 = fmaf(a2, m, c); a3 = fmaf(a3, m, c);
+            a4 = fmaf(a4, m, c); a5 = fmaf(a5, m, c); a6 = fmaf(a6, m, c); a7 = fmaf(a7, m, c);
+        }
+    }
+    float r = ((a0 + a1) + (a2 + a3)) + ((a4 + a5) + (a6 + a7));
+    if (r == 12345.678f) out[0] = r;  // keep the chains live
+}
+
+}  // namespace grd

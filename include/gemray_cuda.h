@@ -1,0 +1,354 @@
+/*
+ * gemray_cuda.h -- C ABI of the B200 spectral-transport engine.
+ *
+ * This is the drop-in boundary for gemray's `gpu`-feature render path.  Every entry
+ * point below replaces one item of the reference's Rust GPU backend; the comment
+ * above each declaration names the reference item (path:line inside the
+ * gemray-studio workspace) whose contract it keeps.
+ *
+ * Conventions
+ *   - Plain C: fixed-width integers, float, pointers and sizes.  No CUDA or torch
+ *     types appear in any signature; streams are passed as `void*` (a cudaStream_t).
+ *   - Every call returns a gr_status.  Nothing aborts the process; a failing call
+ *     leaves caller buffers untouched and records a message readable through
+ *     gr_last_error_string().
+ *   - Struct layouts are frozen (see the static asserts at the end of this file).
+ *     gr_plane, gr_band and gr_material are byte-identical to the reference's
+ *     `GpuFacetPlane`, `GpuAbsorptionBand` and `GpuGemMaterial`
+ *     (crates/gemray/src/geometry/plane.rs:6-9, renderer/buffers.rs:148-165,236-299),
+ *     so a Rust caller can pass `bytemuck::bytes_of(&GpuGemMaterial::encode(m))`.
+ */
+#ifndef GEMRAY_CUDA_H
+#define GEMRAY_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GR_ABI_VERSION 1u
+/* Per-band-set limit, = MAX_ABSORPTION_BANDS (renderer/buffers.rs:148). */
+#define GR_MAX_BANDS 8u
+/* Largest facet-plane count a scene may carry (planes are staged in shared memory). */
+#define GR_MAX_PLANES 512u
+/* Largest bounce cap accepted (= worker MAX_BOUNCES, apps/gemray-worker/src/validate/mod.rs). */
+#define GR_MAX_BOUNCES 4096u
+
+/* Status codes.  GR_DECLINED_* mirror GpuFrameError (renderer/gpu/frame.rs:196-210):
+ * they mean "render this on the CPU tracer instead", exactly like a `false` from
+ * GpuBackend::try_accumulate (renderer/gpu_backend.rs:160-193). */
+typedef enum gr_status {
+    GR_OK = 0,
+    GR_DECLINED_ENV = 1,      /* environment kind not handled on the device */
+    GR_DECLINED_MATERIAL = 2, /* material/finish kind not handled on the device */
+    GR_NO_DEVICE = 3,         /* no usable CUDA device (GpuAcquireError) */
+    GR_EINVAL = 4,            /* bad argument (length mismatch, null pointer, limits) */
+    GR_ENOMEM = 5,            /* device or pinned-host allocation failed */
+    GR_ETIMEOUT = 6,          /* a bounded wait ran out */
+    GR_ECANCELLED = 7,        /* request cancelled before completion */
+    GR_ECUDA = 8,             /* CUDA runtime error; see gr_last_error_string() */
+    GR_EBUSY = 9,             /* admission refused: device-memory budget exhausted */
+    GR_ENOTFOUND = 10         /* unknown scene or request id */
+} gr_status;
+
+/* One half-space: inside <=> dot(normal, x) + d <= 0.  = GpuFacetPlane. */
+typedef struct gr_plane {
+    float normal[3];
+    float d;
+} gr_plane;
+
+/* One Gaussian absorption band.  = GpuAbsorptionBand. */
+typedef struct gr_band {
+    float center_nm;
+    float width_nm;
+    float peak;
+} gr_band;
+
+/* Dispersion model ids, = dispersion_model_type (renderer/buffers.rs:117-121). */
+#define GR_DISP_SELLMEIER1 0u
+#define GR_DISP_SELLMEIER3 1u
+#define GR_DISP_CAUCHY 2u
+
+/* = DispersionParams (renderer/buffers.rs:84-99).  Sellmeier1: a=[b1], b=[c1];
+ * Sellmeier3: a=b[0..3], b=c[0..3]; Cauchy: a=[A, B, C].  c_axis_and_birefringence
+ * = (c_axis.xyz, n_e - n_o). */
+typedef struct gr_dispersion {
+    uint32_t model_type;
+    uint32_t pad0[3];
+    float param_a[4];
+    float param_b[4];
+    float param_c[4];
+    float c_axis_and_birefringence[4];
+    uint32_t is_anisotropic;
+    float biaxial_delta_beta_alpha;
+    uint32_t has_biaxial_delta;
+    float pad_tail;
+} gr_dispersion;
+
+/* Crystal-system ids, = crystal_system (renderer/buffers.rs:170-178). */
+#define GR_CRYSTAL_CUBIC 0u
+
+/* = GpuGemMaterial (renderer/buffers.rs:236-299), 432 bytes. */
+typedef struct gr_material {
+    gr_dispersion dispersion;
+    uint32_t crystal_system;
+    uint32_t optical_character;
+    uint32_t is_pleochroic;
+    uint32_t o_ray_band_count;
+    uint32_t e_ray_band_count;
+    gr_band o_ray_bands[GR_MAX_BANDS];
+    gr_band e_ray_bands[GR_MAX_BANDS];
+    float scattering_sigma_s;
+    float scattering_g;
+    float edge_rounding_radius;
+    uint32_t has_beta_ray;
+    uint32_t beta_ray_band_count;
+    gr_band beta_ray_bands[GR_MAX_BANDS];
+    float absorption_path_scale;
+    uint32_t pad_trailing;
+} gr_material;
+
+/* Pinhole camera, = optics::raytracer::Camera (optics/raytracer/camera.rs:53-59).
+ * The host builds it (Camera::new uses libm sin/cos/tan); the device only reads it. */
+typedef struct gr_camera {
+    float origin[3];
+    float forward[3];
+    float right[3];
+    float up[3];
+    float fov_tan;
+} gr_camera;
+
+/* Environment kinds.  UNIFORM is EnvironmentMap::uniform (renderer/env_map.rs:163-168),
+ * STUDIO is EnvironmentSource::Studio (optics/raytracer/environment.rs:187-196),
+ * LATLONG is EnvironmentSource::HdrMap over an RGB f32 lat-long map. */
+#define GR_ENV_UNIFORM 0u
+#define GR_ENV_STUDIO 1u
+#define GR_ENV_LATLONG 2u
+
+typedef struct gr_environment {
+    uint32_t mode;
+    /* GR_ENV_UNIFORM: the map's single RGB radiance. */
+    float uniform_rgb[3];
+    /* GR_ENV_STUDIO: LightingPreset::params() (temp_k, spot_mult) plus the pose. */
+    float temp_k;
+    float spot_mult;
+    float exposure;
+    float light_yaw;
+    float light_pitch;
+    /* GR_ENV_LATLONG: row-major RGB f32 texels, latlong_w * latlong_h * 3 floats,
+     * row 0 at the +Y pole (v = 0).  Borrowed for the duration of the call. */
+    const float *latlong_rgb;
+    uint32_t latlong_w;
+    uint32_t latlong_h;
+} gr_environment;
+
+/* Optional extension material data (not in the reference model): tabulated
+ * absorption and a wavelength-dependent birefringence.  Pass NULL for reference
+ * behaviour.  Tables are sampled at nm_first + i * nm_step and linearly
+ * interpolated (clamped at the ends). */
+typedef struct gr_material_ext {
+    uint32_t n_absorption;      /* entries per table, 0 = use the Gaussian bands */
+    float absorption_nm_first;
+    float absorption_nm_step;
+    const float *alpha_o_table; /* n_absorption values */
+    const float *alpha_e_table; /* n_absorption values */
+    uint32_t has_cauchy_e;      /* 1 = n_e from its own Cauchy fit below */
+    float cauchy_e[3];          /* n_e(lambda) = a + b/l^2 + c/l^4, lambda in um */
+} gr_material_ext;
+
+/* Scene flags. */
+#define GR_FLAG_KAHAN_FILM 0x1u /* compensated per-pixel sample sum (default: plain f32 in sample order) */
+
+/* One render scene, = GpuSceneRef (renderer/gpu_backend.rs:85-99).  Every pointer is
+ * borrowed for the duration of the call. */
+typedef struct gr_scene {
+    gr_camera camera;
+    uint32_t width;
+    uint32_t height;
+    uint32_t max_bounces;
+    uint32_t n_planes;
+    const gr_plane *planes;    /* n_planes entries */
+    const uint32_t *finishes;  /* NULL or n_planes entries: 0 = polished, 1 = frosted */
+    const gr_material *material;
+    const gr_material_ext *material_ext; /* NULL = reference material model */
+    gr_environment env;
+    uint32_t flags;
+    uint32_t reserved;
+} gr_scene;
+
+/* Context creation options (NULL = defaults). */
+typedef struct gr_create_opts {
+    int32_t device;               /* CUDA device ordinal, -1 = current/0 */
+    uint64_t chunk_budget_bytes;  /* per-launch scratch budget, 0 = default (256 MiB) */
+    uint64_t serve_budget_bytes;  /* device-memory budget for resident scenes/films, 0 = 60 GiB */
+} gr_create_opts;
+
+typedef struct gr_ctx gr_ctx;
+
+/* ---- backend lifecycle ------------------------------------------------------ */
+
+/* Replaces GpuBackend::acquire / GpuFrameRenderer::new (renderer/gpu_backend.rs:114-126,
+ * renderer/gpu/frame.rs:574-594).  On failure *out is NULL and GR_NO_DEVICE/GR_ECUDA
+ * is returned; the caller then behaves like GpuBackend::disabled(). */
+gr_status gr_create(gr_ctx **out, const gr_create_opts *opts);
+
+/* Releases every device resource owned by the context.  NULL is accepted. */
+gr_status gr_destroy(gr_ctx *ctx);
+
+/* Replaces GpuBackend::adapter_label (renderer/gpu_backend.rs:146-153): a
+ * NUL-terminated device description owned by the context. */
+const char *gr_device_label(gr_ctx *ctx);
+
+/* Message for the most recent failing call on this thread ("" if none). */
+const char *gr_last_error_string(void);
+
+/* ABI version of the loaded library (GR_ABI_VERSION at build time). */
+uint32_t gr_abi_version(void);
+
+/* ---- the render path -------------------------------------------------------- */
+
+/* Replaces GpuBackend::try_accumulate -> GpuFrameRenderer::accumulate
+ * (renderer/gpu_backend.rs:160-193, renderer/gpu/frame.rs:632-647,664-814).
+ * Traces samples [sample_offset, sample_offset + spp) of every pixel and ADDS each
+ * pixel's sample sum (summed in sample order, then added once) into accum_xyz, a
+ * host array of width*height*3 floats (Vec3 per pixel).  spp == 0 or an empty frame
+ * is a no-op returning GR_OK.  A declined scene leaves accum_xyz untouched. */
+gr_status gr_accumulate(gr_ctx *ctx, const gr_scene *scene, uint32_t sample_offset,
+                        uint32_t spp, float *accum_xyz);
+
+/* As gr_accumulate, but accum_xyz is a DEVICE pointer (width*height*3 floats) and the
+ * work is enqueued on `stream` (a cudaStream_t, NULL = the context's stream).  The
+ * call returns once the work is enqueued; scene data is uploaded first. */
+gr_status gr_accumulate_device(gr_ctx *ctx, const gr_scene *scene, uint32_t sample_offset,
+                               uint32_t spp, float *accum_xyz_device, void *stream);
+
+/* Per-sample XYZ for samples [sample_offset, sample_offset + spp) of pixels
+ * [first_pixel, first_pixel + n_pixels) into a host array of n_pixels*spp*3 floats,
+ * ordered (pixel, sample) -- the reference kernel's per-tuple output layout
+ * (renderer/shaders/spectral_transport.wgsl:672-691).  Used by parity tests. */
+gr_status gr_trace_samples(gr_ctx *ctx, const gr_scene *scene, uint32_t first_pixel,
+                           uint32_t n_pixels, uint32_t sample_offset, uint32_t spp,
+                           float *xyz_out);
+
+/* Device-side tone map: rgba[i] = ColorSpace::Srgb.encode(xyz[i] * scale, ACES)
+ * (renderer/tonemap.rs:52-108, color/space.rs:290-334).  Host arrays. */
+gr_status gr_tonemap(gr_ctx *ctx, const float *xyz, float scale, uint32_t n_px,
+                     uint8_t *rgba);
+
+/* ---- verification hooks --------------------------------------------------------- */
+
+/* One sampler record, the device analogue of the reference's RngRecord
+ * (renderer/gpu/rng_check.rs:54-109, shaders/rng_equivalence.wgsl:154): the per-sample
+ * seed and stratified draws (optics/raytracer/sampling.rs:232-271) and, for bounces
+ * 0..3, the Fresnel, Russian-roulette, birefringent-split and mode-coupling draws. */
+typedef struct gr_rng_record {
+    uint32_t seed;
+    float jitter_x;
+    float jitter_y;
+    float hero_rand;
+    float draws[4][4]; /* [bounce][fresnel, roulette, split, coupling] */
+} gr_rng_record;
+
+/* Device sampler records for n (pixel, sample) pairs (host arrays). */
+gr_status gr_rng_records(gr_ctx *ctx, const uint32_t *pixels, const uint32_t *samples, uint32_t n,
+                         gr_rng_record *out);
+
+/* Event tallies of an instrumented launch over samples [sample_offset, +spp) of pixels
+ * [first_pixel, +n_pixels) -- the inputs of the algorithmic FLOP model (extends
+ * trace_spectral_ray_with_finish_instrumented, optics/raytracer/transport.rs:512-537).
+ * counts[GR_EVENT_*] must hold GR_EVENT_COUNT entries. */
+#define GR_EVENT_PATHS 0u
+#define GR_EVENT_BOUNCES 1u        /* intersection tests (including the final miss) */
+#define GR_EVENT_ESCAPES 2u
+#define GR_EVENT_TIR 3u
+#define GR_EVENT_REFLECT 4u
+#define GR_EVENT_REFRACT 5u
+#define GR_EVENT_ABSORB 6u         /* interior segments with Beer-Lambert absorption */
+#define GR_EVENT_CHANNEL_TIR 7u    /* per-channel TIR phase evaluations */
+#define GR_EVENT_CHANNEL_REFRACT 8u
+#define GR_EVENT_ROULETTE 9u
+#define GR_EVENT_ROTATIONS 10u     /* Stokes frame rotations */
+#define GR_EVENT_ANISO_BOUNCES 11u
+#define GR_EVENT_WALKOFF 12u
+#define GR_EVENT_ROULETTE_KILLS 13u
+#define GR_EVENT_COUNT 14u
+gr_status gr_event_counts(gr_ctx *ctx, const gr_scene *scene, uint32_t first_pixel, uint32_t n_pixels,
+                          uint32_t sample_offset, uint32_t spp, uint64_t *counts, uint32_t n_counts);
+
+/* Measured dense FP32 FMA throughput of the device (TFLOP/s), the roofline
+ * denominator of the transport kernels. */
+gr_status gr_probe_fp32_peak(gr_ctx *ctx, double *tflops);
+
+/* ---- resident scenes (serving / benchmarks) ------------------------------------- */
+
+/* Copies a scene to the device once (planes, map, tables, encoded constants) and
+ * returns its id.  GR_EBUSY if it does not fit the context's serve budget.  Mirrors
+ * the reference worker keeping a scene across sub-batches
+ * (apps/gemray-worker/src/stream_emit/tracer.rs:64). */
+gr_status gr_scene_upload(gr_ctx *ctx, const gr_scene *scene, uint64_t *scene_id);
+gr_status gr_scene_release(gr_ctx *ctx, uint64_t scene_id);
+
+/* gr_accumulate_device for a resident scene: no host data is read. */
+gr_status gr_render_resident(gr_ctx *ctx, uint64_t scene_id, uint32_t sample_offset, uint32_t spp,
+                             float *film_device, void *stream);
+
+/* ---- engine controls ---------------------------------------------------------- */
+
+/* Transport kernel selection.  PLAIN: one thread per (pixel, sample) tuple, the
+ * reference kernel's launch shape.  PERSISTENT (default): persistent warps that
+ * regenerate finished paths from a global tuple counter.  Results are identical. */
+#define GR_KERNEL_PLAIN 0u
+#define GR_KERNEL_PERSISTENT 1u
+gr_status gr_set_kernel(gr_ctx *ctx, uint32_t kernel);
+
+/* Per-launch timing: while enabled, every trace and film-fold launch is bracketed by
+ * CUDA events on its own stream.  gr_timing_read waits for them, returns the summed
+ * kernel milliseconds and launch counts since the last read (or enable), and resets. */
+gr_status gr_timing_enable(gr_ctx *ctx, uint32_t on);
+gr_status gr_timing_read(gr_ctx *ctx, double *trace_ms, double *fold_ms, uint64_t *trace_launches,
+                         uint64_t *fold_launches);
+
+/* Waits for all work enqueued on the context's stream. */
+gr_status gr_synchronize(gr_ctx *ctx);
+
+/* The context's CUDA stream (a cudaStream_t) for callers that enqueue around it. */
+void *gr_stream(gr_ctx *ctx);
+
+/* ---- scene builders (host only, no device work) --------------------------------- */
+
+/* = Camera::new(yaw, pitch, distance, fov_deg) (optics/raytracer/camera.rs:62-93). */
+gr_status gr_camera_new(float yaw, float pitch, float distance, float fov_deg, gr_camera *out);
+
+/* = StandardGemCuts::standard_round_brilliant (geometry/cuts.rs:45-129): writes up to
+ * cap planes and returns the full count (74). */
+uint32_t gr_standard_round_brilliant(gr_plane *out, uint32_t cap);
+
+/* = GpuGemMaterial::encode(&GemMaterial::by_name(name)) for the 13 built-in materials
+ * (optics/materials.rs:136-1250, renderer/buffers.rs:313-385); exact-name match.
+ * GR_ENOTFOUND for an unknown name. */
+gr_status gr_builtin_material(const char *name, gr_material *out);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#ifdef __cplusplus
+static_assert(sizeof(gr_plane) == 16, "gr_plane = GpuFacetPlane");
+static_assert(sizeof(gr_band) == 12, "gr_band = GpuAbsorptionBand");
+static_assert(sizeof(gr_dispersion) == 96, "gr_dispersion = DispersionParams");
+static_assert(offsetof(gr_dispersion, param_a) == 16, "layout");
+static_assert(offsetof(gr_dispersion, c_axis_and_birefringence) == 64, "layout");
+static_assert(offsetof(gr_dispersion, is_anisotropic) == 80, "layout");
+static_assert(sizeof(gr_material) == 432, "gr_material = GpuGemMaterial");
+static_assert(offsetof(gr_material, crystal_system) == 96, "layout");
+static_assert(offsetof(gr_material, o_ray_bands) == 116, "layout");
+static_assert(offsetof(gr_material, e_ray_bands) == 212, "layout");
+static_assert(offsetof(gr_material, scattering_sigma_s) == 308, "layout");
+static_assert(offsetof(gr_material, beta_ray_bands) == 328, "layout");
+static_assert(offsetof(gr_material, absorption_path_scale) == 424, "layout");
+static_assert(sizeof(gr_camera) == 52, "gr_camera");
+#endif
+
+#endif /* GEMRAY_CUDA_H */

@@ -1,0 +1,280 @@
+// gro_capi.cpp -- C entry points of the oracle for the Python test suite and the
+// CPU-baseline leg of bench.py.
+//
+// TEST INFRASTRUCTURE ONLY (see gr_oracle.hpp).  Threading mirrors the reference
+// worker's `trace_into` (apps/gemray-worker/src/render_core/mod.rs:220-317): one
+// thread per core claiming rows through an atomic counter; each pixel's samples are
+// summed in sample order from zero and the sum is then added once to the film.
+#include <atomic>
+#include <cstdint>
+#include <cstring>
+#include <thread>
+#include <vector>
+
+#include "gr_oracle.hpp"
+#include "gro_scene.hpp"
+
+using namespace gro;
+
+namespace {
+
+template <class R>
+void trace_pixel_samples(const gr_scene &sc, const MaterialCtx<R> &mc, const EnvCtx<R> &env, uint32_t pixel,
+                         uint32_t sample_offset, uint32_t spp, float *per_sample /* spp*3 or null */,
+                         double sum_out[3], EventLog *logs) {
+    uint32_t x = pixel % sc.width, y = pixel / sc.width;
+    PixelRotations rot = pixel_rotations(pixel);
+    V3<R> sum;
+    for (uint32_t s = 0; s < spp; ++s) {
+        uint32_t sample_num = sample_offset + s;
+        SampleDraws d = sample_draws(pixel, sample_num, rot);
+        Ray<float> ray = generate_ray(sc.camera, (float)x, (float)y, (float)sc.width, (float)sc.height, d.jitter_x,
+                                      d.jitter_y);
+        EventLog *lg = logs ? &logs[s] : nullptr;
+        if (lg) std::memset(lg, 0, sizeof(EventLog));
+        V3<R> xyz = trace_spectral_ray<R>(ray, sc.planes, sc.n_planes, mc, env, sc.max_bounces, d.seed, d.hero_rand, lg);
+        if (per_sample) {
+            per_sample[3 * s + 0] = (float)xyz.x;
+            per_sample[3 * s + 1] = (float)xyz.y;
+            per_sample[3 * s + 2] = (float)xyz.z;
+        }
+        sum = sum + xyz;
+    }
+    sum_out[0] = (double)sum.x; sum_out[1] = (double)sum.y; sum_out[2] = (double)sum.z;
+}
+
+template <class R>
+int accumulate_impl(const gr_scene *sc, uint32_t sample_offset, uint32_t spp, float *accum_f, double *accum_d,
+                    int threads) {
+    if (!sc || (!accum_f && !accum_d)) return GR_EINVAL;
+    if (spp == 0 || sc->width == 0 || sc->height == 0) return GR_OK;
+    if (!material_supported(sc->material, sc->finishes, sc->n_planes)) return GR_DECLINED_MATERIAL;
+    MaterialCtx<R> mc = make_material<R>(sc->material, sc->material_ext);
+    EnvCtx<R> env = make_env<R>(sc->env);
+    if (threads <= 0) threads = (int)std::thread::hardware_concurrency();
+    if (threads <= 0) threads = 1;
+    std::atomic<uint32_t> next_row(0);
+    auto worker = [&]() {
+        for (;;) {
+            uint32_t y = next_row.fetch_add(1);
+            if (y >= sc->height) break;
+            for (uint32_t x = 0; x < sc->width; ++x) {
+                uint32_t p = y * sc->width + x;
+                double s[3];
+                trace_pixel_samples<R>(*sc, mc, env, p, sample_offset, spp, nullptr, s, nullptr);
+                for (int c = 0; c < 3; ++c) {
+                    if (accum_f) accum_f[3 * (size_t)p + c] = (float)((R)accum_f[3 * (size_t)p + c] + (R)s[c]);
+                    if (accum_d) accum_d[3 * (size_t)p + c] += s[c];
+                }
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; ++t) pool.emplace_back(worker);
+    for (auto &t : pool) t.join();
+    return GR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t gro_hash_u32(uint32_t x) { return hash_u32(x); }
+
+float gro_rng_draw(uint32_t seed, uint32_t bounce, uint32_t stream) { return rng_draw(seed, bounce, stream); }
+
+float gro_radical_inverse(uint32_t n, uint32_t base) { return radical_inverse_base(n, base); }
+
+// Bulk sampler: (pixel[i], sample[i]) -> seed, jitter_x, jitter_y, hero_rand.
+void gro_sample_draws(const uint32_t *pixels, const uint32_t *samples, uint64_t n, uint32_t *seed, float *jx,
+                      float *jy, float *hero) {
+    for (uint64_t i = 0; i < n; ++i) {
+        PixelRotations r = pixel_rotations(pixels[i]);
+        SampleDraws d = sample_draws(pixels[i], samples[i], r);
+        seed[i] = d.seed; jx[i] = d.jitter_x; jy[i] = d.jitter_y; hero[i] = d.hero_rand;
+    }
+}
+
+void gro_camera_new(float yaw, float pitch, float distance, float fov_deg, gr_camera *out) {
+    *out = camera_new(yaw, pitch, distance, fov_deg);
+}
+
+uint32_t gro_standard_round_brilliant(gr_plane *out, uint32_t cap) {
+    std::vector<gr_plane> p = standard_round_brilliant();
+    for (uint32_t i = 0; i < p.size() && i < cap; ++i) out[i] = p[i];
+    return (uint32_t)p.size();
+}
+
+int gro_builtin_material(const char *name, gr_material *out) { return builtin_material(name, out) ? 0 : -1; }
+
+void gro_white_balance(float temp_k, float out[3]) {
+    V3<float> w = compute_illuminant_white_balance<float>(temp_k);
+    out[0] = w.x; out[1] = w.y; out[2] = w.z;
+}
+
+float gro_studio_env(const float dir[3], float lambda, float temp_k, float spot_mult, float exposure, float yaw,
+                     float pitch) {
+    StudioRig<float> rig = studio_rig_new<float>(yaw, pitch);
+    return studio_radiance<float>(V3<float>(dir[0], dir[1], dir[2]), lambda, temp_k, spot_mult, exposure, rig);
+}
+
+// Studio radiance with the blackbody factor supplied by the caller (isolates libm
+// rounding of the blackbody from the rest of environment.rs:280-321).
+float gro_studio_env_spec(const float dir[3], float spec, float spot_mult, float exposure, float yaw, float pitch) {
+    StudioRig<float> rig = studio_rig_new<float>(yaw, pitch);
+    V3<float> d = V3<float>(dir[0], dir[1], dir[2]).normalize();
+    float bg = rmax(::fmaf(0.012f, ::fmaf(d.y, 0.5f, 0.5f), 0.015f), 0.005f) * exposure;
+    float rad = bg * spec;
+    float key_dot = rmax(d.dot(rig.key), 0.0f);
+    if (key_dot > 0.0f) rad = ::fmaf(powi(key_dot, 28) * 12.0f * spot_mult * exposure, spec, rad);
+    float fill_dot = rmax(d.dot(rig.fill), 0.0f);
+    if (fill_dot > 0.0f) rad = ::fmaf(powi(fill_dot, 18) * 4.5f * exposure, spec, rad);
+    for (int i = 0; i < 16; ++i) {
+        float ring_dot = rmax(d.dot(rig.ring[i]), 0.0f);
+        if (ring_dot > 0.96f) rad = ::fmaf(powi((ring_dot - 0.96f) / 0.04f, 6) * 22.0f * spot_mult * exposure, spec, rad);
+    }
+    return rad;
+}
+
+float gro_exp_poly(float x) { return M<float>::exp_poly(x); }
+
+// One traced sample with an explicit ray (the golden tests' entry point,
+// trace_spectral_ray, transport.rs:420-454).  precision 32 or 64.
+int gro_trace_ray(const gr_scene *sc, const float origin[3], const float dir[3], uint32_t seed, float hero_rand,
+                  uint32_t max_bounces, int precision, double xyz_out[3], uint32_t *bounces, uint32_t *termination) {
+    Ray<float> ray;
+    ray.origin = V3<float>(origin[0], origin[1], origin[2]);
+    ray.dir = V3<float>(dir[0], dir[1], dir[2]);
+    EventLog lg;
+    std::memset(&lg, 0, sizeof(lg));
+    if (precision == 64) {
+        MaterialCtx<double> mc = make_material<double>(sc->material, sc->material_ext);
+        EnvCtx<double> env = make_env<double>(sc->env);
+        V3<double> x = trace_spectral_ray<double>(ray, sc->planes, sc->n_planes, mc, env, max_bounces, seed, hero_rand, &lg);
+        xyz_out[0] = x.x; xyz_out[1] = x.y; xyz_out[2] = x.z;
+    } else {
+        MaterialCtx<float> mc = make_material<float>(sc->material, sc->material_ext);
+        EnvCtx<float> env = make_env<float>(sc->env);
+        V3<float> x = trace_spectral_ray<float>(ray, sc->planes, sc->n_planes, mc, env, max_bounces, seed, hero_rand, &lg);
+        xyz_out[0] = x.x; xyz_out[1] = x.y; xyz_out[2] = x.z;
+    }
+    if (bounces) *bounces = lg.bounces;
+    if (termination) *termination = lg.termination;
+    return 0;
+}
+
+// CPU baseline: the listed rows only; threads claim 16-pixel runs of those rows from
+// an atomic counter (the reference worker claims whole rows, apps/gemray-worker/src/
+// render_core/mod.rs:241-316 -- pixel runs keep every core busy on a small row
+// sample).  accum is the full W*H*3 film; each pixel's samples are summed in sample
+// order and added once.
+int gro_accumulate_rows(const gr_scene *sc, const uint32_t *rows, uint32_t n_rows, uint32_t sample_offset,
+                        uint32_t spp, float *accum, int threads) {
+    if (!sc || !rows || !accum) return GR_EINVAL;
+    if (!material_supported(sc->material, sc->finishes, sc->n_planes)) return GR_DECLINED_MATERIAL;
+    MaterialCtx<float> mc = make_material<float>(sc->material, sc->material_ext);
+    EnvCtx<float> env = make_env<float>(sc->env);
+    if (threads <= 0) threads = (int)std::thread::hardware_concurrency();
+    if (threads <= 0) threads = 1;
+    const uint32_t RUN = 16;
+    const uint64_t runs_per_row = (sc->width + RUN - 1) / RUN;
+    const uint64_t total = runs_per_row * n_rows;
+    std::atomic<uint64_t> next(0);
+    auto worker = [&]() {
+        for (;;) {
+            uint64_t i = next.fetch_add(1);
+            if (i >= total) break;
+            uint32_t y = rows[i / runs_per_row];
+            if (y >= sc->height) continue;
+            uint32_t x0 = (uint32_t)(i % runs_per_row) * RUN;
+            for (uint32_t x = x0; x < x0 + RUN && x < sc->width; ++x) {
+                uint32_t p = y * sc->width + x;
+                double s[3];
+                trace_pixel_samples<float>(*sc, mc, env, p, sample_offset, spp, nullptr, s, nullptr);
+                for (int c = 0; c < 3; ++c) accum[3 * (size_t)p + c] = accum[3 * (size_t)p + c] + (float)s[c];
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; ++t) pool.emplace_back(worker);
+    for (auto &t : pool) t.join();
+    return GR_OK;
+}
+
+// Film accumulation, FP32: accum (W*H*3 floats) += per-pixel sample sums.
+int gro_accumulate(const gr_scene *sc, uint32_t sample_offset, uint32_t spp, float *accum, int threads) {
+    return accumulate_impl<float>(sc, sample_offset, spp, accum, nullptr, threads);
+}
+
+// Film accumulation, FP64 oracle: accum (W*H*3 doubles) += per-pixel sample sums.
+int gro_accumulate_f64(const gr_scene *sc, uint32_t sample_offset, uint32_t spp, double *accum, int threads) {
+    return accumulate_impl<double>(sc, sample_offset, spp, nullptr, accum, threads);
+}
+
+// Per-sample XYZ of pixels [first_pixel, first_pixel+n_pixels), samples
+// [offset, offset+spp) -> xyz_out[(p*spp + s)*3 + c] (FP32 oracle), plus optional
+// per-sample bounce counts / termination reasons / event counts.
+int gro_trace_samples(const gr_scene *sc, uint32_t first_pixel, uint32_t n_pixels, uint32_t sample_offset,
+                      uint32_t spp, float *xyz_out, uint32_t *bounces, uint32_t *term, uint32_t *counts /* 6 per sample */,
+                      int threads) {
+    if (!material_supported(sc->material, sc->finishes, sc->n_planes)) return GR_DECLINED_MATERIAL;
+    MaterialCtx<float> mc = make_material<float>(sc->material, sc->material_ext);
+    EnvCtx<float> env = make_env<float>(sc->env);
+    if (threads <= 0) threads = (int)std::thread::hardware_concurrency();
+    std::atomic<uint32_t> next(0);
+    auto worker = [&]() {
+        std::vector<EventLog> logs(spp);
+        for (;;) {
+            uint32_t i = next.fetch_add(1);
+            if (i >= n_pixels) break;
+            uint32_t p = first_pixel + i;
+            double s[3];
+            trace_pixel_samples<float>(*sc, mc, env, p, sample_offset, spp, xyz_out + (size_t)i * spp * 3, s, logs.data());
+            for (uint32_t k = 0; k < spp; ++k) {
+                size_t o = (size_t)i * spp + k;
+                if (bounces) bounces[o] = logs[k].bounces;
+                if (term) term[o] = logs[k].termination;
+                if (counts) {
+                    counts[6 * o + 0] = logs[k].n_tir;
+                    counts[6 * o + 1] = logs[k].n_reflect;
+                    counts[6 * o + 2] = logs[k].n_refract;
+                    counts[6 * o + 3] = logs[k].n_inside_abs;
+                    counts[6 * o + 4] = logs[k].n_escape;
+                    counts[6 * o + 5] = logs[k].n_chan_tir;
+                }
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; ++t) pool.emplace_back(worker);
+    for (auto &t : pool) t.join();
+    return GR_OK;
+}
+
+// tonemap_to_rgba (renderer/tonemap.rs:52-108): rgba[i] = encode(xyz[i] * scale).
+void gro_tonemap(const float *xyz, float scale, uint32_t n, uint8_t *rgba) {
+    for (uint32_t i = 0; i < n; ++i) {
+        V3<float> c(xyz[3 * (size_t)i], xyz[3 * (size_t)i + 1], xyz[3 * (size_t)i + 2]);
+        srgb_encode(c * scale, rgba + 4 * (size_t)i);
+    }
+}
+
+// Sampler records (renderer/gpu/rng_check.rs cpu_record): seed, jitter, hero and
+// the Fresnel / roulette / split / coupling draws of bounces 0..3 (20 words each).
+void gro_rng_records(const uint32_t *pixels, const uint32_t *samples, uint32_t n, uint32_t *out) {
+    for (uint32_t i = 0; i < n; ++i) {
+        PixelRotations r = pixel_rotations(pixels[i]);
+        SampleDraws d = sample_draws(pixels[i], samples[i], r);
+        uint32_t *o = out + 20 * (size_t)i;
+        float f[19];
+        f[0] = d.jitter_x; f[1] = d.jitter_y; f[2] = d.hero_rand;
+        const uint32_t streams[4] = {FRESNEL_BRANCH_STREAM, RUSSIAN_ROULETTE_STREAM, BIREFRINGENT_SPLIT_STREAM,
+                                     MODE_COUPLING_STREAM};
+        for (uint32_t b = 0; b < 4; ++b)
+            for (int k = 0; k < 4; ++k) f[3 + 4 * b + k] = rng_draw(d.seed, b, streams[k]);
+        o[0] = d.seed;
+        std::memcpy(o + 1, f, sizeof(f));
+    }
+}
+
+}  // extern "C"

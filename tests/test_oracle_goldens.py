@@ -1,0 +1,200 @@
+"""Pins the oracle (C++ restatement of the reference CPU tracer) to the reference's own
+bit-exact golden vectors (tests/golden/reference_goldens.json, extracted from
+crates/gemray/tests/raytracer_tests.rs:1374-1842 by tests/golden/extract_goldens.py).
+
+The goldens were captured on a platform whose f32 libm is not glibc's: its expf is
+faithfully but not correctly rounded (see test_env_golden_residual_is_libm_rounding,
+which reproduces those bits exactly by moving exp() results one ULP).  Every
+golden is therefore pinned to a small ULP distance, and the path decisions (bounce
+count and termination) are checked to agree exactly wherever they are observable.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from gemray_studio_b200 import abi, scene as S
+from helpers import bits, f32_normalize, hash_draw, ulp_distance
+
+GOLD = json.loads((Path(__file__).parent / "golden" / "reference_goldens.json").read_text())
+
+# ULP budgets against the reference platform's bits (glibc vs the capture platform's
+# libm only).  Observed maxima: 63 (materials), 17 (studio cases), 2 (studio env).
+TRACE_ULP_BUDGET = 96
+ENV_ULP_BUDGET = 4
+
+
+def _oracle_planes(oracle):
+    buf = (abi.gr_plane * 128)()
+    n = oracle.gro_standard_round_brilliant(buf, 128)
+    return buf, n
+
+
+def _studio_scene(oracle, material_name, preset, yaw, pitch, planes, n):
+    m = abi.gr_material()
+    assert oracle.gro_builtin_material(material_name.encode(), C.byref(m)) == 0
+    s = abi.gr_scene()
+    s.n_planes, s.planes = n, planes
+    s.material = C.pointer(m)
+    s.env.mode = abi.GR_ENV_STUDIO
+    s.env.temp_k, s.env.spot_mult = S.LIGHTING_PRESETS[preset]
+    s.env.exposure, s.env.light_yaw, s.env.light_pitch = 1.0, yaw, pitch
+    return s, m
+
+
+def _trace(oracle, s, origin, direction, seed, hero, max_bounces, precision=32):
+    xyz = (C.c_double * 3)()
+    b, t = C.c_uint32(), C.c_uint32()
+    oracle.gro_trace_ray(C.byref(s), (C.c_float * 3)(*origin), (C.c_float * 3)(*direction), seed, hero, max_bounces,
+                         precision, xyz, C.byref(b), C.byref(t))
+    return [xyz[0], xyz[1], xyz[2]], b.value, t.value
+
+
+def test_material_goldens(oracle):
+    g = GOLD["materials"]
+    planes, n = _oracle_planes(oracle)
+    assert n == 74
+    d = f32_normalize(g["ray_dir_unnormalized"])
+    worst = 0
+    for case in g["cases"]:
+        s, _m = _studio_scene(oracle, case["material"], g["preset"], g["light_yaw"], g["light_pitch"], planes, n)
+        xyz, _b, term = _trace(oracle, s, g["ray_origin"], d, g["seed"], hash_draw(oracle, g["seed"]), g["max_bounces"])
+        dist = [ulp_distance(bits(v), e) for v, e in zip(xyz, case["xyz_bits"])]
+        worst = max(worst, max(dist))
+        assert max(dist) <= TRACE_ULP_BUDGET, (case["material"], dist)
+        assert term == 0  # escaped
+    assert worst <= TRACE_ULP_BUDGET
+
+
+def test_studio_case_goldens(oracle):
+    g = GOLD["studio_cases"]
+    planes, n = _oracle_planes(oracle)
+    exact = 0
+    for case in g["cases"]:
+        yaw = float(np.float32(np.pi)) if case["light_yaw"] == "PI" else case["light_yaw"]
+        d = f32_normalize(case["dir"]) if case["normalize"] else case["dir"]
+        hero = hash_draw(oracle, case["seed"])
+        for mat, key in (("Diamond", "diamond_bits"), ("Sapphire", "sapphire_bits")):
+            s, _m = _studio_scene(oracle, mat, case["preset"], yaw, case["light_pitch"], planes, n)
+            xyz, _b, _t = _trace(oracle, s, case["origin"], d, case["seed"], hero, g["max_bounces"])
+            dist = [ulp_distance(bits(v), e) for v, e in zip(xyz, case[key])]
+            assert max(dist) <= TRACE_ULP_BUDGET, (case["seed"], mat, dist)
+            exact += sum(1 for x in dist if x == 0)
+    assert exact >= 6  # several components reproduce the reference bits exactly (7 observed)
+
+
+def test_studio_env_goldens(oracle):
+    g = GOLD["studio_env"]
+    temp, spot = S.LIGHTING_PRESETS[g["preset"]]
+    for d0, norm, row in zip(g["dirs_unnormalized"], g["normalize"], g["bits"]):
+        d = f32_normalize(d0) if norm else d0
+        for lam, expect in zip(g["lambdas"], row):
+            v = oracle.gro_studio_env((C.c_float * 3)(*d), lam, temp, spot, g["exposure"], g["light_yaw"], g["light_pitch"])
+            assert ulp_distance(bits(v), expect) <= ENV_ULP_BUDGET
+
+
+def test_env_golden_residual_is_libm_rounding(oracle):
+    """The studio-environment goldens differ from the oracle only through libm rounding:
+    with exp(hc/(lambda * 5000 K)) for 550, 560 and 650 nm taken one ULP above
+    glibc's correctly rounded values (i.e. a faithfully rounded expf), the oracle's f32
+    arithmetic reproduces the reference bits EXACTLY for the two directions whose
+    radiance does not depend on the light rig's sin/cos (backdrop and fill only)."""
+    hck = np.float32(14388000.0)
+
+    def shifted_exp(x, k):
+        e = np.float32(np.exp(np.float64(x)))
+        return np.frombuffer(np.array([bits(e) + k], np.uint32).tobytes(), np.float32)[0]
+
+    def bb(lam, e_shift, e560_shift):
+        lam, t = np.float32(lam), np.float32(5000.0)
+        e = shifted_exp(min(np.float32(hck / np.float32(lam * t)), np.float32(80)), e_shift)
+        e5 = shifted_exp(min(np.float32(hck / np.float32(np.float32(560) * t)), np.float32(80)), e560_shift)
+        d, d5 = max(np.float32(e - np.float32(1)), np.float32(1e-6)), max(np.float32(e5 - np.float32(1)), np.float32(1e-6))
+        x = np.float32(np.float32(560) / lam)
+        x2 = np.float32(x * x)
+        p5 = np.float32(x * np.float32(x2 * x2))
+        return min(max(np.float32(p5 * np.float32(d5 / d)), np.float32(0.01)), np.float32(20))
+
+    g = GOLD["studio_env"]
+    shift = {450.0: 0, 550.0: 1, 650.0: 1}
+    for di in (2, 3):
+        d = f32_normalize(g["dirs_unnormalized"][di]) if g["normalize"][di] else g["dirs_unnormalized"][di]
+        for lam, expect in zip(g["lambdas"], g["bits"][di]):
+            v = oracle.gro_studio_env_spec((C.c_float * 3)(*d), float(bb(lam, shift[lam], 1)), 1.6, 1.0, 0.85, 0.95)
+            assert bits(v) == expect, (di, lam)
+
+
+def test_mode_coupling_draw_seed7_bounce2(oracle):
+    """transport.rs:1005-1010: the MODE_COUPLING_STREAM draw for (seed 7, bounce 2) is < 0.5."""
+    assert oracle.gro_rng_draw(7, 2, 0xCC9E2D51) < 0.5
+
+
+def test_sampler_matches_literal_formula(oracle):
+    """sampling.rs:273-312: pixel_rotations/sample_draws equal the literal formula."""
+    pix = np.repeat(np.arange(4000, dtype=np.uint32), 3)
+    smp = np.tile(np.arange(3, dtype=np.uint32), 4000)
+    seed = np.empty_like(pix)
+    jx, jy, hero = (np.empty(pix.size, np.float32) for _ in range(3))
+    up = C.POINTER(C.c_uint32)
+    fp = C.POINTER(C.c_float)
+    oracle.gro_sample_draws(pix.ctypes.data_as(up), smp.ctypes.data_as(up), pix.size, seed.ctypes.data_as(up),
+                            jx.ctypes.data_as(fp), jy.ctypes.data_as(fp), hero.ctypes.data_as(fp))
+
+    def h(x):
+        x = (x * np.uint32(0x85EBCA6B)) & np.uint32(0xFFFFFFFF)
+        x ^= x >> np.uint32(13)
+        x = (x * np.uint32(0xC2B2AE35)) & np.uint32(0xFFFFFFFF)
+        x ^= x >> np.uint32(16)
+        return x.astype(np.uint32)
+
+    with np.errstate(over="ignore"):
+        expect_seed = h((pix * np.uint32(0x9E3779B9)) ^ (smp * np.uint32(0x85EBCA6B)))
+    assert np.array_equal(seed, expect_seed)
+
+    def rev(v):
+        v = v.astype(np.uint64)
+        out = np.zeros_like(v)
+        for b in range(32):
+            out |= ((v >> np.uint64(b)) & np.uint64(1)) << np.uint64(31 - b)
+        return out.astype(np.uint32)
+
+    def ld2(n):
+        return (rev(n).astype(np.float32) / np.float32(4294967296.0)).astype(np.float32)
+
+    rot_x = ld2(h(pix ^ np.uint32(0xA511E9B3)))
+    s = (ld2(smp) + rot_x).astype(np.float32)
+    expect_jx = (s - np.floor(s)).astype(np.float32) - np.float32(0.5)
+    assert np.array_equal(jx, expect_jx.astype(np.float32))
+    assert np.all((jy >= -0.5) & (jy < 0.5)) and np.all((hero >= 0) & (hero < 1))
+
+
+def test_radical_inverse_values(oracle):
+    """Base-3/5 radical inverses of small n are the exact digit reversals."""
+    for n, b, v in [(1, 3, 1 / 3), (2, 3, 2 / 3), (3, 3, 1 / 9), (1, 5, 0.2), (7, 5, 0.4 + 1 / 25)]:
+        assert abs(oracle.gro_radical_inverse(n, b) - v) < 1e-7
+
+
+def test_exp_poly_properties(oracle):
+    """simd/exp_poly.rs: exp_poly(0) == 1 exactly; a few-ULP match to exp elsewhere."""
+    assert oracle.gro_exp_poly(0.0) == 1.0
+    assert oracle.gro_exp_poly(-0.0) == 1.0
+    xs = np.linspace(-20, 20, 4001, dtype=np.float32)
+    got = np.array([oracle.gro_exp_poly(float(x)) for x in xs], np.float64)
+    ref = np.exp(xs.astype(np.float64))
+    assert np.max(np.abs(got - ref) / ref) < 4e-7
+
+
+def test_fp64_oracle_close_to_fp32(oracle):
+    """The FP64 twin of a golden ray lands within 1e-4 relative of the FP32 oracle."""
+    g = GOLD["materials"]
+    planes, n = _oracle_planes(oracle)
+    d = f32_normalize(g["ray_dir_unnormalized"])
+    s, _m = _studio_scene(oracle, "Diamond", g["preset"], g["light_yaw"], g["light_pitch"], planes, n)
+    x32, b32, _ = _trace(oracle, s, g["ray_origin"], d, 1, hash_draw(oracle, 1), 12, 32)
+    x64, b64, _ = _trace(oracle, s, g["ray_origin"], d, 1, hash_draw(oracle, 1), 12, 64)
+    assert b32 == b64
+    assert np.allclose(x32, x64, rtol=1e-4)

@@ -50,7 +50,7 @@ EVENT_NAMES = ["paths", "bounces", "escapes", "tir", "reflect", "refract", "abso
 GR_EVENT_COUNT = len(EVENT_NAMES)
 
 GR_KERNEL_PLAIN = 0
-GR_KERNEL_PERSISTENT = 1
+GR_KERNEL_WAVEFRONT = 1
 
 
 class gr_plane(C.Structure):

@@ -21,6 +21,8 @@ OUT = PKG / "libgemray_cuda.so"
 SOURCES = ["gr_host.cu", "gr_tonemap.cu", "gr_scene_builders.cpp"]
 HEADERS = ["gr_device.cuh", "gr_trace.cuh", "gr_kernels.cuh", "gr_host.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# Compile-time engine options (see csrc/gr_device.cuh).
+DEFINES: tuple[str, ...] = ()
 
 
 def nvcc() -> str:
@@ -49,19 +51,21 @@ def needs_build() -> bool:
     return OUT.stat().st_mtime < newest
 
 
-def build(force: bool = False, verbose: bool = False) -> Path:
-    if not force and not needs_build():
+def build(force: bool = False, verbose: bool = False, defines: tuple[str, ...] = DEFINES, out: Path | None = None) -> Path:
+    target = Path(out) if out is not None else OUT
+    if out is None and not force and not needs_build():
         return OUT
-    tmp = OUT.with_suffix(".so.tmp")
-    cmd = [nvcc(), *flags(verbose), "-shared", "-o", str(tmp), *[str(CSRC / s) for s in SOURCES]]
+    tmp = target.with_suffix(".so.tmp")
+    cmd = [nvcc(), *flags(verbose), *[f"-D{d}" for d in defines], "-shared", "-o", str(tmp),
+           *[str(CSRC / s) for s in SOURCES]]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
         raise RuntimeError("nvcc failed building libgemray_cuda.so")
     if verbose:
         sys.stderr.write(r.stdout + r.stderr)
-    os.replace(tmp, OUT)
-    return OUT
+    os.replace(tmp, target)
+    return target
 
 
 if __name__ == "__main__":

@@ -60,6 +60,26 @@ struct SceneBuffers {
 };
 
 // ---------------------------------------------------------------------------------
+// libm calls.  With GR_OUTLINE_MATH each CUDA math routine is emitted once and called,
+// keeping the transport kernel's instruction footprint inside the SM instruction
+// cache; the results are the same functions either way.
+// ---------------------------------------------------------------------------------
+#ifdef GR_OUTLINE_MATH
+#define GR_MATH static __device__ __noinline__
+#else
+#define GR_MATH static __device__ __forceinline__
+#endif
+GR_MATH float2 m_sincos(float x) {
+    float s, c;
+    sincosf(x, &s, &c);
+    return make_float2(s, c);
+}
+GR_MATH float m_atan2(float y, float x) { return atan2f(y, x); }
+GR_MATH float m_atan(float x) { return atanf(x); }
+GR_MATH float m_acos(float x) { return acosf(x); }
+GR_MATH float m_exp(float x) { return expf(x); }
+
+// ---------------------------------------------------------------------------------
 // Small vector helpers with glam's scalar semantics (no contraction).
 // ---------------------------------------------------------------------------------
 struct V3 {
@@ -221,7 +241,7 @@ __device__ __forceinline__ float band_sum(const float (*bands)[3], uint32_t n, f
     float acc = -0.0f;
     for (uint32_t i = 0; i < n; ++i) {
         float t = (lambda_nm - bands[i][0]) / bands[i][1];
-        acc = acc + bands[i][2] * expf(-0.5f * t * t);
+        acc = acc + bands[i][2] * m_exp(-0.5f * t * t);
     }
     return acc;
 }
@@ -307,7 +327,7 @@ __device__ __forceinline__ float r_unpol(float rs, float rp) {
 __device__ __forceinline__ float tir_phase_delta(float n1k, float ci, float si) {
     float num = ci * sqrtf(fmaxf(fmaf(n1k * n1k * si, si, -1.0f), 0.0f));
     float den = fmaxf(n1k * si * si, 1e-6f);
-    return 2.0f * atanf(num / den);
+    return 2.0f * m_atan(num / den);
 }
 
 // polarization.rs:197-200 / birefringence.rs:126-131 (same construction)
@@ -321,9 +341,9 @@ __device__ __forceinline__ V3 electric_field_direction(const Stokes &st, V3 s_ax
     V3 s_raw = sub(s_axis, mul(k, dot(k, s_axis)));
     V3 s_hat = dot(s_raw, s_raw) > 1e-8f ? normalize(s_raw) : perp_basis_t(k);
     V3 p_hat = cross(k, s_hat);
-    float psi = 0.5f * atan2f(st.u, st.q);
+    float psi = 0.5f * m_atan2(st.u, st.q);
     float sp, cp;
-    sincosf(psi, &sp, &cp);
+    { float2 sc_ = m_sincos(psi); sp = sc_.x; cp = sc_.y; }
     V3 e = add(smul(cp, s_hat), smul(sp, p_hat));
     return dot(e, e) > 1e-8f ? normalize(e) : s_hat;
 }
@@ -344,22 +364,22 @@ __device__ __forceinline__ float walk_off_angle(float n_o, float n_e, float thet
     if (fabsf(n_o - n_e) < 1e-5f) return 0.0f;
     float n_o2 = n_o * n_o, n_e2 = n_e * n_e;
     float s, c;
-    sincosf(theta, &s, &c);
+    { float2 sc_ = m_sincos(theta); s = sc_.x; c = sc_.y; }
     float num = (n_o2 - n_e2) * s * c;
     float den = fmaxf(fmaf(n_e2 * c, c, n_o2 * s * s), 1e-6f);
-    return atanf(num / den);
+    return m_atan(num / den);
 }
-// :74-91
-__device__ __forceinline__ V3 extraordinary_poynting_dir(V3 wn, V3 c_axis, float n_o, float n_e) {
+// :74-91 (outlined: rare, large)
+static __device__ __noinline__ V3 extraordinary_poynting_dir(V3 wn, V3 c_axis, float n_o, float n_e) {
     float cos_theta = clampf(dot(wn, c_axis), -1.0f, 1.0f);
-    float theta = acosf(fabsf(cos_theta));
+    float theta = m_acos(fabsf(cos_theta));
     float delta = walk_off_angle(n_o, n_e, theta);
     if (fabsf(delta) < 1e-5f) return wn;
     V3 c_proj = normalize_or_zero(sub(c_axis, smul(cos_theta, wn)));
     if (dot(c_proj, c_proj) < 1e-6f) return wn;
     float sign = cos_theta >= 0.0f ? 1.0f : -1.0f;
     float sd, cd;
-    sincosf(delta, &sd, &cd);
+    { float2 sc_ = m_sincos(delta); sd = sc_.x; cd = sc_.y; }
     return normalize(sub(mul(wn, cd), mul(smul(sign, c_proj), sd)));
 }
 // :101-118
@@ -382,7 +402,7 @@ __device__ __forceinline__ float quad_form(const SceneConst &S, float a_o, float
 // environment.rs:12-21 with the lambda-independent 560 nm term host-built.
 __device__ __forceinline__ float blackbody(const SceneConst &S, float lambda_nm) {
     float t_k = fmaxf(S.temp_k, 1000.0f);
-    float e = expf(fminf(14388000.0f / (lambda_nm * t_k), 80.0f));
+    float e = m_exp(fminf(14388000.0f / (lambda_nm * t_k), 80.0f));
     float denom = fmaxf(e - 1.0f, 1e-6f);
     float ratio = S.denom560 / denom;
     return clampf(powi<5>(560.0f / lambda_nm) * ratio, 0.01f, 20.0f);
@@ -410,7 +430,7 @@ __device__ __forceinline__ float studio_radiance(const SceneConst &S, V3 dn, flo
 __device__ __forceinline__ float asym_gauss(float x, float mu, float slo, float shi) {
     float sigma = x < mu ? slo : shi;
     float t = (x - mu) / sigma;
-    return expf(-0.5f * t * t);
+    return m_exp(-0.5f * t * t);
 }
 __device__ __forceinline__ float rgb_to_spectral(float r, float g, float b, float lambda_nm) {
     r = fmaxf(r, 0.0f); g = fmaxf(g, 0.0f); b = fmaxf(b, 0.0f);
@@ -421,8 +441,8 @@ __device__ __forceinline__ float rgb_to_spectral(float r, float g, float b, floa
 __device__ __forceinline__ void latlong_rgb(const SceneConst &S, const float *__restrict__ map, V3 dir, float rgb[3]) {
     const float PI = 3.14159265358979323846f;
     V3 d = normalize_or_zero(dir);
-    float theta = acosf(clampf(d.y, -1.0f, 1.0f));
-    float phi = atan2f(d.x, d.z);
+    float theta = m_acos(clampf(d.y, -1.0f, 1.0f));
+    float phi = m_atan2(d.x, d.z);
     float v = theta / PI;
     float u = rem_euclid(phi / (2.0f * PI), 1.0f);
     uint32_t w = S.map_w, h = S.map_h;

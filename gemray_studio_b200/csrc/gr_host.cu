@@ -22,6 +22,7 @@
 #include "gemray_cuda.h"
 #include "gr_host.h"
 #include "gr_kernels.cuh"
+#include "gr_wavefront.cuh"
 
 using grd::SceneConst;
 
@@ -290,12 +291,15 @@ struct gr_ctx {
     cudaStream_t stream = nullptr;
     std::mutex mu;
     std::string label;
-    size_t chunk_budget = 256ull << 20;
+    size_t chunk_budget = 2048ull << 20;
     uint64_t serve_budget = 60ull << 30;
     int sm_count = 0;
-    int persistent_blocks = 0;
     grh::DeviceBuffer xyz, film, planes, map, ext, counter, rgba;
-    int kernel_mode = GR_KERNEL_PERSISTENT;
+    int kernel_mode = GR_KERNEL_WAVEFRONT;
+    // wavefront engine pool (gr_wavefront.cuh)
+    uint32_t wave_cap = 1u << 18;
+    grh::DeviceBuffer wf_pool, wf_events, wf_queues, wf_cnt;
+    uint32_t *wf_done_host = nullptr;
     // Optional per-launch timing of the trace and fold kernels (CUDA events on the
     // launch stream); read back by gr_timing_read.
     bool timing = false;
@@ -382,6 +386,65 @@ gr_status upload_scene(gr_ctx *ctx, const gr_scene *sc, const SceneConst &S, grd
     return GR_OK;
 }
 
+// Wavefront engine over tuples [0, R.n_tuples) of one chunk (gr_wavefront.cuh).
+gr_status launch_wavefront(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuffers &B, const grd::LaunchRange &R,
+                           float *xyz, cudaStream_t stream) {
+    uint64_t cap64 = R.n_tuples < (uint64_t)ctx->wave_cap ? R.n_tuples : (uint64_t)ctx->wave_cap;
+    uint32_t cap = (uint32_t)((cap64 + 31) & ~31ull);
+    gr_status st;
+    if ((st = ctx->wf_pool.reserve((size_t)cap * sizeof(grd::Path))) != GR_OK) return st;
+    if ((st = ctx->wf_events.reserve((size_t)cap * sizeof(grd::Event))) != GR_OK) return st;
+    if ((st = ctx->wf_queues.reserve((size_t)cap * 6 * sizeof(uint32_t))) != GR_OK) return st;
+    if ((st = ctx->wf_cnt.reserve(grd::W_NCOUNT * sizeof(uint32_t) + 2 * sizeof(unsigned long long))) != GR_OK) return st;
+    if (!ctx->wf_done_host) {
+        void *h = nullptr;
+        GR_CUDA(cudaHostAlloc(&h, sizeof(uint32_t), cudaHostAllocDefault));
+        ctx->wf_done_host = (uint32_t *)h;
+    }
+    grd::WaveBuffers W;
+    W.pool = (grd::Path *)ctx->wf_pool.ptr;
+    W.events = (grd::Event *)ctx->wf_events.ptr;
+    uint32_t *q = (uint32_t *)ctx->wf_queues.ptr;
+    W.q_active0 = q;
+    W.q_active1 = q + cap;
+    W.q_reflect = q + 2 * (size_t)cap;
+    W.q_refract = q + 3 * (size_t)cap;
+    W.q_finish = q + 4 * (size_t)cap;
+    W.q_free = q + 5 * (size_t)cap;
+    W.cnt = (uint32_t *)ctx->wf_cnt.ptr;
+    W.tuples = (unsigned long long *)((char *)ctx->wf_cnt.ptr + grd::W_NCOUNT * sizeof(uint32_t));
+    W.cap = cap;
+    const unsigned T = 256;
+    uint64_t want = (cap + T - 1) / T;
+    const unsigned grid = (unsigned)(want < (uint64_t)ctx->sm_count * 8 ? want : (uint64_t)ctx->sm_count * 8);
+    const size_t smem = (size_t)S.n_planes * sizeof(float4);
+    grd::k_wf_reset<<<grid, T, 0, stream>>>(W);
+    const int BATCH = 4;
+    uint32_t it = 0;
+    for (uint64_t guard = 0;; ++guard) {
+        for (int j = 0; j < BATCH; ++j, ++it) {
+            const uint32_t cur = it & 1u;
+            grd::k_wf_regen_prep<<<1, 1, 0, stream>>>(W, R.n_tuples);
+            grd::k_wf_regen<<<grid, T, 0, stream>>>(S, B, R, W, cur);
+            grd::k_wf_extend<<<grid, T, smem, stream>>>(S, B, W, cur);
+            grd::k_wf_event<false><<<grid, T, 0, stream>>>(S, W, cur ^ 1u);
+            grd::k_wf_event<true><<<grid, T, 0, stream>>>(S, W, cur ^ 1u);
+            grd::k_wf_finish<<<grid, T, 0, stream>>>(S, B, W, xyz);
+            grd::k_wf_bookkeep<<<1, 1, 0, stream>>>(W, cur, R.n_tuples);
+        }
+        GR_CUDA(cudaGetLastError());
+        GR_CUDA(cudaMemcpyAsync(ctx->wf_done_host, W.cnt + grd::W_DONE, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+        GR_CUDA(cudaStreamSynchronize(stream));
+        if (*ctx->wf_done_host) break;
+        // Every path ends within max_bounces iterations of its start and a new batch
+        // of tuples starts every iteration, so this bound is never reached by a
+        // correct engine; it turns a logic error into an error return, not a hang.
+        if (guard > (R.n_tuples / 32 + 4) * ((uint64_t)S.max_bounces + 2))
+            return fail(GR_ETIMEOUT, "wavefront did not drain");
+    }
+    return GR_OK;
+}
+
 // Trace tuples [0, R.n_tuples) of one chunk into xyz (device).
 gr_status launch_trace(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuffers &B, const grd::LaunchRange &R,
                        float *xyz, cudaStream_t stream, int mode) {
@@ -389,19 +452,11 @@ gr_status launch_trace(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuffers
     size_t smem = (size_t)S.n_planes * sizeof(float4);
     if (mode == GR_KERNEL_PLAIN || S.max_bounces == 0) {
         uint64_t blocks = (R.n_tuples + grd::TRACE_THREADS - 1) / grd::TRACE_THREADS;
-        grd::k_trace_plain<<<(unsigned)blocks, grd::TRACE_THREADS, smem, stream>>>(S, B, R, xyz);
-    } else {
-        gr_status st = ctx->counter.reserve(sizeof(unsigned long long));
-        if (st != GR_OK) return st;
-        GR_CUDA(cudaMemsetAsync(ctx->counter.ptr, 0, sizeof(unsigned long long), stream));
-        uint64_t want = (R.n_tuples + grd::TRACE_THREADS - 1) / grd::TRACE_THREADS;
-        uint64_t blocks = (uint64_t)ctx->persistent_blocks;
-        if (want < blocks) blocks = want;
-        grd::k_trace_persistent<grd::NoCounters><<<(unsigned)blocks, grd::TRACE_THREADS, smem, stream>>>(
-            S, B, R, xyz, (unsigned long long *)ctx->counter.ptr, nullptr);
+        grd::k_trace_plain<grd::NoCounters><<<(unsigned)blocks, grd::TRACE_THREADS, smem, stream>>>(S, B, R, xyz, nullptr);
+        GR_CUDA(cudaGetLastError());
+        return GR_OK;
     }
-    GR_CUDA(cudaGetLastError());
-    return GR_OK;
+    return launch_wavefront(ctx, S, B, R, xyz, stream);
 }
 
 gr_status launch_fold(const float *xyz, uint32_t n_pixels, uint32_t spp, uint32_t first_pixel, float *film,
@@ -436,6 +491,7 @@ gr_status render_into(gr_ctx *ctx, const gr_scene *sc, const SceneConst &S, cons
                       uint32_t sample_offset, uint32_t spp, float *film_dev, cudaStream_t stream) {
     const uint64_t n_pixels = (uint64_t)sc->width * sc->height;
     uint64_t budget_tuples = ctx->chunk_budget / (3 * sizeof(float));
+    if (budget_tuples > 0xFFFFFFFFull) budget_tuples = 0xFFFFFFFFull;  // tuple ids are u32 within a launch
     uint64_t chunk_pixels = budget_tuples / spp;
     if (chunk_pixels < 1) chunk_pixels = 1;
     if (chunk_pixels > n_pixels) chunk_pixels = n_pixels;
@@ -512,13 +568,8 @@ gr_status gr_create(gr_ctx **out, const gr_create_opts *opts) {
         return fail(GR_ECUDA, "cudaStreamCreate failed: %s", cudaGetErrorString(e));
     }
     ctx->sm_count = prop.multiProcessorCount;
-    int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grd::k_trace_persistent<grd::NoCounters>, grd::TRACE_THREADS,
-                                                      GR_MAX_PLANES * sizeof(float4));
-    if (e != cudaSuccess || per_sm < 1) per_sm = 1;
-    ctx->persistent_blocks = per_sm * ctx->sm_count;
-    char buf[256];
-    snprintf(buf, sizeof(buf), "%s (CUDA, sm_%d%d, %d SMs)", prop.name, prop.major, prop.minor, prop.multiProcessorCount);
+    char buf[512];
+    snprintf(buf, sizeof(buf), "%.256s (CUDA, sm_%d%d, %d SMs)", prop.name, prop.major, prop.minor, prop.multiProcessorCount);
     ctx->label = buf;
     *out = ctx;
     return GR_OK;
@@ -537,6 +588,11 @@ gr_status gr_destroy(gr_ctx *ctx) {
         ctx->ext.release();
         ctx->counter.release();
         ctx->rgba.release();
+        ctx->wf_pool.release();
+        ctx->wf_events.release();
+        ctx->wf_queues.release();
+        ctx->wf_cnt.release();
+        if (ctx->wf_done_host) cudaFreeHost(ctx->wf_done_host);
         for (auto &p : ctx->trace_ev) { cudaEventDestroy(p.first); cudaEventDestroy(p.second); }
         for (auto &p : ctx->fold_ev) { cudaEventDestroy(p.first); cudaEventDestroy(p.second); }
         for (auto &kv : ctx->scenes) {
@@ -817,10 +873,9 @@ gr_status gr_event_counts(gr_ctx *ctx, const gr_scene *sc, uint32_t first_pixel,
     R.n_tuples = n_tuples;
     unsigned long long *dc = (unsigned long long *)ctx->counter.ptr;
     size_t smem = (size_t)S.n_planes * sizeof(float4);
-    uint64_t want = (n_tuples + grd::TRACE_THREADS - 1) / grd::TRACE_THREADS;
-    uint64_t blocks = want < (uint64_t)ctx->persistent_blocks ? want : (uint64_t)ctx->persistent_blocks;
-    grd::k_trace_persistent<grd::Counters><<<(unsigned)blocks, grd::TRACE_THREADS, smem, ctx->stream>>>(
-        S, B, R, (float *)ctx->xyz.ptr, dc, dc + 1);
+    uint64_t blocks = (n_tuples + grd::TRACE_THREADS - 1) / grd::TRACE_THREADS;
+    grd::k_trace_plain<grd::Counters><<<(unsigned)blocks, grd::TRACE_THREADS, smem, ctx->stream>>>(
+        S, B, R, (float *)ctx->xyz.ptr, dc + 1);
     GR_CUDA(cudaGetLastError());
     unsigned long long host[1 + GR_EVENT_COUNT];
     GR_CUDA(cudaMemcpyAsync(host, dc, sizeof(host), cudaMemcpyDeviceToHost, ctx->stream));
@@ -898,7 +953,7 @@ gr_status gr_timing_read(gr_ctx *ctx, double *trace_ms, double *fold_ms, uint64_
 
 gr_status gr_set_kernel(gr_ctx *ctx, uint32_t kernel) {
     if (!ctx) return fail(GR_EINVAL, "ctx is NULL");
-    if (kernel != GR_KERNEL_PLAIN && kernel != GR_KERNEL_PERSISTENT) return fail(GR_EINVAL, "unknown kernel %u", kernel);
+    if (kernel != GR_KERNEL_PLAIN && kernel != GR_KERNEL_WAVEFRONT) return fail(GR_EINVAL, "unknown kernel %u", kernel);
     std::lock_guard<std::mutex> lk(ctx->mu);
     ctx->kernel_mode = (int)kernel;
     return GR_OK;

@@ -35,94 +35,33 @@ __device__ __forceinline__ void tuple_coords(const LaunchRange &R, uint64_t t, u
     sample = R.sample_offset + s;  // u32 wrapping add, as the reference's wrapping_add
 }
 
-// Plain kernel: one thread traces one tuple start to finish.
+// Plain kernel: one thread traces one tuple start to finish -- the reference
+// kernel's launch shape (one invocation per (pixel, sample), spectral_transport.wgsl:
+// 672-691).  The Counters variant tallies events for the FLOP model.
+template <class CT>
 __global__ void __launch_bounds__(TRACE_THREADS) k_trace_plain(SceneConst S, SceneBuffers B, LaunchRange R,
-                                                               float *__restrict__ xyz) {
+                                                               float *__restrict__ xyz,
+                                                               unsigned long long *__restrict__ tallies) {
     extern __shared__ float4 s_planes[];
     stage_planes(s_planes, B.planes, S.n_planes);
     uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= R.n_tuples) return;
-    uint32_t pixel, sample;
-    tuple_coords(R, t, pixel, sample);
-    Path P;
-    path_init(P, S, B, pixel, sample, (uint32_t)t);
-    P.alive = S.max_bounces > 0;
-    NoCounters nc;
-    while (P.alive) path_step(P, S, s_planes, nc);
-    V3 c = path_finish(P, S, B);
-    xyz[3 * t + 0] = c.x;
-    xyz[3 * t + 1] = c.y;
-    xyz[3 * t + 2] = c.z;
-}
-
-// Persistent kernel with path regeneration: each warp claims up to 32 consecutive
-// tuples at a time from a global counter; a lane whose path ends writes its XYZ and
-// takes the next unassigned tuple of the claim, so every bounce step runs with
-// (nearly) all 32 lanes busy instead of idling behind the warp's longest path.
-// Requires max_bounces >= 1 (the host routes max_bounces == 0 to k_trace_plain).
-template <class CT>
-__global__ void __launch_bounds__(TRACE_THREADS) k_trace_persistent(SceneConst S, SceneBuffers B, LaunchRange R,
-                                                                    float *__restrict__ xyz,
-                                                                    unsigned long long *__restrict__ counter,
-                                                                    unsigned long long *__restrict__ tallies) {
-    extern __shared__ float4 s_planes[];
-    stage_planes(s_planes, B.planes, S.n_planes);
-    const uint32_t lane = threadIdx.x & 31u;
-    const unsigned lt_mask = (1u << lane) - 1u;
-    uint64_t next = 0;     // next unassigned tuple of the warp's claim (warp-uniform)
-    uint32_t avail = 0;    // unassigned tuples left in the claim (warp-uniform)
-    bool exhausted = false;
-    bool have = false;
-    Path P;
     CT ct;
     if constexpr (sizeof(CT) == sizeof(Counters)) {
         for (int i = 0; i < C_COUNT; ++i) ((Counters &)ct).c[i] = 0;
     }
-    for (;;) {
-        unsigned need = __ballot_sync(0xffffffffu, !have);
-        while (need && !exhausted) {
-            if (avail == 0) {
-                unsigned long long b = 0;
-                if (lane == 0) b = atomicAdd(counter, 32ull);
-                b = __shfl_sync(0xffffffffu, b, 0);
-                if (b >= R.n_tuples) {
-                    exhausted = true;
-                    break;
-                }
-                next = b;
-                uint64_t left = R.n_tuples - b;
-                avail = left < 32ull ? (uint32_t)left : 32u;
-            }
-            const uint32_t cnt = (uint32_t)__popc(need);
-            const uint32_t take = cnt < avail ? cnt : avail;
-            const uint32_t rank = (uint32_t)__popc(need & lt_mask);
-            const bool mine = ((need >> lane) & 1u) && rank < take;
-            if (mine) {
-                uint64_t t = next + rank;
-                uint32_t pixel, sample;
-                tuple_coords(R, t, pixel, sample);
-                path_init(P, S, B, pixel, sample, (uint32_t)t);
-                tally(ct, C_PATHS);
-                have = true;
-            }
-            next += take;
-            avail -= take;
-            need &= ~__ballot_sync(0xffffffffu, mine);
-        }
-        if (__ballot_sync(0xffffffffu, have) == 0) break;
-        if (have) {
-            path_step(P, S, s_planes, ct);
-            if (!P.alive) {
-                V3 c = path_finish(P, S, B);
-                const uint64_t t = P.tuple;
-                xyz[3 * t + 0] = c.x;
-                xyz[3 * t + 1] = c.y;
-                xyz[3 * t + 2] = c.z;
-                have = false;
-            }
-        }
+    if (t < R.n_tuples) {
+        uint32_t pixel, sample;
+        tuple_coords(R, t, pixel, sample);
+        Path P;
+        path_init(P, S, B, pixel, sample, (uint32_t)t);
+        tally(ct, C_PATHS);
+        V3 c = trace_path(P, S, B, s_planes, ct);
+        xyz[3 * t + 0] = c.x;
+        xyz[3 * t + 1] = c.y;
+        xyz[3 * t + 2] = c.z;
     }
     if constexpr (sizeof(CT) == sizeof(Counters)) {
+        const uint32_t lane = threadIdx.x & 31u;
         for (int i = 0; i < C_COUNT; ++i) {
             unsigned long long v = ((Counters &)ct).c[i];
             for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);

@@ -1,9 +1,21 @@
 // gr_trace.cuh -- the per-path transport loop (optics/raytracer/transport.rs:684-940)
-// for polished facets of isotropic and uniaxial materials, written as a resumable
-// state machine: path_init() builds a path from its (pixel, sample) tuple,
-// path_step() advances it by one bounce, path_finish() integrates it to XYZ.  The
-// plain kernel runs init/step.../finish per thread; the persistent kernel
-// regenerates finished lanes between steps so warps stay full.
+// for polished facets of isotropic and uniaxial materials, split into resumable
+// stages over a path record:
+//
+//   path_init    sampler draws, camera ray, per-sample wavelength cache
+//   step_hit     one intersection; on a hit: Stokes frame rotation, interior
+//                Beer-Lambert absorption, refraction geometry and the hero's event
+//                decision (TIR / partial reflect / refract) -> Event
+//   step_reflect the TIR and partial-reflect channel updates (one loop: a TIR event
+//                is the reflect update with scale factor exactly 1.0)
+//   step_refract the refract channel updates (chromatic termination, walk-off)
+//   path_finish  escape radiance, spectral MIS, CIE integration, white balance
+//
+// The plain kernel runs the stages back to back in one thread.  The wavefront engine
+// (gr_wavefront.cuh) keeps records in a device pool and runs each stage as its own
+// kernel over a compacted queue, so warps execute one event type at a time.
+// `Path` is a record of float4 rows: in the plain kernel it lives in the thread's
+// local memory, in the wavefront pool in global memory -- the same code serves both.
 #pragma once
 
 #include "gr_device.cuh"
@@ -12,59 +24,91 @@ namespace grd {
 
 constexpr int NCH = 8;
 
-struct Path {
-    Stokes st[NCH];
-    float pdf[NCH];
-    float n_o[NCH];
-    float ne_d[NCH];  // n_e - n_o per channel
-    float a_o[NCH], a_e[NCH];
-    V3 o, d, k, prev_plane;
-    float hero;
-    float rad_scale[NCH];  // radiance multiplier at escape (intensity at escape)
-    uint32_t seed, bounce, tuple;
-    bool inside, is_e, have_prev, absorbing, alive, escaped;
-    V3 escape_dir;
+// Per-path record (352 B).  Flag bits live in k_state.w's integer view.
+struct __align__(16) Path {
+    float4 o_hero;      // ray origin, hero_rand
+    float4 d_seed;      // ray (Poynting) direction S, rng seed bits
+    float4 k_state;     // wave normal k, state bits (bounce | flags)
+    float4 prev_tuple;  // previous plane-of-incidence normal (zero = none), tuple bits
+    float4 st[NCH];     // Stokes (I, Q, U, V) per channel
+    float4 pdf4[2];     // spectral-MIS path pdf per channel
+    float4 n_o4[2];     // ordinary index per channel
+    float4 ne_d4[2];    // n_e - n_o per channel
+    float4 a_o4[2];     // ordinary absorption coefficient per channel
+    float4 a_e4[2];     // extraordinary absorption coefficient per channel
+};
+static_assert(sizeof(Path) == 352, "path record size");
+
+// Event scratch between step_hit and the event stage (64 B).
+struct __align__(16) Event {
+    float4 hp_cos;   // hit point, cos_i (against the wave normal, normal facing the ray)
+    float4 n_ru;     // normal (flipped to face the interior ray), hero r_unpol (0 for TIR)
+    float4 n_med4[2];
 };
 
-// Build the path of tuple (pixel, sample): sampler draws, camera ray, the
-// per-sample wavelength cache (refraction.rs:127-174).
+constexpr uint32_t F_INSIDE = 1u << 0;
+constexpr uint32_t F_IS_E = 1u << 1;
+constexpr uint32_t F_ABSORBING = 1u << 2;
+constexpr uint32_t F_ESCAPED = 1u << 3;
+constexpr uint32_t F_ALIVE = 1u << 4;
+constexpr uint32_t F_TIR = 1u << 5;  // the pending event is a hero TIR
+constexpr uint32_t BOUNCE_SHIFT = 8;
+
+enum EventKind : uint32_t { EV_DONE = 0, EV_REFLECT = 1, EV_REFRACT = 2 };
+
+__device__ __forceinline__ float &arr(float4 (&a)[2], int k) { return reinterpret_cast<float *>(a)[k]; }
+__device__ __forceinline__ float arr(const float4 (&a)[2], int k) { return reinterpret_cast<const float *>(a)[k]; }
+__device__ __forceinline__ V3 xyz(const float4 &v) { return v3(v.x, v.y, v.z); }
+__device__ __forceinline__ void set_xyz(float4 &v, V3 a) { v.x = a.x; v.y = a.y; v.z = a.z; }
+__device__ __forceinline__ uint32_t state_bits(const Path &P) { return __float_as_uint(P.k_state.w); }
+__device__ __forceinline__ void set_state_bits(Path &P, uint32_t s) { P.k_state.w = __uint_as_float(s); }
+__device__ __forceinline__ uint32_t p_bounce(const Path &P) { return state_bits(P) >> BOUNCE_SHIFT; }
+__device__ __forceinline__ uint32_t p_flags(const Path &P) { return state_bits(P) & ((1u << BOUNCE_SHIFT) - 1u); }
+__device__ __forceinline__ uint32_t p_seed(const Path &P) { return __float_as_uint(P.d_seed.w); }
+__device__ __forceinline__ uint32_t p_tuple(const Path &P) { return __float_as_uint(P.prev_tuple.w); }
+__device__ __forceinline__ float p_hero(const Path &P) { return P.o_hero.w; }
+
+// Per-thread event tallies for the instrumented kernel variant (the FLOP model's
+// inputs, cf. trace_spectral_ray_with_finish_instrumented, transport.rs:512-537).
+enum CounterIndex {
+    C_PATHS = 0, C_BOUNCES, C_ESCAPES, C_TIR, C_REFLECT, C_REFRACT, C_ABSORB, C_CH_TIR, C_CH_REFR, C_ROULETTE,
+    C_ROTATIONS, C_ANISO_BOUNCES, C_WALKOFF, C_ROULETTE_KILLS, C_COUNT
+};
+struct Counters {
+    uint32_t c[C_COUNT];
+};
+struct NoCounters {};
+template <class CT> __device__ __forceinline__ void tally(CT &, int, uint32_t = 1) {}
+template <> __device__ __forceinline__ void tally<Counters>(Counters &ct, int i, uint32_t v) { ct.c[i] += v; }
+
+// Build the path of tuple (pixel, sample): sampler draws (sampling.rs:232-271),
+// camera ray (camera.rs:95-114), per-sample wavelength cache (refraction.rs:127-174).
 __device__ __forceinline__ void path_init(Path &P, const SceneConst &S, const SceneBuffers &B, uint32_t pixel,
                                           uint32_t sample, uint32_t tuple) {
     Draws dr = sample_draws(pixel, sample);
     uint32_t x = pixel % S.width, y = pixel / S.width;
-    // camera.rs:95-114
     float aspect = S.width_f / S.height_f;
     float u = (((float)x + dr.jx) / S.width_f - 0.5f) * 2.0f * aspect * S.fov_tan;
     float v = (0.5f - ((float)y + dr.jy) / S.height_f) * 2.0f * S.fov_tan;
     V3 dir = normalize(add(add(ld3(S.cam_f), mul(ld3(S.cam_r), u)), mul(ld3(S.cam_u), v)));
-    P.o = ld3(S.cam_o);
-    P.d = dir;
-    P.k = dir;
-    P.prev_plane = v3(0.f, 0.f, 0.f);
-    P.hero = dr.hero;
-    P.seed = dr.seed;
-    P.bounce = 0;
-    P.tuple = tuple;
-    P.inside = false;
-    P.is_e = false;
-    P.have_prev = false;
-    P.alive = true;
-    P.escaped = false;
+    P.o_hero = make_float4(S.cam_o[0], S.cam_o[1], S.cam_o[2], dr.hero);
+    P.d_seed = make_float4(dir.x, dir.y, dir.z, __uint_as_float(dr.seed));
+    P.prev_tuple = make_float4(0.f, 0.f, 0.f, __uint_as_float(tuple));
     bool any = false;
-#pragma unroll
+#pragma unroll 1
     for (int k = 0; k < NCH; ++k) {
-        P.st[k] = Stokes{1.0f, 0.0f, 0.0f, 0.0f};
-        P.pdf[k] = 1.0f;
-        float lam = lambda_k(P.hero, k);
+        P.st[k] = make_float4(1.0f, 0.0f, 0.0f, 0.0f);
+        arr(P.pdf4, k) = 1.0f;
+        float lam = lambda_k(dr.hero, k);
         float n_o = dispersion(S, lam);
-        P.n_o[k] = n_o;
+        arr(P.n_o4, k) = n_o;
         if (S.has_cauchy_e) {
             float lum = lam * 1e-3f;
             float l2 = lum * lum, l4 = l2 * l2;
             float n_e = S.cauchy_e[0] + S.cauchy_e[1] / l2 + S.cauchy_e[2] / l4;
-            P.ne_d[k] = n_e - n_o;
+            arr(P.ne_d4, k) = n_e - n_o;
         } else {
-            P.ne_d[k] = S.bire;
+            arr(P.ne_d4, k) = S.bire;
         }
         float ao = 0.0f, ae = 0.0f;
         if (S.absorbing) {
@@ -76,32 +120,55 @@ __device__ __forceinline__ void path_init(Path &P, const SceneConst &S, const Sc
                 ae = band_sum(S.e_bands, S.n_e_bands, lam);
             }
         }
-        P.a_o[k] = ao;
-        P.a_e[k] = ae;
+        arr(P.a_o4, k) = ao;
+        arr(P.a_e4, k) = ae;
         any = any || (ao != 0.0f) || (ae != 0.0f);
     }
-    // Every alpha exactly zero makes the Beer-Lambert factor exp_poly(-0) == 1.0
-    // for every channel, so skipping the absorption step is bit-identical.
-    P.absorbing = any;
+    // Every alpha exactly zero makes the Beer-Lambert factor exp_poly(-0) == 1.0 for
+    // every channel, so skipping the absorption step is bit-identical.
+    uint32_t flags = F_ALIVE | (any ? F_ABSORBING : 0u);
+    if (S.max_bounces == 0) flags &= ~F_ALIVE;
+    P.k_state = make_float4(dir.x, dir.y, dir.z, __uint_as_float(flags));
 }
 
 // Convex clip against planes staged in shared memory (intersect.rs:93-132,
 // simd/slab.rs:101-152).  Returns false on a miss.
+//
+// The reference divides t = -side/denom for every plane, but a plane's t only
+// matters if it can raise the running near maximum (denom < 0) or lower the running
+// far minimum (denom > 0).  q' = (-side) * rcp.approx(denom) is within 2^-21 relative
+// of the exact quotient q; if q' + |q'| 2^-19 < t_near then q < t_near, so the
+// correctly rounded fl(q) <= t_near and the plane cannot update (rounding is
+// monotone) -- likewise for the far side.  Only the remaining planes take the IEEE
+// division, so every t that is compared or kept is the reference's own bits.
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 __device__ __forceinline__ bool intersect(const float4 *__restrict__ planes, uint32_t n, V3 o, V3 d, float &t_hit,
                                           int &idx_hit) {
     float t_near = -1e30f, t_far = 1e30f;
     int near_idx = -1, far_idx = -1;
     bool outside = false;
+#pragma unroll 2
     for (uint32_t i = 0; i < n; ++i) {
         float4 p = planes[i];
         float denom = (p.x * d.x + p.y * d.y) + p.z * d.z;
         float side = p.w + ((p.x * o.x + p.y * o.y) + p.z * o.z);
         if (fabsf(denom) > 1e-7f) {
-            float t = (-side) / denom;
+            const float num = -side;
+            const float qa = num * rcp_approx(denom);
+            const float margin = fabsf(qa) * 1.9073486e-6f;  // 2^-19
             if (denom < 0.0f) {
-                if (t > t_near) { t_near = t; near_idx = (int)i; }
-            } else if (t < t_far) {
-                t_far = t; far_idx = (int)i;
+                if (!(qa + margin < t_near)) {
+                    float t = num / denom;
+                    if (t > t_near) { t_near = t; near_idx = (int)i; }
+                }
+            } else if (!(qa - margin > t_far)) {
+                float t = num / denom;
+                if (t < t_far) { t_far = t; far_idx = (int)i; }
             }
         } else if (side > 0.0f) {
             outside = true;
@@ -147,313 +214,340 @@ __device__ __forceinline__ V3 shading_normal(const float4 *planes, uint32_t n, V
     return normalize_or_zero(add(mul(hn, 1.0f - smooth_t), mul(bis, smooth_t)));
 }
 
-// Per-thread event tallies for the instrumented kernel variant (the FLOP model's
-// inputs, cf. trace_spectral_ray_with_finish_instrumented, transport.rs:512-537).
-enum CounterIndex {
-    C_PATHS = 0, C_BOUNCES, C_ESCAPES, C_TIR, C_REFLECT, C_REFRACT, C_ABSORB, C_CH_TIR, C_CH_REFR, C_ROULETTE,
-    C_ROTATIONS, C_ANISO_BOUNCES, C_WALKOFF, C_ROULETTE_KILLS, C_COUNT
-};
-struct Counters {
-    uint32_t c[C_COUNT];
-};
-struct NoCounters {};
-template <class CT> __device__ __forceinline__ void tally(CT &, int, uint32_t = 1) {}
-template <> __device__ __forceinline__ void tally<Counters>(Counters &ct, int i, uint32_t v) { ct.c[i] += v; }
-
-// One bounce of transport.rs:781-929.  Marks the path dead on escape, Russian
-// roulette or the bounce cap.
-template <class CT = NoCounters>
-__device__ __forceinline__ void path_step(Path &P, const SceneConst &S, const float4 *__restrict__ planes, CT &ct) {
-    const uint32_t bounce = P.bounce;
+// One intersection and everything of the bounce up to the hero's event decision
+// (transport.rs:781-895, raytracer/absorption.rs:71-141, refraction.rs:428-547,
+// 1036-1060).  Returns EV_DONE on an escape (F_ESCAPED set, F_ALIVE cleared).
+template <class CT>
+__device__ __forceinline__ uint32_t step_hit(Path &P, const SceneConst &S, const float4 *__restrict__ planes, Event &E,
+                                             CT &ct) {
+    const uint32_t bits = state_bits(P);
+    const uint32_t bounce = bits >> BOUNCE_SHIFT;
+    const bool inside = (bits & F_INSIDE) != 0;
+    const V3 o = xyz(P.o_hero), d = xyz(P.d_seed), kk = xyz(P.k_state);
     float t_hit = 0.0f;
     int fidx = 0;
     tally(ct, C_BOUNCES);
-    if (!intersect(planes, S.n_planes, P.o, P.d, t_hit, fidx)) {
+    if (!intersect(planes, S.n_planes, o, d, t_hit, fidx)) {
+        // accumulate_miss_radiance (transport.rs:67-90) runs in path_finish
         tally(ct, C_ESCAPES);
-        // accumulate_miss_radiance (transport.rs:67-90): radiance_k = I_k * L_k
-        P.escaped = true;
-        P.escape_dir = P.d;
-#pragma unroll
-        for (int k = 0; k < NCH; ++k) P.rad_scale[k] = intensity(P.st[k]);
-        P.alive = false;
-        return;
+        set_state_bits(P, (bits | F_ESCAPED) & ~F_ALIVE);
+        return EV_DONE;
     }
-    V3 hp = add(P.o, smul(t_hit, P.d));
+    V3 hp = add(o, smul(t_hit, d));
     V3 normal = shading_normal(planes, S.n_planes, hp, fidx, plane_normal(planes, fidx), S.edge_radius);
-    const V3 kk = P.k;
 
     // rotate_stokes_to_plane_of_incidence (raytracer/absorption.rs:71-89)
     V3 cur_plane = normalize_or_zero(cross(kk, normal));
-    if (P.have_prev && dot(cur_plane, cur_plane) > 1e-6f && dot(P.prev_plane, P.prev_plane) > 1e-6f) {
-        float cos_psi = clampf(dot(P.prev_plane, cur_plane), -1.0f, 1.0f);
-        float sin_psi = dot(cross(P.prev_plane, cur_plane), normalize_or_zero(kk));
-        float psi = atan2f(sin_psi, cos_psi);
-        float s2, c2;
-        sincosf(2.0f * psi, &s2, &c2);
+    const V3 prev = xyz(P.prev_tuple);
+    if (dot(cur_plane, cur_plane) > 1e-6f && dot(prev, prev) > 1e-6f) {
+        float cos_psi = clampf(dot(prev, cur_plane), -1.0f, 1.0f);
+        float sin_psi = dot(cross(prev, cur_plane), normalize_or_zero(kk));
+        float psi = m_atan2(sin_psi, cos_psi);
+        float2 sc = m_sincos(2.0f * psi);
 #pragma unroll
-        for (int k = 0; k < NCH; ++k) P.st[k] = apply_rotation(P.st[k], c2, s2);
+        for (int k = 0; k < NCH; ++k) {
+            float4 s = P.st[k];
+            Stokes r = apply_rotation(Stokes{s.x, s.y, s.z, s.w}, sc.y, sc.x);
+            P.st[k] = make_float4(r.i, r.q, r.u, r.v);
+        }
         tally(ct, C_ROTATIONS);
     }
-    P.prev_plane = cur_plane;
-    P.have_prev = true;
+    set_xyz(P.prev_tuple, cur_plane);
 
     // apply_interior_segment (transport.rs:586-605) -> apply_absorption (absorption.rs:115-141)
-    if (P.inside) {
+    if (inside) {
         normal = neg(normal);
-        if (P.absorbing) {
+        if (bits & F_ABSORBING) {
             tally(ct, C_ABSORB);
             V3 c_axis = ld3(S.c_axis);
             V3 ea = ordinary_eigen(kk, c_axis);
             V3 eb = extraordinary_eigen_from(kk, ea);
             float scaled = t_hit * S.path_scale;
-            float alpha[NCH];
-#pragma unroll
+            // Every channel's alpha reads that channel's Stokes vector before it is
+            // scaled, so computing and applying per channel is the reference's
+            // two-pass loop (absorption.rs:123-140) in one pass.
+#pragma unroll 1
             for (int k = 0; k < NCH; ++k) {
-                V3 e_hat = electric_field_direction(P.st[k], cur_plane, kk);
-                float p = clampf(dop(P.st[k]), 0.0f, 1.0f);
-                float a_pol = quad_form(S, P.a_o[k], P.a_e[k], e_hat);
-                float a_unp = midpoint(quad_form(S, P.a_o[k], P.a_e[k], ea), quad_form(S, P.a_o[k], P.a_e[k], eb));
-                alpha[k] = fmaf(p, a_pol - a_unp, a_unp);
+                float4 s4 = P.st[k];
+                Stokes s{s4.x, s4.y, s4.z, s4.w};
+                float a_o = arr(P.a_o4, k), a_e = arr(P.a_e4, k);
+                V3 e_hat = electric_field_direction(s, cur_plane, kk);
+                float p = clampf(dop(s), 0.0f, 1.0f);
+                float a_pol = quad_form(S, a_o, a_e, e_hat);
+                float a_unp = midpoint(quad_form(S, a_o, a_e, ea), quad_form(S, a_o, a_e, eb));
+                float alpha = fmaf(p, a_pol - a_unp, a_unp);
+                Stokes r = scale(s, exp_poly(-alpha * scaled));
+                P.st[k] = make_float4(r.i, r.q, r.u, r.v);
             }
-#pragma unroll
-            for (int k = 0; k < NCH; ++k) P.st[k] = scale(P.st[k], exp_poly(-alpha[k] * scaled));
         }
     }
 
     // compute_bounce_refraction_geometry (refraction.rs:428-547), uniaxial branch
-    const bool inside = P.inside;
     const bool aniso = S.anisotropic != 0;
     float cos_i = clampf(dot(neg(kk), normal), 0.0f, 1.0f);
     float one_m_c2 = fmaf(cos_i, -cos_i, 1.0f);
-    float sin_i = sqrtf(fmaxf(one_m_c2, 0.0f));
-    float n_o_hero = P.n_o[0];
-    float n_e_hero = n_o_hero + P.ne_d[0];
-    float n_med[NCH];
+    float n_o_hero = arr(P.n_o4, 0);
     if (aniso) {
         tally(ct, C_ANISO_BOUNCES);
+        float n_e_hero = n_o_hero + arr(P.ne_d4, 0);
         V3 c_axis = ld3(S.c_axis);
         float theta;
         if (!inside) {
             // theta_c_for_bounce entry fixed point (refraction.rs:248-269)
             float n_guess = n_o_hero;
             theta = 0.0f;
-#pragma unroll
+#pragma unroll 1
             for (int it = 0; it < 2; ++it) {
                 float eta = 1.0f / n_guess;
                 float s2 = eta * eta * one_m_c2;
                 if (s2 > 1.0f) break;
-                float ct = sqrtf(fmaxf(1.0f - s2, 0.0f));
-                V3 wd = normalize(add(smul(eta, kk), smul(fmaf(eta, cos_i, -ct), normal)));
-                theta = acosf(fabsf(clampf(dot(wd, c_axis), -1.0f, 1.0f)));
-                float sth, cth;
-                sincosf(theta, &sth, &cth);
-                n_guess = eff_e_index(n_o_hero, n_e_hero, sth, cth);
+                float ctg = sqrtf(fmaxf(1.0f - s2, 0.0f));
+                V3 wd = normalize(add(smul(eta, kk), smul(fmaf(eta, cos_i, -ctg), normal)));
+                theta = m_acos(fabsf(clampf(dot(wd, c_axis), -1.0f, 1.0f)));
+                float2 sc = m_sincos(theta);
+                n_guess = eff_e_index(n_o_hero, n_e_hero, sc.x, sc.y);
             }
         } else {
-            theta = acosf(fabsf(clampf(dot(kk, c_axis), -1.0f, 1.0f)));
+            theta = m_acos(fabsf(clampf(dot(kk, c_axis), -1.0f, 1.0f)));
         }
-        float sth, cth;
-        sincosf(theta, &sth, &cth);
-        const bool use_o = inside && !P.is_e;
-#pragma unroll
-        for (int k = 0; k < NCH; ++k)
-            n_med[k] = use_o ? P.n_o[k] : eff_e_index(P.n_o[k], P.n_o[k] + P.ne_d[k], sth, cth);
-    } else {
-#pragma unroll
-        for (int k = 0; k < NCH; ++k) n_med[k] = P.n_o[k];
-    }
-    const float n1 = inside ? n_med[0] : 1.0f;
-    const float n2 = inside ? 1.0f : n_med[0];
-    float eta0 = n1 / n2;
-    const float sin2_t = eta0 * eta0 * one_m_c2;
-
-    V3 new_k, new_s;
-    bool new_inside = inside;
-    bool has_update = false, update_val = false;
-    if (sin2_t > 1.0f) {
-        // apply_tir_bounce (refraction.rs:599-637)
-        tally(ct, C_TIR);
-#pragma unroll
+        float2 sc = m_sincos(theta);
+        const bool use_o = inside && !(bits & F_IS_E);
+#pragma unroll 1
         for (int k = 0; k < NCH; ++k) {
-            float n1k = inside ? n_med[k] : 1.0f, n2k = inside ? 1.0f : n_med[k];
-            float etak = n1k / n2k;
-            float s2k = etak * etak * one_m_c2;
-            if (s2k > 1.0f) {
-                tally(ct, C_CH_TIR);
-                float dk = tir_phase_delta(n1k, cos_i, sin_i);
-                float sd, cd;
-                sincosf(dk, &sd, &cd);
-                P.st[k] = apply_tir(P.st[k], cd, sd);
-            } else {
-                float ct = sqrtf(fmaxf(1.0f - s2k, 0.0f));
-                float rs, rp, a, b, c;
-                fresnel_rs_rp(n1k, n2k, cos_i, ct, rs, rp);
-                fresnel_reflection_abc(rs, rp, a, b, c);
-                P.st[k] = apply_fresnel(P.st[k], a, b, c);
-                P.pdf[k] = P.pdf[k] * r_unpol(rs, rp);
-            }
+            float n_o = arr(P.n_o4, k);
+            arr(E.n_med4, k) = use_o ? n_o : eff_e_index(n_o, n_o + arr(P.ne_d4, k), sc.x, sc.y);
         }
-        new_k = sub(kk, smul(2.0f * dot(kk, normal), normal));
-        new_s = (inside && aniso && P.is_e) ? extraordinary_poynting_dir(new_k, ld3(S.c_axis), n_o_hero, n_e_hero)
-                                            : new_k;
     } else {
-        // apply_partial_fresnel_bounce (refraction.rs:1036-1086)
-        float cos_t = sqrtf(1.0f - sin2_t);
-        float rs, rp;
-        fresnel_rs_rp(n1, n2, cos_i, cos_t, rs, rp);
-        const float ru = r_unpol(rs, rp);
-        float rng_b = rng_draw(P.seed, bounce, FRESNEL_BRANCH_STREAM);
-        if (rng_b < ru) {
-            // apply_partial_reflect_bounce (refraction.rs:650-690)
-            tally(ct, C_REFLECT);
-            const float inv = 1.0f / ru;
-#pragma unroll
-            for (int k = 0; k < NCH; ++k) {
-                float n1k = inside ? n_med[k] : 1.0f, n2k = inside ? 1.0f : n_med[k];
-                float etak = n1k / n2k;
-                float s2k = etak * etak * one_m_c2;
-                if (s2k > 1.0f) {
-                    tally(ct, C_CH_TIR);
-                    float dk = tir_phase_delta(n1k, cos_i, sin_i);
-                    float sd, cd;
-                    sincosf(dk, &sd, &cd);
-                    P.st[k] = scale(apply_tir(P.st[k], cd, sd), inv);
-                } else {
-                    float ct = sqrtf(fmaxf(1.0f - s2k, 0.0f));
-                    float rsk, rpk, a, b, c;
-                    fresnel_rs_rp(n1k, n2k, cos_i, ct, rsk, rpk);
-                    P.pdf[k] = P.pdf[k] * r_unpol(rsk, rpk);
-                    fresnel_reflection_abc(rsk, rpk, a, b, c);
-                    P.st[k] = scale(apply_fresnel(P.st[k], a, b, c), inv);
-                }
-            }
-            new_k = sub(kk, smul(2.0f * dot(kk, normal), normal));
-            new_s = (inside && aniso && P.is_e)
-                        ? extraordinary_poynting_dir(new_k, ld3(S.c_axis), n_o_hero, n_e_hero)
-                        : new_k;
-        } else {
-            // apply_refract_bounce (refraction.rs:748-867)
-            tally(ct, C_REFRACT);
-            const bool entering_aniso = !inside && aniso;
-            bool use_e = P.is_e;
-            if (entering_aniso) use_e = rng_draw(P.seed, bounce, BIREFRINGENT_SPLIT_STREAM) < 0.5f;
-            const bool ordinary_entry = entering_aniso && !use_e;
-            const bool extra_entry = entering_aniso && use_e;
-            float n2_dir = ordinary_entry ? n_o_hero : n2;
-            float eta_dir = n1 / n2_dir;
-            float s2d = fminf(eta_dir * eta_dir * one_m_c2, 1.0f);
-            float ctd = sqrtf(fmaxf(1.0f - s2d, 0.0f));
-            V3 refr = normalize(add(smul(eta_dir, kk), smul(fmaf(eta_dir, cos_i, -ctd), normal)));
-            V3 c_axis = ld3(S.c_axis);
-            V3 final_dir = extra_entry ? extraordinary_poynting_dir(refr, c_axis, n_o_hero, n_e_hero) : refr;
-            if (extra_entry) tally(ct, C_WALKOFF, 9);
-            const float tinv = 1.0f / (1.0f - ru);
-            const float TOL = 1.0f - 1e-6f;
-            // apply_refract_channel (refraction.rs:883-1011)
-#pragma unroll
-            for (int k = 0; k < NCH; ++k) {
-                float n1k = inside ? n_med[k] : 1.0f;
-                float n2k = ordinary_entry ? P.n_o[k] : (inside ? 1.0f : n_med[k]);
-                float ratio = n1k / n2k;
-                float s2k = (ratio * ratio) * one_m_c2;
-                if (s2k > 1.0f) {
-                    P.st[k] = scale(P.st[k], 0.0f);
-                    P.pdf[k] = 0.0f;
-                    continue;
-                }
-                tally(ct, C_CH_REFR);
-                float ctk = sqrtf(fmaxf(1.0f - s2k, 0.0f));
-                V3 rk = normalize(add(smul(ratio, kk), smul(fmaf(ratio, cos_i, -ctk), normal)));
-                V3 fk = extra_entry ? extraordinary_poynting_dir(rk, c_axis, P.n_o[k], P.n_o[k] + P.ne_d[k]) : rk;
-                if (dot(fk, final_dir) >= TOL) {
-                    float ts = (2.0f * n1k * cos_i) / fmaf(n2k, ctk, n1k * cos_i);
-                    float tp = (2.0f * n1k * cos_i) / fmaf(n1k, ctk, n2k * cos_i);
-                    float a, b, c;
-                    fresnel_transmission_abc(n1k, n2k, cos_i, ctk, ts, tp, a, b, c);
-                    P.st[k] = scale(apply_fresnel(P.st[k], a, b, c), tinv);
-                    float rsk, rpk;
-                    fresnel_rs_rp(n1k, n2k, cos_i, ctk, rsk, rpk);
-                    P.pdf[k] = P.pdf[k] * (1.0f - r_unpol(rsk, rpk));
-                } else {
-                    P.st[k] = scale(P.st[k], 0.0f);
-                    P.pdf[k] = 0.0f;
-                }
-            }
-            new_k = refr;
-            new_s = final_dir;
-            new_inside = !inside;
-            if (entering_aniso) {
-                has_update = true;
-                update_val = use_e;
-            }
-        }
+        E.n_med4[0] = P.n_o4[0];
+        E.n_med4[1] = P.n_o4[1];
     }
-    const bool was_internal_reflection = inside && !has_update && new_inside == inside;
-    P.d = new_s;
-    P.o = add(hp, mul(new_s, 1e-4f));
-    P.k = new_k;
-    P.inside = new_inside;
-    if (has_update) P.is_e = update_val;
-    // maybe_apply_internal_mode_coupling (transport.rs:343-353)
-    if (aniso && was_internal_reflection) P.is_e = rng_draw(P.seed, bounce, MODE_COUPLING_STREAM) < 0.5f;
+    const float n_med0 = arr(E.n_med4, 0);
+    const float n1 = inside ? n_med0 : 1.0f;
+    const float n2 = inside ? 1.0f : n_med0;
+    const float eta0 = n1 / n2;
+    const float sin2_t = eta0 * eta0 * one_m_c2;
+    E.hp_cos = make_float4(hp.x, hp.y, hp.z, cos_i);
 
-    // apply_russian_roulette (transport.rs:204-220)
+    // dispatch_bounce (transport.rs:158-176): hero TIR, or the Fresnel draw of
+    // apply_partial_fresnel_bounce (refraction.rs:1049-1060)
+    if (sin2_t > 1.0f) {
+        E.n_ru = make_float4(normal.x, normal.y, normal.z, 0.0f);
+        set_state_bits(P, bits | F_TIR);
+        return EV_REFLECT;
+    }
+    float cos_t = sqrtf(1.0f - sin2_t);
+    float rs, rp;
+    fresnel_rs_rp(n1, n2, cos_i, cos_t, rs, rp);
+    float ru = r_unpol(rs, rp);
+    E.n_ru = make_float4(normal.x, normal.y, normal.z, ru);
+    set_state_bits(P, bits & ~F_TIR);
+    return rng_draw(p_seed(P), bounce, FRESNEL_BRANCH_STREAM) < ru ? EV_REFLECT : EV_REFRACT;
+}
+
+// Direction / state update after an event, internal mode coupling and Russian
+// roulette (transport.rs:177-193,204-220,343-353,919-928).
+template <class CT>
+__device__ __forceinline__ void step_post(Path &P, const SceneConst &S, V3 hp, V3 new_k, V3 new_s, bool new_inside,
+                                          bool has_update, bool update_val, CT &ct) {
+    uint32_t bits = state_bits(P);
+    const uint32_t bounce = bits >> BOUNCE_SHIFT;
+    const bool inside = (bits & F_INSIDE) != 0;
+    const bool was_internal_reflection = inside && !has_update && new_inside == inside;
+    set_xyz(P.d_seed, new_s);
+    set_xyz(P.o_hero, add(hp, mul(new_s, 1e-4f)));
+    set_xyz(P.k_state, new_k);
+    bits = new_inside ? (bits | F_INSIDE) : (bits & ~F_INSIDE);
+    if (has_update) bits = update_val ? (bits | F_IS_E) : (bits & ~F_IS_E);
+    const uint32_t seed = p_seed(P);
+    if (S.anisotropic && was_internal_reflection)
+        bits = rng_draw(seed, bounce, MODE_COUPLING_STREAM) < 0.5f ? (bits | F_IS_E) : (bits & ~F_IS_E);
     if (bounce > 4) {
         tally(ct, C_ROULETTE);
         float mx = 0.0f;
 #pragma unroll
-        for (int k = 0; k < NCH; ++k) mx = fmaxf(mx, intensity(P.st[k]));
+        for (int k = 0; k < NCH; ++k) mx = fmaxf(mx, fmaxf(P.st[k].x, 0.0f));
         float q = clampf(mx, 0.05f, 1.0f);
-        float rr = rng_draw(P.seed, bounce, RUSSIAN_ROULETTE_STREAM);
-        if (rr > q) {
+        if (rng_draw(seed, bounce, RUSSIAN_ROULETTE_STREAM) > q) {
             tally(ct, C_ROULETTE_KILLS);
-            P.alive = false;
+            set_state_bits(P, bits & ~F_ALIVE);
             return;
         }
         const float iq = 1.0f / q;
 #pragma unroll
-        for (int k = 0; k < NCH; ++k) P.st[k] = scale(P.st[k], iq);
+        for (int k = 0; k < NCH; ++k) {
+            float4 s = P.st[k];
+            P.st[k] = make_float4(s.x * iq, s.y * iq, s.z * iq, s.w * iq);
+        }
     }
-    P.bounce = bounce + 1;
-    if (P.bounce >= S.max_bounces) P.alive = false;
+    const uint32_t nb = bounce + 1;
+    bits = (bits & ((1u << BOUNCE_SHIFT) - 1u)) | (nb << BOUNCE_SHIFT);
+    if (nb >= S.max_bounces) bits &= ~F_ALIVE;
+    set_state_bits(P, bits);
+}
+
+// apply_tir_bounce (refraction.rs:599-637) and apply_partial_reflect_bounce
+// (refraction.rs:650-690) in one channel loop.
+template <class CT>
+__device__ __forceinline__ void step_reflect(Path &P, const SceneConst &S, const Event &E, CT &ct) {
+    const uint32_t bits = state_bits(P);
+    const bool inside = (bits & F_INSIDE) != 0;
+    const bool hero_tir = (bits & F_TIR) != 0;
+    const V3 hp = xyz(E.hp_cos), normal = xyz(E.n_ru), kk = xyz(P.k_state);
+    const float cos_i = E.hp_cos.w;
+    const float one_m_c2 = fmaf(cos_i, -cos_i, 1.0f);
+    const float sin_i = sqrtf(fmaxf(one_m_c2, 0.0f));
+    if (hero_tir) tally(ct, C_TIR); else tally(ct, C_REFLECT);
+    // A TIR event applies each channel's matrix unscaled: the reflect branch's
+    // `.scale(1 / r_unpol)` with factor 1.0 (x * 1.0f == x exactly).
+    const float inv = hero_tir ? 1.0f : 1.0f / E.n_ru.w;
+#pragma unroll 1
+    for (int k = 0; k < NCH; ++k) {
+        const float nm = arr(E.n_med4, k);
+        const float n1k = inside ? nm : 1.0f, n2k = inside ? 1.0f : nm;
+        const float etak = n1k / n2k;
+        const float s2k = etak * etak * one_m_c2;
+        float4 s4 = P.st[k];
+        Stokes s{s4.x, s4.y, s4.z, s4.w};
+        if (s2k > 1.0f) {
+            tally(ct, C_CH_TIR);
+            float2 sc = m_sincos(tir_phase_delta(n1k, cos_i, sin_i));
+            s = scale(apply_tir(s, sc.y, sc.x), inv);
+        } else {
+            float ctk = sqrtf(fmaxf(1.0f - s2k, 0.0f));
+            float rsk, rpk, a, b, c;
+            fresnel_rs_rp(n1k, n2k, cos_i, ctk, rsk, rpk);
+            arr(P.pdf4, k) = arr(P.pdf4, k) * r_unpol(rsk, rpk);
+            fresnel_reflection_abc(rsk, rpk, a, b, c);
+            s = scale(apply_fresnel(s, a, b, c), inv);
+        }
+        P.st[k] = make_float4(s.i, s.q, s.u, s.v);
+    }
+    V3 new_k = sub(kk, smul(2.0f * dot(kk, normal), normal));
+    V3 new_s = new_k;
+    if (inside && S.anisotropic && (bits & F_IS_E)) {
+        float n_o_hero = arr(P.n_o4, 0);
+        new_s = extraordinary_poynting_dir(new_k, ld3(S.c_axis), n_o_hero, n_o_hero + arr(P.ne_d4, 0));
+    }
+    step_post(P, S, hp, new_k, new_s, inside, false, false, ct);
+}
+
+// apply_refract_bounce (refraction.rs:748-867) + apply_refract_channel (:883-1011)
+template <class CT>
+__device__ __forceinline__ void step_refract(Path &P, const SceneConst &S, const Event &E, CT &ct) {
+    const uint32_t bits = state_bits(P);
+    const uint32_t bounce = bits >> BOUNCE_SHIFT;
+    const bool inside = (bits & F_INSIDE) != 0;
+    const bool aniso = S.anisotropic != 0;
+    const V3 hp = xyz(E.hp_cos), normal = xyz(E.n_ru), kk = xyz(P.k_state);
+    const float cos_i = E.hp_cos.w, ru = E.n_ru.w;
+    const float one_m_c2 = fmaf(cos_i, -cos_i, 1.0f);
+    tally(ct, C_REFRACT);
+    const float n_med0 = arr(E.n_med4, 0);
+    const float n1 = inside ? n_med0 : 1.0f;
+    const float n2 = inside ? 1.0f : n_med0;
+    const float n_o_hero = arr(P.n_o4, 0);
+    const float n_e_hero = n_o_hero + arr(P.ne_d4, 0);
+    const bool entering_aniso = !inside && aniso;
+    bool use_e = (bits & F_IS_E) != 0;
+    if (entering_aniso) use_e = rng_draw(p_seed(P), bounce, BIREFRINGENT_SPLIT_STREAM) < 0.5f;
+    const bool ordinary_entry = entering_aniso && !use_e;
+    const bool extra_entry = entering_aniso && use_e;
+    const float n2_dir = ordinary_entry ? n_o_hero : n2;
+    const float eta_dir = n1 / n2_dir;
+    const float s2d = fminf(eta_dir * eta_dir * one_m_c2, 1.0f);
+    const float ctd = sqrtf(fmaxf(1.0f - s2d, 0.0f));
+    const V3 refr = normalize(add(smul(eta_dir, kk), smul(fmaf(eta_dir, cos_i, -ctd), normal)));
+    const V3 c_axis = ld3(S.c_axis);
+    const V3 final_dir = extra_entry ? extraordinary_poynting_dir(refr, c_axis, n_o_hero, n_e_hero) : refr;
+    if (extra_entry) tally(ct, C_WALKOFF, 9);
+    const float tinv = 1.0f / (1.0f - ru);
+    const float TOL = 1.0f - 1e-6f;
+#pragma unroll 1
+    for (int k = 0; k < NCH; ++k) {
+        const float n_o_k = arr(P.n_o4, k);
+        const float n1k = inside ? arr(E.n_med4, k) : 1.0f;
+        const float n2k = ordinary_entry ? n_o_k : (inside ? 1.0f : arr(E.n_med4, k));
+        const float ratio = n1k / n2k;
+        const float s2k = (ratio * ratio) * one_m_c2;
+        float4 s4 = P.st[k];
+        Stokes s{s4.x, s4.y, s4.z, s4.w};
+        bool keep = false;
+        float ctk = 0.0f;
+        if (!(s2k > 1.0f)) {
+            tally(ct, C_CH_REFR);
+            ctk = sqrtf(fmaxf(1.0f - s2k, 0.0f));
+            V3 rk = normalize(add(smul(ratio, kk), smul(fmaf(ratio, cos_i, -ctk), normal)));
+            V3 fk = extra_entry ? extraordinary_poynting_dir(rk, c_axis, n_o_k, n_o_k + arr(P.ne_d4, k)) : rk;
+            keep = dot(fk, final_dir) >= TOL;
+        }
+        if (keep) {
+            float ts = (2.0f * n1k * cos_i) / fmaf(n2k, ctk, n1k * cos_i);
+            float tp = (2.0f * n1k * cos_i) / fmaf(n1k, ctk, n2k * cos_i);
+            float a, b, c;
+            fresnel_transmission_abc(n1k, n2k, cos_i, ctk, ts, tp, a, b, c);
+            s = scale(apply_fresnel(s, a, b, c), tinv);
+            float rsk, rpk;
+            fresnel_rs_rp(n1k, n2k, cos_i, ctk, rsk, rpk);
+            arr(P.pdf4, k) = arr(P.pdf4, k) * (1.0f - r_unpol(rsk, rpk));
+        } else {
+            // chromatic termination / channel cannot transmit (refraction.rs:919-927,1006-1009)
+            s = scale(s, 0.0f);
+            arr(P.pdf4, k) = 0.0f;
+        }
+        P.st[k] = make_float4(s.i, s.q, s.u, s.v);
+    }
+    step_post(P, S, hp, refr, final_dir, !inside, entering_aniso, use_e, ct);
 }
 
 // Escape radiance, spectral MIS and CIE integration (transport.rs:67-90,931-939,
 // raytracer/color.rs:122-164) for a finished path.
 __device__ __forceinline__ V3 path_finish(const Path &P, const SceneConst &S, const SceneBuffers &B) {
-    float rad[NCH];
-    if (P.escaped) {
-        if (S.env_mode == GR_ENV_STUDIO) {
-            V3 dn = normalize(P.escape_dir);
-#pragma unroll
-            for (int k = 0; k < NCH; ++k) rad[k] = fmaf(P.rad_scale[k], studio_radiance(S, dn, lambda_k(P.hero, k)), 0.0f);
-        } else {
-            float rgb[3];
-            if (S.env_mode == GR_ENV_UNIFORM) {
-                rgb[0] = S.uni_rgb[0]; rgb[1] = S.uni_rgb[1]; rgb[2] = S.uni_rgb[2];
-            } else {
-                latlong_rgb(S, B.map, P.escape_dir, rgb);
-            }
-#pragma unroll
-            for (int k = 0; k < NCH; ++k)
-                rad[k] = fmaf(P.rad_scale[k], rgb_to_spectral(rgb[0], rgb[1], rgb[2], lambda_k(P.hero, k)), 0.0f);
-        }
-    } else {
-#pragma unroll
-        for (int k = 0; k < NCH; ++k) rad[k] = 0.0f;
-    }
     float sum = -0.0f;
 #pragma unroll
-    for (int k = 0; k < NCH; ++k) sum = sum + P.pdf[k];
-    float w = sum <= 1e-12f ? 1.0f : 8.0f * P.pdf[0] / sum;
+    for (int k = 0; k < NCH; ++k) sum = sum + arr(P.pdf4, k);
+    const float w = sum <= 1e-12f ? 1.0f : 8.0f * arr(P.pdf4, 0) / sum;
     const float norm = (400.0f / 8.0f) / 106.856f;
-    V3 xyz = v3(0.f, 0.f, 0.f);
-#pragma unroll
-    for (int k = 0; k < NCH; ++k) {
-        float wr = rad[k] * w;
-        xyz = add(xyz, mul(cmf(lambda_k(P.hero, k)), wr * norm));
+    const bool escaped = (p_flags(P) & F_ESCAPED) != 0;
+    const float hero = p_hero(P);
+    const V3 dir = xyz(P.d_seed);
+    float rgb[3] = {0.0f, 0.0f, 0.0f};
+    V3 dn = v3(0.f, 0.f, 0.f);
+    if (escaped) {
+        if (S.env_mode == GR_ENV_STUDIO) {
+            dn = normalize(dir);
+        } else if (S.env_mode == GR_ENV_UNIFORM) {
+            rgb[0] = S.uni_rgb[0]; rgb[1] = S.uni_rgb[1]; rgb[2] = S.uni_rgb[2];
+        } else {
+            latlong_rgb(S, B.map, dir, rgb);
+        }
     }
-    return von_kries(xyz, S.wb);
+    V3 acc = v3(0.f, 0.f, 0.f);
+#pragma unroll 1
+    for (int k = 0; k < NCH; ++k) {
+        const float lam = lambda_k(hero, k);
+        float rad = 0.0f;
+        if (escaped) {
+            float env = S.env_mode == GR_ENV_STUDIO ? studio_radiance(S, dn, lam)
+                                                     : rgb_to_spectral(rgb[0], rgb[1], rgb[2], lam);
+            rad = fmaf(fmaxf(P.st[k].x, 0.0f), env, 0.0f);
+        }
+        float wr = rad * w;
+        acc = add(acc, mul(cmf(lam), wr * norm));
+    }
+    return von_kries(acc, S.wb);
+}
+
+// One whole path in the calling thread (the plain kernel's body).
+template <class CT>
+__device__ __forceinline__ V3 trace_path(Path &P, const SceneConst &S, const SceneBuffers &B,
+                                         const float4 *__restrict__ planes, CT &ct) {
+    while (state_bits(P) & F_ALIVE) {
+        Event E;
+        uint32_t ev = step_hit(P, S, planes, E, ct);
+        if (ev == EV_REFLECT) step_reflect(P, S, E, ct);
+        else if (ev == EV_REFRACT) step_refract(P, S, E, ct);
+    }
+    return path_finish(P, S, B);
 }
 
 }  // namespace grd

@@ -181,7 +181,7 @@ typedef struct gr_scene {
 /* Context creation options (NULL = defaults). */
 typedef struct gr_create_opts {
     int32_t device;               /* CUDA device ordinal, -1 = current/0 */
-    uint64_t chunk_budget_bytes;  /* per-launch scratch budget, 0 = default (256 MiB) */
+    uint64_t chunk_budget_bytes;  /* per-launch scratch budget, 0 = default (2 GiB) */
     uint64_t serve_budget_bytes;  /* device-memory budget for resident scenes/films, 0 = 60 GiB */
 } gr_create_opts;
 
@@ -297,10 +297,11 @@ gr_status gr_render_resident(gr_ctx *ctx, uint64_t scene_id, uint32_t sample_off
 /* ---- engine controls ---------------------------------------------------------- */
 
 /* Transport kernel selection.  PLAIN: one thread per (pixel, sample) tuple, the
- * reference kernel's launch shape.  PERSISTENT (default): persistent warps that
- * regenerate finished paths from a global tuple counter.  Results are identical. */
+ * reference kernel's launch shape.  WAVEFRONT (default): a device pool of path
+ * records advanced by per-stage kernels over compacted event queues.  Results are
+ * identical (same arithmetic per path). */
 #define GR_KERNEL_PLAIN 0u
-#define GR_KERNEL_PERSISTENT 1u
+#define GR_KERNEL_WAVEFRONT 1u
 gr_status gr_set_kernel(gr_ctx *ctx, uint32_t kernel);
 
 /* Per-launch timing: while enabled, every trace and film-fold launch is bracketed by

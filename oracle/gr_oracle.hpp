@@ -1221,4 +1221,182 @@ static inline void srgb_encode(const V3<float> &xyz, uint8_t out[4]) {
     out[0] = encode_channel(toned.x); out[1] = encode_channel(toned.y); out[2] = encode_channel(toned.z);
 }
 
+// ---------------------------------------------------------------------------------
+// a17. Optical metrics -- color/metrics.rs:16-30,118-227,230-284,383-448,504,568-676,
+//      899-975,1082-1237 (FP32, libm, the reference's sequential reduction order)
+// ---------------------------------------------------------------------------------
+static inline void camera_view_basis(float yaw, float pitch, V3<float> &f, V3<float> &r, V3<float> &u) {
+    float cp = ::cosf(pitch), sp = ::sinf(pitch), cy = ::cosf(yaw), sy = ::sinf(yaw);
+    f = V3<float>(-cp * sy, -sp, -cp * cy).normalize();
+    V3<float> up = std::fabs(cp) < 1e-4f ? V3<float>(0.f, 0.f, -1.f) : V3<float>(0.f, 1.f, 0.f);
+    r = f.cross(up).normalize();
+    u = r.cross(f).normalize();
+}
+
+static inline float metric_fresnel_t(float n1, float n2, float ci, float ct) {
+    float ds = ::fmaf(n2, ct, n1 * ci), dp = ::fmaf(n2, ci, n1 * ct);
+    if (std::fabs(ds) < 1e-6f || std::fabs(dp) < 1e-6f) return 0.0f;
+    float a = ::fmaf(n2, -ct, n1 * ci) / ds, b = ::fmaf(n2, -ci, n1 * ct) / dp;
+    float r = midpoint(a * a, b * b);
+    return clampr(1.0f - r, 0.0f, 1.0f);
+}
+
+enum Fate { FATE_ENTRY_BLOCKED = 0, FATE_LEAKED = 1, FATE_EXITED = 2, FATE_ABSORBED = 3 };
+struct ExitPath { V3<float> dir; float transmittance, exit_cos; int facet; uint32_t bounces; };
+
+static inline int trace_wavelength(const V3<float> &entry, const V3<float> &in_dir, const V3<float> &n_entry,
+                                   float cos_i, const gr_plane *planes, uint32_t n, float index, ExitPath &ex) {
+    float sin2_t = (1.0f / (index * index)) * ::fmaf(cos_i, -cos_i, 1.0f);
+    if (sin2_t > 1.0f) return FATE_ENTRY_BLOCKED;
+    float cos_t = ::sqrtf(1.0f - sin2_t);
+    V3<float> dir = ((1.0f / index) * in_dir + ::fmaf(1.0f / index, cos_i, -cos_t) * n_entry).normalize();
+    V3<float> hp = entry + dir * 1e-4f;
+    float sin_crit = 1.0f / index;
+    float entry_t = metric_fresnel_t(1.0f, index, cos_i, cos_t);
+    bool leaked = false, up = false;
+    for (uint32_t bounce = 0; bounce < 10; ++bounce) {
+        Ray<float> r;
+        r.origin = hp;
+        r.dir = dir;
+        Hit<float> h = intersect_polyhedron(r, planes, n);
+        if (!h.hit) break;
+        V3<float> np = r.origin + h.t * r.dir;
+        V3<float> n_out = h.normal;
+        float ct = clampr(dir.dot(n_out), 0.0f, 1.0f);
+        float st = ::sqrtf(rmax(::fmaf(ct, -ct, 1.0f), 0.0f));
+        if (st < sin_crit) {
+            float s2o = (index * index) * ::fmaf(ct, -ct, 1.0f);
+            if (s2o <= 1.0f) {
+                float co = ::sqrtf(1.0f - s2o);
+                V3<float> od = (index * dir + ::fmaf(index, -ct, co) * n_out).normalize();
+                if (n_out.y < -0.05f) {
+                    leaked = true;
+                } else if (od.y > 0.05f) {
+                    up = true;
+                    ex.dir = od;
+                    ex.transmittance = metric_fresnel_t(index, 1.0f, ct, co);
+                    ex.exit_cos = co;
+                    ex.facet = h.facet;
+                    ex.bounces = bounce;
+                }
+                break;
+            }
+        }
+        dir = (dir - (2.0f * ct) * n_out).normalize();
+        hp = np + dir * 1e-4f;
+    }
+    if (leaked) return FATE_LEAKED;
+    if (up) { ex.transmittance = entry_t * ex.transmittance; return FATE_EXITED; }
+    return FATE_ABSORBED;
+}
+
+static inline bool visibly_returned(const V3<float> &d, const V3<float> &fwd, const StudioRig<float> &rig) {
+    bool head = (-d).dot(fwd) > 0.96f;
+    float kd = rmax(d.dot(rig.key), 0.0f), fd = rmax(d.dot(rig.fill), 0.0f);
+    bool ring = std::fabs(::fmaf(rig.sin_lp, -0.8f, d.y)) < 0.35f;
+    bool lit = (kd > 0.70f) || (fd > 0.75f) || (ring && d.y > 0.2f);
+    return !head && lit;
+}
+
+struct MetricsOut { float brilliance, fire, scintillation, windowing, extinction; };
+
+static inline MetricsOut evaluate_gem_optical_metrics(const gr_plane *planes, uint32_t n, const gr_material *m,
+                                                      float cam_yaw, float cam_pitch, float light_yaw, float light_pitch) {
+    if (n == 0) return MetricsOut{85.0f, 25.0f, 75.0f, 5.0f, 5.0f};
+    float nd = rmax(dispersion_evaluate<float>(m->dispersion, 589.3f), 1.1f);
+    float nf = rmax(dispersion_evaluate<float>(m->dispersion, 486.1f), 1.001f);
+    float nc = rmax(dispersion_evaluate<float>(m->dispersion, 656.3f), 1.001f);
+    V3<float> fwd, right, upv;
+    camera_view_basis(cam_yaw, cam_pitch, fwd, right, upv);
+    StudioRig<float> rig = studio_rig_new<float>(light_yaw, light_pitch);
+    const float ap[5][2] = {{0.f, 0.f}, {0.08f, 0.f}, {-0.08f, 0.f}, {0.f, 0.08f}, {0.f, -0.08f}};
+    const float yaw_off[5] = {-3.0f, -1.5f, 0.0f, 1.5f, 3.0f};
+    const float deg2rad = 3.14159265358979323846f / 180.0f;
+    const float rad2deg = 57.2957795130823208767981548141051703f;
+    uint32_t total = 0, windowed = 0, extinct = 0, returned = 0, cell_count = 0;
+    float fire_sum = 0.f, cf_sum = 0.f, cf_sq = 0.f, tv_sum = 0.f;
+    const int grid = 18;
+    for (int ix = 0; ix < grid; ++ix) {
+        for (int iz = 0; iz < grid; ++iz) {
+            float u = ::fmaf(((float)ix + 0.5f) / (float)grid, 2.0f, -1.0f);
+            float v = ::fmaf(((float)iz + 0.5f) / (float)grid, 2.0f, -1.0f);
+            if (::fmaf(v, v, u * u) > 0.70f) continue;
+            uint32_t ct_total = 0, ct_ret = 0;
+            for (int a = 0; a < 5; ++a) {
+                V3<float> rd = (fwd + ap[a][0] * right + ap[a][1] * upv).normalize();
+                V3<float> ro = (-fwd) * 2.5f + (u * 0.95f) * right + (v * 0.95f) * upv;
+                Ray<float> ray;
+                ray.origin = ro;
+                ray.dir = rd;
+                Hit<float> h = intersect_polyhedron(ray, planes, n);
+                if (!h.hit) continue;
+                total++;
+                ct_total++;
+                V3<float> hp = ray.origin + h.t * ray.dir;
+                float ci = clampr((-ray.dir).dot(h.normal), 0.0f, 1.0f);
+                ExitPath e;
+                int fate = trace_wavelength(hp, ray.dir, h.normal, ci, planes, n, nd, e);
+                if (fate == FATE_ENTRY_BLOCKED) continue;
+                if (fate == FATE_LEAKED) { windowed++; continue; }
+                if (fate == FATE_ABSORBED) { extinct++; continue; }
+                if (!visibly_returned(e.dir, fwd, rig)) { extinct++; continue; }
+                returned++;
+                ct_ret++;
+                ExitPath ef, ec;
+                int ff = trace_wavelength(hp, ray.dir, h.normal, ci, planes, n, nf, ef);
+                int fc = trace_wavelength(hp, ray.dir, h.normal, ci, planes, n, nc, ec);
+                if (ff == FATE_EXITED && fc == FATE_EXITED && ef.facet == ec.facet && ef.bounces == ec.bounces) {
+                    float cs = clampr(ef.dir.dot(ec.dir), -1.0f, 1.0f);
+                    float ang = ::acosf(cs) * rad2deg;
+                    float w = (e.transmittance * ef.transmittance * ec.transmittance) *
+                              (rmax(ef.exit_cos, 0.0f) * rmax(ec.exit_cos, 0.0f));
+                    fire_sum = ::fmaf(ang, w, fire_sum);
+                }
+            }
+            if (ct_total > 0) {
+                float frac = (float)ct_ret / (float)ct_total;
+                cf_sum += frac;
+                cf_sq = ::fmaf(frac, frac, cf_sq);
+                cell_count++;
+                uint32_t tr = 0;
+                for (int k = 0; k < 5; ++k) {
+                    V3<float> f2, r2, u2;
+                    camera_view_basis(cam_yaw + yaw_off[k] * deg2rad, cam_pitch, f2, r2, u2);
+                    Ray<float> ray;
+                    ray.origin = (-f2) * 2.5f + (u * 0.95f) * r2 + (v * 0.95f) * u2;
+                    ray.dir = f2;
+                    Hit<float> h = intersect_polyhedron(ray, planes, n);
+                    if (!h.hit) continue;
+                    V3<float> hp = ray.origin + h.t * ray.dir;
+                    float ci = clampr((-ray.dir).dot(h.normal), 0.0f, 1.0f);
+                    ExitPath e;
+                    if (trace_wavelength(hp, ray.dir, h.normal, ci, planes, n, nd, e) == FATE_EXITED &&
+                        visibly_returned(e.dir, f2, rig))
+                        tr++;
+                }
+                float tp = (float)tr / 5.0f;
+                tv_sum += ::fmaf(tp, -tp, tp);
+            }
+        }
+    }
+    float nt = (float)(total > 1 ? total : 1);
+    MetricsOut o;
+    o.windowing = clampr((float)windowed / nt * 100.0f, 0.0f, 100.0f);
+    o.extinction = clampr((float)extinct / nt * 100.0f, 0.0f, 100.0f);
+    o.brilliance = clampr((float)returned / nt * 100.0f, 0.0f, 100.0f);
+    o.fire = rmax(fire_sum / nt * 275.0f, 0.1f);
+    float spatial = 0.0f;
+    if (cell_count > 0) {
+        float mean = cf_sum / (float)cell_count;
+        if (mean > 1e-4f) {
+            float var = rmax(::fmaf(mean, -mean, cf_sq / (float)cell_count), 0.0f);
+            float cv = ::sqrtf(var) / mean;
+            spatial = clampr(cv / (1.0f + cv) * 100.0f, 0.0f, 100.0f);
+        }
+    }
+    float temporal = cell_count > 0 ? clampr((tv_sum / (float)cell_count) / 0.24f * 100.0f, 0.0f, 100.0f) : 0.0f;
+    o.scintillation = clampr(::fmaf(0.4f, temporal, 0.6f * spatial), 0.0f, 100.0f);
+    return o;
+}
+
 }  // namespace gro

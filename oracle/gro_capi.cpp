@@ -277,4 +277,12 @@ void gro_rng_records(const uint32_t *pixels, const uint32_t *samples, uint32_t n
     }
 }
 
+// evaluate_gem_optical_metrics (color/metrics.rs:1082-1237): out = brilliance %,
+// fire index, scintillation %, windowing %, extinction %.
+void gro_metrics(const gr_plane *planes, uint32_t n, const gr_material *m, float cam_yaw, float cam_pitch,
+                 float light_yaw, float light_pitch, float out[5]) {
+    MetricsOut o = evaluate_gem_optical_metrics(planes, n, m, cam_yaw, cam_pitch, light_yaw, light_pitch);
+    out[0] = o.brilliance; out[1] = o.fire; out[2] = o.scintillation; out[3] = o.windowing; out[4] = o.extinction;
+}
+
 }  // extern "C"

@@ -80,6 +80,8 @@ def lib():
     L.gro_trace_samples.argtypes = [sc, U, U, U, U, fp, up, up, up, C.c_int]
     L.gro_accumulate_rows.restype = C.c_int
     L.gro_accumulate_rows.argtypes = [sc, up, U, U, U, fp, C.c_int]
+    L.gro_metrics.restype = None
+    L.gro_metrics.argtypes = [C.POINTER(abi.gr_plane), U, C.POINTER(abi.gr_material), F, F, F, F, fp]
     L.gro_tonemap.restype = None
     L.gro_tonemap.argtypes = [fp, F, U, C.POINTER(C.c_uint8)]
     L.gro_rng_records.restype = None

@@ -198,3 +198,15 @@ def test_fp64_oracle_close_to_fp32(oracle):
     x64, b64, _ = _trace(oracle, s, g["ray_origin"], d, 1, hash_draw(oracle, 1), 12, 64)
     assert b32 == b64
     assert np.allclose(x32, x64, rtol=1e-4)
+
+
+def test_metric_goldens_bit_exact(oracle):
+    """evaluate_gem_optical_metrics(SRB, Diamond, 0, 0.45, 0.85, 0.95) reproduces the
+    reference's five f32 bit patterns exactly (raytracer_tests.rs:1818-1842)."""
+    g = GOLD["metrics"]
+    planes, n = _oracle_planes(oracle)
+    m = abi.gr_material()
+    oracle.gro_builtin_material(g["material"].encode(), C.byref(m))
+    out = (C.c_float * 5)()
+    oracle.gro_metrics(planes, n, C.byref(m), g["cam_yaw"], g["cam_pitch"], g["light_yaw"], g["light_pitch"], out)
+    assert [bits(v) for v in out] == g["bits"]

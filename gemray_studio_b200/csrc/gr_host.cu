@@ -295,7 +295,7 @@ struct gr_ctx {
     uint64_t serve_budget = 60ull << 30;
     int sm_count = 0;
     grh::DeviceBuffer xyz, film, planes, map, ext, counter, rgba;
-    int kernel_mode = GR_KERNEL_WAVEFRONT;
+    int kernel_mode = GR_KERNEL_PLAIN;
     // wavefront engine pool (gr_wavefront.cuh)
     uint32_t wave_cap = 1u << 18;
     grh::DeviceBuffer wf_pool, wf_events, wf_queues, wf_cnt;

@@ -53,7 +53,7 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_trace_plain(SceneConst S, Sce
         uint32_t pixel, sample;
         tuple_coords(R, t, pixel, sample);
         Path P;
-        path_init(P, S, B, pixel, sample, (uint32_t)t);
+        path_init<1>(P, S, B, pixel, sample, (uint32_t)t);
         tally(ct, C_PATHS);
         V3 c = trace_path(P, S, B, s_planes, ct);
         xyz[3 * t + 0] = c.x;

@@ -83,6 +83,7 @@ template <> __device__ __forceinline__ void tally<Counters>(Counters &ct, int i,
 
 // Build the path of tuple (pixel, sample): sampler draws (sampling.rs:232-271),
 // camera ray (camera.rs:95-114), per-sample wavelength cache (refraction.rs:127-174).
+template <int U = 1>
 __device__ __forceinline__ void path_init(Path &P, const SceneConst &S, const SceneBuffers &B, uint32_t pixel,
                                           uint32_t sample, uint32_t tuple) {
     Draws dr = sample_draws(pixel, sample);
@@ -95,7 +96,7 @@ __device__ __forceinline__ void path_init(Path &P, const SceneConst &S, const Sc
     P.d_seed = make_float4(dir.x, dir.y, dir.z, __uint_as_float(dr.seed));
     P.prev_tuple = make_float4(0.f, 0.f, 0.f, __uint_as_float(tuple));
     bool any = false;
-#pragma unroll 1
+#pragma unroll U
     for (int k = 0; k < NCH; ++k) {
         P.st[k] = make_float4(1.0f, 0.0f, 0.0f, 0.0f);
         arr(P.pdf4, k) = 1.0f;
@@ -217,7 +218,7 @@ __device__ __forceinline__ V3 shading_normal(const float4 *planes, uint32_t n, V
 // One intersection and everything of the bounce up to the hero's event decision
 // (transport.rs:781-895, raytracer/absorption.rs:71-141, refraction.rs:428-547,
 // 1036-1060).  Returns EV_DONE on an escape (F_ESCAPED set, F_ALIVE cleared).
-template <class CT>
+template <int U, class CT>
 __device__ __forceinline__ uint32_t step_hit(Path &P, const SceneConst &S, const float4 *__restrict__ planes, Event &E,
                                              CT &ct) {
     const uint32_t bits = state_bits(P);
@@ -266,7 +267,7 @@ __device__ __forceinline__ uint32_t step_hit(Path &P, const SceneConst &S, const
             // Every channel's alpha reads that channel's Stokes vector before it is
             // scaled, so computing and applying per channel is the reference's
             // two-pass loop (absorption.rs:123-140) in one pass.
-#pragma unroll 1
+#pragma unroll U
             for (int k = 0; k < NCH; ++k) {
                 float4 s4 = P.st[k];
                 Stokes s{s4.x, s4.y, s4.z, s4.w};
@@ -296,7 +297,7 @@ __device__ __forceinline__ uint32_t step_hit(Path &P, const SceneConst &S, const
             // theta_c_for_bounce entry fixed point (refraction.rs:248-269)
             float n_guess = n_o_hero;
             theta = 0.0f;
-#pragma unroll 1
+#pragma unroll U
             for (int it = 0; it < 2; ++it) {
                 float eta = 1.0f / n_guess;
                 float s2 = eta * eta * one_m_c2;
@@ -312,7 +313,7 @@ __device__ __forceinline__ uint32_t step_hit(Path &P, const SceneConst &S, const
         }
         float2 sc = m_sincos(theta);
         const bool use_o = inside && !(bits & F_IS_E);
-#pragma unroll 1
+#pragma unroll U
         for (int k = 0; k < NCH; ++k) {
             float n_o = arr(P.n_o4, k);
             arr(E.n_med4, k) = use_o ? n_o : eff_e_index(n_o, n_o + arr(P.ne_d4, k), sc.x, sc.y);
@@ -387,7 +388,7 @@ __device__ __forceinline__ void step_post(Path &P, const SceneConst &S, V3 hp, V
 
 // apply_tir_bounce (refraction.rs:599-637) and apply_partial_reflect_bounce
 // (refraction.rs:650-690) in one channel loop.
-template <class CT>
+template <int U, class CT>
 __device__ __forceinline__ void step_reflect(Path &P, const SceneConst &S, const Event &E, CT &ct) {
     const uint32_t bits = state_bits(P);
     const bool inside = (bits & F_INSIDE) != 0;
@@ -400,7 +401,7 @@ __device__ __forceinline__ void step_reflect(Path &P, const SceneConst &S, const
     // A TIR event applies each channel's matrix unscaled: the reflect branch's
     // `.scale(1 / r_unpol)` with factor 1.0 (x * 1.0f == x exactly).
     const float inv = hero_tir ? 1.0f : 1.0f / E.n_ru.w;
-#pragma unroll 1
+#pragma unroll U
     for (int k = 0; k < NCH; ++k) {
         const float nm = arr(E.n_med4, k);
         const float n1k = inside ? nm : 1.0f, n2k = inside ? 1.0f : nm;
@@ -432,7 +433,7 @@ __device__ __forceinline__ void step_reflect(Path &P, const SceneConst &S, const
 }
 
 // apply_refract_bounce (refraction.rs:748-867) + apply_refract_channel (:883-1011)
-template <class CT>
+template <int U, class CT>
 __device__ __forceinline__ void step_refract(Path &P, const SceneConst &S, const Event &E, CT &ct) {
     const uint32_t bits = state_bits(P);
     const uint32_t bounce = bits >> BOUNCE_SHIFT;
@@ -462,7 +463,7 @@ __device__ __forceinline__ void step_refract(Path &P, const SceneConst &S, const
     if (extra_entry) tally(ct, C_WALKOFF, 9);
     const float tinv = 1.0f / (1.0f - ru);
     const float TOL = 1.0f - 1e-6f;
-#pragma unroll 1
+#pragma unroll U
     for (int k = 0; k < NCH; ++k) {
         const float n_o_k = arr(P.n_o4, k);
         const float n1k = inside ? arr(E.n_med4, k) : 1.0f;
@@ -501,6 +502,7 @@ __device__ __forceinline__ void step_refract(Path &P, const SceneConst &S, const
 
 // Escape radiance, spectral MIS and CIE integration (transport.rs:67-90,931-939,
 // raytracer/color.rs:122-164) for a finished path.
+template <int U = 1>
 __device__ __forceinline__ V3 path_finish(const Path &P, const SceneConst &S, const SceneBuffers &B) {
     float sum = -0.0f;
 #pragma unroll
@@ -522,7 +524,7 @@ __device__ __forceinline__ V3 path_finish(const Path &P, const SceneConst &S, co
         }
     }
     V3 acc = v3(0.f, 0.f, 0.f);
-#pragma unroll 1
+#pragma unroll U
     for (int k = 0; k < NCH; ++k) {
         const float lam = lambda_k(hero, k);
         float rad = 0.0f;
@@ -543,11 +545,11 @@ __device__ __forceinline__ V3 trace_path(Path &P, const SceneConst &S, const Sce
                                          const float4 *__restrict__ planes, CT &ct) {
     while (state_bits(P) & F_ALIVE) {
         Event E;
-        uint32_t ev = step_hit(P, S, planes, E, ct);
-        if (ev == EV_REFLECT) step_reflect(P, S, E, ct);
-        else if (ev == EV_REFRACT) step_refract(P, S, E, ct);
+        uint32_t ev = step_hit<1>(P, S, planes, E, ct);
+        if (ev == EV_REFLECT) step_reflect<1>(P, S, E, ct);
+        else if (ev == EV_REFRACT) step_refract<1>(P, S, E, ct);
     }
-    return path_finish(P, S, B);
+    return path_finish<1>(P, S, B);
 }
 
 }  // namespace grd

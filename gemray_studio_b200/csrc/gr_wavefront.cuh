@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(256) k_wf_regen(SceneConst S, SceneBuffers B, 
         const uint64_t t = t0 + i;
         uint32_t pixel, sample;
         tuple_coords(R, t, pixel, sample);
-        path_init(W.pool[slot], S, B, pixel, sample, (uint32_t)t);
+        path_init<1>(W.pool[slot], S, B, pixel, sample, (uint32_t)t);
         wq_push(act, W.cnt + (cur ? W_ACT1 : W_ACT0), slot);
     }
 }
@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(256) k_wf_extend(SceneConst S, SceneBuffers B,
     NoCounters nc;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const uint32_t slot = act[i];
-        const uint32_t ev = step_hit(W.pool[slot], S, s_planes, W.events[slot], nc);
+        const uint32_t ev = step_hit<1>(W.pool[slot], S, s_planes, W.events[slot], nc);
         if (ev == EV_REFLECT) wq_push(W.q_reflect, W.cnt + W_REFL, slot);
         else if (ev == EV_REFRACT) wq_push(W.q_refract, W.cnt + W_REFR, slot);
         else wq_push(W.q_finish, W.cnt + W_FIN, slot);
@@ -115,8 +115,8 @@ __global__ void __launch_bounds__(256) k_wf_event(SceneConst S, WaveBuffers W, u
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const uint32_t slot = q[i];
         Path &P = W.pool[slot];
-        if (REFRACT) step_refract(P, S, W.events[slot], nc);
-        else step_reflect(P, S, W.events[slot], nc);
+        if (REFRACT) step_refract<1>(P, S, W.events[slot], nc);
+        else step_reflect<1>(P, S, W.events[slot], nc);
         if (state_bits(P) & F_ALIVE) wq_push(act, W.cnt + (nxt ? W_ACT1 : W_ACT0), slot);
         else wq_push(W.q_finish, W.cnt + W_FIN, slot);
     }
@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(256) k_wf_finish(SceneConst S, SceneBuffers B,
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const uint32_t slot = W.q_finish[i];
         const Path &P = W.pool[slot];
-        const V3 c = path_finish(P, S, B);
+        const V3 c = path_finish<1>(P, S, B);
         const uint64_t t = p_tuple(P);
         xyz[3 * t + 0] = c.x;
         xyz[3 * t + 1] = c.y;

@@ -51,6 +51,8 @@ GR_EVENT_COUNT = len(EVENT_NAMES)
 
 GR_KERNEL_PLAIN = 0
 GR_KERNEL_WAVEFRONT = 1
+GR_STATIC_SCRATCH_BYTES = 16 << 20
+GR_STATIC_SCRATCH_TUPLES = GR_STATIC_SCRATCH_BYTES // 12
 
 
 class gr_plane(C.Structure):
@@ -170,6 +172,7 @@ EXPORTS = [
     ("gr_scene_upload", C.c_int, [_ctx_p, C.POINTER(gr_scene), C.POINTER(C.c_uint64)]),
     ("gr_scene_release", C.c_int, [_ctx_p, C.c_uint64]),
     ("gr_render_resident", C.c_int, [_ctx_p, C.c_uint64, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]),
+    ("gr_render_resident_static", C.c_int, [_ctx_p, C.c_uint64, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]),
     ("gr_timing_enable", C.c_int, [_ctx_p, C.c_uint32]),
     ("gr_timing_read", C.c_int, [_ctx_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_uint64),
                                  C.POINTER(C.c_uint64)]),

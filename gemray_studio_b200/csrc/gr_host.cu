@@ -843,6 +843,43 @@ gr_status gr_render_resident(gr_ctx *ctx, uint64_t id, uint32_t sample_offset, u
     return grh::render_into(ctx, &shape, rs->S, resident_buffers(rs), sample_offset, spp, film_dev, s);
 }
 
+gr_status gr_render_resident_static(gr_ctx *ctx, uint64_t id, uint32_t sample_offset, uint32_t spp, float *film_dev,
+                                    void *stream) {
+    if (!ctx) return fail(GR_EINVAL, "ctx is NULL");
+    if (spp > GR_STATIC_SCRATCH_TUPLES)
+        return fail(GR_EINVAL, "spp %u does not fit the static scratch: at most %u samples per pixel per call", spp,
+                    (unsigned)GR_STATIC_SCRATCH_TUPLES);
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    auto it = ctx->scenes.find(id);
+    if (it == ctx->scenes.end()) return fail(GR_ENOTFOUND, "unknown scene id %llu", (unsigned long long)id);
+    ResidentScene *rs = it->second;
+    const uint64_t n_pixels = (uint64_t)rs->S.width * rs->S.height;
+    if (spp == 0 || n_pixels == 0) return GR_OK;
+    if (!film_dev) return fail(GR_EINVAL, "film is NULL");
+    GR_CUDA(cudaSetDevice(ctx->device));
+    float *scratch = nullptr;
+    GR_CUDA((cudaError_t)grh::static_scratch(ctx->device, &scratch));
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    const grd::SceneBuffers B = resident_buffers(rs);
+    uint64_t chunk_pixels = GR_STATIC_SCRATCH_TUPLES / spp;
+    if (chunk_pixels > n_pixels) chunk_pixels = n_pixels;
+    for (uint64_t first = 0; first < n_pixels; first += chunk_pixels) {
+        const uint64_t np = n_pixels - first < chunk_pixels ? n_pixels - first : chunk_pixels;
+        grd::LaunchRange R;
+        R.first_pixel = (uint32_t)first;
+        R.n_pixels = (uint32_t)np;
+        R.sample_offset = sample_offset;
+        R.spp = spp;
+        R.n_tuples = np * spp;
+        gr_status st = grh::launch_trace(ctx, rs->S, B, R, scratch, s, GR_KERNEL_PLAIN);
+        if (st != GR_OK) return st;
+        st = grh::launch_fold(scratch, (uint32_t)np, spp, (uint32_t)first, film_dev,
+                              (rs->S.flags & GR_FLAG_KAHAN_FILM) ? 1u : 0u, s);
+        if (st != GR_OK) return st;
+    }
+    return GR_OK;
+}
+
 gr_status gr_event_counts(gr_ctx *ctx, const gr_scene *sc, uint32_t first_pixel, uint32_t n_pixels,
                           uint32_t sample_offset, uint32_t spp, uint64_t *counts, uint32_t n_counts) {
     if (!ctx || !sc || !counts) return fail(GR_EINVAL, "NULL argument");

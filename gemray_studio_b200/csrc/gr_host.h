@@ -20,4 +20,9 @@ struct DeviceBuffer {
 // Device tone map (gr_tonemap.cu): rgba_dev[i] = sRGB ACES encode of xyz_dev[i] * scale.
 gr_status tonemap_device(const float *xyz_dev, float scale, uint32_t n, void *rgba_dev, struct CUstream_st *s);
 
+// The fixed scratch of gr_render_resident_static (gr_static.cu): its address on
+// `device` (the current device), looked up once per device.  Returns a cudaError_t.
+constexpr int kStaticMaxDevices = 64;
+int static_scratch(int device, float **out);
+
 }  // namespace grh

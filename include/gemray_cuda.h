@@ -294,6 +294,33 @@ gr_status gr_scene_release(gr_ctx *ctx, uint64_t scene_id);
 gr_status gr_render_resident(gr_ctx *ctx, uint64_t scene_id, uint32_t sample_offset, uint32_t spp,
                              float *film_device, void *stream);
 
+/* gr_render_resident that allocates no device memory.  No counterpart in the
+ * reference (its frame renderer grows its buffers on demand, renderer/gpu/frame.rs:
+ * 868-879); it exists for callers that must not allocate inside a render call.
+ *
+ * The per-tuple XYZ scratch is a fixed file-scope device array of
+ * GR_STATIC_SCRATCH_BYTES (one per device per process) instead of the context's
+ * growable buffer; the call makes no cudaMalloc / cudaFree and no library call that
+ * allocates, always runs the PLAIN kernel and records no timing events.  The frame is
+ * traced in chunks of floor(GR_STATIC_SCRATCH_TUPLES / spp) pixels, each folded into
+ * the film before the next is traced (stream order), so results are identical to
+ * gr_render_resident.  spp > GR_STATIC_SCRATCH_TUPLES (one pixel's samples do not fit)
+ * is rejected with GR_EINVAL before any work.
+ *
+ * Nothing in the scratch needs to start at zero: each chunk's trace launch writes
+ * every slot its fold then reads.  The film must hold the caller's running sum (the
+ * call ADDS to it), exactly as for gr_render_resident.
+ *
+ * Set-up: the first call on each device looks up the array's address once
+ * (cudaGetSymbolAddress, which may load the module); make that first call before any
+ * stream capture begins.  Races: the scratch is shared by every context on the
+ * device, so calls whose device work may overlap (other contexts, or different
+ * streams not ordered with each other) race on it; the caller must serialise them. */
+#define GR_STATIC_SCRATCH_BYTES (16u << 20)
+#define GR_STATIC_SCRATCH_TUPLES (GR_STATIC_SCRATCH_BYTES / 12u) /* 1,398,101 */
+gr_status gr_render_resident_static(gr_ctx *ctx, uint64_t scene_id, uint32_t sample_offset, uint32_t spp,
+                                    float *film_device, void *stream);
+
 /* ---- engine controls ---------------------------------------------------------- */
 
 /* Transport kernel selection.  PLAIN (default): one thread per (pixel, sample)

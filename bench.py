@@ -17,7 +17,7 @@ Prints ONE JSON line (rank 0):
   e2e     the same metric through the reference-facing C-ABI call gr_accumulate with
           host buffers (host->device upload of scene + film and the film readback
           inside the timed region);
-  roofline  FP32 bound of the dominant kernel (k_trace_persistent): algorithmic
+  roofline  FP32 bound of the dominant kernel (k_trace_plain): algorithmic
           flops from the event-tallied FLOP model / its event-timed duration, against
           the FP32 FMA throughput measured on this device;
   cpu_baseline  the C++ restatement of the reference CPU tracer on this host's cores.
@@ -48,6 +48,8 @@ WORKLOADS = {
     "c1": dict(width=256, height=256, spp=64, max_bounces=32, env="uniform", stone="rb57"),
     "c2": dict(width=1920, height=1080, spp=256, max_bounces=32, env="latlong", stone="rb57"),
     "c3": dict(width=1024, height=1024, spp=1024, max_bounces=64, env="studio", stone="em49"),
+    # c2's scene at 480x270, 64 spp: the small case the ncu captures run on
+    "c2s": dict(width=480, height=270, spp=64, max_bounces=32, env="latlong", stone="rb57"),
 }
 
 
@@ -233,6 +235,17 @@ def run_reference(args):
     }), flush=True)
 
 
+def traffic_per_launch(tuples_per_launch: float):
+    """DRAM bytes (read + write) of one k_trace_plain launch: the per-tuple traffic of
+    the committed ncu capture (profiles/k_trace_plain_traffic.json) times the tuples
+    one launch processes, or None without a capture."""
+    p = ROOT / "profiles" / "k_trace_plain_traffic.json"
+    if not p.exists():
+        return None
+    per_tuple = json.loads(p.read_text())["dram_bytes_per_tuple"]
+    return per_tuple * tuples_per_launch
+
+
 def run_engine(args):
     world, rank, local = dist_setup()
     import torch
@@ -330,15 +343,16 @@ def run_engine(args):
             "config": workload_config(args.workload, w, f"sample-range shards x{world}" if world > 1 else "single GPU"),
             "e2e": {"value": e2e_value, "unit": "path-samples/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
-            "roofline": {"bound": "fp32", "kernel": "k_trace_persistent", "achieved": achieved, "peak": fp32_peak,
-                         "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
+            "roofline": {"bound": "fp32", "kernel": "k_trace_plain", "achieved": achieved, "peak": fp32_peak,
+                         "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                         "traffic": traffic_per_launch(samples_per_step / max(1, ntr.value / frames)),
                          "peak_source": "measured on this device by gr_probe_fp32_peak (8 independent FFMA chains)",
                          "flops_per_sample": model.flops_per_sample,
                          "sfu_ops_per_sample": model.sfu / max(1, model.paths),
                          "kernel_ms_per_step": tr.value / frames, "fold_ms_per_step": fo.value / frames,
                          "launches_per_step": (ntr.value + nfo.value) / frames},
             "events_per_sample": {k: v / max(1, tallies["paths"]) for k, v in tallies.items() if k != "paths"},
-            "gpu_launches": int(ntr.value + nfo.value + args.steps),  # + the L2 flush fills
+            "gpu_launches": int(ntr.value + nfo.value),  # this library's trace + fold launches
             "clocks": clk,
             "device": r.adapter_label(),
         }

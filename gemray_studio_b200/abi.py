@@ -51,6 +51,7 @@ GR_EVENT_COUNT = len(EVENT_NAMES)
 
 GR_KERNEL_PLAIN = 0
 GR_KERNEL_WAVEFRONT = 1
+GR_KERNEL_REGEN = 2
 GR_STATIC_SCRATCH_BYTES = 16 << 20
 GR_STATIC_SCRATCH_TUPLES = GR_STATIC_SCRATCH_BYTES // 12
 
@@ -92,6 +93,18 @@ class gr_camera(C.Structure):
         ("origin", C.c_float * 3), ("forward", C.c_float * 3), ("right", C.c_float * 3),
         ("up", C.c_float * 3), ("fov_tan", C.c_float),
     ]
+
+
+class gr_metrics_out(C.Structure):
+    _fields_ = [("brilliance_pct", C.c_float), ("fire_index", C.c_float), ("scintillation_pct", C.c_float),
+                ("windowing_pct", C.c_float), ("extinction_pct", C.c_float)]
+
+
+class gr_pose(C.Structure):
+    _fields_ = [("cam_yaw", C.c_float), ("cam_pitch", C.c_float), ("light_yaw", C.c_float), ("light_pitch", C.c_float)]
+
+
+GR_METRICS_FP64_SUMS = 0x1
 
 
 class gr_environment(C.Structure):
@@ -169,6 +182,10 @@ EXPORTS = [
     ("gr_event_counts", C.c_int, [_ctx_p, C.POINTER(gr_scene), C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                   C.POINTER(C.c_uint64), C.c_uint32]),
     ("gr_probe_fp32_peak", C.c_int, [_ctx_p, C.POINTER(C.c_double)]),
+    ("gr_optical_metrics", C.c_int, [_ctx_p, C.c_void_p, C.c_uint32, C.POINTER(gr_material), C.POINTER(gr_pose),
+                                     C.c_uint32, C.c_uint32, C.POINTER(gr_metrics_out)]),
+    ("gr_angular_profile", C.c_int, [_ctx_p, C.c_void_p, C.c_uint32, C.POINTER(gr_material), C.c_float, C.c_float,
+                                     C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     ("gr_scene_upload", C.c_int, [_ctx_p, C.POINTER(gr_scene), C.POINTER(C.c_uint64)]),
     ("gr_scene_release", C.c_int, [_ctx_p, C.c_uint64]),
     ("gr_render_resident", C.c_int, [_ctx_p, C.c_uint64, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]),

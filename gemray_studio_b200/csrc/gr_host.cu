@@ -294,7 +294,7 @@ struct gr_ctx {
     size_t chunk_budget = 2048ull << 20;
     uint64_t serve_budget = 60ull << 30;
     int sm_count = 0;
-    grh::DeviceBuffer xyz, film, planes, map, ext, counter, rgba;
+    grh::DeviceBuffer xyz, film, planes, map, ext, counter, rgba, metrics;
     int kernel_mode = GR_KERNEL_PLAIN;
     // wavefront engine pool (gr_wavefront.cuh)
     uint32_t wave_cap = 1u << 18;
@@ -417,7 +417,7 @@ gr_status launch_wavefront(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuf
     const unsigned T = 256;
     uint64_t want = (cap + T - 1) / T;
     const unsigned grid = (unsigned)(want < (uint64_t)ctx->sm_count * 8 ? want : (uint64_t)ctx->sm_count * 8);
-    const size_t smem = (size_t)S.n_planes * sizeof(float4);
+    const size_t smem = grd::planes_smem_bytes(S.n_planes);
     grd::k_wf_reset<<<grid, T, 0, stream>>>(W);
     const int BATCH = 4;
     uint32_t it = 0;
@@ -449,10 +449,17 @@ gr_status launch_wavefront(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuf
 gr_status launch_trace(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuffers &B, const grd::LaunchRange &R,
                        float *xyz, cudaStream_t stream, int mode) {
     if (R.n_tuples == 0) return GR_OK;
-    size_t smem = (size_t)S.n_planes * sizeof(float4);
+    size_t smem = grd::planes_smem_bytes(S.n_planes);
     if (mode == GR_KERNEL_PLAIN || S.max_bounces == 0) {
         uint64_t blocks = (R.n_tuples + grd::TRACE_THREADS - 1) / grd::TRACE_THREADS;
         grd::k_trace_plain<grd::NoCounters><<<(unsigned)blocks, grd::TRACE_THREADS, smem, stream>>>(S, B, R, xyz, nullptr);
+        GR_CUDA(cudaGetLastError());
+        return GR_OK;
+    }
+    if (mode == GR_KERNEL_REGEN) {
+        const uint64_t warps = (R.n_tuples + grd::REGEN_TUPLES - 1) / grd::REGEN_TUPLES;
+        const uint64_t blocks = (warps * 32 + grd::TRACE_THREADS - 1) / grd::TRACE_THREADS;
+        grd::k_trace_regen<<<(unsigned)blocks, grd::TRACE_THREADS, smem, stream>>>(S, B, R, xyz);
         GR_CUDA(cudaGetLastError());
         return GR_OK;
     }
@@ -588,6 +595,7 @@ gr_status gr_destroy(gr_ctx *ctx) {
         ctx->ext.release();
         ctx->counter.release();
         ctx->rgba.release();
+        ctx->metrics.release();
         ctx->wf_pool.release();
         ctx->wf_events.release();
         ctx->wf_queues.release();
@@ -909,7 +917,7 @@ gr_status gr_event_counts(gr_ctx *ctx, const gr_scene *sc, uint32_t first_pixel,
     R.spp = spp;
     R.n_tuples = n_tuples;
     unsigned long long *dc = (unsigned long long *)ctx->counter.ptr;
-    size_t smem = (size_t)S.n_planes * sizeof(float4);
+    size_t smem = grd::planes_smem_bytes(S.n_planes);
     uint64_t blocks = (n_tuples + grd::TRACE_THREADS - 1) / grd::TRACE_THREADS;
     grd::k_trace_plain<grd::Counters><<<(unsigned)blocks, grd::TRACE_THREADS, smem, ctx->stream>>>(
         S, B, R, (float *)ctx->xyz.ptr, dc + 1);
@@ -988,9 +996,46 @@ gr_status gr_timing_read(gr_ctx *ctx, double *trace_ms, double *fold_ms, uint64_
     return GR_OK;
 }
 
+gr_status gr_optical_metrics(gr_ctx *ctx, const gr_plane *planes, uint32_t n_planes, const gr_material *material,
+                             const gr_pose *poses, uint32_t n_poses, uint32_t flags, gr_metrics_out *out) {
+    if (!ctx || !material || (n_poses && (!poses || !out))) return fail(GR_EINVAL, "NULL argument");
+    if (n_planes > GR_MAX_PLANES) return fail(GR_EINVAL, "n_planes %u exceeds GR_MAX_PLANES", n_planes);
+    if (n_planes && !planes) return fail(GR_EINVAL, "planes is NULL");
+    if (n_poses == 0) return GR_OK;
+    if (n_planes == 0) {
+        // color/metrics.rs:1090-1103: no geometry -> the reference's placeholder values
+        for (uint32_t i = 0; i < n_poses; ++i) out[i] = gr_metrics_out{85.0f, 25.0f, 75.0f, 5.0f, 5.0f};
+        return GR_OK;
+    }
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    GR_CUDA(cudaSetDevice(ctx->device));
+    gr_status st = grh::metrics_device(planes, n_planes, material, poses, n_poses, out, flags, ctx->stream, ctx->metrics);
+    if (st == GR_ECUDA) return fail(st, "metrics launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    return st;
+}
+
+gr_status gr_angular_profile(gr_ctx *ctx, const gr_plane *planes, uint32_t n_planes, const gr_material *material,
+                             float cam_yaw, float light_yaw, float light_pitch, float *brilliance_19,
+                             float *extinction_19, float *windowing_19) {
+    if (!brilliance_19 || !extinction_19 || !windowing_19) return fail(GR_EINVAL, "NULL curve");
+    gr_pose poses[19];
+    const float to_rad = 3.14159265358979323846f / 180.0f;  // f32::to_radians
+    for (int i = 0; i < 19; ++i) poses[i] = gr_pose{cam_yaw, (5.0f * (float)i) * to_rad, light_yaw, light_pitch};
+    gr_metrics_out m[19];
+    gr_status st = gr_optical_metrics(ctx, planes, n_planes, material, poses, 19, 0u, m);
+    if (st != GR_OK) return st;
+    for (int i = 0; i < 19; ++i) {
+        brilliance_19[i] = m[i].brilliance_pct;
+        extinction_19[i] = m[i].extinction_pct;
+        windowing_19[i] = m[i].windowing_pct;
+    }
+    return GR_OK;
+}
+
 gr_status gr_set_kernel(gr_ctx *ctx, uint32_t kernel) {
     if (!ctx) return fail(GR_EINVAL, "ctx is NULL");
-    if (kernel != GR_KERNEL_PLAIN && kernel != GR_KERNEL_WAVEFRONT) return fail(GR_EINVAL, "unknown kernel %u", kernel);
+    if (kernel != GR_KERNEL_PLAIN && kernel != GR_KERNEL_WAVEFRONT && kernel != GR_KERNEL_REGEN)
+        return fail(GR_EINVAL, "unknown kernel %u", kernel);
     std::lock_guard<std::mutex> lk(ctx->mu);
     ctx->kernel_mode = (int)kernel;
     return GR_OK;

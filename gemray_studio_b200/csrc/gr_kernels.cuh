@@ -23,9 +23,19 @@ struct LaunchRange {
     uint64_t n_tuples;  // n_pixels * spp
 };
 
-__device__ __forceinline__ void stage_planes(float4 *sp, const float4 *__restrict__ gp, uint32_t n) {
+// Both shared-memory layouts of the paired scan (planes_smem_bytes(n) bytes at sp).
+__device__ __forceinline__ Planes stage_plane_set(float4 *sp, const float4 *__restrict__ gp, uint32_t n) {
+    float4 *pairs = sp + n;
+    const uint32_t np = (n + 1u) >> 1;
     for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) sp[i] = gp[i];
+    for (uint32_t j = threadIdx.x; j < np; j += blockDim.x) {
+        const float4 a = gp[2 * j];
+        const float4 b = 2 * j + 1 < n ? gp[2 * j + 1] : make_float4(0.0f, 0.0f, 0.0f, -1.0f);
+        pairs[2 * j] = make_float4(a.x, b.x, a.y, b.y);
+        pairs[2 * j + 1] = make_float4(a.z, b.z, a.w, b.w);
+    }
     __syncthreads();
+    return Planes{sp, pairs, n};
 }
 
 __device__ __forceinline__ void tuple_coords(const LaunchRange &R, uint64_t t, uint32_t &pixel, uint32_t &sample) {
@@ -38,12 +48,18 @@ __device__ __forceinline__ void tuple_coords(const LaunchRange &R, uint64_t t, u
 // Plain kernel: one thread traces one tuple start to finish -- the reference
 // kernel's launch shape (one invocation per (pixel, sample), spectral_transport.wgsl:
 // 672-691).  The Counters variant tallies events for the FLOP model.
+// 9 resident blocks of 128 threads per SM caps the kernel at 56 registers; measured
+// on B200 this beats the unconstrained 64-72 registers by 2-5% (more warps to hide
+// the latency of the scalar physics code outweighs a few spilled values).
+#ifndef GR_TRACE_MIN_BLOCKS
+#define GR_TRACE_MIN_BLOCKS 9
+#endif
 template <class CT>
-__global__ void __launch_bounds__(TRACE_THREADS) k_trace_plain(SceneConst S, SceneBuffers B, LaunchRange R,
+__global__ void __launch_bounds__(TRACE_THREADS, GR_TRACE_MIN_BLOCKS) k_trace_plain(SceneConst S, SceneBuffers B, LaunchRange R,
                                                                float *__restrict__ xyz,
                                                                unsigned long long *__restrict__ tallies) {
     extern __shared__ float4 s_planes[];
-    stage_planes(s_planes, B.planes, S.n_planes);
+    const Planes PL = stage_plane_set(s_planes, B.planes, S.n_planes);
     uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     CT ct;
     if constexpr (sizeof(CT) == sizeof(Counters)) {
@@ -55,7 +71,7 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_trace_plain(SceneConst S, Sce
         Path P;
         path_init<1>(P, S, B, pixel, sample, (uint32_t)t);
         tally(ct, C_PATHS);
-        V3 c = trace_path(P, S, B, s_planes, ct);
+        V3 c = trace_path(P, S, B, PL, ct);
         xyz[3 * t + 0] = c.x;
         xyz[3 * t + 1] = c.y;
         xyz[3 * t + 2] = c.z;
@@ -66,6 +82,71 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_trace_plain(SceneConst S, Sce
             unsigned long long v = ((Counters &)ct).c[i];
             for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
             if (lane == 0 && v) atomicAdd(tallies + i, v);
+        }
+    }
+}
+
+// Path-regeneration kernel.  Path lengths within a warp vary widely (on a brilliant
+// the mean is ~3.7 bounces but the warp's longest path averages ~12), so a warp
+// that runs each lane's path to its end idles most lanes most of the time.  Here
+// each warp owns GR_REGEN_BATCH * 32 consecutive tuples; a lane whose path has ended
+// waits until at least GR_REGEN_MIN_IDLE lanes are idle (or all are), then every
+// idle lane finishes its path (writes its XYZ) and starts the warp's next unclaimed
+// tuple, while the warp's live lanes carry on bouncing.  Each tuple still runs the
+// same functions in the same order as in the plain kernel, so every XYZ is
+// bit-identical; only the schedule differs.
+#ifndef GR_REGEN_BATCH
+#define GR_REGEN_BATCH 16
+#endif
+#ifndef GR_REGEN_MIN_IDLE
+#define GR_REGEN_MIN_IDLE 16
+#endif
+constexpr uint32_t REGEN_TUPLES = 32u * GR_REGEN_BATCH;
+
+__global__ void __launch_bounds__(TRACE_THREADS) k_trace_regen(SceneConst S, SceneBuffers B, LaunchRange R,
+                                                               float *__restrict__ xyz) {
+    extern __shared__ float4 s_planes[];
+    const Planes PL = stage_plane_set(s_planes, B.planes, S.n_planes);
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t w_end0 = (warp + 1) * REGEN_TUPLES;
+    const uint64_t w_end = w_end0 < R.n_tuples ? w_end0 : R.n_tuples;
+    uint64_t next = warp * REGEN_TUPLES;  // warp-uniform: first unclaimed tuple
+    if (next >= R.n_tuples) return;       // whole warp (n_tuples and the grid are warp-uniform)
+    NoCounters nc;
+    Path P;
+    bool have = false;  // this lane holds a started, not yet finished path
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    for (;;) {
+        bool alive = have && (state_bits(P) & F_ALIVE);
+        const uint32_t idle = __ballot_sync(0xffffffffu, !alive);
+        const uint32_t n_idle = __popc(idle);
+        if (n_idle >= GR_REGEN_MIN_IDLE || idle == 0xffffffffu) {
+            if (!alive) {
+                if (have) {
+                    const V3 c = path_finish<1>(P, S, B);
+                    const uint64_t t = p_tuple(P);
+                    xyz[3 * t + 0] = c.x;
+                    xyz[3 * t + 1] = c.y;
+                    xyz[3 * t + 2] = c.z;
+                }
+                const uint64_t t = next + __popc(idle & lt_mask);
+                have = t < w_end;
+                if (have) {
+                    uint32_t pixel, sample;
+                    tuple_coords(R, t, pixel, sample);
+                    path_init<1>(P, S, B, pixel, sample, (uint32_t)t);
+                }
+            }
+            next += n_idle;
+            if (__ballot_sync(0xffffffffu, have) == 0u) break;
+            alive = have && (state_bits(P) & F_ALIVE);
+        }
+        if (alive) {
+            Event E;
+            const uint32_t ev = step_hit<1>(P, S, PL, E, nc);
+            if (ev == EV_REFLECT) step_reflect<1>(P, S, E, nc);
+            else if (ev == EV_REFRACT) step_refract<1>(P, S, E, nc);
         }
     }
 }

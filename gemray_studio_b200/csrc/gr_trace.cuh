@@ -24,6 +24,16 @@ namespace grd {
 
 constexpr int NCH = 8;
 
+// Unroll factors of the per-channel loops on the bounce path (code size vs. issue).
+#ifndef GR_ROT_UNROLL
+#define GR_ROT_UNROLL 8
+#endif
+#ifndef GR_RR_UNROLL
+#define GR_RR_UNROLL 8
+#endif
+constexpr int ROT_UNROLL = GR_ROT_UNROLL;
+constexpr int RR_UNROLL = GR_RR_UNROLL;
+
 // Per-path record (352 B).  Flag bits live in k_state.w's integer view.
 struct __align__(16) Path {
     float4 o_hero;      // ray origin, hero_rand
@@ -190,6 +200,114 @@ __device__ __forceinline__ bool intersect(const float4 *__restrict__ planes, uin
     return false;
 }
 
+// ---------------------------------------------------------------------------------
+// Paired plane scan for the transport kernels.
+//
+// Planes are staged twice in shared memory: as float4 (n.xyz, d) for lookups by
+// index, and pair-interleaved as {nx0, nx1, ny0, ny1}, {nz0, nz1, d0, d1}, so that
+// one packed mul.rn.f32x2 (sm_100: two IEEE round-to-nearest products) forms the
+// same product for two planes.  The sums stay scalar: a fully packed evaluation
+// (packed sums as well) did not reproduce the scalar scan's results on B200, while
+// packed products with scalar sums are bit-identical to it.  An odd tail is padded
+// with the plane n = 0, d = -1 (denom = 0, side = -1), which never acts.
+//
+// The per-plane decisions are those of the reference loop, reduced by two exact
+// rules (intersect.rs:93-132):
+//   * an entering plane (denom < -1e-7) with side <= 0 has t = -side/denom <= 0.
+//     Such t can only matter through t_near > t_far or t_near > 1e-4; the second is
+//     false for t <= 0, and if t_far < t <= 0 the far test (t_far > 1e-4) fails as
+//     well, so the outcome is a miss either way -- the plane is skipped;
+//   * a plane with side > 0 that the ray does not enter (denom >= -1e-7) is either
+//     parallel and outside (SlabScan::Outside) or gives t < 0 as a far candidate,
+//     forcing t_far < 0 and hence a miss -- the scan returns a miss at once.
+// Every t that is compared or kept is still the IEEE quotient -side / denom.
+// ---------------------------------------------------------------------------------
+struct Planes {
+    const float4 *aos;    // n x (n.xyz, d)
+    const float4 *pairs;  // ceil(n / 2) x 2 float4, interleaved as above
+    uint32_t n;
+};
+
+__host__ __device__ constexpr size_t planes_smem_bytes(uint32_t n) {
+    return (size_t)(n + 2u * ((n + 1u) / 2u)) * 16u;
+}
+
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 pk2(float lo, float hi) {
+    f32x2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void upk2(f32x2 v, float &lo, float &hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b) {
+    f32x2 r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+
+// One plane's contribution; returns false when the scan ends in a miss.
+__device__ __forceinline__ bool scan_plane(float denom, float side, int i, float &t_near, int &near_idx, float &t_far,
+                                           int &far_idx) {
+    if (denom < -1e-7f) {
+        if (side > 0.0f) {
+            const float num = -side;
+            const float qa = num * rcp_approx(denom);
+            if (!(qa + fabsf(qa) * 1.9073486e-6f < t_near)) {
+                const float t = num / denom;
+                if (t > t_near) { t_near = t; near_idx = i; }
+            }
+        }
+    } else if (side > 0.0f) {
+        return false;
+    } else if (denom > 1e-7f) {
+        const float num = -side;
+        const float qa = num * rcp_approx(denom);
+        if (!(qa - fabsf(qa) * 1.9073486e-6f > t_far)) {
+            const float t = num / denom;
+            if (t < t_far) { t_far = t; far_idx = i; }
+        }
+    }
+    return true;
+}
+
+__device__ __forceinline__ bool intersect(const Planes &PL, V3 o, V3 d, float &t_hit, int &idx_hit) {
+    float t_near = -1e30f, t_far = 1e30f;
+    int near_idx = -1, far_idx = -1;
+    const f32x2 dx = pk2(d.x, d.x), dy = pk2(d.y, d.y), dz = pk2(d.z, d.z);
+    const f32x2 ox = pk2(o.x, o.x), oy = pk2(o.y, o.y), oz = pk2(o.z, o.z);
+    const uint32_t np = (PL.n + 1u) >> 1;
+    for (uint32_t j = 0; j < np; ++j) {
+        const float4 a = PL.pairs[2 * j], b = PL.pairs[2 * j + 1];
+        const f32x2 nx = pk2(a.x, a.y), ny = pk2(a.z, a.w), nz = pk2(b.x, b.y);
+        float xd0, xd1, yd0, yd1, zd0, zd1, xo0, xo1, yo0, yo1, zo0, zo1;
+        upk2(mul2(nx, dx), xd0, xd1);
+        upk2(mul2(ny, dy), yd0, yd1);
+        upk2(mul2(nz, dz), zd0, zd1);
+        upk2(mul2(nx, ox), xo0, xo1);
+        upk2(mul2(ny, oy), yo0, yo1);
+        upk2(mul2(nz, oz), zo0, zo1);
+        // denom = (nx*dx + ny*dy) + nz*dz;  side = d + ((nx*ox + ny*oy) + nz*oz)
+        const float den0 = (xd0 + yd0) + zd0, den1 = (xd1 + yd1) + zd1;
+        const float sid0 = b.z + ((xo0 + yo0) + zo0), sid1 = b.w + ((xo1 + yo1) + zo1);
+        if (!scan_plane(den0, sid0, (int)(2 * j), t_near, near_idx, t_far, far_idx)) return false;
+        if (!scan_plane(den1, sid1, (int)(2 * j + 1), t_near, near_idx, t_far, far_idx)) return false;
+    }
+    if (t_near > t_far) return false;
+    if (t_near > 1e-4f) {
+        t_hit = t_near;
+        idx_hit = near_idx;
+        return true;
+    }
+    if (t_far > 1e-4f) {
+        t_hit = t_far;
+        idx_hit = far_idx;
+        return true;
+    }
+    return false;
+}
+
 __device__ __forceinline__ V3 plane_normal(const float4 *planes, int idx) {
     if (idx < 0) return v3(0.f, 0.f, 0.f);
     float4 p = planes[idx];
@@ -219,8 +337,7 @@ __device__ __forceinline__ V3 shading_normal(const float4 *planes, uint32_t n, V
 // (transport.rs:781-895, raytracer/absorption.rs:71-141, refraction.rs:428-547,
 // 1036-1060).  Returns EV_DONE on an escape (F_ESCAPED set, F_ALIVE cleared).
 template <int U, class CT>
-__device__ __forceinline__ uint32_t step_hit(Path &P, const SceneConst &S, const float4 *__restrict__ planes, Event &E,
-                                             CT &ct) {
+__device__ __forceinline__ uint32_t step_hit(Path &P, const SceneConst &S, const Planes &PL, Event &E, CT &ct) {
     const uint32_t bits = state_bits(P);
     const uint32_t bounce = bits >> BOUNCE_SHIFT;
     const bool inside = (bits & F_INSIDE) != 0;
@@ -228,14 +345,14 @@ __device__ __forceinline__ uint32_t step_hit(Path &P, const SceneConst &S, const
     float t_hit = 0.0f;
     int fidx = 0;
     tally(ct, C_BOUNCES);
-    if (!intersect(planes, S.n_planes, o, d, t_hit, fidx)) {
+    if (!intersect(PL, o, d, t_hit, fidx)) {
         // accumulate_miss_radiance (transport.rs:67-90) runs in path_finish
         tally(ct, C_ESCAPES);
         set_state_bits(P, (bits | F_ESCAPED) & ~F_ALIVE);
         return EV_DONE;
     }
     V3 hp = add(o, smul(t_hit, d));
-    V3 normal = shading_normal(planes, S.n_planes, hp, fidx, plane_normal(planes, fidx), S.edge_radius);
+    V3 normal = shading_normal(PL.aos, PL.n, hp, fidx, plane_normal(PL.aos, fidx), S.edge_radius);
 
     // rotate_stokes_to_plane_of_incidence (raytracer/absorption.rs:71-89)
     V3 cur_plane = normalize_or_zero(cross(kk, normal));
@@ -245,7 +362,7 @@ __device__ __forceinline__ uint32_t step_hit(Path &P, const SceneConst &S, const
         float sin_psi = dot(cross(prev, cur_plane), normalize_or_zero(kk));
         float psi = m_atan2(sin_psi, cos_psi);
         float2 sc = m_sincos(2.0f * psi);
-#pragma unroll
+#pragma unroll ROT_UNROLL
         for (int k = 0; k < NCH; ++k) {
             float4 s = P.st[k];
             Stokes r = apply_rotation(Stokes{s.x, s.y, s.z, s.w}, sc.y, sc.x);
@@ -365,7 +482,7 @@ __device__ __forceinline__ void step_post(Path &P, const SceneConst &S, V3 hp, V
     if (bounce > 4) {
         tally(ct, C_ROULETTE);
         float mx = 0.0f;
-#pragma unroll
+#pragma unroll RR_UNROLL
         for (int k = 0; k < NCH; ++k) mx = fmaxf(mx, fmaxf(P.st[k].x, 0.0f));
         float q = clampf(mx, 0.05f, 1.0f);
         if (rng_draw(seed, bounce, RUSSIAN_ROULETTE_STREAM) > q) {
@@ -374,7 +491,7 @@ __device__ __forceinline__ void step_post(Path &P, const SceneConst &S, V3 hp, V
             return;
         }
         const float iq = 1.0f / q;
-#pragma unroll
+#pragma unroll RR_UNROLL
         for (int k = 0; k < NCH; ++k) {
             float4 s = P.st[k];
             P.st[k] = make_float4(s.x * iq, s.y * iq, s.z * iq, s.w * iq);
@@ -541,11 +658,11 @@ __device__ __forceinline__ V3 path_finish(const Path &P, const SceneConst &S, co
 
 // One whole path in the calling thread (the plain kernel's body).
 template <class CT>
-__device__ __forceinline__ V3 trace_path(Path &P, const SceneConst &S, const SceneBuffers &B,
-                                         const float4 *__restrict__ planes, CT &ct) {
+__device__ __forceinline__ V3 trace_path(Path &P, const SceneConst &S, const SceneBuffers &B, const Planes &PL,
+                                         CT &ct) {
     while (state_bits(P) & F_ALIVE) {
         Event E;
-        uint32_t ev = step_hit<1>(P, S, planes, E, ct);
+        uint32_t ev = step_hit<1>(P, S, PL, E, ct);
         if (ev == EV_REFLECT) step_reflect<1>(P, S, E, ct);
         else if (ev == EV_REFRACT) step_refract<1>(P, S, E, ct);
     }

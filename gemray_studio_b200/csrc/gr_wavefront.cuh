@@ -91,14 +91,14 @@ __global__ void __launch_bounds__(256) k_wf_regen(SceneConst S, SceneBuffers B, 
 
 __global__ void __launch_bounds__(256) k_wf_extend(SceneConst S, SceneBuffers B, WaveBuffers W, uint32_t cur) {
     extern __shared__ float4 s_planes[];
-    stage_planes(s_planes, B.planes, S.n_planes);
+    const Planes PL = stage_plane_set(s_planes, B.planes, S.n_planes);
     const uint32_t n = W.cnt[cur ? W_ACT1 : W_ACT0];
     const uint32_t *act = active_q(W, cur);
     const uint32_t stride = gridDim.x * blockDim.x;
     NoCounters nc;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const uint32_t slot = act[i];
-        const uint32_t ev = step_hit<1>(W.pool[slot], S, s_planes, W.events[slot], nc);
+        const uint32_t ev = step_hit<1>(W.pool[slot], S, PL, W.events[slot], nc);
         if (ev == EV_REFLECT) wq_push(W.q_reflect, W.cnt + W_REFL, slot);
         else if (ev == EV_REFRACT) wq_push(W.q_refract, W.cnt + W_REFR, slot);
         else wq_push(W.q_finish, W.cnt + W_FIN, slot);

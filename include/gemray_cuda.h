@@ -281,6 +281,46 @@ gr_status gr_event_counts(gr_ctx *ctx, const gr_scene *scene, uint32_t first_pix
  * denominator of the transport kernels. */
 gr_status gr_probe_fp32_peak(gr_ctx *ctx, double *tflops);
 
+/* ---- optical metrics ------------------------------------------------------------ */
+
+/* = GemOpticalMetrics (color/metrics.rs:33-39). */
+typedef struct gr_metrics_out {
+    float brilliance_pct;
+    float fire_index;
+    float scintillation_pct;
+    float windowing_pct;
+    float extinction_pct;
+} gr_metrics_out;
+
+/* One viewing pose (radians), the four scalar arguments of
+ * evaluate_gem_optical_metrics. */
+typedef struct gr_pose {
+    float cam_yaw;
+    float cam_pitch;
+    float light_yaw;
+    float light_pitch;
+} gr_pose;
+
+/* Form the fire / scintillation sums in f64 instead of the reference's f32 running
+ * sums (counts are exact either way). */
+#define GR_METRICS_FP64_SUMS 0x1u
+
+/* evaluate_gem_optical_metrics (color/metrics.rs:1082-1237) for n_poses poses in one
+ * device pass: one thread per (pose, 18x18 grid cell, aperture ray or temporal yaw
+ * offset), then a per-pose reduction in the reference's cell order.  Classification
+ * counts (brilliance, windowing, extinction, the cells' return fractions) are the
+ * reference's exactly; fire can differ in its last bits through acosf.  n_planes == 0
+ * gives the reference's placeholder values (85, 25, 75, 5, 5). */
+gr_status gr_optical_metrics(gr_ctx *ctx, const gr_plane *planes, uint32_t n_planes, const gr_material *material,
+                             const gr_pose *poses, uint32_t n_poses, uint32_t flags, gr_metrics_out *out);
+
+/* evaluate_angular_profile_at_azimuth (color/metrics.rs:1262-1289): the 19 tilt
+ * elevations 0, 5, ..., 90 degrees (pitch = deg * (pi / 180) in f32, as
+ * f32::to_radians) as one batch; writes 19 values to each curve. */
+gr_status gr_angular_profile(gr_ctx *ctx, const gr_plane *planes, uint32_t n_planes, const gr_material *material,
+                             float cam_yaw, float light_yaw, float light_pitch, float *brilliance_19,
+                             float *extinction_19, float *windowing_19);
+
 /* ---- resident scenes (serving / benchmarks) ------------------------------------- */
 
 /* Copies a scene to the device once (planes, map, tables, encoded constants) and
@@ -326,10 +366,13 @@ gr_status gr_render_resident_static(gr_ctx *ctx, uint64_t scene_id, uint32_t sam
 /* Transport kernel selection.  PLAIN (default): one thread per (pixel, sample)
  * tuple, the reference kernel's launch shape.  WAVEFRONT: a device pool of path
  * records advanced by per-stage kernels over compacted event queues (about 3x slower
- * on B200: each bounce moves ~1 KB of record traffic).  Results are identical (same
+ * on B200: each bounce moves ~1 KB of record traffic).  REGEN: path regeneration,
+ * each warp owns a run of consecutive tuples and lanes whose path has ended start the
+ * next ones while the rest of the warp keeps bouncing.  Results are identical (same
  * arithmetic per path). */
 #define GR_KERNEL_PLAIN 0u
 #define GR_KERNEL_WAVEFRONT 1u
+#define GR_KERNEL_REGEN 2u
 gr_status gr_set_kernel(gr_ctx *ctx, uint32_t kernel);
 
 /* Per-launch timing: while enabled, every trace and film-fold launch is bracketed by
@@ -378,6 +421,7 @@ static_assert(offsetof(gr_material, scattering_sigma_s) == 308, "layout");
 static_assert(offsetof(gr_material, beta_ray_bands) == 328, "layout");
 static_assert(offsetof(gr_material, absorption_path_scale) == 424, "layout");
 static_assert(sizeof(gr_camera) == 52, "gr_camera");
+static_assert(sizeof(gr_metrics_out) == 20, "gr_metrics_out = GemOpticalMetrics");
 #endif
 
 #endif /* GEMRAY_CUDA_H */

@@ -107,6 +107,14 @@ class gr_pose(C.Structure):
 GR_METRICS_FP64_SUMS = 0x1
 
 
+class gr_batch_item(C.Structure):
+    _fields_ = [("scene_id", C.c_uint64), ("film_device", C.c_void_p), ("sample_offset", C.c_uint32),
+                ("spp", C.c_uint32)]
+
+
+GR_BATCH_GRAPH = 0x1
+
+
 class gr_environment(C.Structure):
     _fields_ = [
         ("mode", C.c_uint32), ("uniform_rgb", C.c_float * 3),
@@ -190,6 +198,7 @@ EXPORTS = [
     ("gr_scene_release", C.c_int, [_ctx_p, C.c_uint64]),
     ("gr_render_resident", C.c_int, [_ctx_p, C.c_uint64, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]),
     ("gr_render_resident_static", C.c_int, [_ctx_p, C.c_uint64, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]),
+    ("gr_render_batch", C.c_int, [_ctx_p, C.POINTER(gr_batch_item), C.c_uint32, C.c_uint32, C.c_void_p]),
     ("gr_timing_enable", C.c_int, [_ctx_p, C.c_uint32]),
     ("gr_timing_read", C.c_int, [_ctx_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_uint64),
                                  C.POINTER(C.c_uint64)]),

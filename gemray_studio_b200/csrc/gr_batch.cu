@@ -1,0 +1,197 @@
+// gr_batch.cu -- gr_render_batch: many resident scenes in shared launches.
+//
+// The planner cuts every item (resident scene, film, sample range) into segments of
+// whole pixels and packs them, in item order, into launches of at most the context's
+// per-launch tuple budget (chunk_budget / 12 B of per-tuple XYZ scratch).  Each launch
+// is one k_trace_batch grid over all of its segments followed by one k_fold_batch
+// grid, so scenes with few pixels or few samples share the device with the others
+// instead of each paying a launch, a tail and a host round trip.  Per-tuple arithmetic
+// and the per-pixel fold order are those of the single-scene kernels: every film is
+// bit-identical to rendering its item alone with gr_render_resident.
+//
+// With GR_BATCH_GRAPH the launch sequence is captured once as a CUDA graph and
+// replayed whenever the same batch shape recurs (same scenes, films, spp, frame sizes
+// and tables); only the device tables, which carry the sample offsets, are uploaded
+// again before each replay.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <unordered_map>
+#include <vector>
+
+#include "gr_batch.cuh"
+#include "gr_ctx.h"
+
+using grh::fail;
+
+namespace {
+
+struct Launch {
+    uint32_t seg_first, seg_count;
+    uint64_t blocks, warps;
+    uint32_t max_planes;
+};
+
+struct Plan {
+    std::vector<grd::SceneSlot> slots;
+    std::vector<grd::BatchSegment> segs;
+    std::vector<Launch> launches;
+    uint64_t max_tuples = 0;  // scratch tuples one launch needs
+};
+
+// Cuts the items into launches of at most `budget` tuples (a pixel whose spp alone
+// exceeds the budget gets a launch of its own).  xyz pointers are offsets from 0
+// until the scratch is placed.
+gr_status make_plan(gr_ctx *ctx, const gr_batch_item *items, uint32_t n_items, uint64_t budget, Plan &P) {
+    std::unordered_map<uint64_t, uint32_t> slot_of;
+    Launch cur{0, 0, 0, 0, 0};
+    uint64_t used = 0;
+    auto close = [&]() {
+        if (cur.seg_count) P.launches.push_back(cur);
+        P.max_tuples = std::max(P.max_tuples, used);
+        cur = Launch{(uint32_t)P.segs.size(), 0, 0, 0, 0};
+        used = 0;
+    };
+    for (uint32_t i = 0; i < n_items; ++i) {
+        const gr_batch_item &it = items[i];
+        auto f = ctx->scenes.find(it.scene_id);
+        if (f == ctx->scenes.end()) return fail(GR_ENOTFOUND, "item %u: unknown scene id %llu", i, (unsigned long long)it.scene_id);
+        ResidentScene *rs = f->second;
+        const uint64_t n_px = (uint64_t)rs->S.width * rs->S.height;
+        if (it.spp == 0 || n_px == 0) continue;
+        if (!it.film_device) return fail(GR_EINVAL, "item %u: film is NULL", i);
+        auto sl = slot_of.find(it.scene_id);
+        uint32_t slot;
+        if (sl == slot_of.end()) {
+            slot = (uint32_t)P.slots.size();
+            grd::SceneSlot s;
+            std::memset(&s, 0, sizeof(s));
+            s.S = rs->S;
+            s.B = resident_buffers(rs);
+            P.slots.push_back(s);
+            slot_of[it.scene_id] = slot;
+        } else {
+            slot = sl->second;
+        }
+        uint64_t next = 0;
+        while (next < n_px) {
+            uint64_t room = used < budget ? (budget - used) / it.spp : 0;
+            if (room == 0) {
+                if (used > 0) {
+                    close();
+                    continue;
+                }
+                room = 1;
+            }
+            const uint64_t np = std::min(room, n_px - next);
+            grd::BatchSegment g;
+            std::memset(&g, 0, sizeof(g));
+            g.R.first_pixel = (uint32_t)next;
+            g.R.n_pixels = (uint32_t)np;
+            g.R.sample_offset = it.sample_offset;
+            g.R.spp = it.spp;
+            g.R.n_tuples = np * it.spp;
+            g.xyz = reinterpret_cast<float *>((uintptr_t)(3 * used * sizeof(float)));
+            g.film = it.film_device;
+            g.block_begin = cur.blocks;
+            g.warp_begin = cur.warps;
+            g.scene = slot;
+            g.kahan = (rs->S.flags & GR_FLAG_KAHAN_FILM) ? 1u : 0u;
+            P.segs.push_back(g);
+            cur.seg_count++;
+            cur.blocks += (g.R.n_tuples + grd::TRACE_THREADS - 1) / grd::TRACE_THREADS;
+            cur.warps += np;
+            cur.max_planes = std::max(cur.max_planes, rs->S.n_planes);
+            used += g.R.n_tuples;
+            next += np;
+        }
+    }
+    close();
+    return GR_OK;
+}
+
+gr_status launch_plan(const Plan &P, const grd::SceneSlot *slots, const grd::BatchSegment *segs, cudaStream_t s) {
+    for (const Launch &L : P.launches) {
+        grd::k_trace_batch<<<(unsigned)L.blocks, grd::TRACE_THREADS, grd::planes_smem_bytes(L.max_planes), s>>>(
+            slots, segs + L.seg_first, L.seg_count);
+        const unsigned T = 256;
+        grd::k_fold_batch<<<(unsigned)((L.warps * 32 + T - 1) / T), T, 0, s>>>(segs + L.seg_first, L.seg_count);
+    }
+    GR_CUDA(cudaGetLastError());
+    return GR_OK;
+}
+
+// The shape a captured graph is valid for: everything but the sample offsets.
+std::vector<uint64_t> graph_key(const Plan &P, const void *tables, const void *xyz) {
+    std::vector<uint64_t> k;
+    k.push_back((uint64_t)(uintptr_t)tables);
+    k.push_back((uint64_t)(uintptr_t)xyz);
+    k.push_back(P.slots.size());
+    for (const grd::BatchSegment &g : P.segs) {
+        k.push_back((uint64_t)(uintptr_t)g.film);
+        k.push_back(((uint64_t)g.R.first_pixel << 32) | g.R.n_pixels);
+        k.push_back(((uint64_t)g.R.spp << 32) | g.scene);
+    }
+    for (const Launch &L : P.launches) k.push_back(((uint64_t)L.seg_count << 32) | L.max_planes);
+    return k;
+}
+
+}  // namespace
+
+extern "C" gr_status gr_render_batch(gr_ctx *ctx, const gr_batch_item *items, uint32_t n_items, uint32_t flags,
+                                     void *stream) {
+    if (!ctx) return fail(GR_EINVAL, "ctx is NULL");
+    if (n_items && !items) return fail(GR_EINVAL, "items is NULL");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    GR_CUDA(cudaSetDevice(ctx->device));
+    uint64_t budget = ctx->chunk_budget / (3 * sizeof(float));
+    if (budget > 0xFFFFFFFFull) budget = 0xFFFFFFFFull;  // tuple ids are u32 within a segment
+    Plan P;
+    gr_status st = make_plan(ctx, items, n_items, budget, P);
+    if (st != GR_OK) return st;
+    if (P.launches.empty()) return GR_OK;
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+
+    st = ctx->xyz.reserve((size_t)P.max_tuples * 3 * sizeof(float));
+    if (st != GR_OK) return st;
+    const size_t slot_bytes = (P.slots.size() * sizeof(grd::SceneSlot) + 255) & ~(size_t)255;
+    const size_t seg_bytes = P.segs.size() * sizeof(grd::BatchSegment);
+    st = ctx->batch_tables.reserve(slot_bytes + seg_bytes);
+    if (st != GR_OK) return st;
+    float *xyz = (float *)ctx->xyz.ptr;
+    for (grd::BatchSegment &g : P.segs) g.xyz = xyz + ((uintptr_t)g.xyz) / sizeof(float);
+    grd::SceneSlot *d_slots = (grd::SceneSlot *)ctx->batch_tables.ptr;
+    grd::BatchSegment *d_segs = (grd::BatchSegment *)((char *)ctx->batch_tables.ptr + slot_bytes);
+    // Pageable-source copies: the host vectors may be freed once these calls return.
+    GR_CUDA(cudaMemcpyAsync(d_slots, P.slots.data(), P.slots.size() * sizeof(grd::SceneSlot), cudaMemcpyHostToDevice, s));
+    GR_CUDA(cudaMemcpyAsync(d_segs, P.segs.data(), seg_bytes, cudaMemcpyHostToDevice, s));
+
+    if (!(flags & GR_BATCH_GRAPH)) return launch_plan(P, d_slots, d_segs, s);
+
+    const std::vector<uint64_t> key = graph_key(P, ctx->batch_tables.ptr, ctx->xyz.ptr);
+    cudaGraphExec_t exec = nullptr;
+    for (const BatchGraph &g : ctx->batch_graphs)
+        if (g.key == key) exec = g.exec;
+    if (!exec) {
+        cudaGraph_t graph = nullptr;
+        GR_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        st = launch_plan(P, d_slots, d_segs, s);
+        cudaError_t e = cudaStreamEndCapture(s, &graph);
+        if (st != GR_OK) {
+            if (graph) cudaGraphDestroy(graph);
+            return st;
+        }
+        if (e != cudaSuccess) return fail(GR_ECUDA, "batch graph capture failed: %s", cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return fail(GR_ECUDA, "batch graph instantiation failed: %s", cudaGetErrorString(e));
+        if (ctx->batch_graphs.size() >= kMaxBatchGraphs) {
+            cudaGraphExecDestroy(ctx->batch_graphs.front().exec);
+            ctx->batch_graphs.erase(ctx->batch_graphs.begin());
+        }
+        ctx->batch_graphs.push_back(BatchGraph{key, exec});
+    }
+    GR_CUDA(cudaGraphLaunch(exec, s));
+    return GR_OK;
+}

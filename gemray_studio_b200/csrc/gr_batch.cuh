@@ -1,0 +1,83 @@
+// gr_batch.cuh -- batched launches: many scenes (each with its own planes, material,
+// environment and film) in one grid.  Included by gr_batch.cu only.
+#pragma once
+
+#include "gr_launch.cuh"
+
+namespace grd {
+
+// A segment is one scene's run of whole pixels for one sample
+// range; every block of the trace kernel (every warp of the fold kernel) belongs to
+// exactly one segment, found by binary search over the segments' first block (warp).
+// The scene's constants are copied into shared memory, so per-tuple arithmetic is
+// that of the single-scene kernel and results are bit-identical to rendering each
+// scene alone.
+struct SceneSlot {
+    SceneConst S;
+    SceneBuffers B;
+};
+
+struct BatchSegment {
+    LaunchRange R;         // pixels / samples of this segment
+    float *xyz;            // its per-tuple XYZ (3 f32 per tuple)
+    float *film;           // the scene's film (W*H*3 f32), ADDed into by the fold
+    uint64_t block_begin;  // first trace block of the segment
+    uint64_t warp_begin;   // first fold warp of the segment
+    uint32_t scene;        // index into the SceneSlot table
+    uint32_t kahan;
+};
+
+template <bool BY_WARP>
+__device__ __forceinline__ uint32_t find_segment(const BatchSegment *__restrict__ segs, uint32_t n, uint64_t key) {
+    uint32_t lo = 0, hi = n;  // last segment whose begin <= key
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        const uint64_t b = BY_WARP ? segs[mid].warp_begin : segs[mid].block_begin;
+        if (b <= key) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(TRACE_THREADS, GR_TRACE_MIN_BLOCKS)
+    k_trace_batch(const SceneSlot *__restrict__ slots, const BatchSegment *__restrict__ segs, uint32_t n_segs) {
+    __shared__ SceneSlot s_slot;
+    __shared__ uint32_t s_seg;
+    extern __shared__ float4 s_planes[];
+    if (threadIdx.x == 0) s_seg = find_segment<false>(segs, n_segs, blockIdx.x);
+    __syncthreads();
+    const BatchSegment &G = segs[s_seg];
+    {
+        const uint32_t *src = reinterpret_cast<const uint32_t *>(slots + G.scene);
+        uint32_t *dst = reinterpret_cast<uint32_t *>(&s_slot);
+        for (uint32_t i = threadIdx.x; i < sizeof(SceneSlot) / 4; i += blockDim.x) dst[i] = src[i];
+    }
+    __syncthreads();
+    const SceneConst &S = s_slot.S;
+    const SceneBuffers &B = s_slot.B;
+    const Planes PL = stage_plane_set(s_planes, B.planes, S.n_planes);
+    const LaunchRange R = G.R;
+    const uint64_t t = (uint64_t)(blockIdx.x - G.block_begin) * blockDim.x + threadIdx.x;
+    if (t < R.n_tuples) {
+        uint32_t pixel, sample;
+        tuple_coords(R, t, pixel, sample);
+        Path P;
+        path_init<1>(P, S, B, pixel, sample, (uint32_t)t);
+        NoCounters nc;
+        const V3 c = trace_path(P, S, B, PL, nc);
+        float *xyz = G.xyz;
+        xyz[3 * t + 0] = c.x;
+        xyz[3 * t + 1] = c.y;
+        xyz[3 * t + 2] = c.z;
+    }
+}
+
+__global__ void k_fold_batch(const BatchSegment *__restrict__ segs, uint32_t n_segs) {
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const BatchSegment &G = segs[find_segment<true>(segs, n_segs, warp)];
+    const uint64_t px = warp - G.warp_begin;
+    if (px >= G.R.n_pixels) return;  // the grid's last warps past the final segment
+    fold_pixel(G.xyz, px, G.R.spp, G.R.first_pixel + (uint32_t)px, G.film, G.kahan);
+}
+
+}  // namespace grd

@@ -1,0 +1,72 @@
+// gr_ctx.h -- the engine context and resident scenes, shared by the host translation
+// units (gr_host.cu, gr_batch.cu).  Internal: not part of the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <mutex>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include "gemray_cuda.h"
+#include "gr_device.cuh"
+#include "gr_host.h"
+
+using grd::SceneConst;
+
+namespace grh {
+// Records a formatted message for gr_last_error_string() and returns st.
+gr_status fail(gr_status st, const char *fmt, ...);
+}  // namespace grh
+
+#define GR_CUDA(call)                                                                                       \
+    do {                                                                                                    \
+        cudaError_t e_ = (call);                                                                            \
+        if (e_ != cudaSuccess) return grh::fail(GR_ECUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+struct ResidentScene {
+    SceneConst S;
+    grh::DeviceBuffer planes, map, ext;
+    uint64_t bytes = 0;
+};
+
+// A captured batch launch sequence and the batch shape it is valid for.
+struct BatchGraph {
+    std::vector<uint64_t> key;
+    cudaGraphExec_t exec;
+};
+constexpr size_t kMaxBatchGraphs = 16;
+
+struct gr_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::mutex mu;
+    std::string label;
+    size_t chunk_budget = 2048ull << 20;
+    uint64_t serve_budget = 60ull << 30;
+    int sm_count = 0;
+    grh::DeviceBuffer xyz, film, planes, map, ext, counter, rgba, metrics;
+    int kernel_mode = GR_KERNEL_PLAIN;
+    // wavefront engine pool (gr_wavefront.cuh)
+    uint32_t wave_cap = 1u << 18;
+    grh::DeviceBuffer wf_pool, wf_events, wf_queues, wf_cnt;
+    uint32_t *wf_done_host = nullptr;
+    // Optional per-launch timing of the trace and fold kernels (CUDA events on the
+    // launch stream); read back by gr_timing_read.
+    bool timing = false;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> trace_ev, fold_ev;
+    size_t trace_used = 0, fold_used = 0;
+    uint64_t trace_launches = 0, fold_launches = 0;
+    // gr_render_batch: scene-slot + segment tables, captured launch sequences
+    grh::DeviceBuffer batch_tables;
+    std::vector<BatchGraph> batch_graphs;
+    std::map<uint64_t, ResidentScene *> scenes;
+    uint64_t next_scene_id = 1;
+    uint64_t resident_bytes = 0;
+};
+
+// Device pointers of a resident scene in the layout the kernels take.
+grd::SceneBuffers resident_buffers(ResidentScene *rs);

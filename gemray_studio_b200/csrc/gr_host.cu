@@ -20,13 +20,14 @@
 #include <vector>
 
 #include "gemray_cuda.h"
+#include "gr_ctx.h"
 #include "gr_host.h"
 #include "gr_kernels.cuh"
 #include "gr_wavefront.cuh"
 
 using grd::SceneConst;
 
-namespace {
+namespace grh {
 
 thread_local std::string g_last_error;
 
@@ -40,13 +41,9 @@ gr_status fail(gr_status st, const char *fmt, ...) {
     return st;
 }
 
-#define GR_CUDA(call)                                                                                 \
-    do {                                                                                              \
-        cudaError_t e_ = (call);                                                                      \
-        if (e_ != cudaSuccess) return fail(GR_ECUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
-    } while (0)
+}  // namespace grh
 
-}  // namespace
+using grh::fail;
 
 // ---------------------------------------------------------------------------------
 // Host-side f32 helpers (glam scalar semantics).
@@ -280,36 +277,6 @@ void encode_scene(const gr_scene *sc, SceneConst &S) {
 // ---------------------------------------------------------------------------------
 // A scene kept on the device between calls (serving / benchmark): encoded
 // constants plus its own copies of the planes, map and extension tables.
-struct ResidentScene {
-    SceneConst S;
-    grh::DeviceBuffer planes, map, ext;
-    uint64_t bytes = 0;
-};
-
-struct gr_ctx {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    std::mutex mu;
-    std::string label;
-    size_t chunk_budget = 2048ull << 20;
-    uint64_t serve_budget = 60ull << 30;
-    int sm_count = 0;
-    grh::DeviceBuffer xyz, film, planes, map, ext, counter, rgba, metrics;
-    int kernel_mode = GR_KERNEL_PLAIN;
-    // wavefront engine pool (gr_wavefront.cuh)
-    uint32_t wave_cap = 1u << 18;
-    grh::DeviceBuffer wf_pool, wf_events, wf_queues, wf_cnt;
-    uint32_t *wf_done_host = nullptr;
-    // Optional per-launch timing of the trace and fold kernels (CUDA events on the
-    // launch stream); read back by gr_timing_read.
-    bool timing = false;
-    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> trace_ev, fold_ev;
-    size_t trace_used = 0, fold_used = 0;
-    uint64_t trace_launches = 0, fold_launches = 0;
-    std::map<uint64_t, ResidentScene *> scenes;
-    uint64_t next_scene_id = 1;
-    uint64_t resident_bytes = 0;
-};
 
 namespace grd {
 __global__ void k_rng_records(const uint32_t *__restrict__ pixels, const uint32_t *__restrict__ samples, uint32_t n,
@@ -543,11 +510,24 @@ gr_status prepare(gr_ctx *ctx, const gr_scene *sc, SceneConst &S, grd::SceneBuff
 // ---------------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------------
+// Device pointers of a resident scene in the layout the kernels take.
+grd::SceneBuffers resident_buffers(ResidentScene *rs) {
+    grd::SceneBuffers B;
+    std::memset(&B, 0, sizeof(B));
+    B.planes = (const float4 *)rs->planes.ptr;
+    B.map = (const float *)rs->map.ptr;
+    if (rs->S.ext_n) {
+        B.ext_alpha_o = (const float *)rs->ext.ptr;
+        B.ext_alpha_e = (const float *)rs->ext.ptr + rs->S.ext_n;
+    }
+    return B;
+}
+
 extern "C" {
 
 uint32_t gr_abi_version(void) { return GR_ABI_VERSION; }
 
-const char *gr_last_error_string(void) { return g_last_error.c_str(); }
+const char *gr_last_error_string(void) { return grh::g_last_error.c_str(); }
 
 gr_status gr_create(gr_ctx **out, const gr_create_opts *opts) {
     if (!out) return fail(GR_EINVAL, "out is NULL");
@@ -596,6 +576,9 @@ gr_status gr_destroy(gr_ctx *ctx) {
         ctx->counter.release();
         ctx->rgba.release();
         ctx->metrics.release();
+        for (BatchGraph &g : ctx->batch_graphs) cudaGraphExecDestroy(g.exec);
+        ctx->batch_graphs.clear();
+        ctx->batch_tables.release();
         ctx->wf_pool.release();
         ctx->wf_events.release();
         ctx->wf_queues.release();
@@ -818,18 +801,6 @@ gr_status gr_scene_release(gr_ctx *ctx, uint64_t id) {
     delete rs;
     ctx->scenes.erase(it);
     return GR_OK;
-}
-
-static grd::SceneBuffers resident_buffers(ResidentScene *rs) {
-    grd::SceneBuffers B;
-    std::memset(&B, 0, sizeof(B));
-    B.planes = (const float4 *)rs->planes.ptr;
-    B.map = (const float *)rs->map.ptr;
-    if (rs->S.ext_n) {
-        B.ext_alpha_o = (const float *)rs->ext.ptr;
-        B.ext_alpha_e = (const float *)rs->ext.ptr + rs->S.ext_n;
-    }
-    return B;
 }
 
 gr_status gr_render_resident(gr_ctx *ctx, uint64_t id, uint32_t sample_offset, uint32_t spp, float *film_dev,

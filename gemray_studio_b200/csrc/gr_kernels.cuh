@@ -1,59 +1,15 @@
-// gr_kernels.cuh -- transport and film kernels (sm_100a).
-//
-// Work unit: a tuple t in [0, n_pixels * spp) of one launch maps to
-//   pixel = first_pixel + t / spp, absolute sample = sample_offset + t % spp,
-// the reference kernel's `idx = pixel * spp + s` numbering
-// (renderer/shaders/spectral_transport.wgsl:672-691), and its XYZ lands in
-// xyz[3 * t .. 3 * t + 3).  A film kernel then folds each pixel's spp samples in
-// sample order and adds the sum once to the film -- the reference's per-pixel
-// `sum += sample; accum[p] += sum` (renderer/gpu/frame.rs:799-814).
+// gr_kernels.cuh -- transport and film kernels of the single-scene path (sm_100a);
+// tuple numbering and the ordered fold are in gr_launch.cuh.  Included by gr_host.cu
+// only (the kernels here are not templates and must be defined once).
 #pragma once
 
-#include "gr_trace.cuh"
+#include "gr_launch.cuh"
 
 namespace grd {
-
-constexpr int TRACE_THREADS = 128;
-
-struct LaunchRange {
-    uint32_t first_pixel;
-    uint32_t n_pixels;
-    uint32_t sample_offset;
-    uint32_t spp;
-    uint64_t n_tuples;  // n_pixels * spp
-};
-
-// Both shared-memory layouts of the paired scan (planes_smem_bytes(n) bytes at sp).
-__device__ __forceinline__ Planes stage_plane_set(float4 *sp, const float4 *__restrict__ gp, uint32_t n) {
-    float4 *pairs = sp + n;
-    const uint32_t np = (n + 1u) >> 1;
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) sp[i] = gp[i];
-    for (uint32_t j = threadIdx.x; j < np; j += blockDim.x) {
-        const float4 a = gp[2 * j];
-        const float4 b = 2 * j + 1 < n ? gp[2 * j + 1] : make_float4(0.0f, 0.0f, 0.0f, -1.0f);
-        pairs[2 * j] = make_float4(a.x, b.x, a.y, b.y);
-        pairs[2 * j + 1] = make_float4(a.z, b.z, a.w, b.w);
-    }
-    __syncthreads();
-    return Planes{sp, pairs, n};
-}
-
-__device__ __forceinline__ void tuple_coords(const LaunchRange &R, uint64_t t, uint32_t &pixel, uint32_t &sample) {
-    uint32_t local_pixel = (uint32_t)(t / R.spp);
-    uint32_t s = (uint32_t)(t - (uint64_t)local_pixel * R.spp);
-    pixel = R.first_pixel + local_pixel;
-    sample = R.sample_offset + s;  // u32 wrapping add, as the reference's wrapping_add
-}
 
 // Plain kernel: one thread traces one tuple start to finish -- the reference
 // kernel's launch shape (one invocation per (pixel, sample), spectral_transport.wgsl:
 // 672-691).  The Counters variant tallies events for the FLOP model.
-// 9 resident blocks of 128 threads per SM caps the kernel at 56 registers; measured
-// on B200 this beats the unconstrained 64-72 registers by 2-5% (more warps to hide
-// the latency of the scalar physics code outweighs a few spilled values).
-#ifndef GR_TRACE_MIN_BLOCKS
-#define GR_TRACE_MIN_BLOCKS 9
-#endif
 template <class CT>
 __global__ void __launch_bounds__(TRACE_THREADS, GR_TRACE_MIN_BLOCKS) k_trace_plain(SceneConst S, SceneBuffers B, LaunchRange R,
                                                                float *__restrict__ xyz,
@@ -151,48 +107,11 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_trace_regen(SceneConst S, Sce
     }
 }
 
-// Film kernel: one warp per pixel.  Lanes load 32 samples at a time (coalesced);
-// every lane then folds them in sample order with shuffles, so the sum is the exact
-// sequential f32 sum the reference forms on the host.  Kahan mode keeps a
-// compensation term instead (flags & GR_FLAG_KAHAN_FILM).
 __global__ void k_film_fold(const float *__restrict__ xyz, uint32_t n_pixels, uint32_t spp, uint32_t first_pixel,
                             float *__restrict__ film, uint32_t kahan) {
-    const uint32_t lane = threadIdx.x & 31u;
     const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (warp >= n_pixels) return;
-    const float *src = xyz + (size_t)warp * spp * 3;
-    float sx = 0.0f, sy = 0.0f, sz = 0.0f;
-    float cx = 0.0f, cy = 0.0f, cz = 0.0f;
-    for (uint32_t s0 = 0; s0 < spp; s0 += 32) {
-        uint32_t s = s0 + lane;
-        float x = 0.f, y = 0.f, z = 0.f;
-        if (s < spp) {
-            x = src[3 * s + 0];
-            y = src[3 * s + 1];
-            z = src[3 * s + 2];
-        }
-        uint32_t cnt = spp - s0 < 32u ? spp - s0 : 32u;
-        for (uint32_t j = 0; j < cnt; ++j) {
-            float vx = __shfl_sync(0xffffffffu, x, j);
-            float vy = __shfl_sync(0xffffffffu, y, j);
-            float vz = __shfl_sync(0xffffffffu, z, j);
-            if (kahan) {
-                float yx = vx - cx, tx = sx + yx; cx = (tx - sx) - yx; sx = tx;
-                float yy = vy - cy, ty = sy + yy; cy = (ty - sy) - yy; sy = ty;
-                float yz = vz - cz, tz = sz + yz; cz = (tz - sz) - yz; sz = tz;
-            } else {
-                sx = sx + vx;
-                sy = sy + vy;
-                sz = sz + vz;
-            }
-        }
-    }
-    if (lane == 0) {
-        size_t p = (size_t)(first_pixel + (uint32_t)warp) * 3;
-        film[p + 0] = film[p + 0] + sx;
-        film[p + 1] = film[p + 1] + sy;
-        film[p + 2] = film[p + 2] + sz;
-    }
+    fold_pixel(xyz, warp, spp, first_pixel + (uint32_t)warp, film, kahan);
 }
 
 static_assert(C_COUNT == GR_EVENT_COUNT, "counter layout");

@@ -334,6 +334,30 @@ gr_status gr_scene_release(gr_ctx *ctx, uint64_t scene_id);
 gr_status gr_render_resident(gr_ctx *ctx, uint64_t scene_id, uint32_t sample_offset, uint32_t spp,
                              float *film_device, void *stream);
 
+/* ---- batched launches ------------------------------------------------------------ */
+
+/* One scene's sample range in a batched render: ADD samples [sample_offset,
+ * sample_offset + spp) of every pixel of a resident scene into film_device
+ * (W*H*3 f32 on the context's device). */
+typedef struct gr_batch_item {
+    uint64_t scene_id;
+    float *film_device;
+    uint32_t sample_offset;
+    uint32_t spp;
+} gr_batch_item;
+
+/* Capture the batch's launch sequence as a CUDA graph and replay it whenever the same
+ * batch shape (scenes, films, spp, frame sizes) recurs; sample offsets may change. */
+#define GR_BATCH_GRAPH 0x1u
+
+/* Renders all items in shared launches (no counterpart in the reference, whose
+ * frame renderer takes one scene per dispatch, renderer/gpu/frame.rs:632-814): scenes
+ * of any plane count, material and frame size are packed into launches of at most
+ * the context's chunk budget of per-tuple scratch.  Each film is bit-identical to
+ * gr_render_resident of its item alone.  Work is queued on `stream` (NULL = the
+ * context stream) and the call returns without waiting for it. */
+gr_status gr_render_batch(gr_ctx *ctx, const gr_batch_item *items, uint32_t n_items, uint32_t flags, void *stream);
+
 /* gr_render_resident that allocates no device memory.  No counterpart in the
  * reference (its frame renderer grows its buffers on demand, renderer/gpu/frame.rs:
  * 868-879); it exists for callers that must not allocate inside a render call.

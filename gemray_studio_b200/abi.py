@@ -115,6 +115,23 @@ class gr_batch_item(C.Structure):
 GR_BATCH_GRAPH = 0x1
 
 
+GR_REQ_RENDER, GR_REQ_METRICS = 0, 1
+GR_REQ_QUEUED, GR_REQ_RUNNING, GR_REQ_DONE, GR_REQ_CANCELLED, GR_REQ_FAILED = 0, 1, 2, 3, 4
+REQUEST_STATES = {0: "queued", 1: "running", 2: "done", 3: "cancelled", 4: "failed"}
+
+
+class gr_request(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("slice_spp", C.c_uint32), ("scene_id", C.c_uint64),
+                ("sample_offset", C.c_uint32), ("spp", C.c_uint32), ("flags", C.c_uint32), ("n_planes", C.c_uint32),
+                ("planes", C.c_void_p), ("material", C.c_void_p), ("poses", C.c_void_p), ("n_poses", C.c_uint32),
+                ("reserved", C.c_uint32)]
+
+
+class gr_request_status(C.Structure):
+    _fields_ = [("state", C.c_uint32), ("samples_done", C.c_uint32), ("error", C.c_int), ("reserved", C.c_uint32),
+                ("queued_ms", C.c_double), ("latency_ms", C.c_double)]
+
+
 class gr_environment(C.Structure):
     _fields_ = [
         ("mode", C.c_uint32), ("uniform_rgb", C.c_float * 3),
@@ -199,6 +216,13 @@ EXPORTS = [
     ("gr_render_resident", C.c_int, [_ctx_p, C.c_uint64, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]),
     ("gr_render_resident_static", C.c_int, [_ctx_p, C.c_uint64, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]),
     ("gr_render_batch", C.c_int, [_ctx_p, C.POINTER(gr_batch_item), C.c_uint32, C.c_uint32, C.c_void_p]),
+    ("gr_submit", C.c_int, [_ctx_p, C.POINTER(gr_request), C.POINTER(C.c_uint64)]),
+    ("gr_poll", C.c_int, [_ctx_p, C.c_uint64, C.POINTER(gr_request_status)]),
+    ("gr_wait", C.c_int, [_ctx_p, C.c_uint64, C.c_uint32, C.POINTER(gr_request_status)]),
+    ("gr_cancel", C.c_int, [_ctx_p, C.c_uint64]),
+    ("gr_request_film", C.c_int, [_ctx_p, C.c_uint64, C.POINTER(C.c_float)]),
+    ("gr_request_metrics", C.c_int, [_ctx_p, C.c_uint64, C.POINTER(gr_metrics_out)]),
+    ("gr_request_release", C.c_int, [_ctx_p, C.c_uint64]),
     ("gr_timing_enable", C.c_int, [_ctx_p, C.c_uint32]),
     ("gr_timing_read", C.c_int, [_ctx_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_uint64),
                                  C.POINTER(C.c_uint64)]),

@@ -62,9 +62,11 @@ def _raise_for(lib, status: int) -> None:
 class GpuFrameRenderer:
     """Owns one engine context (device buffers, stream); see renderer/gpu/frame.rs:566-647."""
 
-    def __init__(self, device: int = -1, chunk_budget_bytes: int = 0, kernel: int | None = None):
+    def __init__(self, device: int = -1, chunk_budget_bytes: int = 0, kernel: int | None = None,
+                 serve_budget_bytes: int = 0):
         self._lib = abi.load_library()
-        opts = abi.gr_create_opts(device=device, chunk_budget_bytes=chunk_budget_bytes, serve_budget_bytes=0)
+        opts = abi.gr_create_opts(device=device, chunk_budget_bytes=chunk_budget_bytes,
+                                  serve_budget_bytes=serve_budget_bytes)
         ctx = C.c_void_p()
         _raise_for(self._lib, self._lib.gr_create(C.byref(ctx), C.byref(opts)))
         self._ctx = ctx

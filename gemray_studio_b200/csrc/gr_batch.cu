@@ -139,19 +139,16 @@ std::vector<uint64_t> graph_key(const Plan &P, const void *tables, const void *x
 
 }  // namespace
 
-extern "C" gr_status gr_render_batch(gr_ctx *ctx, const gr_batch_item *items, uint32_t n_items, uint32_t flags,
-                                     void *stream) {
-    if (!ctx) return fail(GR_EINVAL, "ctx is NULL");
-    if (n_items && !items) return fail(GR_EINVAL, "items is NULL");
-    std::lock_guard<std::mutex> lk(ctx->mu);
-    GR_CUDA(cudaSetDevice(ctx->device));
+namespace grh {
+
+gr_status batch_enqueue(gr_ctx *ctx, const gr_batch_item *items, uint32_t n_items, uint32_t flags, cudaStream_t stream) {
     uint64_t budget = ctx->chunk_budget / (3 * sizeof(float));
     if (budget > 0xFFFFFFFFull) budget = 0xFFFFFFFFull;  // tuple ids are u32 within a segment
     Plan P;
     gr_status st = make_plan(ctx, items, n_items, budget, P);
     if (st != GR_OK) return st;
     if (P.launches.empty()) return GR_OK;
-    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    cudaStream_t s = stream ? stream : ctx->stream;
 
     st = ctx->xyz.reserve((size_t)P.max_tuples * 3 * sizeof(float));
     if (st != GR_OK) return st;
@@ -194,4 +191,15 @@ extern "C" gr_status gr_render_batch(gr_ctx *ctx, const gr_batch_item *items, ui
     }
     GR_CUDA(cudaGraphLaunch(exec, s));
     return GR_OK;
+}
+
+}  // namespace grh
+
+extern "C" gr_status gr_render_batch(gr_ctx *ctx, const gr_batch_item *items, uint32_t n_items, uint32_t flags,
+                                     void *stream) {
+    if (!ctx) return fail(GR_EINVAL, "ctx is NULL");
+    if (n_items && !items) return fail(GR_EINVAL, "items is NULL");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    GR_CUDA(cudaSetDevice(ctx->device));
+    return grh::batch_enqueue(ctx, items, n_items, flags, (cudaStream_t)stream);
 }

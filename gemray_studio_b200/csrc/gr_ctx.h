@@ -33,6 +33,8 @@ struct ResidentScene {
     uint64_t bytes = 0;
 };
 
+struct ServeState;  // gr_serve.cu
+
 // A captured batch launch sequence and the batch shape it is valid for.
 struct BatchGraph {
     std::vector<uint64_t> key;
@@ -63,6 +65,8 @@ struct gr_ctx {
     // gr_render_batch: scene-slot + segment tables, captured launch sequences
     grh::DeviceBuffer batch_tables;
     std::vector<BatchGraph> batch_graphs;
+    // gr_submit / gr_poll request loop (created by the first submit)
+    ServeState *serve = nullptr;
     std::map<uint64_t, ResidentScene *> scenes;
     uint64_t next_scene_id = 1;
     uint64_t resident_bytes = 0;
@@ -70,3 +74,13 @@ struct gr_ctx {
 
 // Device pointers of a resident scene in the layout the kernels take.
 grd::SceneBuffers resident_buffers(ResidentScene *rs);
+
+namespace grh {
+// gr_render_batch's body; the caller holds ctx->mu and has made ctx->device current.
+gr_status batch_enqueue(gr_ctx *ctx, const gr_batch_item *items, uint32_t n_items, uint32_t flags, cudaStream_t stream);
+}  // namespace grh
+
+namespace grh {
+// Stops the request loop and frees its requests; the caller holds no lock.
+void serve_shutdown(gr_ctx *ctx);
+}  // namespace grh

@@ -564,6 +564,7 @@ gr_status gr_create(gr_ctx **out, const gr_create_opts *opts) {
 
 gr_status gr_destroy(gr_ctx *ctx) {
     if (!ctx) return GR_OK;
+    grh::serve_shutdown(ctx);  // joins the request loop, which takes ctx->mu itself
     {
         std::lock_guard<std::mutex> lk(ctx->mu);
         cudaSetDevice(ctx->device);

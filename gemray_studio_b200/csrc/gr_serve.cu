@@ -1,0 +1,460 @@
+// gr_serve.cu -- the render-request loop: gr_submit / gr_poll / gr_wait / gr_cancel.
+//
+// Requests mirror RenderRequest{request_id, first_sample, samples}
+// (crates/gemray-net/src/messages/render.rs:65-70) over resident scenes.  A worker
+// thread per context runs continuous batching:
+//   * admission -- queued requests are admitted in arrival order while their film
+//     fits the context's device-memory budget next to the resident scenes and the
+//     films of running requests; a film is allocated and zeroed on admission;
+//   * ticks -- each tick every running render contributes its next slice
+//     (slice_spp samples of every pixel) to ONE batched launch (gr_batch.cu), so
+//     requests that arrive while others run share the device with them at the next
+//     tick; up to two ticks are in flight, so the host plans tick k+1 while tick k runs;
+//   * retirement -- when a tick's event completes its slices count as folded;
+//     a render is DONE when all its samples are; cancellation takes effect between
+//     slices;
+//   * metric requests (pose sweeps) run between ticks on the same stream.
+// A request's film is what gr_render_resident adds when called once per slice over
+// the same sample range (each slice's per-pixel sum is folded in sample order and
+// added once, like a worker accumulating sub-batches), so a result depends on its own
+// slice size but is bit-identical alone and in any mix.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "gr_ctx.h"
+
+using grh::fail;
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+    uint64_t id = 0;
+    gr_request r{};
+    std::vector<gr_pose> poses;          // metrics
+    std::vector<gr_plane> planes;        // metrics
+    gr_material material{};              // metrics
+    std::vector<gr_metrics_out> metrics; // metrics results
+    uint32_t state = GR_REQ_QUEUED;
+    gr_status error = GR_OK;
+    uint64_t film_bytes = 0;
+    grh::DeviceBuffer film;
+    uint32_t issued = 0, done = 0, in_flight = 0;  // samples per pixel
+    bool cancel = false;
+    Clock::time_point t_submit, t_admit, t_done;
+};
+
+struct Tick {
+    cudaEvent_t ev = nullptr;
+    std::vector<std::pair<uint64_t, uint32_t>> slices;  // (request id, spp)
+};
+
+double ms_between(Clock::time_point a, Clock::time_point b) {
+    return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+}  // namespace
+
+struct ServeState {
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::unordered_map<uint64_t, Request *> reqs;
+    std::deque<uint64_t> queue;   // admission order
+    std::vector<uint64_t> running;
+    uint64_t next_id = 1;
+    uint64_t film_bytes = 0;      // films of admitted requests
+    bool stop = false;
+    std::thread worker;
+};
+
+namespace {
+
+void finish(ServeState &sv, Request *q, uint32_t state, gr_status err = GR_OK) {
+    q->state = state;
+    q->error = err;
+    q->t_done = Clock::now();
+    if (q->t_admit.time_since_epoch().count() == 0) q->t_admit = q->t_done;  // ended while queued
+    sv.cv_done.notify_all();
+}
+
+// Admission in arrival order while films fit the budget (caller holds sv.mu).
+void admit(gr_ctx *ctx, ServeState &sv, uint64_t resident_bytes) {
+    while (!sv.queue.empty()) {
+        Request *q = sv.reqs[sv.queue.front()];
+        if (q->cancel) {
+            sv.queue.pop_front();
+            finish(sv, q, GR_REQ_CANCELLED);
+            continue;
+        }
+        if (q->r.kind == GR_REQ_METRICS) {
+            sv.queue.pop_front();
+            q->state = GR_REQ_RUNNING;
+            q->t_admit = Clock::now();
+            sv.running.push_back(q->id);
+            continue;
+        }
+        if (resident_bytes + q->film_bytes > ctx->serve_budget) {  // can never fit, even with no other film
+            sv.queue.pop_front();
+            finish(sv, q, GR_REQ_FAILED, GR_EBUSY);
+            continue;
+        }
+        if (resident_bytes + sv.film_bytes + q->film_bytes > ctx->serve_budget) break;  // wait for releases
+        if (q->film.reserve(q->film_bytes) != GR_OK ||
+            cudaMemsetAsync(q->film.ptr, 0, q->film_bytes, ctx->stream) != cudaSuccess) {
+            sv.queue.pop_front();
+            q->film.release();
+            finish(sv, q, GR_REQ_FAILED, GR_ENOMEM);
+            continue;
+        }
+        sv.queue.pop_front();
+        sv.film_bytes += q->film_bytes;
+        q->state = GR_REQ_RUNNING;
+        q->t_admit = Clock::now();
+        sv.running.push_back(q->id);
+    }
+}
+
+void worker_main(gr_ctx *ctx, ServeState *sv) {
+    cudaSetDevice(ctx->device);
+    std::deque<Tick> flight;
+    std::vector<cudaEvent_t> spare;
+    auto retire = [&](Tick &t) {  // caller holds sv->mu; the tick's event has completed
+        for (auto &s : t.slices) {
+            auto it = sv->reqs.find(s.first);
+            if (it == sv->reqs.end()) continue;
+            Request *q = it->second;
+            q->in_flight -= s.second;
+            q->done += s.second;
+        }
+        spare.push_back(t.ev);
+    };
+    for (;;) {
+        // 1. retire finished ticks (always the oldest first: ticks complete in order)
+        while (!flight.empty()) {
+            const bool must_wait = flight.size() >= 2;
+            cudaError_t e = must_wait ? cudaEventSynchronize(flight.front().ev) : cudaEventQuery(flight.front().ev);
+            if (e == cudaErrorNotReady) break;
+            std::lock_guard<std::mutex> lk(sv->mu);
+            retire(flight.front());
+            flight.pop_front();
+        }
+        std::vector<gr_batch_item> items;
+        std::vector<std::pair<uint64_t, uint32_t>> slices;
+        std::vector<Request *> metric_jobs;
+        {
+            std::unique_lock<std::mutex> lk(sv->mu);
+            // 2. completions and cancellations of running requests
+            std::vector<uint64_t> keep;
+            for (uint64_t id : sv->running) {
+                Request *q = sv->reqs[id];
+                if (q->r.kind == GR_REQ_METRICS && q->cancel) {
+                    finish(*sv, q, GR_REQ_CANCELLED);
+                    continue;
+                }
+                if (q->r.kind == GR_REQ_RENDER && q->in_flight == 0 && (q->cancel || q->done >= q->r.spp)) {
+                    finish(*sv, q, q->done >= q->r.spp ? GR_REQ_DONE : GR_REQ_CANCELLED);
+                    continue;
+                }
+                keep.push_back(id);
+            }
+            sv->running.swap(keep);
+            // 3. admission (resident_bytes is read without ctx->mu: a stale value only
+            //    delays or advances an admission by one tick)
+            admit(ctx, *sv, ctx->resident_bytes);
+            // 4. this tick's slices
+            for (uint64_t id : sv->running) {
+                Request *q = sv->reqs[id];
+                if (q->r.kind == GR_REQ_METRICS) {
+                    if (q->state == GR_REQ_RUNNING && !q->cancel) metric_jobs.push_back(q);
+                    continue;
+                }
+                if (q->cancel || q->issued >= q->r.spp) continue;
+                const uint32_t slice = std::min(q->r.slice_spp ? q->r.slice_spp : 16u, q->r.spp - q->issued);
+                items.push_back(gr_batch_item{q->r.scene_id, (float *)q->film.ptr, q->r.sample_offset + q->issued, slice});
+                slices.emplace_back(id, slice);
+                q->issued += slice;
+                q->in_flight += slice;
+            }
+            if (items.empty() && metric_jobs.empty()) {
+                if (flight.empty()) {
+                    if (sv->stop) break;
+                    sv->cv_work.wait_for(lk, std::chrono::milliseconds(20));
+                    continue;
+                }
+                lk.unlock();
+                cudaEventSynchronize(flight.front().ev);  // nothing new to issue: wait for the oldest tick
+                continue;
+            }
+        }
+        // 5. metric sweeps between ticks
+        for (Request *q : metric_jobs) {
+            gr_status st;
+            {
+                std::lock_guard<std::mutex> lk(ctx->mu);
+                st = grh::metrics_device(q->planes.data(), (uint32_t)q->planes.size(), &q->material, q->poses.data(),
+                                         (uint32_t)q->poses.size(), q->metrics.data(), q->r.flags, ctx->stream,
+                                         ctx->metrics);
+            }
+            std::lock_guard<std::mutex> lk(sv->mu);
+            std::vector<uint64_t> keep;
+            for (uint64_t id : sv->running)
+                if (id != q->id) keep.push_back(id);
+            sv->running.swap(keep);
+            finish(*sv, q, st == GR_OK ? GR_REQ_DONE : GR_REQ_FAILED, st);
+        }
+        // 6. launch the tick
+        if (!items.empty()) {
+            Tick t;
+            t.slices = slices;
+            if (!spare.empty()) {
+                t.ev = spare.back();
+                spare.pop_back();
+            } else if (cudaEventCreateWithFlags(&t.ev, cudaEventDisableTiming) != cudaSuccess) {
+                t.ev = nullptr;
+            }
+            gr_status st;
+            {
+                std::lock_guard<std::mutex> lk(ctx->mu);
+                st = grh::batch_enqueue(ctx, items.data(), (uint32_t)items.size(), 0u, ctx->stream);
+                if (st == GR_OK && t.ev && cudaEventRecord(t.ev, ctx->stream) != cudaSuccess) st = GR_ECUDA;
+                if (st == GR_OK && !t.ev) st = GR_ECUDA;
+            }
+            if (st != GR_OK) {
+                // the whole tick failed: fail its requests (they may have partial films)
+                cudaStreamSynchronize(ctx->stream);
+                std::lock_guard<std::mutex> lk(sv->mu);
+                for (auto &s : slices) {
+                    Request *q = sv->reqs[s.first];
+                    q->in_flight -= s.second;
+                    q->cancel = true;
+                    q->error = st;
+                }
+                if (t.ev) spare.push_back(t.ev);
+                for (auto &s : slices) {
+                    Request *q = sv->reqs[s.first];
+                    std::vector<uint64_t> keep;
+                    for (uint64_t id : sv->running)
+                        if (id != q->id) keep.push_back(id);
+                    sv->running.swap(keep);
+                    finish(*sv, q, GR_REQ_FAILED, st);
+                }
+            } else {
+                flight.push_back(std::move(t));
+            }
+        }
+    }
+    for (Tick &t : flight) cudaEventSynchronize(t.ev), spare.push_back(t.ev);
+    for (cudaEvent_t e : spare)
+        if (e) cudaEventDestroy(e);
+}
+
+ServeState *serve_state(gr_ctx *ctx) {
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!ctx->serve) {
+        ctx->serve = new ServeState();
+        ctx->serve->worker = std::thread(worker_main, ctx, ctx->serve);
+    }
+    return ctx->serve;
+}
+
+Request *find(ServeState *sv, uint64_t id) {
+    auto it = sv->reqs.find(id);
+    return it == sv->reqs.end() ? nullptr : it->second;
+}
+
+void fill_status(const Request *q, gr_request_status *out) {
+    out->state = q->state;
+    out->samples_done = q->done;
+    out->error = q->error;
+    out->queued_ms = q->state == GR_REQ_QUEUED ? ms_between(q->t_submit, Clock::now()) : ms_between(q->t_submit, q->t_admit);
+    const bool ended = q->state == GR_REQ_DONE || q->state == GR_REQ_CANCELLED || q->state == GR_REQ_FAILED;
+    out->latency_ms = ended ? ms_between(q->t_submit, q->t_done) : 0.0;
+}
+
+}  // namespace
+
+namespace grh {
+void serve_shutdown(gr_ctx *ctx) {
+    ServeState *sv = ctx->serve;
+    if (!sv) return;
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        sv->stop = true;
+        for (auto &kv : sv->reqs) kv.second->cancel = true;
+    }
+    sv->cv_work.notify_all();
+    if (sv->worker.joinable()) sv->worker.join();
+    for (auto &kv : sv->reqs) {
+        kv.second->film.release();
+        delete kv.second;
+    }
+    delete sv;
+    ctx->serve = nullptr;
+}
+}  // namespace grh
+
+extern "C" {
+
+gr_status gr_submit(gr_ctx *ctx, const gr_request *req, uint64_t *request_id) {
+    if (!ctx || !req || !request_id) return fail(GR_EINVAL, "NULL argument");
+    Request *q = new Request();
+    q->r = *req;
+    if (req->kind == GR_REQ_RENDER) {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        auto it = ctx->scenes.find(req->scene_id);
+        if (it == ctx->scenes.end()) {
+            delete q;
+            return fail(GR_ENOTFOUND, "unknown scene id %llu", (unsigned long long)req->scene_id);
+        }
+        q->film_bytes = (uint64_t)it->second->S.width * it->second->S.height * 3 * sizeof(float);
+    } else if (req->kind == GR_REQ_METRICS) {
+        if (!req->material || !req->poses || (req->n_planes && !req->planes) || req->n_planes > GR_MAX_PLANES) {
+            delete q;
+            return fail(GR_EINVAL, "metrics request needs material, poses and at most GR_MAX_PLANES planes");
+        }
+        q->poses.assign(req->poses, req->poses + req->n_poses);
+        q->planes.assign(req->planes, req->planes + req->n_planes);
+        q->material = *req->material;
+        q->metrics.resize(req->n_poses);
+        q->r.poses = nullptr;
+        q->r.planes = nullptr;
+        q->r.material = nullptr;
+    } else {
+        delete q;
+        return fail(GR_EINVAL, "unknown request kind %u", req->kind);
+    }
+    ServeState *sv = serve_state(ctx);
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        q->id = sv->next_id++;
+        q->t_submit = Clock::now();
+        if (q->r.kind == GR_REQ_METRICS && q->r.n_planes == 0) {
+            for (auto &m : q->metrics) m = gr_metrics_out{85.0f, 25.0f, 75.0f, 5.0f, 5.0f};  // color/metrics.rs:1090-1103
+            q->t_admit = q->t_submit;
+            finish(*sv, q, GR_REQ_DONE);
+        } else if (q->r.kind == GR_REQ_RENDER && q->r.spp == 0) {
+            q->t_admit = q->t_submit;
+            finish(*sv, q, GR_REQ_DONE);
+        } else {
+            sv->queue.push_back(q->id);
+        }
+        sv->reqs[q->id] = q;
+        *request_id = q->id;
+    }
+    sv->cv_work.notify_all();
+    return GR_OK;
+}
+
+gr_status gr_poll(gr_ctx *ctx, uint64_t id, gr_request_status *out) {
+    if (!ctx || !out) return fail(GR_EINVAL, "NULL argument");
+    if (!ctx->serve) return fail(GR_ENOTFOUND, "unknown request id %llu", (unsigned long long)id);
+    ServeState *sv = ctx->serve;
+    std::lock_guard<std::mutex> lk(sv->mu);
+    Request *q = find(sv, id);
+    if (!q) return fail(GR_ENOTFOUND, "unknown request id %llu", (unsigned long long)id);
+    fill_status(q, out);
+    return GR_OK;
+}
+
+gr_status gr_wait(gr_ctx *ctx, uint64_t id, uint32_t timeout_ms, gr_request_status *out) {
+    if (!ctx) return fail(GR_EINVAL, "ctx is NULL");
+    if (!ctx->serve) return fail(GR_ENOTFOUND, "unknown request id %llu", (unsigned long long)id);
+    ServeState *sv = ctx->serve;
+    std::unique_lock<std::mutex> lk(sv->mu);
+    Request *q = find(sv, id);
+    if (!q) return fail(GR_ENOTFOUND, "unknown request id %llu", (unsigned long long)id);
+    auto ended = [&] { return q->state == GR_REQ_DONE || q->state == GR_REQ_CANCELLED || q->state == GR_REQ_FAILED; };
+    if (!sv->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), ended)) {
+        if (out) fill_status(q, out);
+        return fail(GR_ETIMEOUT, "request %llu not finished after %u ms", (unsigned long long)id, timeout_ms);
+    }
+    if (out) fill_status(q, out);
+    return GR_OK;
+}
+
+gr_status gr_cancel(gr_ctx *ctx, uint64_t id) {
+    if (!ctx) return fail(GR_EINVAL, "ctx is NULL");
+    if (!ctx->serve) return fail(GR_ENOTFOUND, "unknown request id %llu", (unsigned long long)id);
+    ServeState *sv = ctx->serve;
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        Request *q = find(sv, id);
+        if (!q) return fail(GR_ENOTFOUND, "unknown request id %llu", (unsigned long long)id);
+        q->cancel = true;
+    }
+    sv->cv_work.notify_all();
+    return GR_OK;
+}
+
+gr_status gr_request_film(gr_ctx *ctx, uint64_t id, float *xyz_host) {
+    if (!ctx || !xyz_host) return fail(GR_EINVAL, "NULL argument");
+    if (!ctx->serve) return fail(GR_ENOTFOUND, "unknown request id %llu", (unsigned long long)id);
+    ServeState *sv = ctx->serve;
+    void *src = nullptr;
+    uint64_t bytes = 0;
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        Request *q = find(sv, id);
+        if (!q) return fail(GR_ENOTFOUND, "unknown request id %llu", (unsigned long long)id);
+        if (q->r.kind != GR_REQ_RENDER) return fail(GR_EINVAL, "request %llu is not a render", (unsigned long long)id);
+        if (q->state != GR_REQ_DONE && q->state != GR_REQ_CANCELLED)
+            return fail(GR_EINVAL, "request %llu has not finished", (unsigned long long)id);
+        src = q->film.ptr;
+        bytes = q->film_bytes;
+    }
+    if (!src) {
+        std::memset(xyz_host, 0, bytes);  // finished before admission: no samples
+        return GR_OK;
+    }
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    GR_CUDA(cudaSetDevice(ctx->device));
+    GR_CUDA(cudaMemcpyAsync(xyz_host, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    GR_CUDA(cudaStreamSynchronize(ctx->stream));
+    return GR_OK;
+}
+
+gr_status gr_request_metrics(gr_ctx *ctx, uint64_t id, gr_metrics_out *out) {
+    if (!ctx || !out) return fail(GR_EINVAL, "NULL argument");
+    if (!ctx->serve) return fail(GR_ENOTFOUND, "unknown request id %llu", (unsigned long long)id);
+    ServeState *sv = ctx->serve;
+    std::lock_guard<std::mutex> lk(sv->mu);
+    Request *q = find(sv, id);
+    if (!q) return fail(GR_ENOTFOUND, "unknown request id %llu", (unsigned long long)id);
+    if (q->r.kind != GR_REQ_METRICS || q->state != GR_REQ_DONE)
+        return fail(GR_EINVAL, "request %llu is not a finished metrics request", (unsigned long long)id);
+    for (size_t i = 0; i < q->metrics.size(); ++i) out[i] = q->metrics[i];
+    return GR_OK;
+}
+
+gr_status gr_request_release(gr_ctx *ctx, uint64_t id) {
+    if (!ctx) return fail(GR_EINVAL, "ctx is NULL");
+    if (!ctx->serve) return fail(GR_ENOTFOUND, "unknown request id %llu", (unsigned long long)id);
+    ServeState *sv = ctx->serve;
+    Request *q = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(sv->mu);
+        q = find(sv, id);
+        if (!q) return fail(GR_ENOTFOUND, "unknown request id %llu", (unsigned long long)id);
+        if (q->state == GR_REQ_QUEUED || q->state == GR_REQ_RUNNING)
+            return fail(GR_EBUSY, "request %llu is still active (cancel it first)", (unsigned long long)id);
+        if (q->film.ptr) sv->film_bytes -= q->film_bytes;
+        sv->reqs.erase(id);
+    }
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    q->film.release();
+    delete q;
+    return GR_OK;
+}
+
+}  // extern "C"

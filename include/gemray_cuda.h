@@ -358,6 +358,69 @@ typedef struct gr_batch_item {
  * context stream) and the call returns without waiting for it. */
 gr_status gr_render_batch(gr_ctx *ctx, const gr_batch_item *items, uint32_t n_items, uint32_t flags, void *stream);
 
+/* ---- serving: render requests over resident scenes ------------------------------ */
+
+/* Request kinds. */
+#define GR_REQ_RENDER 0u  /* ADD samples [sample_offset, sample_offset + spp) into a fresh film */
+#define GR_REQ_METRICS 1u /* a brilliance/fire/scintillation pose sweep (gr_optical_metrics) */
+
+/* One request, = RenderRequest{request_id, first_sample, samples}
+ * (crates/gemray-net/src/messages/render.rs:65-70) for a resident scene, or a metric
+ * sweep.  Pointers are copied at submit. */
+typedef struct gr_request {
+    uint32_t kind;
+    uint32_t slice_spp;      /* render: samples per scheduling slice, 0 = 16; progress, interleaving and
+                                cancellation happen between slices */
+    uint64_t scene_id;       /* render: resident scene */
+    uint32_t sample_offset;  /* render: first absolute sample */
+    uint32_t spp;            /* render: samples per pixel */
+    uint32_t flags;          /* metrics: GR_METRICS_* */
+    uint32_t n_planes;       /* metrics */
+    const gr_plane *planes;  /* metrics */
+    const gr_material *material; /* metrics */
+    const gr_pose *poses;    /* metrics */
+    uint32_t n_poses;        /* metrics */
+    uint32_t reserved;
+} gr_request;
+
+/* Request states. */
+#define GR_REQ_QUEUED 0u
+#define GR_REQ_RUNNING 1u
+#define GR_REQ_DONE 2u
+#define GR_REQ_CANCELLED 3u
+#define GR_REQ_FAILED 4u
+
+typedef struct gr_request_status {
+    uint32_t state;         /* GR_REQ_* */
+    uint32_t samples_done;  /* render: samples per pixel folded into the film so far */
+    gr_status error;        /* GR_REQ_FAILED: why (GR_EBUSY = can never fit the memory budget) */
+    uint32_t reserved;
+    double queued_ms;       /* submit -> admission */
+    double latency_ms;      /* submit -> finished (0 while active) */
+} gr_request_status;
+
+/* Queues a request and returns at once (no counterpart in the reference's GPU path,
+ * which renders one dispatch at a time; the worker's render loop is
+ * apps/gemray-worker/src/render_core/mod.rs).  A worker thread admits requests in
+ * arrival order while their film (W*H*3 f32) fits the context's serve budget next to
+ * the resident scenes and unreleased films, and advances every running render by one
+ * slice per tick in a shared batched launch.  A film is bit-identical to
+ * gr_render_resident called once per slice over the same sample range (each slice's
+ * per-pixel sum is added once, as a worker accumulating sub-batches does), alone or
+ * in any mix. */
+gr_status gr_submit(gr_ctx *ctx, const gr_request *request, uint64_t *request_id);
+gr_status gr_poll(gr_ctx *ctx, uint64_t request_id, gr_request_status *status);
+/* Blocks until the request has finished or timeout_ms passed (GR_ETIMEOUT). */
+gr_status gr_wait(gr_ctx *ctx, uint64_t request_id, uint32_t timeout_ms, gr_request_status *status);
+/* Stops a request between slices; its film keeps the slices already folded. */
+gr_status gr_cancel(gr_ctx *ctx, uint64_t request_id);
+/* Copies a finished (or cancelled) render's film, W*H*3 f32, to host memory. */
+gr_status gr_request_film(gr_ctx *ctx, uint64_t request_id, float *xyz_host);
+/* Copies a finished metrics request's n_poses results. */
+gr_status gr_request_metrics(gr_ctx *ctx, uint64_t request_id, gr_metrics_out *out);
+/* Frees a finished request and its film (GR_EBUSY while it is active). */
+gr_status gr_request_release(gr_ctx *ctx, uint64_t request_id);
+
 /* gr_render_resident that allocates no device memory.  No counterpart in the
  * reference (its frame renderer grows its buffers on demand, renderer/gpu/frame.rs:
  * 868-879); it exists for callers that must not allocate inside a render call.
@@ -446,6 +509,8 @@ static_assert(offsetof(gr_material, beta_ray_bands) == 328, "layout");
 static_assert(offsetof(gr_material, absorption_path_scale) == 424, "layout");
 static_assert(sizeof(gr_camera) == 52, "gr_camera");
 static_assert(sizeof(gr_metrics_out) == 20, "gr_metrics_out = GemOpticalMetrics");
+static_assert(sizeof(gr_request) == 64, "gr_request");
+static_assert(sizeof(gr_request_status) == 32, "gr_request_status");
 #endif
 
 #endif /* GEMRAY_CUDA_H */

@@ -50,6 +50,9 @@ WORKLOADS = {
     "c3": dict(width=1024, height=1024, spp=1024, max_bounces=64, env="studio", stone="em49"),
     # c2's scene at 480x270, 64 spp: the small case the ncu captures run on
     "c2s": dict(width=480, height=270, spp=64, max_bounces=32, env="latlong", stone="rb57"),
+    # batched and served forms (run_batch / run_serve; their scenes come from workloads.py)
+    "c4": dict(width=0, height=0, spp=0, max_bounces=32, env="latlong", stone="random"),
+    "c5": dict(width=0, height=0, spp=0, max_bounces=32, env="latlong", stone="random"),
 }
 
 
@@ -328,6 +331,15 @@ def run_engine(args):
     h2d = n_px * 12 + sc.planes.nbytes + C.sizeof(abi.gr_material) + map_bytes
     d2h = n_px * 12
 
+    # C2's metric output: brilliance / fire / scintillation over 16 tilts in [-20, +20] deg
+    from gemray_studio_b200 import metrics as M
+    from gemray_studio_b200 import workloads as W
+    poses = W.c2_tilt_poses(16)
+    M.evaluate_poses(r, sc.planes, sc.material, poses)  # warm
+    t1 = time.perf_counter()
+    mvals = M.evaluate_poses(r, sc.planes, sc.material, poses)
+    metrics_ms = (time.perf_counter() - t1) * 1e3
+
     trace_ms_per_launch = tr.value / max(1, ntr.value)
     frames = args.steps
     flops_per_frame = model.flops_per_sample * samples_per_step
@@ -352,6 +364,10 @@ def run_engine(args):
                          "kernel_ms_per_step": tr.value / frames, "fold_ms_per_step": fo.value / frames,
                          "launches_per_step": (ntr.value + nfo.value) / frames},
             "events_per_sample": {k: v / max(1, tallies["paths"]) for k, v in tallies.items() if k != "paths"},
+            "metrics_16_tilts": {"ms": metrics_ms, "how": "gr_optical_metrics, one device batch, host wall clock",
+                                 "brilliance_pct": [round(float(v), 3) for v in mvals[:, 0]],
+                                 "fire_index": [round(float(v), 3) for v in mvals[:, 1]],
+                                 "scintillation_pct": [round(float(v), 3) for v in mvals[:, 2]]},
             "gpu_launches": int(ntr.value + nfo.value),  # this library's trace + fold launches
             "clocks": clk,
             "device": r.adapter_label(),
@@ -359,10 +375,200 @@ def run_engine(args):
         if world == 1 and not args.no_cpu_baseline:
             out["cpu_baseline"] = cpu_baseline(sc, w)
         print(json.dumps(out), flush=True)
+    del film, flush  # torch tensors used on the context stream go before the context
+    torch.cuda.synchronize()
     r.close()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def _flush_l2(flush, i, stream):
+    import torch
+    with torch.cuda.stream(stream):
+        flush.fill_(i & 0xFF)
+
+
+def run_batch(args):
+    """C4: 64 random stones (17-145 planes, six materials, Kahan films) rendered by
+    one batched call per step (gr_render_batch, CUDA-graph replay) against the same
+    renders issued one scene at a time with gr_render_resident (the plain kernel)."""
+    import torch
+
+    from gemray_studio_b200 import GpuFrameRenderer, abi, build
+    from gemray_studio_b200 import workloads as W
+    build.build()
+    s = args.scale
+    stones = W.random_stones(64, seed=0, side=(max(16, int(128 * s)), max(16, int(1024 * s))), spp=(32, 512))
+    r = GpuFrameRenderer()
+    lib, ctx = r.lib, r.ctx
+    stream_ptr = lib.gr_stream(ctx)
+    stream = torch.cuda.ExternalStream(stream_ptr)
+    ids = []
+    for st in stones:
+        sid = C.c_uint64()
+        assert lib.gr_scene_upload(ctx, C.byref(st.scene.c_scene()), C.byref(sid)) == abi.GR_OK
+        ids.append(sid.value)
+    with torch.cuda.stream(stream):
+        films = [torch.zeros((st.scene.width * st.scene.height, 3), dtype=torch.float32, device="cuda") for st in stones]
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    tuples = sum(st.scene.width * st.scene.height * st.spp for st in stones)
+    stride = max(st.spp for st in stones)
+
+    def serial(i):
+        for k, st in enumerate(stones):
+            assert lib.gr_render_resident(ctx, ids[k], i * stride, st.spp, C.c_void_p(films[k].data_ptr()),
+                                          None) == abi.GR_OK
+
+    def batched(i):
+        items = (abi.gr_batch_item * len(stones))(*[abi.gr_batch_item(ids[k], films[k].data_ptr(), i * stride, st.spp)
+                                                    for k, st in enumerate(stones)])
+        assert lib.gr_render_batch(ctx, items, len(stones), abi.GR_BATCH_GRAPH, None) == abi.GR_OK
+
+    def timed(fn, base):
+        for i in range(args.warmup):
+            fn(base + i)
+        torch.cuda.synchronize()
+        evs = []
+        for i in range(args.steps):
+            _flush_l2(flush, i, stream)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn(base + args.warmup + i)
+            b.record(stream)
+            evs.append((a, b))
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(b) for a, b in evs) / args.steps
+
+    with ClockSampler(0) as clocks:
+        ms_serial = timed(serial, 0)
+        ms_batch = timed(batched, 1000)
+    # e2e: films from pinned host memory in, batched render, films back out
+    host = [torch.zeros(f.shape, dtype=torch.float32).pin_memory() for f in films]
+    e_evs = []
+    for i in range(args.steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        with torch.cuda.stream(stream):
+            for h, f in zip(host, films):
+                f.copy_(h, non_blocking=True)
+        batched(2000 + i)
+        with torch.cuda.stream(stream):
+            for h, f in zip(host, films):
+                h.copy_(f, non_blocking=True)
+        b.record(stream)
+        e_evs.append((a, b))
+    torch.cuda.synchronize()
+    ms_e2e = sum(a.elapsed_time(b) for a, b in e_evs) / args.steps
+    film_bytes = sum(f.numel() * 4 for f in films)
+    planes = [st.n_planes for st in stones]
+    print(json.dumps({
+        "metric": "path-samples/s", "value": tuples / (ms_batch * 1e-3), "unit": "path-samples/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_batch, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"c4: 64 random convex stones ({min(planes)}-{max(planes)} planes), six materials "
+                               f"(n_d 1.47-2.42), films {stones[0].scene.width}..{max(st.scene.width for st in stones)}"
+                               f" px square, spp 32-512, Kahan films, one gr_render_batch call per step (CUDA graph)",
+                   "path_samples_per_step": tuples, "scale": s, "l2": "flushed between steps (256 MiB device write)"},
+        "serial_plain": {"value": tuples / (ms_serial * 1e-3), "ms_per_step": ms_serial,
+                         "how": "the same 64 renders, one gr_render_resident call (plain kernel) per stone"},
+        "batched_over_serial": ms_serial / ms_batch,
+        "e2e": {"value": tuples / (ms_e2e * 1e-3), "unit": "path-samples/s", "h2d_bytes_per_step": film_bytes,
+                "d2h_bytes_per_step": film_bytes},
+        "clocks": clocks.summary(), "device": r.adapter_label(),
+    }), flush=True)
+    del host, films, flush  # torch tensors used on the context stream go before the context
+    torch.cuda.synchronize()
+    r.close()
+
+
+def run_serve(args):
+    """C5: Poisson render requests (plus 10% metric-only 64-tilt sweeps) over random
+    stones through the request loop (gr_submit / gr_wait), against a FIFO server that
+    renders each request alone with the plain kernel (its measured service times)."""
+    import torch
+
+    from gemray_studio_b200 import abi, build, metrics as M
+    from gemray_studio_b200 import workloads as W
+    from gemray_studio_b200.serve import RenderServer
+    build.build()
+    stones = W.random_stones(32, seed=0, side=(args.serve_side[0], args.serve_side[1]), spp=(16, 128))
+    reqs = W.request_stream(stones, args.rate, args.duration, seed=1, spp=(args.serve_spp[0], args.serve_spp[1]))
+    srv = RenderServer()
+    ids = [srv.upload(st.scene) for st in stones]
+    w = srv.submit_render(ids[0], 0, 16)  # warm the worker and the kernels
+    srv.wait(w)
+    srv.release(w)
+    rids = []
+    t0 = time.perf_counter()
+    with ClockSampler(0) as clocks:
+        for q in reqs:
+            dt = t0 + q.arrival_s - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            st = stones[q.stone]
+            if q.is_metrics:
+                rids.append(srv.submit_metrics(st.scene.planes, st.scene.material, q.poses))
+            else:
+                rids.append(srv.submit_render(ids[q.stone], 0, q.spp))  # slices sized per tick
+        stats = [srv.wait(r) for r in rids]
+    t_end = time.perf_counter()
+    for r in rids:
+        srv.release(r)
+    render_tuples = sum(stones[q.stone].scene.width * stones[q.stone].scene.height * q.spp for q in reqs
+                        if not q.is_metrics)
+    lat = np.array([s.latency_ms for s in stats])
+    # serial plain-kernel server: each request alone, in arrival order, one at a time
+    lib, ctx = srv.lib, srv.ctx
+    stream = torch.cuda.ExternalStream(lib.gr_stream(ctx))
+    films = {}
+    service = []
+    for q in reqs:
+        st = stones[q.stone]
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if q.is_metrics:
+            t1 = time.perf_counter()
+            M.evaluate_poses(srv.r, st.scene.planes, st.scene.material, q.poses)
+            service.append((time.perf_counter() - t1) * 1e3)
+            continue
+        f = films.get(q.stone)
+        if f is None:
+            f = films[q.stone] = torch.zeros((st.scene.width * st.scene.height, 3), dtype=torch.float32, device="cuda")
+            torch.cuda.synchronize()
+        a.record(stream)
+        assert lib.gr_render_resident(ctx, ids[q.stone], 0, q.spp, C.c_void_p(f.data_ptr()), None) == abi.GR_OK
+        b.record(stream)
+        b.synchronize()
+        service.append(a.elapsed_time(b))
+    finish, lat_ser = 0.0, []
+    for q, sv_ms in zip(reqs, service):
+        start = max(q.arrival_s * 1e3, finish)
+        finish = start + sv_ms
+        lat_ser.append(finish - q.arrival_s * 1e3)
+    lat_ser = np.array(lat_ser)
+    ser_span = max(finish, reqs[-1].arrival_s * 1e3) if reqs else 1.0
+    print(json.dumps({
+        "metric": "path-samples/s", "value": render_tuples / (t_end - t0), "unit": "path-samples/s", "n_gpus": 1,
+        "steps": 1, "warmup": 1, "ms_per_step": (t_end - t0) * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"c5: Poisson arrivals {args.rate}/s for {args.duration} s ({len(reqs)} requests, "
+                               f"{sum(q.is_metrics for q in reqs)} metric-only 64-tilt sweeps) over 32 random stones, "
+                               f"films {args.serve_side[0]}-{args.serve_side[1]} px square, spp {args.serve_spp[0]}-"
+                               f"{args.serve_spp[1]}, ticks of ~16.8 M path-samples filled in arrival order",
+                   "render_path_samples": render_tuples},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                       "max": float(lat.max())},
+        "serial_plain": {"value": render_tuples / (ser_span * 1e-3), "p50": float(np.percentile(lat_ser, 50)),
+                         "p99": float(np.percentile(lat_ser, 99)),
+                         "how": "FIFO single server: each request rendered alone with gr_render_resident (device-"
+                                "timed service times), queued in arrival order"},
+        "wall_clock": "arrivals, latencies and throughput are host wall-clock (a request stream has no device-side "
+                      "clock)",
+        "clocks": clocks.summary(), "device": srv.r.adapter_label(),
+    }), flush=True)
+    del films
+    torch.cuda.synchronize()
+    srv.close()
 
 
 def main():
@@ -373,9 +579,18 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--scale", type=float, default=1.0, help="c4: film side scale")
+    ap.add_argument("--rate", type=float, default=40.0, help="c5: arrivals per second")
+    ap.add_argument("--duration", type=float, default=10.0, help="c5: seconds of arrivals")
+    ap.add_argument("--serve-side", type=int, nargs=2, default=(128, 384), help="c5: film side range")
+    ap.add_argument("--serve-spp", type=int, nargs=2, default=(16, 128), help="c5: spp range")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "c4":
+        run_batch(args)
+    elif args.workload == "c5":
+        run_serve(args)
     else:
         run_engine(args)
 

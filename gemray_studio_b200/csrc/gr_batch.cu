@@ -43,7 +43,7 @@ struct Plan {
 // Cuts the items into launches of at most `budget` tuples (a pixel whose spp alone
 // exceeds the budget gets a launch of its own).  xyz pointers are offsets from 0
 // until the scratch is placed.
-gr_status make_plan(gr_ctx *ctx, const gr_batch_item *items, uint32_t n_items, uint64_t budget, Plan &P) {
+gr_status make_plan(gr_ctx *ctx, const grh::BatchItem *items, uint32_t n_items, uint64_t budget, Plan &P) {
     std::unordered_map<uint64_t, uint32_t> slot_of;
     Launch cur{0, 0, 0, 0, 0};
     uint64_t used = 0;
@@ -54,7 +54,7 @@ gr_status make_plan(gr_ctx *ctx, const gr_batch_item *items, uint32_t n_items, u
         used = 0;
     };
     for (uint32_t i = 0; i < n_items; ++i) {
-        const gr_batch_item &it = items[i];
+        const gr_batch_item &it = items[i].it;
         auto f = ctx->scenes.find(it.scene_id);
         if (f == ctx->scenes.end()) return fail(GR_ENOTFOUND, "item %u: unknown scene id %llu", i, (unsigned long long)it.scene_id);
         ResidentScene *rs = f->second;
@@ -98,6 +98,9 @@ gr_status make_plan(gr_ctx *ctx, const gr_batch_item *items, uint32_t n_items, u
             g.warp_begin = cur.warps;
             g.scene = slot;
             g.kahan = (rs->S.flags & GR_FLAG_KAHAN_FILM) ? 1u : 0u;
+            g.cont = items[i].cont;
+            g.comp = items[i].comp;
+            if (g.cont && g.kahan && !g.comp) return fail(GR_EINVAL, "item %u: continue mode with Kahan needs comp", i);
             P.segs.push_back(g);
             cur.seg_count++;
             cur.blocks += (g.R.n_tuples + grd::TRACE_THREADS - 1) / grd::TRACE_THREADS;
@@ -132,6 +135,7 @@ std::vector<uint64_t> graph_key(const Plan &P, const void *tables, const void *x
         k.push_back((uint64_t)(uintptr_t)g.film);
         k.push_back(((uint64_t)g.R.first_pixel << 32) | g.R.n_pixels);
         k.push_back(((uint64_t)g.R.spp << 32) | g.scene);
+        k.push_back((uint64_t)(uintptr_t)g.comp ^ g.cont);
     }
     for (const Launch &L : P.launches) k.push_back(((uint64_t)L.seg_count << 32) | L.max_planes);
     return k;
@@ -141,7 +145,7 @@ std::vector<uint64_t> graph_key(const Plan &P, const void *tables, const void *x
 
 namespace grh {
 
-gr_status batch_enqueue(gr_ctx *ctx, const gr_batch_item *items, uint32_t n_items, uint32_t flags, cudaStream_t stream) {
+gr_status batch_enqueue(gr_ctx *ctx, const BatchItem *items, uint32_t n_items, uint32_t flags, cudaStream_t stream) {
     uint64_t budget = ctx->chunk_budget / (3 * sizeof(float));
     if (budget > 0xFFFFFFFFull) budget = 0xFFFFFFFFull;  // tuple ids are u32 within a segment
     Plan P;
@@ -160,9 +164,26 @@ gr_status batch_enqueue(gr_ctx *ctx, const gr_batch_item *items, uint32_t n_item
     for (grd::BatchSegment &g : P.segs) g.xyz = xyz + ((uintptr_t)g.xyz) / sizeof(float);
     grd::SceneSlot *d_slots = (grd::SceneSlot *)ctx->batch_tables.ptr;
     grd::BatchSegment *d_segs = (grd::BatchSegment *)((char *)ctx->batch_tables.ptr + slot_bytes);
-    // Pageable-source copies: the host vectors may be freed once these calls return.
-    GR_CUDA(cudaMemcpyAsync(d_slots, P.slots.data(), P.slots.size() * sizeof(grd::SceneSlot), cudaMemcpyHostToDevice, s));
-    GR_CUDA(cudaMemcpyAsync(d_segs, P.segs.data(), seg_bytes, cudaMemcpyHostToDevice, s));
+    // Stage both tables in the next pinned ring slot (once its previous upload has
+    // been consumed) and upload them in one copy.  The device tables are shared by
+    // every batch: stream order puts this copy after the previous batch's kernels.
+    const int k = ctx->stage_next;
+    ctx->stage_next = (k + 1) % gr_ctx::kStageSlots;
+    if (ctx->stage_ev[k]) GR_CUDA(cudaEventSynchronize(ctx->stage_ev[k]));
+    else GR_CUDA(cudaEventCreateWithFlags(&ctx->stage_ev[k], cudaEventDisableTiming));
+    if (ctx->stage_cap[k] < slot_bytes + seg_bytes) {
+        if (ctx->stage_host[k]) cudaFreeHost(ctx->stage_host[k]);
+        ctx->stage_host[k] = nullptr;
+        ctx->stage_cap[k] = 0;
+        const size_t want = std::max<size_t>(slot_bytes + seg_bytes, 64 << 10);
+        GR_CUDA(cudaHostAlloc(&ctx->stage_host[k], want, cudaHostAllocDefault));
+        ctx->stage_cap[k] = want;
+    }
+    char *h = (char *)ctx->stage_host[k];
+    std::memcpy(h, P.slots.data(), P.slots.size() * sizeof(grd::SceneSlot));
+    std::memcpy(h + slot_bytes, P.segs.data(), seg_bytes);
+    GR_CUDA(cudaMemcpyAsync(ctx->batch_tables.ptr, h, slot_bytes + seg_bytes, cudaMemcpyHostToDevice, s));
+    GR_CUDA(cudaEventRecord(ctx->stage_ev[k], s));
 
     if (!(flags & GR_BATCH_GRAPH)) return launch_plan(P, d_slots, d_segs, s);
 
@@ -199,7 +220,9 @@ extern "C" gr_status gr_render_batch(gr_ctx *ctx, const gr_batch_item *items, ui
                                      void *stream) {
     if (!ctx) return fail(GR_EINVAL, "ctx is NULL");
     if (n_items && !items) return fail(GR_EINVAL, "items is NULL");
+    std::vector<grh::BatchItem> bi(n_items);
+    for (uint32_t i = 0; i < n_items; ++i) bi[i] = grh::BatchItem{items[i], nullptr, 0u};
     std::lock_guard<std::mutex> lk(ctx->mu);
     GR_CUDA(cudaSetDevice(ctx->device));
-    return grh::batch_enqueue(ctx, items, n_items, flags, (cudaStream_t)stream);
+    return grh::batch_enqueue(ctx, bi.data(), n_items, flags, (cudaStream_t)stream);
 }

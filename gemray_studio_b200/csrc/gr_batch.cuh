@@ -20,11 +20,14 @@ struct SceneSlot {
 struct BatchSegment {
     LaunchRange R;         // pixels / samples of this segment
     float *xyz;            // its per-tuple XYZ (3 f32 per tuple)
-    float *film;           // the scene's film (W*H*3 f32), ADDed into by the fold
+    float *film;           // the scene's film (W*H*3 f32), folded into (fold_pixel)
+    float *comp;           // continue mode with Kahan: the film's compensation terms
     uint64_t block_begin;  // first trace block of the segment
     uint64_t warp_begin;   // first fold warp of the segment
     uint32_t scene;        // index into the SceneSlot table
     uint32_t kahan;
+    uint32_t cont;         // fold_pixel continue mode
+    uint32_t pad;
 };
 
 template <bool BY_WARP>
@@ -77,7 +80,7 @@ __global__ void k_fold_batch(const BatchSegment *__restrict__ segs, uint32_t n_s
     const BatchSegment &G = segs[find_segment<true>(segs, n_segs, warp)];
     const uint64_t px = warp - G.warp_begin;
     if (px >= G.R.n_pixels) return;  // the grid's last warps past the final segment
-    fold_pixel(G.xyz, px, G.R.spp, G.R.first_pixel + (uint32_t)px, G.film, G.kahan);
+    fold_pixel(G.xyz, px, G.R.spp, G.R.first_pixel + (uint32_t)px, G.film, G.kahan, G.cont, G.comp);
 }
 
 }  // namespace grd

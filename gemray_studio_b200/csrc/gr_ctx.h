@@ -62,8 +62,15 @@ struct gr_ctx {
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> trace_ev, fold_ev;
     size_t trace_used = 0, fold_used = 0;
     uint64_t trace_launches = 0, fold_launches = 0;
-    // gr_render_batch: scene-slot + segment tables, captured launch sequences
+    // gr_render_batch: scene-slot + segment tables, captured launch sequences, and a
+    // ring of pinned host staging buffers for the table uploads (a pageable source
+    // would make each upload wait for the previous batch to reach its copy)
     grh::DeviceBuffer batch_tables;
+    static constexpr int kStageSlots = 4;
+    void *stage_host[kStageSlots] = {};
+    size_t stage_cap[kStageSlots] = {};
+    cudaEvent_t stage_ev[kStageSlots] = {};
+    int stage_next = 0;
     std::vector<BatchGraph> batch_graphs;
     // gr_submit / gr_poll request loop (created by the first submit)
     ServeState *serve = nullptr;
@@ -76,8 +83,16 @@ struct gr_ctx {
 grd::SceneBuffers resident_buffers(ResidentScene *rs);
 
 namespace grh {
+// One batch item plus its fold mode: cont = 0 adds each call's per-pixel sum once
+// (gr_render_batch); cont = 1 continues the film's running sum (serving slices; comp
+// holds the Kahan compensation for scenes with GR_FLAG_KAHAN_FILM).
+struct BatchItem {
+    gr_batch_item it;
+    float *comp;
+    uint32_t cont;
+};
 // gr_render_batch's body; the caller holds ctx->mu and has made ctx->device current.
-gr_status batch_enqueue(gr_ctx *ctx, const gr_batch_item *items, uint32_t n_items, uint32_t flags, cudaStream_t stream);
+gr_status batch_enqueue(gr_ctx *ctx, const BatchItem *items, uint32_t n_items, uint32_t flags, cudaStream_t stream);
 }  // namespace grh
 
 namespace grh {

@@ -577,6 +577,10 @@ gr_status gr_destroy(gr_ctx *ctx) {
         ctx->counter.release();
         ctx->rgba.release();
         ctx->metrics.release();
+        for (int k = 0; k < gr_ctx::kStageSlots; ++k) {
+            if (ctx->stage_host[k]) cudaFreeHost(ctx->stage_host[k]);
+            if (ctx->stage_ev[k]) cudaEventDestroy(ctx->stage_ev[k]);
+        }
         for (BatchGraph &g : ctx->batch_graphs) cudaGraphExecDestroy(g.exec);
         ctx->batch_graphs.clear();
         ctx->batch_tables.release();

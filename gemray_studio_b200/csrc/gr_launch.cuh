@@ -54,13 +54,30 @@ __device__ __forceinline__ void tuple_coords(const LaunchRange &R, uint64_t t, u
 #define GR_TRACE_MIN_BLOCKS 9
 #endif
 
-// One warp folds pixel `px` (local to its xyz block) and adds the sum into film.
+// One warp folds pixel `px` (local to its xyz block) into film pixel `film_pixel`.
+// Add mode (cont == 0): the samples are summed in order from zero and the sum is
+// added to the film once -- the reference's per-call semantics.  Continue mode
+// (cont != 0): the sum starts from the film's current value (and, with Kahan, from
+// the compensation kept in comp) and is written back, so successive slices of one
+// sample range on a zero film form exactly one sequential sum, whatever the slicing.
 __device__ __forceinline__ void fold_pixel(const float *__restrict__ xyz, uint64_t px, uint32_t spp, uint32_t film_pixel,
-                                           float *__restrict__ film, uint32_t kahan) {
+                                           float *__restrict__ film, uint32_t kahan, uint32_t cont = 0,
+                                           float *__restrict__ comp = nullptr) {
     const uint32_t lane = threadIdx.x & 31u;
     const float *src = xyz + (size_t)px * spp * 3;
+    const size_t p = (size_t)film_pixel * 3;
     float sx = 0.0f, sy = 0.0f, sz = 0.0f;
     float cx = 0.0f, cy = 0.0f, cz = 0.0f;
+    if (cont) {
+        sx = film[p + 0];
+        sy = film[p + 1];
+        sz = film[p + 2];
+        if (kahan) {
+            cx = comp[p + 0];
+            cy = comp[p + 1];
+            cz = comp[p + 2];
+        }
+    }
     for (uint32_t s0 = 0; s0 < spp; s0 += 32) {
         uint32_t s = s0 + lane;
         float x = 0.f, y = 0.f, z = 0.f;
@@ -86,10 +103,20 @@ __device__ __forceinline__ void fold_pixel(const float *__restrict__ xyz, uint64
         }
     }
     if (lane == 0) {
-        size_t p = (size_t)film_pixel * 3;
-        film[p + 0] = film[p + 0] + sx;
-        film[p + 1] = film[p + 1] + sy;
-        film[p + 2] = film[p + 2] + sz;
+        if (cont) {
+            film[p + 0] = sx;
+            film[p + 1] = sy;
+            film[p + 2] = sz;
+            if (kahan) {
+                comp[p + 0] = cx;
+                comp[p + 1] = cy;
+                comp[p + 2] = cz;
+            }
+        } else {
+            film[p + 0] = film[p + 0] + sx;
+            film[p + 1] = film[p + 1] + sy;
+            film[p + 2] = film[p + 2] + sz;
+        }
     }
 }
 

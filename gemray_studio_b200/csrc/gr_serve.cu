@@ -6,18 +6,21 @@
 //   * admission -- queued requests are admitted in arrival order while their film
 //     fits the context's device-memory budget next to the resident scenes and the
 //     films of running requests; a film is allocated and zeroed on admission;
-//   * ticks -- each tick every running render contributes its next slice
-//     (slice_spp samples of every pixel) to ONE batched launch (gr_batch.cu), so
-//     requests that arrive while others run share the device with them at the next
-//     tick; up to two ticks are in flight, so the host plans tick k+1 while tick k runs;
+//   * ticks -- each tick is ONE batched launch (gr_batch.cu) filled from the running
+//     renders in arrival order, each contributing all of its remaining samples until
+//     the tick's tuple budget is spent, so small requests finish in a single tick and
+//     share it with others; up to two ticks are in flight, so the host plans tick k+1
+//     while tick k runs;
 //   * retirement -- when a tick's event completes its slices count as folded;
 //     a render is DONE when all its samples are; cancellation takes effect between
 //     slices;
 //   * metric requests (pose sweeps) run between ticks on the same stream.
-// A request's film is what gr_render_resident adds when called once per slice over
-// the same sample range (each slice's per-pixel sum is folded in sample order and
-// added once, like a worker accumulating sub-batches), so a result depends on its own
-// slice size but is bit-identical alone and in any mix.
+// Slices fold in continue mode (fold_pixel): each slice carries the pixel's running
+// sum on from the film (and the Kahan compensation from a side buffer), and a request
+// starts on a zero film, so its film is one sequential per-pixel sum over all of its
+// samples -- bit-identical to one gr_render_resident call over the same sample range
+// on a zero film, whatever the slicing and whatever else is running.  Slices are
+// therefore sized freely by the scheduler.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -37,6 +40,25 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
+// A request's film (or Kahan compensation) from the stream-ordered allocator: taking
+// and returning it never synchronises the device, so admissions and releases do not
+// stall the ticks in flight.
+struct StreamBuffer {
+    void *ptr = nullptr;
+    cudaError_t alloc(size_t bytes, cudaStream_t s) {
+        cudaError_t e = cudaMallocAsync(&ptr, bytes, s);
+        if (e != cudaSuccess) {
+            ptr = nullptr;
+            return e;
+        }
+        return cudaMemsetAsync(ptr, 0, bytes, s);
+    }
+    void release(cudaStream_t s) {
+        if (ptr) cudaFreeAsync(ptr, s);
+        ptr = nullptr;
+    }
+};
+
 struct Request {
     uint64_t id = 0;
     gr_request r{};
@@ -46,12 +68,18 @@ struct Request {
     std::vector<gr_metrics_out> metrics; // metrics results
     uint32_t state = GR_REQ_QUEUED;
     gr_status error = GR_OK;
-    uint64_t film_bytes = 0;
-    grh::DeviceBuffer film;
+    uint64_t film_bytes = 0;     // film (+ Kahan compensation) bytes held on the device
+    uint64_t n_px = 0;
+    bool kahan = false;
+    StreamBuffer film, comp;
     uint32_t issued = 0, done = 0, in_flight = 0;  // samples per pixel
     bool cancel = false;
     Clock::time_point t_submit, t_admit, t_done;
 };
+
+// Path-samples one tick carries: ~20-60 ms of transport on B200, the latency quantum
+// of the request loop (a new arrival joins the tick after the ones in flight).
+constexpr uint64_t kTickTuples = 16ull << 20;
 
 struct Tick {
     cudaEvent_t ev = nullptr;
@@ -66,6 +94,8 @@ double ms_between(Clock::time_point a, Clock::time_point b) {
 
 struct ServeState {
     std::mutex mu;
+    cudaStream_t metrics_stream = nullptr;  // metric sweeps run beside the ticks
+    grh::DeviceBuffer metrics_scratch;
     std::condition_variable cv_work, cv_done;
     std::unordered_map<uint64_t, Request *> reqs;
     std::deque<uint64_t> queue;   // admission order
@@ -108,10 +138,11 @@ void admit(gr_ctx *ctx, ServeState &sv, uint64_t resident_bytes) {
             continue;
         }
         if (resident_bytes + sv.film_bytes + q->film_bytes > ctx->serve_budget) break;  // wait for releases
-        if (q->film.reserve(q->film_bytes) != GR_OK ||
-            cudaMemsetAsync(q->film.ptr, 0, q->film_bytes, ctx->stream) != cudaSuccess) {
+        const size_t fb = (size_t)q->n_px * 3 * sizeof(float);
+        if (q->film.alloc(fb, ctx->stream) != cudaSuccess || (q->kahan && q->comp.alloc(fb, ctx->stream) != cudaSuccess)) {
             sv.queue.pop_front();
-            q->film.release();
+            q->film.release(ctx->stream);
+            q->comp.release(ctx->stream);
             finish(sv, q, GR_REQ_FAILED, GR_ENOMEM);
             continue;
         }
@@ -147,7 +178,7 @@ void worker_main(gr_ctx *ctx, ServeState *sv) {
             retire(flight.front());
             flight.pop_front();
         }
-        std::vector<gr_batch_item> items;
+        std::vector<grh::BatchItem> items;
         std::vector<std::pair<uint64_t, uint32_t>> slices;
         std::vector<Request *> metric_jobs;
         {
@@ -170,7 +201,17 @@ void worker_main(gr_ctx *ctx, ServeState *sv) {
             // 3. admission (resident_bytes is read without ctx->mu: a stale value only
             //    delays or advances an admission by one tick)
             admit(ctx, *sv, ctx->resident_bytes);
-            // 4. this tick's slices
+            // 4. this tick's slices: running requests in arrival order, each taking all of
+            //    its remaining samples until the tick's tuple budget is spent (no single
+            //    request more than half of it while others wait); a fixed slice_spp caps
+            //    a request's share per tick instead
+            uint32_t n_active = 0;
+            for (uint64_t id : sv->running) {
+                Request *q = sv->reqs[id];
+                n_active += q->r.kind == GR_REQ_RENDER && !q->cancel && q->issued < q->r.spp;
+            }
+            const uint64_t cap = n_active > 1 ? kTickTuples / 2 : kTickTuples;
+            uint64_t budget = kTickTuples;
             for (uint64_t id : sv->running) {
                 Request *q = sv->reqs[id];
                 if (q->r.kind == GR_REQ_METRICS) {
@@ -178,8 +219,18 @@ void worker_main(gr_ctx *ctx, ServeState *sv) {
                     continue;
                 }
                 if (q->cancel || q->issued >= q->r.spp) continue;
-                const uint32_t slice = std::min(q->r.slice_spp ? q->r.slice_spp : 16u, q->r.spp - q->issued);
-                items.push_back(gr_batch_item{q->r.scene_id, (float *)q->film.ptr, q->r.sample_offset + q->issued, slice});
+                const uint64_t px = std::max<uint64_t>(1, q->n_px);
+                uint64_t want = std::min(budget, cap) / px;
+                if (want == 0) {
+                    if (!items.empty()) continue;  // the next tick
+                    want = 1;                      // a lone pixel-heavy request still advances
+                }
+                if (q->r.slice_spp) want = std::min<uint64_t>(want, q->r.slice_spp);
+                const uint32_t slice = (uint32_t)std::min<uint64_t>(want, q->r.spp - q->issued);
+                budget -= std::min<uint64_t>(budget, (uint64_t)slice * px);
+                items.push_back(grh::BatchItem{
+                    gr_batch_item{q->r.scene_id, (float *)q->film.ptr, q->r.sample_offset + q->issued, slice},
+                    (float *)q->comp.ptr, 1u});
                 slices.emplace_back(id, slice);
                 q->issued += slice;
                 q->in_flight += slice;
@@ -190,20 +241,19 @@ void worker_main(gr_ctx *ctx, ServeState *sv) {
                     sv->cv_work.wait_for(lk, std::chrono::milliseconds(20));
                     continue;
                 }
-                lk.unlock();
-                cudaEventSynchronize(flight.front().ev);  // nothing new to issue: wait for the oldest tick
+                // nothing new to issue: sleep until the oldest tick ends or a request
+                // arrives (polling the event keeps arrivals from waiting on the tick)
+                if (cudaEventQuery(flight.front().ev) == cudaErrorNotReady)
+                    sv->cv_work.wait_for(lk, std::chrono::microseconds(200));
                 continue;
             }
         }
         // 5. metric sweeps between ticks
         for (Request *q : metric_jobs) {
-            gr_status st;
-            {
-                std::lock_guard<std::mutex> lk(ctx->mu);
-                st = grh::metrics_device(q->planes.data(), (uint32_t)q->planes.size(), &q->material, q->poses.data(),
-                                         (uint32_t)q->poses.size(), q->metrics.data(), q->r.flags, ctx->stream,
-                                         ctx->metrics);
-            }
+            // its own stream and scratch: no context lock, and the ticks in flight keep running
+            const gr_status st = grh::metrics_device(q->planes.data(), (uint32_t)q->planes.size(), &q->material,
+                                                     q->poses.data(), (uint32_t)q->poses.size(), q->metrics.data(),
+                                                     q->r.flags, sv->metrics_stream, sv->metrics_scratch);
             std::lock_guard<std::mutex> lk(sv->mu);
             std::vector<uint64_t> keep;
             for (uint64_t id : sv->running)
@@ -261,6 +311,8 @@ ServeState *serve_state(gr_ctx *ctx) {
     std::lock_guard<std::mutex> lk(ctx->mu);
     if (!ctx->serve) {
         ctx->serve = new ServeState();
+        cudaSetDevice(ctx->device);
+        cudaStreamCreateWithFlags(&ctx->serve->metrics_stream, cudaStreamNonBlocking);
         ctx->serve->worker = std::thread(worker_main, ctx, ctx->serve);
     }
     return ctx->serve;
@@ -293,10 +345,15 @@ void serve_shutdown(gr_ctx *ctx) {
     }
     sv->cv_work.notify_all();
     if (sv->worker.joinable()) sv->worker.join();
+    cudaSetDevice(ctx->device);
     for (auto &kv : sv->reqs) {
-        kv.second->film.release();
+        kv.second->film.release(ctx->stream);
+        kv.second->comp.release(ctx->stream);
         delete kv.second;
     }
+    cudaStreamSynchronize(ctx->stream);  // stream-ordered frees above complete
+    sv->metrics_scratch.release();
+    if (sv->metrics_stream) cudaStreamDestroy(sv->metrics_stream);
     delete sv;
     ctx->serve = nullptr;
 }
@@ -315,7 +372,9 @@ gr_status gr_submit(gr_ctx *ctx, const gr_request *req, uint64_t *request_id) {
             delete q;
             return fail(GR_ENOTFOUND, "unknown scene id %llu", (unsigned long long)req->scene_id);
         }
-        q->film_bytes = (uint64_t)it->second->S.width * it->second->S.height * 3 * sizeof(float);
+        q->n_px = (uint64_t)it->second->S.width * it->second->S.height;
+        q->kahan = (it->second->S.flags & GR_FLAG_KAHAN_FILM) != 0;
+        q->film_bytes = q->n_px * 3 * sizeof(float) * (q->kahan ? 2 : 1);
     } else if (req->kind == GR_REQ_METRICS) {
         if (!req->material || !req->poses || (req->n_planes && !req->planes) || req->n_planes > GR_MAX_PLANES) {
             delete q;
@@ -409,7 +468,7 @@ gr_status gr_request_film(gr_ctx *ctx, uint64_t id, float *xyz_host) {
         if (q->state != GR_REQ_DONE && q->state != GR_REQ_CANCELLED)
             return fail(GR_EINVAL, "request %llu has not finished", (unsigned long long)id);
         src = q->film.ptr;
-        bytes = q->film_bytes;
+        bytes = q->n_px * 3 * sizeof(float);
     }
     if (!src) {
         std::memset(xyz_host, 0, bytes);  // finished before admission: no samples
@@ -451,8 +510,8 @@ gr_status gr_request_release(gr_ctx *ctx, uint64_t id) {
     }
     std::lock_guard<std::mutex> lk(ctx->mu);
     cudaSetDevice(ctx->device);
-    cudaStreamSynchronize(ctx->stream);
-    q->film.release();
+    q->film.release(ctx->stream);  // stream-ordered: after every tick that wrote it
+    q->comp.release(ctx->stream);
     delete q;
     return GR_OK;
 }

@@ -5,9 +5,10 @@ the reference's ``RenderRequest{request_id, first_sample, samples}``
 (crates/gemray-net/src/messages/render.rs:65-70): each adds samples
 ``[first_sample, first_sample + samples)`` of every pixel into a film of its own.
 The library's worker thread admits requests by device-memory budget and advances all
-running renders together, one slice per tick, in shared batched launches; a film is
-bit-identical to rendering its request alone.  Metric sweeps (brilliance / fire /
-scintillation over a list of poses) share the same queue.
+running renders together, one slice per tick, in shared batched launches.  Slices
+continue each pixel's running sum, so a film is bit-identical to rendering the whole
+sample range alone in one call, however it was sliced and whatever else ran.  Metric
+sweeps (brilliance / fire / scintillation over a list of poses) share the same queue.
 """
 from __future__ import annotations
 
@@ -62,7 +63,9 @@ class RenderServer:
         self._shapes.pop(scene_id, None)
 
     # -- requests -------------------------------------------------------------------
-    def submit_render(self, scene_id: int, first_sample: int, samples: int, slice_spp: int = 16) -> int:
+    def submit_render(self, scene_id: int, first_sample: int, samples: int, slice_spp: int = 0) -> int:
+        """slice_spp caps the samples per pixel one tick may take (0 = no cap); the film
+        never depends on it."""
         q = abi.gr_request(kind=abi.GR_REQ_RENDER, slice_spp=slice_spp, scene_id=scene_id, sample_offset=first_sample,
                            spp=samples)
         rid = C.c_uint64()

@@ -369,8 +369,10 @@ gr_status gr_render_batch(gr_ctx *ctx, const gr_batch_item *items, uint32_t n_it
  * sweep.  Pointers are copied at submit. */
 typedef struct gr_request {
     uint32_t kind;
-    uint32_t slice_spp;      /* render: samples per scheduling slice, 0 = 16; progress, interleaving and
-                                cancellation happen between slices */
+    uint32_t slice_spp;      /* render: at most this many samples per pixel per tick, 0 = no cap (a tick
+                                carries ~16.8 M path-samples, filled from the running renders in arrival
+                                order).  Progress, interleaving and cancellation happen between slices;
+                                the film does not depend on the slicing */
     uint64_t scene_id;       /* render: resident scene */
     uint32_t sample_offset;  /* render: first absolute sample */
     uint32_t spp;            /* render: samples per pixel */
@@ -404,10 +406,9 @@ typedef struct gr_request_status {
  * apps/gemray-worker/src/render_core/mod.rs).  A worker thread admits requests in
  * arrival order while their film (W*H*3 f32) fits the context's serve budget next to
  * the resident scenes and unreleased films, and advances every running render by one
- * slice per tick in a shared batched launch.  A film is bit-identical to
- * gr_render_resident called once per slice over the same sample range (each slice's
- * per-pixel sum is added once, as a worker accumulating sub-batches does), alone or
- * in any mix. */
+ * slice per tick in a shared batched launch.  Slices continue each pixel's running
+ * sum, so a film is bit-identical to one gr_render_resident call over the same sample
+ * range on a zero film -- for any slicing, alone or in any mix. */
 gr_status gr_submit(gr_ctx *ctx, const gr_request *request, uint64_t *request_id);
 gr_status gr_poll(gr_ctx *ctx, uint64_t request_id, gr_request_status *status);
 /* Blocks until the request has finished or timeout_ms passed (GR_ETIMEOUT). */

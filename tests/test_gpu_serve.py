@@ -1,10 +1,9 @@
 """Serving (gr_submit / gr_poll / gr_wait / gr_cancel): continuous batching of render
 requests and metric sweeps over resident scenes.
 
-The bar: a request's film is bit-identical alone and in a mix (and to
-gr_render_resident called once per slice over the same sample range: each slice's
-per-pixel sum is added to the film once, as a worker accumulating sub-batches does);
-metric sweeps equal
+The bar: a request's film is bit-identical alone and in a mix, for any slicing, to
+one gr_render_resident call over its whole sample range on a zero film (slices carry
+each pixel's running sum on, Kahan compensation included); metric sweeps equal
 gr_optical_metrics; cancellation stops a render between slices; admission holds
 requests back until their film fits the device-memory budget and fails the ones that
 never can.
@@ -34,20 +33,14 @@ def _scenes():
                     max_bounces=16, env_mode=abi.GR_ENV_UNIFORM, flags=abi.GR_FLAG_KAHAN_FILM)]
 
 
-def _resident(srv: RenderServer, sid: int, shape, offset: int, spp: int, slice_spp: int) -> np.ndarray:
-    """gr_render_resident over the same sample range, one call per slice: a request's
-    film is defined by its slices (each slice's per-pixel sum is added once), exactly
-    as a worker that accumulates sub-batches."""
+def _resident(srv: RenderServer, sid: int, shape, offset: int, spp: int) -> np.ndarray:
+    """One gr_render_resident call over the whole sample range on a zero film."""
     import torch
     w, h = shape
     film = torch.zeros((w * h, 3), dtype=torch.float32, device="cuda")
     torch.cuda.synchronize()
-    done = 0
-    while done < spp:
-        n = min(slice_spp, spp - done)
-        st = srv.lib.gr_render_resident(srv.ctx, sid, offset + done, n, C.c_void_p(film.data_ptr()), None)
-        assert st == abi.GR_OK
-        done += n
+    st = srv.lib.gr_render_resident(srv.ctx, sid, offset, spp, C.c_void_p(film.data_ptr()), None)
+    assert st == abi.GR_OK
     assert srv.lib.gr_synchronize(srv.ctx) == abi.GR_OK
     return film.cpu().numpy()
 
@@ -57,22 +50,22 @@ def test_results_identical_alone_and_in_mix(engine_lib):
     try:
         scenes = _scenes()
         ids = [srv.upload(sc) for sc in scenes]
-        alone = srv.submit_render(ids[0], 100, 48, slice_spp=16)
+        alone = srv.submit_render(ids[0], 100, 48)  # slices sized by the library
         st = srv.wait(alone)
         assert st.state == "done" and st.samples_done == 48 and st.latency_ms > 0
         film_alone = srv.film(alone)
         # the same request again, now mixed with two renders of other scenes and a metric sweep
         poses = np.array([[0.0, 0.45 + 0.05 * k, 0.85, 0.95] for k in range(8)], np.float32)
-        rids = [srv.submit_render(ids[1], 7, 40, slice_spp=8), srv.submit_render(ids[0], 100, 48, slice_spp=16),
+        rids = [srv.submit_render(ids[1], 7, 40, slice_spp=8), srv.submit_render(ids[0], 100, 48, slice_spp=5),
                 srv.submit_render(ids[2], 0, 33, slice_spp=16)]
         mid = srv.submit_metrics(S.standard_round_brilliant(), S.builtin_material("Diamond"), poses)
         for r in rids + [mid]:
             assert srv.wait(r).state == "done"
         mixed = srv.film(rids[1])
         assert np.array_equal(film_alone.view(np.uint32), mixed.view(np.uint32))
-        assert np.array_equal(mixed.view(np.uint32), _resident(srv, ids[0], (48, 40), 100, 48, 16).view(np.uint32))
-        assert np.array_equal(srv.film(rids[0]).view(np.uint32), _resident(srv, ids[1], (32, 32), 7, 40, 8).view(np.uint32))
-        assert np.array_equal(srv.film(rids[2]).view(np.uint32), _resident(srv, ids[2], (24, 30), 0, 33, 16).view(np.uint32))
+        assert np.array_equal(mixed.view(np.uint32), _resident(srv, ids[0], (48, 40), 100, 48).view(np.uint32))
+        assert np.array_equal(srv.film(rids[0]).view(np.uint32), _resident(srv, ids[1], (32, 32), 7, 40).view(np.uint32))
+        assert np.array_equal(srv.film(rids[2]).view(np.uint32), _resident(srv, ids[2], (24, 30), 0, 33).view(np.uint32))
         ref = M.evaluate_poses(srv.r, S.standard_round_brilliant(), S.builtin_material("Diamond"), poses)
         assert np.array_equal(srv.metrics(mid).view(np.uint32), ref.view(np.uint32))
         for r in [alone] + rids + [mid]:
@@ -94,7 +87,7 @@ def test_cancel_between_slices(engine_lib):
         assert st.state == "cancelled" and st.samples_done < (1 << 20) and st.samples_done % 4 == 0
         film = srv.film(rid)   # the slices folded before the cancel
         if st.samples_done:
-            assert np.array_equal(film.view(np.uint32), _resident(srv, sid, (48, 40), 0, st.samples_done, 4).view(np.uint32))
+            assert np.array_equal(film.view(np.uint32), _resident(srv, sid, (48, 40), 0, st.samples_done).view(np.uint32))
         srv.release(rid)
     finally:
         srv.close()
@@ -116,7 +109,7 @@ def test_admission_by_memory_budget(engine_lib):
         srv.release(a)
         sb = srv.wait(b)
         assert sb.state == "done" and sb.queued_ms >= 0.9 * sa.latency_ms
-        assert np.array_equal(srv.film(b).view(np.uint32), _resident(srv, ids[0], (48, 40), 32, 32, 8).view(np.uint32))
+        assert np.array_equal(srv.film(b).view(np.uint32), _resident(srv, ids[0], (48, 40), 32, 32).view(np.uint32))
         srv.release(b)
         big = S.Scene(width=512, height=512, planes=S.round_brilliant_57(), material=S.builtin_material("Diamond"),
                       cam=S.camera(0.35, 0.28, 5.0, 18.0), max_bounces=8)

@@ -44,6 +44,7 @@ GR_ENV_STUDIO = 1
 GR_ENV_LATLONG = 2
 
 GR_FLAG_KAHAN_FILM = 0x1
+GR_FLAG_FP64_RESOLVE = 0x2
 
 EVENT_NAMES = ["paths", "bounces", "escapes", "tir", "reflect", "refract", "absorb", "channel_tir",
                "channel_refract", "roulette", "rotations", "aniso_bounces", "walkoff", "roulette_kills"]

@@ -61,6 +61,8 @@ gr_status make_plan(gr_ctx *ctx, const grh::BatchItem *items, uint32_t n_items, 
         const uint64_t n_px = (uint64_t)rs->S.width * rs->S.height;
         if (it.spp == 0 || n_px == 0) continue;
         if (!it.film_device) return fail(GR_EINVAL, "item %u: film is NULL", i);
+        if (rs->S.flags & GR_FLAG_FP64_RESOLVE)
+            return fail(GR_EINVAL, "item %u: GR_FLAG_FP64_RESOLVE scenes render through the single-scene calls", i);
         auto sl = slot_of.find(it.scene_id);
         uint32_t slot;
         if (sl == slot_of.end()) {

@@ -417,6 +417,13 @@ gr_status launch_trace(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuffers
                        float *xyz, cudaStream_t stream, int mode) {
     if (R.n_tuples == 0) return GR_OK;
     size_t smem = grd::planes_smem_bytes(S.n_planes);
+    if (S.flags & GR_FLAG_FP64_RESOLVE) {  // the re-solve variant exists for the plain kernel only
+        const uint64_t blocks = (R.n_tuples + grd::TRACE_THREADS - 1) / grd::TRACE_THREADS;
+        grd::k_trace_plain<grd::NoCounters, true><<<(unsigned)blocks, grd::TRACE_THREADS, smem, stream>>>(S, B, R, xyz,
+                                                                                                        nullptr);
+        GR_CUDA(cudaGetLastError());
+        return GR_OK;
+    }
     if (mode == GR_KERNEL_PLAIN || S.max_bounces == 0) {
         uint64_t blocks = (R.n_tuples + grd::TRACE_THREADS - 1) / grd::TRACE_THREADS;
         grd::k_trace_plain<grd::NoCounters><<<(unsigned)blocks, grd::TRACE_THREADS, smem, stream>>>(S, B, R, xyz, nullptr);

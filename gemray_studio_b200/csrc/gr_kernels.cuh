@@ -9,8 +9,9 @@ namespace grd {
 
 // Plain kernel: one thread traces one tuple start to finish -- the reference
 // kernel's launch shape (one invocation per (pixel, sample), spectral_transport.wgsl:
-// 672-691).  The Counters variant tallies events for the FLOP model.
-template <class CT>
+// 672-691).  The Counters variant tallies events for the FLOP model; RESOLVE is the
+// GR_FLAG_FP64_RESOLVE variant (FP64 re-solve of ambiguous exits and TIR decisions).
+template <class CT, bool RESOLVE = false>
 __global__ void __launch_bounds__(TRACE_THREADS, GR_TRACE_MIN_BLOCKS) k_trace_plain(SceneConst S, SceneBuffers B, LaunchRange R,
                                                                float *__restrict__ xyz,
                                                                unsigned long long *__restrict__ tallies) {
@@ -27,7 +28,7 @@ __global__ void __launch_bounds__(TRACE_THREADS, GR_TRACE_MIN_BLOCKS) k_trace_pl
         Path P;
         path_init<1>(P, S, B, pixel, sample, (uint32_t)t);
         tally(ct, C_PATHS);
-        V3 c = trace_path(P, S, B, PL, ct);
+        V3 c = trace_path<CT, RESOLVE>(P, S, B, PL, ct);
         xyz[3 * t + 0] = c.x;
         xyz[3 * t + 1] = c.y;
         xyz[3 * t + 2] = c.z;

@@ -247,16 +247,27 @@ __device__ __forceinline__ f32x2 mul2(f32x2 a, f32x2 b) {
     return r;
 }
 
-// One plane's contribution; returns false when the scan ends in a miss.
+// One plane's contribution; returns false when the scan ends in a miss.  With R
+// (FP64 re-solve) the division-skip margin widens to 2^-15 and the runner-up t of
+// each side is tracked: every plane whose t lies within ~2.9e-5 (relative) of the
+// running extremum is divided exactly, so a runner-up within 1e-5 is never missed.
+template <bool R>
 __device__ __forceinline__ bool scan_plane(float denom, float side, int i, float &t_near, int &near_idx, float &t_far,
-                                           int &far_idx) {
+                                           int &far_idx, float &t_near2, float &t_far2) {
+    constexpr float M = R ? 3.0517578e-5f : 1.9073486e-6f;  // 2^-15 : 2^-19
     if (denom < -1e-7f) {
         if (side > 0.0f) {
             const float num = -side;
             const float qa = num * rcp_approx(denom);
-            if (!(qa + fabsf(qa) * 1.9073486e-6f < t_near)) {
+            if (!(qa + fabsf(qa) * M < t_near)) {
                 const float t = num / denom;
-                if (t > t_near) { t_near = t; near_idx = i; }
+                if (t > t_near) {
+                    if (R) t_near2 = t_near;
+                    t_near = t;
+                    near_idx = i;
+                } else if (R && t > t_near2) {
+                    t_near2 = t;
+                }
             }
         }
     } else if (side > 0.0f) {
@@ -264,16 +275,54 @@ __device__ __forceinline__ bool scan_plane(float denom, float side, int i, float
     } else if (denom > 1e-7f) {
         const float num = -side;
         const float qa = num * rcp_approx(denom);
-        if (!(qa - fabsf(qa) * 1.9073486e-6f > t_far)) {
+        if (!(qa - fabsf(qa) * M > t_far)) {
             const float t = num / denom;
-            if (t < t_far) { t_far = t; far_idx = i; }
+            if (t < t_far) {
+                if (R) t_far2 = t_far;
+                t_far = t;
+                far_idx = i;
+            } else if (R && t < t_far2) {
+                t_far2 = t;
+            }
         }
     }
     return true;
 }
 
+// The reference clip (intersect.rs:93-132) in FP64, t rounded back to f32: the
+// re-solve for rays whose f32 exit facet is ambiguous.  Out of line: it runs for
+// only a tiny fraction of rays.
+static __device__ __noinline__ bool intersect_fp64(const float4 *__restrict__ planes, uint32_t n, V3 o, V3 d,
+                                                   float &t_hit, int &idx_hit) {
+    double tn = -1e30, tf = 1e30;
+    int ni = -1, fi = -1;
+    for (uint32_t i = 0; i < n; ++i) {
+        const float4 p = planes[i];
+        const double denom = ((double)p.x * d.x + (double)p.y * d.y) + (double)p.z * d.z;
+        const double side = (double)p.w + (((double)p.x * o.x + (double)p.y * o.y) + (double)p.z * o.z);
+        if (fabs(denom) > 1e-7) {
+            const double t = -side / denom;
+            if (denom < 0.0) {
+                if (t > tn) { tn = t; ni = (int)i; }
+            } else if (t < tf) {
+                tf = t;
+                fi = (int)i;
+            }
+        } else if (side > 0.0) {
+            return false;
+        }
+    }
+    if (tn > tf) return false;
+    if (tn > 1e-4) { t_hit = (float)tn; idx_hit = ni; return true; }
+    if (tf > 1e-4) { t_hit = (float)tf; idx_hit = fi; return true; }
+    return false;
+}
+
+// R: re-solve in FP64 when the chosen exit is within 1e-5 (relative) of the
+// runner-up plane or of the other side's extremum (a ray grazing an edge).
+template <bool R = false>
 __device__ __forceinline__ bool intersect(const Planes &PL, V3 o, V3 d, float &t_hit, int &idx_hit) {
-    float t_near = -1e30f, t_far = 1e30f;
+    float t_near = -1e30f, t_far = 1e30f, t_near2 = -1e30f, t_far2 = 1e30f;
     int near_idx = -1, far_idx = -1;
     const f32x2 dx = pk2(d.x, d.x), dy = pk2(d.y, d.y), dz = pk2(d.z, d.z);
     const f32x2 ox = pk2(o.x, o.x), oy = pk2(o.y, o.y), oz = pk2(o.z, o.z);
@@ -291,8 +340,16 @@ __device__ __forceinline__ bool intersect(const Planes &PL, V3 o, V3 d, float &t
         // denom = (nx*dx + ny*dy) + nz*dz;  side = d + ((nx*ox + ny*oy) + nz*oz)
         const float den0 = (xd0 + yd0) + zd0, den1 = (xd1 + yd1) + zd1;
         const float sid0 = b.z + ((xo0 + yo0) + zo0), sid1 = b.w + ((xo1 + yo1) + zo1);
-        if (!scan_plane(den0, sid0, (int)(2 * j), t_near, near_idx, t_far, far_idx)) return false;
-        if (!scan_plane(den1, sid1, (int)(2 * j + 1), t_near, near_idx, t_far, far_idx)) return false;
+        if (!scan_plane<R>(den0, sid0, (int)(2 * j), t_near, near_idx, t_far, far_idx, t_near2, t_far2)) return false;
+        if (!scan_plane<R>(den1, sid1, (int)(2 * j + 1), t_near, near_idx, t_far, far_idx, t_near2, t_far2))
+            return false;
+    }
+    if (R) {
+        const float tol = 1e-5f;
+        bool amb = fabsf(t_near - t_far) <= tol * fmaxf(fabsf(t_near), fabsf(t_far));
+        if (t_near > 1e-4f) amb = amb || (t_near - t_near2 <= tol * t_near);
+        else if (t_far > 1e-4f) amb = amb || (t_far2 - t_far <= tol * t_far);
+        if (amb) return intersect_fp64(PL.aos, PL.n, o, d, t_hit, idx_hit);
     }
     if (t_near > t_far) return false;
     if (t_near > 1e-4f) {
@@ -336,7 +393,7 @@ __device__ __forceinline__ V3 shading_normal(const float4 *planes, uint32_t n, V
 // One intersection and everything of the bounce up to the hero's event decision
 // (transport.rs:781-895, raytracer/absorption.rs:71-141, refraction.rs:428-547,
 // 1036-1060).  Returns EV_DONE on an escape (F_ESCAPED set, F_ALIVE cleared).
-template <int U, class CT>
+template <int U, class CT, bool R = false>
 __device__ __forceinline__ uint32_t step_hit(Path &P, const SceneConst &S, const Planes &PL, Event &E, CT &ct) {
     const uint32_t bits = state_bits(P);
     const uint32_t bounce = bits >> BOUNCE_SHIFT;
@@ -345,7 +402,7 @@ __device__ __forceinline__ uint32_t step_hit(Path &P, const SceneConst &S, const
     float t_hit = 0.0f;
     int fidx = 0;
     tally(ct, C_BOUNCES);
-    if (!intersect(PL, o, d, t_hit, fidx)) {
+    if (!intersect<R>(PL, o, d, t_hit, fidx)) {
         // accumulate_miss_radiance (transport.rs:67-90) runs in path_finish
         tally(ct, C_ESCAPES);
         set_state_bits(P, (bits | F_ESCAPED) & ~F_ALIVE);
@@ -448,12 +505,19 @@ __device__ __forceinline__ uint32_t step_hit(Path &P, const SceneConst &S, const
 
     // dispatch_bounce (transport.rs:158-176): hero TIR, or the Fresnel draw of
     // apply_partial_fresnel_bounce (refraction.rs:1049-1060)
-    if (sin2_t > 1.0f) {
+    bool tir = sin2_t > 1.0f;
+    if (R && fabsf(sin2_t - 1.0f) < 1e-5f) {
+        // near the critical angle: decide TIR in FP64 (refraction.rs:428-547 in double)
+        const double ci = fmin(fmax(-((double)kk.x * normal.x + (double)kk.y * normal.y) - (double)kk.z * normal.z, 0.0), 1.0);
+        const double eta = (double)n1 / (double)n2;
+        tir = eta * eta * (1.0 - ci * ci) > 1.0;
+    }
+    if (tir) {
         E.n_ru = make_float4(normal.x, normal.y, normal.z, 0.0f);
         set_state_bits(P, bits | F_TIR);
         return EV_REFLECT;
     }
-    float cos_t = sqrtf(1.0f - sin2_t);
+    float cos_t = sqrtf(R ? fmaxf(1.0f - sin2_t, 0.0f) : 1.0f - sin2_t);
     float rs, rp;
     fresnel_rs_rp(n1, n2, cos_i, cos_t, rs, rp);
     float ru = r_unpol(rs, rp);
@@ -657,12 +721,12 @@ __device__ __forceinline__ V3 path_finish(const Path &P, const SceneConst &S, co
 }
 
 // One whole path in the calling thread (the plain kernel's body).
-template <class CT>
+template <class CT, bool R = false>
 __device__ __forceinline__ V3 trace_path(Path &P, const SceneConst &S, const SceneBuffers &B, const Planes &PL,
                                          CT &ct) {
     while (state_bits(P) & F_ALIVE) {
         Event E;
-        uint32_t ev = step_hit<1>(P, S, PL, E, ct);
+        uint32_t ev = step_hit<1, CT, R>(P, S, PL, E, ct);
         if (ev == EV_REFLECT) step_reflect<1>(P, S, E, ct);
         else if (ev == EV_REFRACT) step_refract<1>(P, S, E, ct);
     }

@@ -54,6 +54,41 @@ def standard_round_brilliant() -> np.ndarray:
     return np.ctypeslib.as_array(buf).view(np.float32).reshape(-1, 4)[:n].copy()
 
 
+def custom_material(mean_ri: float, dispersion_delta: float, birefringence_delta: float,
+                    absorption_rgb=(0.0, 0.0, 0.0)) -> abi.gr_material:
+    """= GpuGemMaterial::encode(&GemMaterial::new_custom(..)) (optics/materials.rs:1257-1316,
+    renderer/buffers.rs:655-800): a Cauchy fit through n_d with the given F-C
+    dispersion (f32 arithmetic as the reference), c-axis +Y, trigonal / uniaxial when
+    |birefringence| > 1e-4, absorption as legacy_rgb_bands (optics/absorption.rs:179-185)
+    on both eigenmodes."""
+    f = np.float32
+    ld, lf, lc = f(0.5893), f(0.4861), f(0.6563)
+    k_fc = f(1.0) / (f(1.0) / (lf * lf) - f(1.0) / (lc * lc))
+    b = max(f(dispersion_delta) * k_fc, f(0.0))
+    a = max(f(mean_ri) - b / (ld * ld), f(1.0))
+    bire = f(birefringence_delta)
+    m = abi.gr_material()
+    d = m.dispersion
+    d.model_type = abi.GR_DISP_CAUCHY
+    d.param_a[0], d.param_a[1] = float(a), float(b)
+    d.c_axis_and_birefringence[1] = 1.0
+    d.c_axis_and_birefringence[3] = float(bire)
+    aniso = abs(float(bire)) > 1e-4
+    d.is_anisotropic = 1 if aniso else 0
+    m.crystal_system = 3 if aniso else 0  # Trigonal / Cubic
+    m.optical_character = 1 if bire > 1e-4 else (2 if bire < -1e-4 else 0)
+    for k, (c, w, p) in enumerate(((620.0, 55.0, absorption_rgb[0]), (540.0, 45.0, absorption_rgb[1]),
+                                    (450.0, 45.0, absorption_rgb[2]))):
+        for bands in (m.o_ray_bands, m.e_ray_bands):
+            bands[k].center_nm, bands[k].width_nm, bands[k].peak = c, w, p
+    for first, bands in ((3, m.o_ray_bands), (3, m.e_ray_bands), (0, m.beta_ray_bands)):  # unused slots: width 1
+        for k in range(first, abi.GR_MAX_BANDS):
+            bands[k].width_nm = 1.0
+    m.o_ray_band_count = m.e_ray_band_count = 3
+    m.absorption_path_scale = 1.0
+    return m
+
+
 def builtin_material(name: str) -> abi.gr_material:
     m = abi.gr_material()
     st = _lib().gr_builtin_material(name.encode(), C.byref(m))

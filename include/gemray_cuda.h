@@ -160,6 +160,13 @@ typedef struct gr_material_ext {
 
 /* Scene flags. */
 #define GR_FLAG_KAHAN_FILM 0x1u /* compensated per-pixel sample sum (default: plain f32 in sample order) */
+/* FP64 re-solve of ambiguous f32 decisions (an extension, off by default): a ray whose
+ * f32 exit facet is within 1e-5 (relative) of another plane's, or of the other side's
+ * extremum, is re-clipped in FP64, and a hero TIR decision with |sin^2(t) - 1| < 1e-5
+ * is re-made in FP64.  Results then differ from the reference's f32 tracer on those
+ * few rays (towards the FP64 result).  Single-scene calls only (gr_accumulate*,
+ * gr_render_resident*, gr_trace_samples); gr_render_batch and gr_submit reject it. */
+#define GR_FLAG_FP64_RESOLVE 0x2u
 
 /* One render scene, = GpuSceneRef (renderer/gpu_backend.rs:85-99).  Every pointer is
  * borrowed for the duration of the call. */

@@ -112,6 +112,21 @@ void gro_white_balance(float temp_k, float out[3]) {
     out[0] = w.x; out[1] = w.y; out[2] = w.z;
 }
 
+// White-furnace analytic target (crates/gemray/tests/raytracer_tests.rs:2594-2600):
+// sum over lambda = 380..780 nm of cie_1931_cmf(lambda) * rgb_to_spectral_radiance(
+// [L0, L0, L0], lambda), then / 106.856, in the reference's f32 order.
+void gro_furnace_target(float l0, float out[3]) {
+    float t[3] = {0.0f, 0.0f, 0.0f};
+    for (int step = 0; step <= 400; ++step) {
+        const float lambda = 380.0f + (float)step;
+        const float spec = rgb_to_spectral<float>(l0, l0, l0, lambda);
+        float c[3];
+        cmf_scalar<float>(lambda, c);
+        for (int k = 0; k < 3; ++k) t[k] = t[k] + c[k] * spec;
+    }
+    for (int k = 0; k < 3; ++k) out[k] = t[k] / 106.856f;
+}
+
 float gro_studio_env(const float dir[3], float lambda, float temp_k, float spot_mult, float exposure, float yaw,
                      float pitch) {
     StudioRig<float> rig = studio_rig_new<float>(yaw, pitch);
@@ -243,6 +258,30 @@ int gro_trace_samples(const gr_scene *sc, uint32_t first_pixel, uint32_t n_pixel
                     counts[6 * o + 5] = logs[k].n_chan_tir;
                 }
             }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; ++t) pool.emplace_back(worker);
+    for (auto &t : pool) t.join();
+    return GR_OK;
+}
+
+// Per-sample XYZ of the FP64 twin (values rounded to f32), for per-sample agreement
+// checks against the f32 engine.
+int gro_trace_samples_f64(const gr_scene *sc, uint32_t first_pixel, uint32_t n_pixels, uint32_t sample_offset,
+                          uint32_t spp, float *xyz_out, int threads) {
+    if (!material_supported(sc->material, sc->finishes, sc->n_planes)) return GR_DECLINED_MATERIAL;
+    MaterialCtx<double> mc = make_material<double>(sc->material, sc->material_ext);
+    EnvCtx<double> env = make_env<double>(sc->env);
+    if (threads <= 0) threads = (int)std::thread::hardware_concurrency();
+    std::atomic<uint32_t> next(0);
+    auto worker = [&]() {
+        for (;;) {
+            uint32_t i = next.fetch_add(1);
+            if (i >= n_pixels) break;
+            double s[3];
+            trace_pixel_samples<double>(*sc, mc, env, first_pixel + i, sample_offset, spp,
+                                        xyz_out + (size_t)i * spp * 3, s, nullptr);
         }
     };
     std::vector<std::thread> pool;

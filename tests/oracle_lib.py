@@ -64,6 +64,10 @@ def lib():
     L.gro_builtin_material.argtypes = [C.c_char_p, C.POINTER(abi.gr_material)]
     L.gro_white_balance.restype = None
     L.gro_white_balance.argtypes = [F, fp]
+    L.gro_trace_samples_f64.restype = C.c_int
+    L.gro_trace_samples_f64.argtypes = [C.POINTER(abi.gr_scene), U, U, U, U, fp, C.c_int]
+    L.gro_furnace_target.restype = None
+    L.gro_furnace_target.argtypes = [F, fp]
     L.gro_studio_env.restype = F
     L.gro_studio_env.argtypes = [fp, F, F, F, F, F, F]
     L.gro_studio_env_spec.restype = F

@@ -48,3 +48,25 @@ def test_synthetic_geometry_is_valid():
     assert S.face_count(S.emerald_cut_49()) == 49          # every plane bounds a face
     assert S.face_count(S.round_brilliant_57()) == 73      # 57 facets + 16 girdle planes
     assert S.face_count(S.standard_round_brilliant()) == 74
+
+
+def test_custom_material_matches_new_custom_encoding():
+    """GemMaterial::new_custom (optics/materials.rs:1257-1316) as GpuGemMaterial::encode
+    writes it: Cauchy a = n_d - b / 0.5893^2 with b = dispersion x k_FC, c-axis +Y,
+    trigonal + uniaxial-positive above |dn| > 1e-4, legacy RGB bands on both modes."""
+    import numpy as np
+
+    from gemray_studio_b200 import abi, scene as S
+    m = S.custom_material(1.5, 0.0, 0.03)
+    d = m.dispersion
+    assert d.model_type == abi.GR_DISP_CAUCHY and d.param_a[0] == np.float32(1.5) and d.param_a[1] == 0.0
+    assert list(d.c_axis_and_birefringence) == [0.0, 1.0, 0.0, np.float32(0.03)]
+    assert d.is_anisotropic == 1 and m.crystal_system == 3 and m.optical_character == 1
+    assert m.o_ray_band_count == 3 and m.o_ray_bands[0].center_nm == 620.0 and m.e_ray_bands[2].width_nm == 45.0
+    assert m.beta_ray_band_count == 0 and m.beta_ray_bands[0].width_nm == 1.0 and m.absorption_path_scale == 1.0
+    iso = S.custom_material(2.417, 0.044, 0.0)
+    f = np.float32
+    k = f(1) / (f(1) / (f(0.4861) * f(0.4861)) - f(1) / (f(0.6563) * f(0.6563)))
+    b = f(0.044) * k
+    assert iso.dispersion.param_a[1] == b and iso.dispersion.param_a[0] == f(2.417) - b / (f(0.5893) * f(0.5893))
+    assert iso.dispersion.is_anisotropic == 0 and iso.crystal_system == 0 and iso.optical_character == 0

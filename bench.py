@@ -249,6 +249,20 @@ def traffic_per_launch(tuples_per_launch: float):
     return per_tuple * tuples_per_launch
 
 
+def hbm_view(tuples_per_launch: float, ms_per_launch: float):
+    """The transport kernel against the measured HBM copy bandwidth: its DRAM traffic
+    per launch (from the committed ncu capture) over its event-timed duration.  Shows
+    how far the kernel is from being memory-bound."""
+    t = traffic_per_launch(tuples_per_launch)
+    p = ROOT / "MEASURED_PEAKS.json"
+    if t is None or ms_per_launch <= 0:
+        return None
+    gbs = t / (ms_per_launch * 1e-3) / 1e9
+    peak = json.loads(p.read_text()).get("hbm_gbs") if p.exists() else None
+    return {"achieved": gbs, "unit": "GB/s", "peak": peak, "frac": gbs / peak if peak else None,
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peak else None}
+
+
 def run_engine(args):
     world, rank, local = dist_setup()
     import torch
@@ -358,6 +372,8 @@ def run_engine(args):
             "roofline": {"bound": "fp32", "kernel": "k_trace_plain", "achieved": achieved, "peak": fp32_peak,
                          "unit": "TFLOP/s", "frac": achieved / fp32_peak,
                          "traffic": traffic_per_launch(samples_per_step / max(1, ntr.value / frames)),
+                         "hbm_view": hbm_view(samples_per_step / max(1, ntr.value / frames),
+                                              tr.value / max(1, ntr.value)),
                          "peak_source": "measured on this device by gr_probe_fp32_peak (8 independent FFMA chains)",
                          "flops_per_sample": model.flops_per_sample,
                          "sfu_ops_per_sample": model.sfu / max(1, model.paths),

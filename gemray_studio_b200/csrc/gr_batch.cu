@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <cstring>
 #include <unordered_map>
 #include <vector>
@@ -116,6 +117,17 @@ gr_status make_plan(gr_ctx *ctx, const grh::BatchItem *items, uint32_t n_items, 
     return GR_OK;
 }
 
+// Capacity to reserve for `need` bytes: unchanged while it fits, else at least double
+// the old capacity (and 1 MiB), capped at `limit` when that still covers `need`.  A
+// regrowth frees the old buffer, which synchronises the device (and, for pinned
+// memory, pins pages): geometric growth makes that rare in a long-running loop.
+size_t grown(size_t cap, size_t need, size_t limit) {
+    if (need <= cap) return need;
+    size_t want = std::max<size_t>({need, 2 * cap, (size_t)1 << 20});
+    if (want > limit) want = std::max(need, limit);
+    return want;
+}
+
 gr_status launch_plan(const Plan &P, const grd::SceneSlot *slots, const grd::BatchSegment *segs, cudaStream_t s) {
     for (const Launch &L : P.launches) {
         grd::k_trace_batch<<<(unsigned)L.blocks, grd::TRACE_THREADS, grd::planes_smem_bytes(L.max_planes), s>>>(
@@ -156,11 +168,11 @@ gr_status batch_enqueue(gr_ctx *ctx, const BatchItem *items, uint32_t n_items, u
     if (P.launches.empty()) return GR_OK;
     cudaStream_t s = stream ? stream : ctx->stream;
 
-    st = ctx->xyz.reserve((size_t)P.max_tuples * 3 * sizeof(float));
+    st = ctx->xyz.reserve(grown(ctx->xyz.cap, (size_t)P.max_tuples * 3 * sizeof(float), ctx->chunk_budget));
     if (st != GR_OK) return st;
     const size_t slot_bytes = (P.slots.size() * sizeof(grd::SceneSlot) + 255) & ~(size_t)255;
     const size_t seg_bytes = P.segs.size() * sizeof(grd::BatchSegment);
-    st = ctx->batch_tables.reserve(slot_bytes + seg_bytes);
+    st = ctx->batch_tables.reserve(grown(ctx->batch_tables.cap, slot_bytes + seg_bytes, SIZE_MAX));
     if (st != GR_OK) return st;
     float *xyz = (float *)ctx->xyz.ptr;
     for (grd::BatchSegment &g : P.segs) g.xyz = xyz + ((uintptr_t)g.xyz) / sizeof(float);
@@ -177,7 +189,7 @@ gr_status batch_enqueue(gr_ctx *ctx, const BatchItem *items, uint32_t n_items, u
         if (ctx->stage_host[k]) cudaFreeHost(ctx->stage_host[k]);
         ctx->stage_host[k] = nullptr;
         ctx->stage_cap[k] = 0;
-        const size_t want = std::max<size_t>(slot_bytes + seg_bytes, 64 << 10);
+        const size_t want = grown(ctx->stage_cap[k], slot_bytes + seg_bytes, SIZE_MAX);
         GR_CUDA(cudaHostAlloc(&ctx->stage_host[k], want, cudaHostAllocDefault));
         ctx->stage_cap[k] = want;
     }

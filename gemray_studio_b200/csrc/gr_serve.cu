@@ -9,8 +9,7 @@
 //   * ticks -- each tick is ONE batched launch (gr_batch.cu) filled from the running
 //     renders in arrival order, each contributing all of its remaining samples until
 //     the tick's tuple budget is spent, so small requests finish in a single tick and
-//     share it with others; up to two ticks are in flight, so the host plans tick k+1
-//     while tick k runs;
+//     share it with others; one tick is in flight at a time;
 //   * retirement -- when a tick's event completes its slices count as folded;
 //     a render is DONE when all its samples are; cancellation takes effect between
 //     slices;
@@ -77,9 +76,13 @@ struct Request {
     Clock::time_point t_submit, t_admit, t_done;
 };
 
-// Path-samples one tick carries: ~20-60 ms of transport on B200, the latency quantum
-// of the request loop (a new arrival joins the tick after the ones in flight).
-constexpr uint64_t kTickTuples = 16ull << 20;
+// Path-samples one tick carries: ~10-30 ms of transport on B200, the latency quantum
+// of the request loop (a new arrival joins the tick after the one in flight).
+constexpr uint64_t kTickTuples = 8ull << 20;
+// Ticks queued on the device at once.  One: the host plans the next tick in ~0.1 ms,
+// so a second tick in flight buys no throughput and would make an arrival wait
+// behind two ticks instead of one.
+constexpr size_t kTicksInFlight = 1;
 
 struct Tick {
     cudaEvent_t ev = nullptr;
@@ -171,7 +174,7 @@ void worker_main(gr_ctx *ctx, ServeState *sv) {
     for (;;) {
         // 1. retire finished ticks (always the oldest first: ticks complete in order)
         while (!flight.empty()) {
-            const bool must_wait = flight.size() >= 2;
+            const bool must_wait = flight.size() >= kTicksInFlight;
             cudaError_t e = must_wait ? cudaEventSynchronize(flight.front().ev) : cudaEventQuery(flight.front().ev);
             if (e == cudaErrorNotReady) break;
             std::lock_guard<std::mutex> lk(sv->mu);

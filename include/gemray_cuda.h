@@ -377,7 +377,7 @@ gr_status gr_render_batch(gr_ctx *ctx, const gr_batch_item *items, uint32_t n_it
 typedef struct gr_request {
     uint32_t kind;
     uint32_t slice_spp;      /* render: at most this many samples per pixel per tick, 0 = no cap (a tick
-                                carries ~16.8 M path-samples, filled from the running renders in arrival
+                                carries ~8.4 M path-samples, filled from the running renders in arrival
                                 order).  Progress, interleaving and cancellation happen between slices;
                                 the film does not depend on the slicing */
     uint64_t scene_id;       /* render: resident scene */

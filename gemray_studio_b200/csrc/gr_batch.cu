@@ -32,6 +32,7 @@ struct Launch {
     uint32_t seg_first, seg_count;
     uint64_t blocks, warps;
     uint32_t max_planes;
+    bool extras;  // a segment's scene has frosted facets or scattering
 };
 
 struct Plan {
@@ -46,12 +47,12 @@ struct Plan {
 // until the scratch is placed.
 gr_status make_plan(gr_ctx *ctx, const grh::BatchItem *items, uint32_t n_items, uint64_t budget, Plan &P) {
     std::unordered_map<uint64_t, uint32_t> slot_of;
-    Launch cur{0, 0, 0, 0, 0};
+    Launch cur{0, 0, 0, 0, 0, false};
     uint64_t used = 0;
     auto close = [&]() {
         if (cur.seg_count) P.launches.push_back(cur);
         P.max_tuples = std::max(P.max_tuples, used);
-        cur = Launch{(uint32_t)P.segs.size(), 0, 0, 0, 0};
+        cur = Launch{(uint32_t)P.segs.size(), 0, 0, 0, 0, false};
         used = 0;
     };
     for (uint32_t i = 0; i < n_items; ++i) {
@@ -109,6 +110,7 @@ gr_status make_plan(gr_ctx *ctx, const grh::BatchItem *items, uint32_t n_items, 
             cur.blocks += (g.R.n_tuples + grd::TRACE_THREADS - 1) / grd::TRACE_THREADS;
             cur.warps += np;
             cur.max_planes = std::max(cur.max_planes, rs->S.n_planes);
+            cur.extras = cur.extras || rs->S.any_frosted || rs->S.sigma_s > 0.0f;
             used += g.R.n_tuples;
             next += np;
         }
@@ -130,8 +132,12 @@ size_t grown(size_t cap, size_t need, size_t limit) {
 
 gr_status launch_plan(const Plan &P, const grd::SceneSlot *slots, const grd::BatchSegment *segs, cudaStream_t s) {
     for (const Launch &L : P.launches) {
-        grd::k_trace_batch<<<(unsigned)L.blocks, grd::TRACE_THREADS, grd::planes_smem_bytes(L.max_planes), s>>>(
-            slots, segs + L.seg_first, L.seg_count);
+        if (L.extras)
+            grd::k_trace_batch<true><<<(unsigned)L.blocks, grd::TRACE_THREADS, grd::planes_smem_bytes(L.max_planes), s>>>(
+                slots, segs + L.seg_first, L.seg_count);
+        else
+            grd::k_trace_batch<false><<<(unsigned)L.blocks, grd::TRACE_THREADS, grd::planes_smem_bytes(L.max_planes), s>>>(
+                slots, segs + L.seg_first, L.seg_count);
         const unsigned T = 256;
         grd::k_fold_batch<<<(unsigned)((L.warps * 32 + T - 1) / T), T, 0, s>>>(segs + L.seg_first, L.seg_count);
     }
@@ -151,7 +157,7 @@ std::vector<uint64_t> graph_key(const Plan &P, const void *tables, const void *x
         k.push_back(((uint64_t)g.R.spp << 32) | g.scene);
         k.push_back((uint64_t)(uintptr_t)g.comp ^ g.cont);
     }
-    for (const Launch &L : P.launches) k.push_back(((uint64_t)L.seg_count << 32) | L.max_planes);
+    for (const Launch &L : P.launches) k.push_back(((uint64_t)L.seg_count << 32) | L.max_planes | ((uint64_t)L.extras << 31));
     return k;
 }
 

@@ -42,6 +42,8 @@ __device__ __forceinline__ uint32_t find_segment(const BatchSegment *__restrict_
     return lo;
 }
 
+// EXTRAS: the variant for launches holding a scene with frosted facets or scattering.
+template <bool EXTRAS>
 __global__ void __launch_bounds__(TRACE_THREADS, GR_TRACE_MIN_BLOCKS)
     k_trace_batch(const SceneSlot *__restrict__ slots, const BatchSegment *__restrict__ segs, uint32_t n_segs) {
     __shared__ SceneSlot s_slot;
@@ -67,7 +69,7 @@ __global__ void __launch_bounds__(TRACE_THREADS, GR_TRACE_MIN_BLOCKS)
         Path P;
         path_init<1>(P, S, B, pixel, sample, (uint32_t)t);
         NoCounters nc;
-        const V3 c = trace_path(P, S, B, PL, nc);
+        const V3 c = trace_path<NoCounters, false, EXTRAS>(P, S, B, PL, nc);
         float *xyz = G.xyz;
         xyz[3 * t + 0] = c.x;
         xyz[3 * t + 1] = c.y;

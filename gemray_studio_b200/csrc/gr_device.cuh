@@ -50,6 +50,10 @@ struct SceneConst {
     float key[3], fill[3], ring[16][3];  // StudioRig::new, host-built
     uint32_t map_w, map_h;
     uint32_t flags;
+    // frosted facet finishes (bit i = plane i) and Henyey-Greenstein volume scattering
+    uint32_t any_frosted;
+    uint32_t frosted[GR_MAX_PLANES / 32];
+    float sigma_s, hg_g;
 };
 
 struct SceneBuffers {
@@ -78,6 +82,7 @@ GR_MATH float m_atan2(float y, float x) { return atan2f(y, x); }
 GR_MATH float m_atan(float x) { return atanf(x); }
 GR_MATH float m_acos(float x) { return acosf(x); }
 GR_MATH float m_exp(float x) { return expf(x); }
+GR_MATH float m_log(float x) { return logf(x); }
 
 // ---------------------------------------------------------------------------------
 // Small vector helpers with glam's scalar semantics (no contraction).
@@ -192,6 +197,11 @@ constexpr uint32_t MODE_COUPLING_STREAM = 0xCC9E2D51u;
 constexpr uint32_t PIXEL_JITTER_X_ROTATION_STREAM = 0xA511E9B3u;
 constexpr uint32_t PIXEL_JITTER_Y_ROTATION_STREAM = 0x63D81B23u;
 constexpr uint32_t HERO_WAVELENGTH_ROTATION_STREAM = 0x1B873593u;
+constexpr uint32_t FROSTED_DIR_U_STREAM = 0x27D4EB2Fu;    // sampling.rs:28-41
+constexpr uint32_t FROSTED_DIR_V_STREAM = 0x165667B1u;
+constexpr uint32_t DISTANCE_SAMPLE_STREAM = 0xA24BAED4u;
+constexpr uint32_t PHASE_DIR_U_STREAM = 0x9FB21C65u;
+constexpr uint32_t PHASE_DIR_V_STREAM = 0x1CE4E5B9u;
 
 struct Draws {
     uint32_t seed;
@@ -493,6 +503,47 @@ __device__ __forceinline__ V3 von_kries(V3 xyz, const float wb[3]) {
     return v3(fmaf(0.986993f, lms.x, fmaf(-0.147054f, lms.y, 0.159963f * lms.z)),
               fmaf(0.432305f, lms.x, fmaf(0.518360f, lms.y, 0.049291f * lms.z)),
               fmaf(-0.008529f, lms.x, fmaf(0.040043f, lms.y, 0.968487f * lms.z)));
+}
+
+// ---------------------------------------------------------------------------------
+// Frosted facets and Henyey-Greenstein scattering (raytracer/scattering.rs:337-443)
+// ---------------------------------------------------------------------------------
+__device__ __forceinline__ void frosted_basis(V3 n, V3 &t, V3 &b) {
+    const V3 a = fabsf(n.x) > 0.9f ? v3(0.f, 1.f, 0.f) : v3(1.f, 0.f, 0.f);
+    t = normalize_or_zero(sub(a, mul(n, dot(n, a))));
+    b = cross(n, t);
+}
+
+__device__ __forceinline__ V3 cosine_weighted_hemisphere(float u1, float u2, V3 n) {
+    const float r = sqrtf(u1);
+    const float theta = (2.0f * 3.14159265358979323846f) * u2;
+    const float2 sc = m_sincos(theta);
+    V3 t, b;
+    frosted_basis(n, t, b);
+    return normalize_or_zero(add(add(mul(t, r * sc.y), mul(b, r * sc.x)), mul(n, sqrtf(fmaxf(1.0f - u1, 0.0f)))));
+}
+
+__device__ __forceinline__ V3 sample_hg_direction(float u1, float u2, float g, V3 fwd) {
+    float cos_theta;
+    if (fabsf(g) < 1e-3f) {
+        cos_theta = fmaf(2.0f, -u1, 1.0f);
+    } else {
+        const float one_minus_g2 = fmaf(g, -g, 1.0f);
+        const float denom = fmaf(2.0f * g, u1, 1.0f - g);
+        const float sq = one_minus_g2 / denom;
+        cos_theta = fmaf(sq, -sq, fmaf(g, g, 1.0f)) / (2.0f * g);
+    }
+    cos_theta = clampf(cos_theta, -1.0f, 1.0f);
+    const float sin_theta = sqrtf(fmaxf(fmaf(cos_theta, -cos_theta, 1.0f), 0.0f));
+    const float phi = (2.0f * 3.14159265358979323846f) * u2;
+    const float2 sc = m_sincos(phi);
+    V3 t, b;
+    frosted_basis(fwd, t, b);
+    return normalize_or_zero(add(add(mul(t, sin_theta * sc.y), mul(b, sin_theta * sc.x)), mul(fwd, cos_theta)));
+}
+
+__device__ __forceinline__ bool frosted_facet(const SceneConst &S, int idx) {
+    return S.any_frosted && idx >= 0 && ((S.frosted[idx >> 5] >> (idx & 31)) & 1u);
 }
 
 }  // namespace grd

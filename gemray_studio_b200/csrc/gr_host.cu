@@ -197,10 +197,6 @@ gr_status check_supported(const gr_scene *sc) {
     const gr_material *m = sc->material;
     if (m->dispersion.has_biaxial_delta) return fail(GR_DECLINED_MATERIAL, "biaxial materials are not handled on the device");
     if (m->has_beta_ray) return fail(GR_DECLINED_MATERIAL, "trichroic (beta-ray) absorption is not handled on the device");
-    if (m->scattering_sigma_s > 0.0f) return fail(GR_DECLINED_MATERIAL, "volumetric scattering is not handled on the device");
-    if (sc->finishes)
-        for (uint32_t i = 0; i < sc->n_planes; ++i)
-            if (sc->finishes[i] != 0) return fail(GR_DECLINED_MATERIAL, "frosted facets are not handled on the device");
     return GR_OK;
 }
 
@@ -240,6 +236,15 @@ void encode_scene(const gr_scene *sc, SceneConst &S) {
         S.e_bands[i][2] = m->e_ray_bands[i].peak;
     }
     S.path_scale = m->absorption_path_scale;
+    S.sigma_s = m->scattering_sigma_s;
+    S.hg_g = m->scattering_g;
+    S.any_frosted = 0;
+    if (sc->finishes)
+        for (uint32_t i = 0; i < sc->n_planes; ++i)
+            if (sc->finishes[i] != 0) {
+                S.frosted[i >> 5] |= 1u << (i & 31);
+                S.any_frosted = 1;
+            }
     S.edge_radius = m->edge_rounding_radius;
     tensor_frame(S.c_axis, S.ax0, S.ax1, S.ax2);
     const gr_material_ext *ext = sc->material_ext;
@@ -417,16 +422,25 @@ gr_status launch_trace(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuffers
                        float *xyz, cudaStream_t stream, int mode) {
     if (R.n_tuples == 0) return GR_OK;
     size_t smem = grd::planes_smem_bytes(S.n_planes);
+    const bool extras = S.any_frosted || S.sigma_s > 0.0f;
+    const uint64_t plain_blocks = (R.n_tuples + grd::TRACE_THREADS - 1) / grd::TRACE_THREADS;
     if (S.flags & GR_FLAG_FP64_RESOLVE) {  // the re-solve variant exists for the plain kernel only
-        const uint64_t blocks = (R.n_tuples + grd::TRACE_THREADS - 1) / grd::TRACE_THREADS;
-        grd::k_trace_plain<grd::NoCounters, true><<<(unsigned)blocks, grd::TRACE_THREADS, smem, stream>>>(S, B, R, xyz,
-                                                                                                        nullptr);
+        if (extras)
+            grd::k_trace_plain<grd::NoCounters, true, true><<<(unsigned)plain_blocks, grd::TRACE_THREADS, smem, stream>>>(
+                S, B, R, xyz, nullptr);
+        else
+            grd::k_trace_plain<grd::NoCounters, true><<<(unsigned)plain_blocks, grd::TRACE_THREADS, smem, stream>>>(
+                S, B, R, xyz, nullptr);
         GR_CUDA(cudaGetLastError());
         return GR_OK;
     }
     if (mode == GR_KERNEL_PLAIN || S.max_bounces == 0) {
-        uint64_t blocks = (R.n_tuples + grd::TRACE_THREADS - 1) / grd::TRACE_THREADS;
-        grd::k_trace_plain<grd::NoCounters><<<(unsigned)blocks, grd::TRACE_THREADS, smem, stream>>>(S, B, R, xyz, nullptr);
+        if (extras)
+            grd::k_trace_plain<grd::NoCounters, false, true><<<(unsigned)plain_blocks, grd::TRACE_THREADS, smem, stream>>>(
+                S, B, R, xyz, nullptr);
+        else
+            grd::k_trace_plain<grd::NoCounters><<<(unsigned)plain_blocks, grd::TRACE_THREADS, smem, stream>>>(S, B, R, xyz,
+                                                                                                           nullptr);
         GR_CUDA(cudaGetLastError());
         return GR_OK;
     }
@@ -902,8 +916,12 @@ gr_status gr_event_counts(gr_ctx *ctx, const gr_scene *sc, uint32_t first_pixel,
     unsigned long long *dc = (unsigned long long *)ctx->counter.ptr;
     size_t smem = grd::planes_smem_bytes(S.n_planes);
     uint64_t blocks = (n_tuples + grd::TRACE_THREADS - 1) / grd::TRACE_THREADS;
-    grd::k_trace_plain<grd::Counters><<<(unsigned)blocks, grd::TRACE_THREADS, smem, ctx->stream>>>(
-        S, B, R, (float *)ctx->xyz.ptr, dc + 1);
+    if (S.any_frosted || S.sigma_s > 0.0f)
+        grd::k_trace_plain<grd::Counters, false, true><<<(unsigned)blocks, grd::TRACE_THREADS, smem, ctx->stream>>>(
+            S, B, R, (float *)ctx->xyz.ptr, dc + 1);
+    else
+        grd::k_trace_plain<grd::Counters><<<(unsigned)blocks, grd::TRACE_THREADS, smem, ctx->stream>>>(
+            S, B, R, (float *)ctx->xyz.ptr, dc + 1);
     GR_CUDA(cudaGetLastError());
     unsigned long long host[1 + GR_EVENT_COUNT];
     GR_CUDA(cudaMemcpyAsync(host, dc, sizeof(host), cudaMemcpyDeviceToHost, ctx->stream));

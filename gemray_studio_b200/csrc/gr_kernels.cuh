@@ -10,8 +10,9 @@ namespace grd {
 // Plain kernel: one thread traces one tuple start to finish -- the reference
 // kernel's launch shape (one invocation per (pixel, sample), spectral_transport.wgsl:
 // 672-691).  The Counters variant tallies events for the FLOP model; RESOLVE is the
-// GR_FLAG_FP64_RESOLVE variant (FP64 re-solve of ambiguous exits and TIR decisions).
-template <class CT, bool RESOLVE = false>
+// GR_FLAG_FP64_RESOLVE variant (FP64 re-solve of ambiguous exits and TIR decisions);
+// EXTRAS the variant for scenes with frosted facets or volume scattering.
+template <class CT, bool RESOLVE = false, bool EXTRAS = false>
 __global__ void __launch_bounds__(TRACE_THREADS, GR_TRACE_MIN_BLOCKS) k_trace_plain(SceneConst S, SceneBuffers B, LaunchRange R,
                                                                float *__restrict__ xyz,
                                                                unsigned long long *__restrict__ tallies) {
@@ -28,7 +29,7 @@ __global__ void __launch_bounds__(TRACE_THREADS, GR_TRACE_MIN_BLOCKS) k_trace_pl
         Path P;
         path_init<1>(P, S, B, pixel, sample, (uint32_t)t);
         tally(ct, C_PATHS);
-        V3 c = trace_path<CT, RESOLVE>(P, S, B, PL, ct);
+        V3 c = trace_path<CT, RESOLVE, EXTRAS>(P, S, B, PL, ct);
         xyz[3 * t + 0] = c.x;
         xyz[3 * t + 1] = c.y;
         xyz[3 * t + 2] = c.z;
@@ -101,7 +102,7 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_trace_regen(SceneConst S, Sce
         }
         if (alive) {
             Event E;
-            const uint32_t ev = step_hit<1>(P, S, PL, E, nc);
+            const uint32_t ev = step_hit<1, NoCounters, false, true>(P, S, PL, E, nc);
             if (ev == EV_REFLECT) step_reflect<1>(P, S, E, nc);
             else if (ev == EV_REFRACT) step_refract<1>(P, S, E, nc);
         }

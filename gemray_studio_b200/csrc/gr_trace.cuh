@@ -64,7 +64,9 @@ constexpr uint32_t F_ALIVE = 1u << 4;
 constexpr uint32_t F_TIR = 1u << 5;  // the pending event is a hero TIR
 constexpr uint32_t BOUNCE_SHIFT = 8;
 
-enum EventKind : uint32_t { EV_DONE = 0, EV_REFLECT = 1, EV_REFRACT = 2 };
+// EV_HANDLED: the bounce was completed inside step_hit (a frosted facet or a volume
+// scattering event); the path continues with the next intersection if still alive.
+enum EventKind : uint32_t { EV_DONE = 0, EV_REFLECT = 1, EV_REFRACT = 2, EV_HANDLED = 3 };
 
 __device__ __forceinline__ float &arr(float4 (&a)[2], int k) { return reinterpret_cast<float *>(a)[k]; }
 __device__ __forceinline__ float arr(const float4 (&a)[2], int k) { return reinterpret_cast<const float *>(a)[k]; }
@@ -390,10 +392,115 @@ __device__ __forceinline__ V3 shading_normal(const float4 *planes, uint32_t n, V
     return normalize_or_zero(add(mul(hn, 1.0f - smooth_t), mul(bis, smooth_t)));
 }
 
+// Per-channel pleochroic alpha of the current segment (channel_absorption_alphas,
+// raytracer/absorption.rs:175-216) against plane-of-incidence normal `s_axis`.
+template <int U>
+__device__ __forceinline__ void segment_alphas(const Path &P, const SceneConst &S, V3 s_axis, V3 kk, float alpha[NCH]) {
+    if (!(state_bits(P) & F_ABSORBING)) {
+#pragma unroll
+        for (int k = 0; k < NCH; ++k) alpha[k] = 0.0f;
+        return;
+    }
+    const V3 ea = ordinary_eigen(kk, ld3(S.c_axis));
+    const V3 eb = extraordinary_eigen_from(kk, ea);
+#pragma unroll U
+    for (int k = 0; k < NCH; ++k) {
+        const float4 s4 = P.st[k];
+        const Stokes st{s4.x, s4.y, s4.z, s4.w};
+        const float a_o = arr(P.a_o4, k), a_e = arr(P.a_e4, k);
+        const V3 e_hat = electric_field_direction(st, s_axis, kk);
+        const float p = clampf(dop(st), 0.0f, 1.0f);
+        const float a_pol = quad_form(S, a_o, a_e, e_hat);
+        const float a_unp = midpoint(quad_form(S, a_o, a_e, ea), quad_form(S, a_o, a_e, eb));
+        alpha[k] = fmaf(p, a_pol - a_unp, a_unp);
+    }
+}
+
+// Roulette and the bounce count after a step that does not go through step_post
+// (apply_russian_roulette, transport.rs:204-220, then the loop's next bounce).
+__device__ __forceinline__ void advance_bounce(Path &P, const SceneConst &S) {
+    uint32_t bits = state_bits(P);
+    const uint32_t bounce = bits >> BOUNCE_SHIFT;
+    if (bounce > 4) {
+        float mx = 0.0f;
+#pragma unroll RR_UNROLL
+        for (int k = 0; k < NCH; ++k) mx = fmaxf(mx, fmaxf(P.st[k].x, 0.0f));
+        const float q = clampf(mx, 0.05f, 1.0f);
+        if (rng_draw(p_seed(P), bounce, RUSSIAN_ROULETTE_STREAM) > q) {
+            set_state_bits(P, bits & ~F_ALIVE);
+            return;
+        }
+        const float iq = 1.0f / q;
+#pragma unroll RR_UNROLL
+        for (int k = 0; k < NCH; ++k) {
+            const float4 s4 = P.st[k];
+            P.st[k] = make_float4(s4.x * iq, s4.y * iq, s4.z * iq, s4.w * iq);
+        }
+    }
+    const uint32_t nb = bounce + 1;
+    bits = (bits & ((1u << BOUNCE_SHIFT) - 1u)) | (nb << BOUNCE_SHIFT);
+    if (nb >= S.max_bounces) bits &= ~F_ALIVE;
+    set_state_bits(P, bits);
+}
+
+// maybe_scatter_or_extinguish (raytracer/scattering.rs:132-212) for the interior
+// segment of length t_hit from the path's origin (out of line, like frosted_bounce:
+// rare paths kept out of the transport loop's registers).  Returns true when a scattering
+// event happened (the path moved to the event point with a new direction, and the
+// bounce is complete); false when the segment was crossed, its extinction applied.
+template <int U, class CT>
+__device__ __noinline__ bool scatter_step(Path &P, const SceneConst &S, float t_hit, CT &) {
+    const uint32_t bounce = p_bounce(P);
+    const uint32_t seed = p_seed(P);
+    const V3 kk = xyz(P.k_state);
+    float alpha[NCH];
+    segment_alphas<U>(P, S, xyz(P.prev_tuple), kk, alpha);
+    const float sigma_s = S.sigma_s;
+    const float sigma_t_hero = alpha[0] + sigma_s;  // the hero is channel 0
+    const float omu = fmaxf(1.0f - rng_draw(seed, bounce, DISTANCE_SAMPLE_STREAM), 1e-7f);
+    const float t_free = -(m_log(omu)) / sigma_t_hero;
+    const float hit_scaled = t_hit * S.path_scale;
+    if (t_free < hit_scaled) {
+        const float pdf_hero = sigma_t_hero * omu;
+#pragma unroll U
+        for (int k = 0; k < NCH; ++k) {
+            const float sigma_t_k = alpha[k] + sigma_s;
+            const float tr = exp_poly(-(alpha[k] + sigma_s) * t_free);
+            const float w = tr * sigma_s / pdf_hero;
+            P.st[k] = make_float4(fmaxf(P.st[k].x, 0.0f) * w, 0.0f, 0.0f, 0.0f);
+            arr(P.pdf4, k) = arr(P.pdf4, k) * (sigma_t_k * tr);
+        }
+        const float u1 = rng_draw(seed, bounce, PHASE_DIR_U_STREAM);
+        const float u2 = rng_draw(seed, bounce, PHASE_DIR_V_STREAM);
+        const V3 d = xyz(P.d_seed);
+        const V3 nd = sample_hg_direction(u1, u2, S.hg_g, d);
+        set_xyz(P.o_hero, add(xyz(P.o_hero), smul(t_free / S.path_scale, d)));
+        set_xyz(P.d_seed, nd);
+        set_xyz(P.k_state, nd);
+        set_xyz(P.prev_tuple, v3(0.f, 0.f, 0.f));  // depolarized: no previous plane of incidence
+        advance_bounce(P, S);
+        return true;
+    }
+    float sv[NCH];
+#pragma unroll U
+    for (int k = 0; k < NCH; ++k) sv[k] = exp_poly(-(alpha[k] + sigma_s) * hit_scaled);
+    const float sh = fmaxf(sv[0], 1e-30f);
+#pragma unroll U
+    for (int k = 0; k < NCH; ++k) {
+        const float f = sv[k] / sh;
+        const float4 s4 = P.st[k];
+        P.st[k] = make_float4(s4.x * f, s4.y * f, s4.z * f, s4.w * f);
+        arr(P.pdf4, k) = arr(P.pdf4, k) * sv[k];
+    }
+    return false;
+}
+
 // One intersection and everything of the bounce up to the hero's event decision
 // (transport.rs:781-895, raytracer/absorption.rs:71-141, refraction.rs:428-547,
 // 1036-1060).  Returns EV_DONE on an escape (F_ESCAPED set, F_ALIVE cleared).
-template <int U, class CT, bool R = false>
+// X: the instantiation that handles frosted facets and volume scattering (scenes
+// without either run the X = false code, which has neither branch).
+template <int U, class CT, bool R = false, bool X = false>
 __device__ __forceinline__ uint32_t step_hit(Path &P, const SceneConst &S, const Planes &PL, Event &E, CT &ct) {
     const uint32_t bits = state_bits(P);
     const uint32_t bounce = bits >> BOUNCE_SHIFT;
@@ -407,6 +514,13 @@ __device__ __forceinline__ uint32_t step_hit(Path &P, const SceneConst &S, const
         tally(ct, C_ESCAPES);
         set_state_bits(P, (bits | F_ESCAPED) & ~F_ALIVE);
         return EV_DONE;
+    }
+    bool extinguished = false;  // the segment's extinction was applied by the scattering step
+    if (X && inside && S.sigma_s > 0.0f) {
+        // try_scatter_step / maybe_scatter_or_extinguish (raytracer/scattering.rs:132-315):
+        // a Henyey-Greenstein event along this interior segment, drawn before the facet
+        if (scatter_step<U>(P, S, t_hit, ct)) return EV_HANDLED;
+        extinguished = true;
     }
     V3 hp = add(o, smul(t_hit, d));
     V3 normal = shading_normal(PL.aos, PL.n, hp, fidx, plane_normal(PL.aos, fidx), S.edge_radius);
@@ -432,7 +546,7 @@ __device__ __forceinline__ uint32_t step_hit(Path &P, const SceneConst &S, const
     // apply_interior_segment (transport.rs:586-605) -> apply_absorption (absorption.rs:115-141)
     if (inside) {
         normal = neg(normal);
-        if (bits & F_ABSORBING) {
+        if ((bits & F_ABSORBING) && !extinguished) {
             tally(ct, C_ABSORB);
             V3 c_axis = ld3(S.c_axis);
             V3 ea = ordinary_eigen(kk, c_axis);
@@ -505,6 +619,10 @@ __device__ __forceinline__ uint32_t step_hit(Path &P, const SceneConst &S, const
 
     // dispatch_bounce (transport.rs:158-176): hero TIR, or the Fresnel draw of
     // apply_partial_fresnel_bounce (refraction.rs:1049-1060)
+    if (X && frosted_facet(S, fidx)) {
+        frosted_bounce(P, S, hp, normal, inside, n1, n2, cos_i, sin2_t, ct);
+        return EV_HANDLED;
+    }
     bool tir = sin2_t > 1.0f;
     if (R && fabsf(sin2_t - 1.0f) < 1e-5f) {
         // near the critical angle: decide TIR in FP64 (refraction.rs:428-547 in double)
@@ -565,6 +683,51 @@ __device__ __forceinline__ void step_post(Path &P, const SceneConst &S, V3 hp, V
     bits = (bits & ((1u << BOUNCE_SHIFT) - 1u)) | (nb << BOUNCE_SHIFT);
     if (nb >= S.max_bounces) bits &= ~F_ALIVE;
     set_state_bits(P, bits);
+}
+
+// apply_frosted_bounce (raytracer/scattering.rs:522-602): a Lambertian lobe on either
+// side of the facet, every channel depolarized; the forced (TIR) branch takes no pdf.
+template <class CT>
+__device__ __noinline__ void frosted_bounce(Path &P, const SceneConst &S, V3 hp, V3 normal, bool inside, float n1,
+                                               float n2, float cos_i, float sin2_t, CT &ct) {
+    const uint32_t bits = state_bits(P);
+    const uint32_t bounce = bits >> BOUNCE_SHIFT;
+    const uint32_t seed = p_seed(P);
+    const float u1 = rng_draw(seed, bounce, FROSTED_DIR_U_STREAM);
+    const float u2 = rng_draw(seed, bounce, FROSTED_DIR_V_STREAM);
+    V3 nd;
+    bool new_inside = inside, has_update = false, use_e = false;
+    if (sin2_t > 1.0f) {
+        nd = cosine_weighted_hemisphere(u1, u2, normal);
+#pragma unroll
+        for (int k = 0; k < NCH; ++k) P.st[k] = make_float4(fmaxf(P.st[k].x, 0.0f), 0.0f, 0.0f, 0.0f);
+    } else {
+        const float c_t = sqrtf(fmaxf(1.0f - sin2_t, 0.0f));
+        const float r_s = fmaf(n2, -c_t, n1 * cos_i) / fmaf(n2, c_t, n1 * cos_i);
+        const float r_p = fmaf(n1, -c_t, n2 * cos_i) / fmaf(n1, c_t, n2 * cos_i);
+        const float ru = clampf(0.5f * fmaf(r_p, r_p, r_s * r_s), 1e-4f, 1.0f - 1e-4f);
+        if (rng_draw(seed, bounce, FRESNEL_BRANCH_STREAM) < ru) {
+            nd = cosine_weighted_hemisphere(u1, u2, normal);
+#pragma unroll
+            for (int k = 0; k < NCH; ++k) {
+                P.st[k] = make_float4(fmaxf(P.st[k].x, 0.0f) / ru, 0.0f, 0.0f, 0.0f);
+                arr(P.pdf4, k) = arr(P.pdf4, k) * ru;
+            }
+        } else {
+            nd = cosine_weighted_hemisphere(u1, u2, neg(normal));
+            const bool entering_aniso = !inside && S.anisotropic;
+            use_e = entering_aniso ? rng_draw(seed, bounce, BIREFRINGENT_SPLIT_STREAM) < 0.5f : (bits & F_IS_E) != 0;
+            has_update = entering_aniso;
+            const float tu = 1.0f - ru;
+#pragma unroll
+            for (int k = 0; k < NCH; ++k) {
+                P.st[k] = make_float4(fmaxf(P.st[k].x, 0.0f) / tu, 0.0f, 0.0f, 0.0f);
+                arr(P.pdf4, k) = arr(P.pdf4, k) * tu;
+            }
+            new_inside = !inside;
+        }
+    }
+    step_post(P, S, hp, nd, nd, new_inside, has_update, use_e, ct);
 }
 
 // apply_tir_bounce (refraction.rs:599-637) and apply_partial_reflect_bounce
@@ -721,12 +884,12 @@ __device__ __forceinline__ V3 path_finish(const Path &P, const SceneConst &S, co
 }
 
 // One whole path in the calling thread (the plain kernel's body).
-template <class CT, bool R = false>
+template <class CT, bool R = false, bool X = false>
 __device__ __forceinline__ V3 trace_path(Path &P, const SceneConst &S, const SceneBuffers &B, const Planes &PL,
                                          CT &ct) {
     while (state_bits(P) & F_ALIVE) {
         Event E;
-        uint32_t ev = step_hit<1, CT, R>(P, S, PL, E, ct);
+        uint32_t ev = step_hit<1, CT, R, X>(P, S, PL, E, ct);
         if (ev == EV_REFLECT) step_reflect<1>(P, S, E, ct);
         else if (ev == EV_REFRACT) step_refract<1>(P, S, E, ct);
     }

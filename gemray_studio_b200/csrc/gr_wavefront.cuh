@@ -98,9 +98,11 @@ __global__ void __launch_bounds__(256) k_wf_extend(SceneConst S, SceneBuffers B,
     NoCounters nc;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const uint32_t slot = act[i];
-        const uint32_t ev = step_hit<1>(W.pool[slot], S, PL, W.events[slot], nc);
+        const uint32_t ev = step_hit<1, NoCounters, false, true>(W.pool[slot], S, PL, W.events[slot], nc);
         if (ev == EV_REFLECT) wq_push(W.q_reflect, W.cnt + W_REFL, slot);
         else if (ev == EV_REFRACT) wq_push(W.q_refract, W.cnt + W_REFR, slot);
+        else if (ev == EV_HANDLED && (state_bits(W.pool[slot]) & F_ALIVE))  // frosted / scattered: next round
+            wq_push(active_q(W, cur ^ 1u), W.cnt + (cur ? W_ACT0 : W_ACT1), slot);
         else wq_push(W.q_finish, W.cnt + W_FIN, slot);
     }
 }

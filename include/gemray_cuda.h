@@ -42,7 +42,7 @@ extern "C" {
 typedef enum gr_status {
     GR_OK = 0,
     GR_DECLINED_ENV = 1,      /* environment kind not handled on the device */
-    GR_DECLINED_MATERIAL = 2, /* material/finish kind not handled on the device */
+    GR_DECLINED_MATERIAL = 2, /* biaxial indicatrix or trichroic beta-ray material: not handled on the device */
     GR_NO_DEVICE = 3,         /* no usable CUDA device (GpuAcquireError) */
     GR_EINVAL = 4,            /* bad argument (length mismatch, null pointer, limits) */
     GR_ENOMEM = 5,            /* device or pinned-host allocation failed */
@@ -100,8 +100,9 @@ typedef struct gr_material {
     uint32_t e_ray_band_count;
     gr_band o_ray_bands[GR_MAX_BANDS];
     gr_band e_ray_bands[GR_MAX_BANDS];
-    float scattering_sigma_s;
-    float scattering_g;
+    float scattering_sigma_s;  /* > 0: Henyey-Greenstein volume scattering inside the stone
+                                  (maybe_scatter_or_extinguish, optics/raytracer/scattering.rs:132) */
+    float scattering_g;        /* HG asymmetry, > 0 forward */
     float edge_rounding_radius;
     uint32_t has_beta_ray;
     uint32_t beta_ray_band_count;
@@ -177,7 +178,9 @@ typedef struct gr_scene {
     uint32_t max_bounces;
     uint32_t n_planes;
     const gr_plane *planes;    /* n_planes entries */
-    const uint32_t *finishes;  /* NULL or n_planes entries: 0 = polished, 1 = frosted */
+    const uint32_t *finishes;  /* NULL or n_planes entries: 0 = polished, 1 = frosted (diffuse
+                                  reflect/transmit, apply_frosted_bounce, optics/raytracer/
+                                  scattering.rs:522-602) */
     const gr_material *material;
     const gr_material_ext *material_ext; /* NULL = reference material model */
     gr_environment env;

@@ -41,6 +41,7 @@ template <> struct M<float> {
     static float atan2(float y, float x) { return ::atan2f(y, x); }
     static float acos(float x) { return ::acosf(x); }
     static float exp(float x) { return ::expf(x); }
+    static float log(float x) { return ::logf(x); }
     static float sqrt(float x) { return ::sqrtf(x); }
     static float floor(float x) { return ::floorf(x); }
     static float fma(float a, float b, float c) { return ::fmaf(a, b, c); }
@@ -85,6 +86,7 @@ template <> struct M<double> {
     static double atan2(double y, double x) { return std::atan2(y, x); }
     static double acos(double x) { return std::acos(x); }
     static double exp(double x) { return std::exp(x); }
+    static double log(double x) { return std::log(x); }
     static double sqrt(double x) { return std::sqrt(x); }
     static double floor(double x) { return std::floor(x); }
     static double fma(double a, double b, double c) { return std::fma(a, b, c); }
@@ -161,6 +163,11 @@ static const uint32_t MODE_COUPLING_STREAM = 0xCC9E2D51u;      // sampling.rs:23
 static const uint32_t PIXEL_JITTER_X_ROTATION_STREAM = 0xA511E9B3u; // sampling.rs:111
 static const uint32_t PIXEL_JITTER_Y_ROTATION_STREAM = 0x63D81B23u; // sampling.rs:112
 static const uint32_t HERO_WAVELENGTH_ROTATION_STREAM = 0x1B873593u; // sampling.rs:113
+static const uint32_t FROSTED_DIR_U_STREAM = 0x27D4EB2Fu;    // sampling.rs:28
+static const uint32_t FROSTED_DIR_V_STREAM = 0x165667B1u;    // sampling.rs:29
+static const uint32_t DISTANCE_SAMPLE_STREAM = 0xA24BAED4u;  // sampling.rs:35
+static const uint32_t PHASE_DIR_U_STREAM = 0x9FB21C65u;      // sampling.rs:40
+static const uint32_t PHASE_DIR_V_STREAM = 0x1CE4E5B9u;      // sampling.rs:41
 
 // sampling.rs:45-51
 static inline uint32_t hash_u32(uint32_t x) {
@@ -827,12 +834,10 @@ template <class R> static inline MaterialCtx<R> make_material(const gr_material 
 // materials; the others are declined (the reference's decline => CPU fallback
 // contract, renderer/gpu_backend.rs:27-44).
 static inline bool material_supported(const gr_material *m, const uint32_t *finishes, uint32_t n_planes) {
+    (void)finishes;
+    (void)n_planes;
     if (m->dispersion.has_biaxial_delta) return false;
-    if (m->scattering_sigma_s > 0.0f) return false;
     if (m->has_beta_ray) return false;
-    if (finishes)
-        for (uint32_t i = 0; i < n_planes; ++i)
-            if (finishes[i] != 0) return false;
     return true;
 }
 
@@ -956,6 +961,43 @@ template <class R> static inline R r_unpol_clamped(R rs, R rp) {
     return clampr(R(0.5f) * M<R>::fma(rp, rp, rs * rs), R(1e-4f), R(1) - R(1e-4f));
 }
 
+// ---------------------------------------------------------------------------------
+// Frosted facets and Henyey-Greenstein volume scattering -- raytracer/scattering.rs
+// ---------------------------------------------------------------------------------
+template <class R> static inline void frosted_orthonormal_basis(const V3<R> &n, V3<R> &t, V3<R> &b) {  // :337-342
+    V3<R> a = std::fabs(n.x) > R(0.9f) ? V3<R>(R(0), R(1), R(0)) : V3<R>(R(1), R(0), R(0));
+    t = (a - n * n.dot(a)).normalize_or_zero();
+    b = n.cross(t);
+}
+
+template <class R> static inline V3<R> cosine_weighted_hemisphere(R u1, R u2, const V3<R> &n) {  // :356-362
+    const R r = M<R>::sqrt(u1);
+    const R theta = R(2.0f * 3.14159265358979323846f) * u2;
+    const R sin_t = M<R>::sin(theta), cos_t = M<R>::cos(theta);
+    V3<R> t, b;
+    frosted_orthonormal_basis(n, t, b);
+    return (t * (r * cos_t) + b * (r * sin_t) + n * M<R>::sqrt(rmax(R(1) - u1, R(0)))).normalize_or_zero();
+}
+
+template <class R> static inline V3<R> sample_hg_direction(R u1, R u2, R g, const V3<R> &fwd) {  // :428-443
+    R cos_theta;
+    if (std::fabs(g) < R(1e-3f)) {
+        cos_theta = M<R>::fma(R(2), -u1, R(1));
+    } else {
+        const R one_minus_g2 = M<R>::fma(g, -g, R(1));
+        const R denom = M<R>::fma(R(2) * g, u1, R(1) - g);
+        const R sq = one_minus_g2 / denom;
+        cos_theta = M<R>::fma(sq, -sq, M<R>::fma(g, g, R(1))) / (R(2) * g);
+    }
+    cos_theta = clampr(cos_theta, R(-1), R(1));
+    const R sin_theta = M<R>::sqrt(rmax(M<R>::fma(cos_theta, -cos_theta, R(1)), R(0)));
+    const R phi = R(2.0f * 3.14159265358979323846f) * u2;
+    const R sin_p = M<R>::sin(phi), cos_p = M<R>::cos(phi);
+    V3<R> t, b;
+    frosted_orthonormal_basis(fwd, t, b);
+    return (t * (sin_theta * cos_p) + b * (sin_theta * sin_p) + fwd * cos_theta).normalize_or_zero();
+}
+
 // Optional per-bounce event record (extends trace_spectral_ray_with_finish_instrumented,
 // transport.rs:512-537).
 struct EventLog {
@@ -963,6 +1005,7 @@ struct EventLog {
     uint32_t termination;
     uint32_t n_tir, n_reflect, n_refract, n_inside_abs, n_escape;
     uint32_t n_chan_tir;  // per-channel TIR-phase evaluations
+    uint32_t n_scatter;   // Henyey-Greenstein volume events
     int32_t facets[64];
     uint8_t events[64];
 };
@@ -976,7 +1019,8 @@ struct TraceOpts {
 template <class R>
 static inline V3<R> trace_spectral_ray(const Ray<float> &initial, const gr_plane *planes, uint32_t n_planes,
                                        const MaterialCtx<R> &mc, const EnvCtx<R> &env, uint32_t max_bounces,
-                                       uint32_t rng_seed, float hero_rand, EventLog *log) {
+                                       uint32_t rng_seed, float hero_rand, EventLog *log,
+                                       const uint32_t *finishes = nullptr) {
     R lam[8];
     wrapped_hero_wavelengths<R>(hero_rand, lam);
     Stokes<R> st[8];
@@ -1004,6 +1048,63 @@ static inline V3<R> trace_spectral_ray(const Ray<float> &initial, const gr_plane
             break;
         }
         if (log && bounce < 64) log->facets[bounce] = hit.facet;
+        // try_scatter_step (raytracer/scattering.rs:246-315, maybe_scatter_or_extinguish
+        // :132-212): a Henyey-Greenstein event somewhere along this interior segment,
+        // drawn before the facet is processed; on no event, the segment's extinction
+        // (which then replaces apply_absorption below).
+        if (inside && mat->scattering_sigma_s > 0.0f) {
+            const V3<R> s_axis = have_prev ? prev_plane : V3<R>();
+            const V3<R> ea = ordinary_eigen_polarization(cur_k, mc.c_axis);
+            const V3<R> eb = extraordinary_eigen_polarization(cur_k, mc.c_axis);
+            R alphas[8];
+            for (int k = 0; k < 8; ++k) {
+                V3<R> e_hat = electric_field_direction(st[k], s_axis, cur_k);
+                alphas[k] = effective_pleochroic_alpha(wc.tensor[k], e_hat, ea, eb, st[k].degree_of_polarization());
+            }
+            const R sigma_s = R(mat->scattering_sigma_s);
+            const R sigma_t_hero = alphas[0] + sigma_s;  // the hero is channel 0
+            const R dist_rand = R(rng_draw(rng_seed, bounce, DISTANCE_SAMPLE_STREAM));
+            const R omu = rmax(R(1) - dist_rand, R(1e-7f));
+            const R t_free = -(M<R>::log(omu)) / sigma_t_hero;
+            const R hit_scaled = hit.t * R(mat->absorption_path_scale);
+            if (t_free < hit_scaled) {
+                const R pdf_hero = sigma_t_hero * omu;
+                for (int k = 0; k < 8; ++k) {
+                    const R sigma_t_k = alphas[k] + sigma_s;
+                    const R tr = M<R>::exp_poly(-(alphas[k] + sigma_s) * t_free);
+                    const R w = tr * sigma_s / pdf_hero;
+                    st[k] = Stokes<R>{st[k].intensity() * w, R(0), R(0), R(0)};
+                    pdf[k] = pdf[k] * (sigma_t_k * tr);
+                }
+                const R u1 = R(rng_draw(rng_seed, bounce, PHASE_DIR_U_STREAM));
+                const R u2 = R(rng_draw(rng_seed, bounce, PHASE_DIR_V_STREAM));
+                const V3<R> new_dir = sample_hg_direction(u1, u2, R(mat->scattering_g), ray.dir);
+                ray.origin = ray.origin + (t_free / R(mat->absorption_path_scale)) * ray.dir;
+                ray.dir = new_dir;
+                cur_k = new_dir;
+                have_prev = false;  // depolarized: no previous plane of incidence
+                if (log) log->n_scatter++;
+                if (bounce > 4) {   // apply_russian_roulette (transport.rs:204-220)
+                    R mx = R(0);
+                    for (int k = 0; k < 8; ++k) mx = rmax(mx, st[k].intensity());
+                    R q = clampr(mx, R(0.05f), R(1));
+                    R rr = R(rng_draw(rng_seed, bounce, RUSSIAN_ROULETTE_STREAM));
+                    if (rr > q) {
+                        if (log) { log->bounces = bounce; log->termination = TERM_RUSSIAN_ROULETTE; }
+                        break;
+                    }
+                    for (int k = 0; k < 8; ++k) st[k] = st[k].scale(R(1) / q);
+                }
+                continue;
+            }
+            R sv[8];
+            for (int k = 0; k < 8; ++k) sv[k] = M<R>::exp_poly(-(alphas[k] + sigma_s) * hit_scaled);
+            const R sh = rmax(sv[0], R(1e-30f));
+            for (int k = 0; k < 8; ++k) {
+                st[k] = st[k].scale(sv[k] / sh);
+                pdf[k] = pdf[k] * sv[k];
+            }
+        }
         V3<R> hp = ray.origin + hit.t * ray.dir;
         V3<R> normal = shading_normal_near_edge(planes, n_planes, hp, hit.facet, hit.normal, R(mat->edge_rounding_radius));
 
@@ -1041,11 +1142,50 @@ static inline V3<R> trace_spectral_ray(const Ray<float> &initial, const gr_plane
 
         Geo<R> g = bounce_geometry(mc, wc, normal, cur_k, inside, is_e);
 
-        // dispatch_bounce (transport.rs:128-193), polished facets
+        // dispatch_bounce (transport.rs:128-193)
         V3<R> new_k, new_s;
         bool new_inside = inside;
         bool has_update = false, update_val = false;
-        if (g.sin2_t > R(1)) {
+        if (finishes && finishes[hit.facet] != 0) {
+            // apply_frosted_bounce (raytracer/scattering.rs:522-602): a Lambertian lobe
+            // on either side, depolarizing, no pdf division on the forced (TIR) branch
+            const R u1 = R(rng_draw(rng_seed, bounce, FROSTED_DIR_U_STREAM));
+            const R u2 = R(rng_draw(rng_seed, bounce, FROSTED_DIR_V_STREAM));
+            V3<R> nd;
+            if (g.sin2_t > R(1)) {
+                nd = cosine_weighted_hemisphere(u1, u2, normal);
+                for (int k = 0; k < 8; ++k) st[k] = Stokes<R>{st[k].intensity(), R(0), R(0), R(0)};
+                if (log) { log->n_tir++; if (bounce < 64) log->events[bounce] = EV_TIR; }
+            } else {
+                const R ct = M<R>::sqrt(rmax(R(1) - g.sin2_t, R(0)));
+                const R r_s = M<R>::fma(g.n2, -ct, g.n1 * g.cos_i) / M<R>::fma(g.n2, ct, g.n1 * g.cos_i);
+                const R r_p = M<R>::fma(g.n1, -ct, g.n2 * g.cos_i) / M<R>::fma(g.n1, ct, g.n2 * g.cos_i);
+                const R ru = clampr(R(0.5f) * M<R>::fma(r_p, r_p, r_s * r_s), R(1e-4f), R(1) - R(1e-4f));
+                const R rng_b = R(rng_draw(rng_seed, bounce, FRESNEL_BRANCH_STREAM));
+                if (rng_b < ru) {
+                    nd = cosine_weighted_hemisphere(u1, u2, normal);
+                    for (int k = 0; k < 8; ++k) {
+                        st[k] = Stokes<R>{st[k].intensity() / ru, R(0), R(0), R(0)};
+                        pdf[k] = pdf[k] * ru;
+                    }
+                    if (log) { log->n_reflect++; if (bounce < 64) log->events[bounce] = EV_REFLECT; }
+                } else {
+                    nd = cosine_weighted_hemisphere(u1, u2, -normal);
+                    const bool entering_aniso = !inside && mc.anisotropic;
+                    const bool use_e = entering_aniso ? rng_draw(rng_seed, bounce, BIREFRINGENT_SPLIT_STREAM) < 0.5f : is_e;
+                    const R tu = R(1) - ru;
+                    for (int k = 0; k < 8; ++k) {
+                        st[k] = Stokes<R>{st[k].intensity() / tu, R(0), R(0), R(0)};
+                        pdf[k] = pdf[k] * tu;
+                    }
+                    new_inside = !inside;
+                    if (entering_aniso) { has_update = true; update_val = use_e; }
+                    if (log) { log->n_refract++; if (bounce < 64) log->events[bounce] = EV_REFRACT; }
+                }
+            }
+            new_k = nd;
+            new_s = nd;
+        } else if (g.sin2_t > R(1)) {
             // apply_tir_bounce (refraction.rs:599-637)
             for (int k = 0; k < 8; ++k) {
                 R n1k = g.n1_ch[k], n2k = g.n2_ch[k];

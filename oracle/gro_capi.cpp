@@ -32,7 +32,8 @@ void trace_pixel_samples(const gr_scene &sc, const MaterialCtx<R> &mc, const Env
                                       d.jitter_y);
         EventLog *lg = logs ? &logs[s] : nullptr;
         if (lg) std::memset(lg, 0, sizeof(EventLog));
-        V3<R> xyz = trace_spectral_ray<R>(ray, sc.planes, sc.n_planes, mc, env, sc.max_bounces, d.seed, d.hero_rand, lg);
+        V3<R> xyz = trace_spectral_ray<R>(ray, sc.planes, sc.n_planes, mc, env, sc.max_bounces, d.seed, d.hero_rand, lg,
+                                          sc.finishes);
         if (per_sample) {
             per_sample[3 * s + 0] = (float)xyz.x;
             per_sample[3 * s + 1] = (float)xyz.y;
@@ -154,7 +155,8 @@ float gro_studio_env_spec(const float dir[3], float spec, float spot_mult, float
 float gro_exp_poly(float x) { return M<float>::exp_poly(x); }
 
 // One traced sample with an explicit ray (the golden tests' entry point,
-// trace_spectral_ray, transport.rs:420-454).  precision 32 or 64.
+// trace_spectral_ray / trace_spectral_ray_with_finish, transport.rs:420-454; the
+// scene's finishes, when given, select frosted facets).  precision 32 or 64.
 int gro_trace_ray(const gr_scene *sc, const float origin[3], const float dir[3], uint32_t seed, float hero_rand,
                   uint32_t max_bounces, int precision, double xyz_out[3], uint32_t *bounces, uint32_t *termination) {
     Ray<float> ray;
@@ -165,17 +167,65 @@ int gro_trace_ray(const gr_scene *sc, const float origin[3], const float dir[3],
     if (precision == 64) {
         MaterialCtx<double> mc = make_material<double>(sc->material, sc->material_ext);
         EnvCtx<double> env = make_env<double>(sc->env);
-        V3<double> x = trace_spectral_ray<double>(ray, sc->planes, sc->n_planes, mc, env, max_bounces, seed, hero_rand, &lg);
+        V3<double> x = trace_spectral_ray<double>(ray, sc->planes, sc->n_planes, mc, env, max_bounces, seed, hero_rand, &lg,
+                                                  sc->finishes);
         xyz_out[0] = x.x; xyz_out[1] = x.y; xyz_out[2] = x.z;
     } else {
         MaterialCtx<float> mc = make_material<float>(sc->material, sc->material_ext);
         EnvCtx<float> env = make_env<float>(sc->env);
-        V3<float> x = trace_spectral_ray<float>(ray, sc->planes, sc->n_planes, mc, env, max_bounces, seed, hero_rand, &lg);
+        V3<float> x = trace_spectral_ray<float>(ray, sc->planes, sc->n_planes, mc, env, max_bounces, seed, hero_rand, &lg,
+                                                 sc->finishes);
         xyz_out[0] = x.x; xyz_out[1] = x.y; xyz_out[2] = x.z;
     }
     if (bounces) *bounces = lg.bounces;
     if (termination) *termination = lg.termination;
     return 0;
+}
+
+// The sample loop of the reference's CPU property tests (raytracer_tests.rs:2322-2372,
+// 2411-2460, 2710-2760; scattering.rs scattering_tests): a grid x grid view through the
+// scene's camera at pixel centres, sample s of pixel p seeded hash(p ^ hash(s ^ salt)),
+// hero_rand = hash(seed) / 4294967295, radiance summed in a Vec3 of f32 and divided
+// once by the sample count.  Declined materials return GR_DECLINED_MATERIAL.
+int gro_probe_grid(const gr_scene *sc, uint32_t grid, uint32_t spp, uint32_t salt, uint32_t max_bounces,
+                   float mean_out[3]) {
+    if (!sc || !mean_out || grid == 0 || spp == 0) return GR_EINVAL;
+    if (!material_supported(sc->material, sc->finishes, sc->n_planes)) return GR_DECLINED_MATERIAL;
+    MaterialCtx<float> mc = make_material<float>(sc->material, sc->material_ext);
+    EnvCtx<float> env = make_env<float>(sc->env);
+    const float g = (float)grid;
+    V3<float> sum(0.f, 0.f, 0.f);
+    uint32_t count = 0;
+    for (uint32_t iy = 0; iy < grid; ++iy) {
+        for (uint32_t ix = 0; ix < grid; ++ix) {
+            const Ray<float> ray = generate_ray(sc->camera, (float)ix, (float)iy, g, g, 0.5f, 0.5f);
+            const uint32_t pixel_id = iy * grid + ix;
+            for (uint32_t s = 0; s < spp; ++s) {
+                const uint32_t seed = hash_u32(pixel_id ^ hash_u32(s ^ salt));
+                const float hero = (float)hash_u32(seed) / 4294967295.0f;
+                EventLog lg;
+                std::memset(&lg, 0, sizeof(lg));
+                sum = sum + trace_spectral_ray<float>(ray, sc->planes, sc->n_planes, mc, env, max_bounces, seed, hero,
+                                                      &lg, sc->finishes);
+                ++count;
+            }
+        }
+    }
+    const float c = (float)count;
+    mean_out[0] = sum.x / c; mean_out[1] = sum.y / c; mean_out[2] = sum.z / c;
+    return GR_OK;
+}
+
+// The two direction samplers of the frosted and scattering paths (scattering.rs:
+// 356-362 cosine_weighted_hemisphere, 428-443 sample_henyey_greenstein_direction).
+void gro_cosine_hemisphere(float u1, float u2, const float n[3], float out[3]) {
+    const V3<float> d = cosine_weighted_hemisphere<float>(u1, u2, V3<float>(n[0], n[1], n[2]));
+    out[0] = d.x; out[1] = d.y; out[2] = d.z;
+}
+
+void gro_sample_hg(float u1, float u2, float g, const float fwd[3], float out[3]) {
+    const V3<float> d = sample_hg_direction<float>(u1, u2, g, V3<float>(fwd[0], fwd[1], fwd[2]));
+    out[0] = d.x; out[1] = d.y; out[2] = d.z;
 }
 
 // CPU baseline: the listed rows only; threads claim 16-pixel runs of those rows from

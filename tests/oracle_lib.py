@@ -76,6 +76,12 @@ def lib():
     L.gro_exp_poly.argtypes = [F]
     L.gro_trace_ray.restype = C.c_int
     L.gro_trace_ray.argtypes = [sc, fp, fp, U, F, U, C.c_int, C.POINTER(C.c_double), up, up]
+    L.gro_probe_grid.restype = C.c_int
+    L.gro_probe_grid.argtypes = [sc, U, U, U, U, fp]
+    L.gro_cosine_hemisphere.restype = None
+    L.gro_cosine_hemisphere.argtypes = [F, F, fp, fp]
+    L.gro_sample_hg.restype = None
+    L.gro_sample_hg.argtypes = [F, F, F, fp, fp]
     L.gro_accumulate.restype = C.c_int
     L.gro_accumulate.argtypes = [sc, U, U, fp, C.c_int]
     L.gro_accumulate_f64.restype = C.c_int

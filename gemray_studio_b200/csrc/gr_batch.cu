@@ -32,7 +32,7 @@ struct Launch {
     uint32_t seg_first, seg_count;
     uint64_t blocks, warps;
     uint32_t max_planes;
-    bool extras;  // a segment's scene has frosted facets or scattering
+    bool extras;  // a segment's scene has frosted facets, scattering or a biaxial material
 };
 
 struct Plan {
@@ -110,7 +110,7 @@ gr_status make_plan(gr_ctx *ctx, const grh::BatchItem *items, uint32_t n_items, 
             cur.blocks += (g.R.n_tuples + grd::TRACE_THREADS - 1) / grd::TRACE_THREADS;
             cur.warps += np;
             cur.max_planes = std::max(cur.max_planes, rs->S.n_planes);
-            cur.extras = cur.extras || rs->S.any_frosted || rs->S.sigma_s > 0.0f;
+            cur.extras = cur.extras || grd::needs_extras(rs->S);
             used += g.R.n_tuples;
             next += np;
         }

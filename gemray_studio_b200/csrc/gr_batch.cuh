@@ -67,7 +67,7 @@ __global__ void __launch_bounds__(TRACE_THREADS, GR_TRACE_MIN_BLOCKS)
         uint32_t pixel, sample;
         tuple_coords(R, t, pixel, sample);
         Path P;
-        path_init<1>(P, S, B, pixel, sample, (uint32_t)t);
+        path_init<1, EXTRAS>(P, S, B, pixel, sample, (uint32_t)t);
         NoCounters nc;
         const V3 c = trace_path<NoCounters, false, EXTRAS>(P, S, B, PL, nc);
         float *xyz = G.xyz;

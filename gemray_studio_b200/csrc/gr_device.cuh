@@ -12,6 +12,7 @@
 //     is bit-identical to the reference on every input.
 #pragma once
 
+#include <cfloat>
 #include <cstdint>
 
 #include "gemray_cuda.h"
@@ -54,7 +55,21 @@ struct SceneConst {
     uint32_t any_frosted;
     uint32_t frosted[GR_MAX_PLANES / 32];
     float sigma_s, hg_g;
+    // biaxial indicatrix (optics/birefringence.rs:349-839): per channel n_beta = the
+    // dispersion index, n_alpha = n_beta - d_beta_alpha, n_gamma = n_alpha + bire, in
+    // the frame ax0/ax1/ax2; beta-ray absorption bands (trichroism, biaxial only)
+    uint32_t biaxial;
+    float d_beta_alpha;
+    uint32_t has_beta, n_b_bands;
+    float b_bands[GR_MAX_BANDS][3];
 };
+
+// Scenes that need the extension instantiation of the transport kernels (frosted
+// facets, volume scattering, biaxial materials); every other scene runs the default
+// instantiation, which contains none of that code.
+__host__ __device__ inline bool needs_extras(const SceneConst &S) {
+    return S.any_frosted || S.sigma_s > 0.0f || S.biaxial;
+}
 
 struct SceneBuffers {
     const float4 *planes;      // n_planes
@@ -404,6 +419,166 @@ __device__ __forceinline__ V3 extraordinary_eigen_from(V3 wn, V3 o) { return nor
 __device__ __forceinline__ float quad_form(const SceneConst &S, float a_o, float a_e, V3 e) {
     float l0 = dot(ld3(S.ax0), e), l1 = dot(ld3(S.ax1), e), l2 = dot(ld3(S.ax2), e);
     return (a_o * (l0 * l0) + a_o * (l1 * l1)) + a_e * (l2 * l2);
+}
+// ... and for AbsorptionTensor3::biaxial (:238-245), alpha = (a_o, a_b, a_e).
+__device__ __forceinline__ float quad_form3(const SceneConst &S, float a_o, float a_b, float a_e, V3 e) {
+    float l0 = dot(ld3(S.ax0), e), l1 = dot(ld3(S.ax1), e), l2 = dot(ld3(S.ax2), e);
+    return (a_o * (l0 * l0) + a_b * (l1 * l1)) + a_e * (l2 * l2);
+}
+
+// ---------------------------------------------------------------------------------
+// Biaxial indicatrix -- optics/birefringence.rs:133-170,349-839.  The principal frame
+// is the scene's tensor frame (ax0, ax1, ax2) = (stable_orthonormal_basis(c), c), the
+// construction BiaxialIndicatrix::from_gamma_axis and AbsorptionTensor3 share.
+// ---------------------------------------------------------------------------------
+struct Ind {
+    float na, nb, ng;
+};
+// GemMaterial::biaxial_indicatrix (materials.rs:1508-1519) at the channel whose
+// dispersion index is n_beta.
+__device__ __forceinline__ Ind make_ind(const SceneConst &S, float n_beta) {
+    Ind I;
+    I.nb = n_beta;
+    I.na = n_beta - S.d_beta_alpha;
+    I.ng = I.na + S.bire;
+    return I;
+}
+// axes^T * v and axes * v (glam Mat3::mul_vec3: column sums left to right)
+__device__ __forceinline__ V3 ind_local(const SceneConst &S, V3 v) {
+    return v3(dot(ld3(S.ax0), v), dot(ld3(S.ax1), v), dot(ld3(S.ax2), v));
+}
+__device__ __forceinline__ V3 ind_world(const SceneConst &S, V3 v) {
+    return add(add(mul(ld3(S.ax0), v.x), mul(ld3(S.ax1), v.y)), mul(ld3(S.ax2), v.z));
+}
+// indices_are_degenerate (:508-511)
+__device__ __forceinline__ bool ind_degenerate(float a, float b) {
+    const float scale = fmaxf(fmaxf(fabsf(a), fabsf(b)), 1.0f);
+    return fabsf(a - b) <= sqrtf(FLT_EPSILON) * scale;
+}
+// wave_indices (:435-498): Fresnel's equation of wave normals -> (n_slow, n_fast);
+// degenerate pairs take the uniaxial closed form.
+__device__ __forceinline__ void wave_indices(const SceneConst &S, const Ind &I, V3 wave_normal, float &ns, float &nf) {
+    const V3 k = normalize_or_zero(wave_normal);
+    const bool ab = ind_degenerate(I.na, I.nb), bg = ind_degenerate(I.nb, I.ng);
+    if (ab && bg) {
+        const float n = ((I.na + I.nb) + I.ng) / 3.0f;
+        ns = n;
+        nf = n;
+        return;
+    }
+    if (ab || bg) {
+        const V3 c = ab ? ld3(S.ax2) : ld3(S.ax0);
+        const float n_o = ab ? midpoint(I.na, I.nb) : midpoint(I.nb, I.ng);
+        const float n_e = ab ? I.ng : I.na;
+        const float theta = m_acos(fabsf(clampf(dot(k, c), -1.0f, 1.0f)));
+        const float2 sc = m_sincos(theta);
+        const float n_eff = eff_e_index(n_o, n_e, sc.x, sc.y);
+        ns = fmaxf(n_o, n_eff);
+        nf = fminf(n_o, n_eff);
+        return;
+    }
+    const V3 l = ind_local(S, k);
+    const float a2 = l.x * l.x, b2 = l.y * l.y, g2 = l.z * l.z;
+    const float b1 = 1.0f / (I.na * I.na), b2c = 1.0f / (I.nb * I.nb), b3 = 1.0f / (I.ng * I.ng);
+    const float big_b = fmaf(a2, b2c + b3, fmaf(b2, b1 + b3, g2 * (b1 + b2c)));
+    const float big_c = fmaf(a2, b2c * b3, fmaf(b2, b1 * b3, (g2 * b1) * b2c));
+    const float disc = sqrtf(fmaxf(fmaf(big_b, big_b, -4.0f * big_c), 0.0f));
+    const float x_lo = 0.5f * (big_b - disc);
+    const float x_hi = midpoint(big_b, disc);
+    ns = 1.0f / sqrtf(fmaxf(x_lo, 1e-12f));
+    nf = 1.0f / sqrtf(fmaxf(x_hi, 1e-12f));
+}
+__device__ __forceinline__ V3 cross_fma(V3 a, V3 b) {
+    return v3(fmaf(a.y, b.z, -(a.z * b.y)), fmaf(a.z, b.x, -(a.x * b.z)), fmaf(a.x, b.y, -(a.y * b.x)));
+}
+__device__ __forceinline__ float dot_fma(V3 a, V3 b) { return fmaf(a.x, b.x, fmaf(a.y, b.y, a.z * b.z)); }
+// eigenvector_world (:659-702) with precise_root_near (:717-749): the D direction of
+// the mode whose root is nearest x, in world space, its largest component positive.
+static __device__ __noinline__ V3 eigenvector_world(const SceneConst &S, V3 l, float b0, float b1, float b2, float x_in,
+                                                    V3 k_hat) {
+    const float a = l.x * l.x, bb = l.y * l.y, cc = l.z * l.z;
+    float x;
+    {
+        const float big_b = fmaf(a, b1 + b2, fmaf(bb, b0 + b2, cc * (b0 + b1)));
+        const float xdiff = b0 - b1, ydiff = b2 - b0;
+        const float a_plus_c = a + cc, a_plus_bb = a + bb;
+        const float two_a_minus_bc = 2.0f * fmaf(bb, -cc, a);
+        const float disc_sq = fmaf(a_plus_c * a_plus_c, xdiff * xdiff,
+                                   fmaf(a_plus_bb * a_plus_bb, ydiff * ydiff, (two_a_minus_bc * xdiff) * ydiff));
+        const float disc = sqrtf(fmaxf(disc_sq, 0.0f));
+        const float x_lo = 0.5f * (big_b - disc);
+        const float x_hi = midpoint(big_b, disc);
+        x = fabsf(x_in - x_lo) <= fabsf(x_in - x_hi) ? x_lo : x_hi;
+    }
+    const float s = fmaf(b0, a, fmaf(b1, bb, (b2 * l.z) * l.z));
+    const float m00 = fmaf(a, fmaf(2.0f, -b0, s), b0 - x);
+    const float m11 = fmaf(bb, fmaf(2.0f, -b1, s), b1 - x);
+    const float m22 = fmaf(cc, fmaf(2.0f, -b2, s), b2 - x);
+    const float m01 = (l.x * l.y) * ((s - b0) - b1);
+    const float m02 = (l.x * l.z) * ((s - b0) - b2);
+    const float m12 = (l.y * l.z) * ((s - b1) - b2);
+    const V3 r0 = v3(m00, m01, m02), r1 = v3(m01, m11, m12), r2 = v3(m02, m12, m22);
+    const V3 c01 = cross_fma(r0, r1), c02 = cross_fma(r0, r2), c12 = cross_fma(r1, r2);
+    const float s02 = dot_fma(c01, c02) < 0.0f ? -1.0f : 1.0f;
+    const float s12 = dot_fma(c01, c12) < 0.0f ? -1.0f : 1.0f;
+    const V3 vl = add(add(c01, mul(c02, s02)), mul(c12, s12));
+    const V3 vw = ind_world(S, vl);
+    if (dot(vw, vw) > 1e-12f) {
+        const float ax = fabsf(vw.x), ay = fabsf(vw.y), az = fabsf(vw.z);
+        const float largest = (ax >= ay && ax >= az) ? vw.x : (ay >= az ? vw.y : vw.z);
+        return normalize(largest < 0.0f ? neg(vw) : vw);
+    }
+    return perp_basis_t(k_hat);
+}
+// eigen_polarizations (:542-554): the (slow, fast) D directions
+__device__ __forceinline__ void eigen_pair(const SceneConst &S, const Ind &I, V3 wave_normal, V3 &d_slow, V3 &d_fast) {
+    const V3 k = normalize_or_zero(wave_normal);
+    const V3 l = ind_local(S, k);
+    const float b0 = 1.0f / (I.na * I.na), b1 = 1.0f / (I.nb * I.nb), b2 = 1.0f / (I.ng * I.ng);
+    float ns, nf;
+    wave_indices(S, I, wave_normal, ns, nf);
+    d_slow = eigenvector_world(S, l, b0, b1, b2, 1.0f / (ns * ns), k);
+    d_fast = eigenvector_world(S, l, b0, b1, b2, 1.0f / (nf * nf), k);
+}
+// mode_poynting_dir (:831-836) = poynting_direction(k, d_to_e_direction(D of the mode))
+// (:760-768, :860-870).  Only the requested mode's eigenvector is formed: the two are
+// computed independently, so this is the reference's value.
+static __device__ __noinline__ V3 mode_poynting_dir(const SceneConst &S, Ind I, V3 wave_normal, bool want_slow) {
+    const V3 k = normalize_or_zero(wave_normal);
+    const V3 l = ind_local(S, k);
+    const float b0 = 1.0f / (I.na * I.na), b1 = 1.0f / (I.nb * I.nb), b2 = 1.0f / (I.ng * I.ng);
+    float ns, nf;
+    wave_indices(S, I, wave_normal, ns, nf);
+    const float n = want_slow ? ns : nf;
+    const V3 d = eigenvector_world(S, l, b0, b1, b2, 1.0f / (n * n), k);
+    const V3 dl = ind_local(S, d);
+    const V3 el = v3(dl.x / (I.na * I.na), dl.y / (I.nb * I.nb), dl.z / (I.ng * I.ng));
+    // d_to_e_direction normalizes, and poynting_direction normalizes its input again
+    const V3 e = normalize_or_zero(normalize_or_zero(ind_world(S, el)));
+    const V3 perp = sub(k, mul(e, dot(e, k)));
+    const float len2 = dot(perp, perp);
+    if (len2 > 1e-10f) {
+        const float len = sqrtf(len2);
+        return v3(perp.x / len, perp.y / len, perp.z / len);
+    }
+    return k;
+}
+// resolve_entry_mode (:795-818): two fixed-point steps of the refracted wave normal
+static __device__ __noinline__ V3 resolve_entry_mode(const SceneConst &S, Ind I, V3 incident, V3 normal, float cos_i,
+                                                     float n_seed, bool want_slow) {
+    float n_guess = n_seed;
+    V3 wave_dir = incident;
+    for (int it = 0; it < 2; ++it) {
+        const float eta = 1.0f / n_guess;
+        const float s2 = eta * eta * fmaf(cos_i, -cos_i, 1.0f);
+        if (s2 > 1.0f) break;
+        const float ct = sqrtf(fmaxf(1.0f - s2, 0.0f));
+        wave_dir = normalize(add(smul(eta, incident), smul(fmaf(eta, cos_i, -ct), normal)));
+        float ns, nf;
+        wave_indices(S, I, wave_dir, ns, nf);
+        n_guess = want_slow ? ns : nf;
+    }
+    return wave_dir;
 }
 
 // ---------------------------------------------------------------------------------

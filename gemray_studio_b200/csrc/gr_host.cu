@@ -190,15 +190,6 @@ gr_status validate_scene(const gr_scene *sc) {
     return GR_OK;
 }
 
-// v1 device coverage: polished facets of isotropic / uniaxial, non-scattering
-// materials.  Anything else is declined (GpuFrameError::UnsupportedMaterial
-// semantics: the caller renders it on the CPU tracer).
-gr_status check_supported(const gr_scene *sc) {
-    const gr_material *m = sc->material;
-    if (m->dispersion.has_biaxial_delta) return fail(GR_DECLINED_MATERIAL, "biaxial materials are not handled on the device");
-    if (m->has_beta_ray) return fail(GR_DECLINED_MATERIAL, "trichroic (beta-ray) absorption is not handled on the device");
-    return GR_OK;
-}
 
 void encode_scene(const gr_scene *sc, SceneConst &S) {
     std::memset(&S, 0, sizeof(S));
@@ -255,7 +246,18 @@ void encode_scene(const gr_scene *sc, SceneConst &S) {
         S.has_cauchy_e = ext->has_cauchy_e ? 1u : 0u;
         for (int i = 0; i < 3; ++i) S.cauchy_e[i] = ext->cauchy_e[i];
     }
-    S.absorbing = (S.ext_n > 0 || S.n_o_bands > 0 || S.n_e_bands > 0) ? 1u : 0u;
+    // biaxial indicatrix and the beta-ray band set (read by biaxial materials only,
+    // build_ray_wavelength_cache, refraction.rs:140-166)
+    S.biaxial = m->dispersion.has_biaxial_delta ? 1u : 0u;
+    S.d_beta_alpha = m->dispersion.biaxial_delta_beta_alpha;
+    S.has_beta = (S.biaxial && m->has_beta_ray) ? 1u : 0u;
+    S.n_b_bands = S.has_beta ? m->beta_ray_band_count : 0u;
+    for (uint32_t i = 0; i < GR_MAX_BANDS; ++i) {
+        S.b_bands[i][0] = m->beta_ray_bands[i].center_nm;
+        S.b_bands[i][1] = m->beta_ray_bands[i].width_nm;
+        S.b_bands[i][2] = m->beta_ray_bands[i].peak;
+    }
+    S.absorbing = (S.ext_n > 0 || S.n_o_bands > 0 || S.n_e_bands > 0 || S.n_b_bands > 0) ? 1u : 0u;
     S.env_mode = sc->env.mode;
     for (int i = 0; i < 3; ++i) S.uni_rgb[i] = sc->env.uniform_rgb[i];
     S.temp_k = sc->env.temp_k;
@@ -422,7 +424,7 @@ gr_status launch_trace(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuffers
                        float *xyz, cudaStream_t stream, int mode) {
     if (R.n_tuples == 0) return GR_OK;
     size_t smem = grd::planes_smem_bytes(S.n_planes);
-    const bool extras = S.any_frosted || S.sigma_s > 0.0f;
+    const bool extras = grd::needs_extras(S);
     const uint64_t plain_blocks = (R.n_tuples + grd::TRACE_THREADS - 1) / grd::TRACE_THREADS;
     if (S.flags & GR_FLAG_FP64_RESOLVE) {  // the re-solve variant exists for the plain kernel only
         if (extras)
@@ -519,8 +521,6 @@ gr_status render_into(gr_ctx *ctx, const gr_scene *sc, const SceneConst &S, cons
 
 gr_status prepare(gr_ctx *ctx, const gr_scene *sc, SceneConst &S, grd::SceneBuffers &B) {
     gr_status st = validate_scene(sc);
-    if (st != GR_OK) return st;
-    st = check_supported(sc);
     if (st != GR_OK) return st;
     encode_scene(sc, S);
     return upload_scene(ctx, sc, S, B);
@@ -766,8 +766,6 @@ gr_status gr_scene_upload(gr_ctx *ctx, const gr_scene *sc, uint64_t *out_id) {
     if (!ctx || !out_id) return fail(GR_EINVAL, "ctx or out_id is NULL");
     gr_status st = grh::validate_scene(sc);
     if (st != GR_OK) return st;
-    st = grh::check_supported(sc);
-    if (st != GR_OK) return st;
     std::lock_guard<std::mutex> lk(ctx->mu);
     GR_CUDA(cudaSetDevice(ctx->device));
     ResidentScene *rs = new ResidentScene();
@@ -916,7 +914,7 @@ gr_status gr_event_counts(gr_ctx *ctx, const gr_scene *sc, uint32_t first_pixel,
     unsigned long long *dc = (unsigned long long *)ctx->counter.ptr;
     size_t smem = grd::planes_smem_bytes(S.n_planes);
     uint64_t blocks = (n_tuples + grd::TRACE_THREADS - 1) / grd::TRACE_THREADS;
-    if (S.any_frosted || S.sigma_s > 0.0f)
+    if (grd::needs_extras(S))
         grd::k_trace_plain<grd::Counters, false, true><<<(unsigned)blocks, grd::TRACE_THREADS, smem, ctx->stream>>>(
             S, B, R, (float *)ctx->xyz.ptr, dc + 1);
     else

@@ -11,7 +11,8 @@ namespace grd {
 // kernel's launch shape (one invocation per (pixel, sample), spectral_transport.wgsl:
 // 672-691).  The Counters variant tallies events for the FLOP model; RESOLVE is the
 // GR_FLAG_FP64_RESOLVE variant (FP64 re-solve of ambiguous exits and TIR decisions);
-// EXTRAS the variant for scenes with frosted facets or volume scattering.
+// EXTRAS the variant for scenes with frosted facets, volume scattering or a biaxial
+// material.
 template <class CT, bool RESOLVE = false, bool EXTRAS = false>
 __global__ void __launch_bounds__(TRACE_THREADS, GR_TRACE_MIN_BLOCKS) k_trace_plain(SceneConst S, SceneBuffers B, LaunchRange R,
                                                                float *__restrict__ xyz,
@@ -27,7 +28,7 @@ __global__ void __launch_bounds__(TRACE_THREADS, GR_TRACE_MIN_BLOCKS) k_trace_pl
         uint32_t pixel, sample;
         tuple_coords(R, t, pixel, sample);
         Path P;
-        path_init<1>(P, S, B, pixel, sample, (uint32_t)t);
+        path_init<1, EXTRAS>(P, S, B, pixel, sample, (uint32_t)t);
         tally(ct, C_PATHS);
         V3 c = trace_path<CT, RESOLVE, EXTRAS>(P, S, B, PL, ct);
         xyz[3 * t + 0] = c.x;
@@ -93,7 +94,7 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_trace_regen(SceneConst S, Sce
                 if (have) {
                     uint32_t pixel, sample;
                     tuple_coords(R, t, pixel, sample);
-                    path_init<1>(P, S, B, pixel, sample, (uint32_t)t);
+                    path_init<1, true>(P, S, B, pixel, sample, (uint32_t)t);
                 }
             }
             next += n_idle;
@@ -103,8 +104,8 @@ __global__ void __launch_bounds__(TRACE_THREADS) k_trace_regen(SceneConst S, Sce
         if (alive) {
             Event E;
             const uint32_t ev = step_hit<1, NoCounters, false, true>(P, S, PL, E, nc);
-            if (ev == EV_REFLECT) step_reflect<1>(P, S, E, nc);
-            else if (ev == EV_REFRACT) step_refract<1>(P, S, E, nc);
+            if (ev == EV_REFLECT) step_reflect<1, NoCounters, true>(P, S, E, nc);
+            else if (ev == EV_REFRACT) step_refract<1, NoCounters, true>(P, S, E, nc);
         }
     }
 }

@@ -43,7 +43,7 @@ struct __align__(16) Path {
     float4 st[NCH];     // Stokes (I, Q, U, V) per channel
     float4 pdf4[2];     // spectral-MIS path pdf per channel
     float4 n_o4[2];     // ordinary index per channel
-    float4 ne_d4[2];    // n_e - n_o per channel
+    float4 ne_d4[2];    // n_e - n_o per channel (biaxial materials: beta-ray absorption coefficient)
     float4 a_o4[2];     // ordinary absorption coefficient per channel
     float4 a_e4[2];     // extraordinary absorption coefficient per channel
 };
@@ -95,7 +95,10 @@ template <> __device__ __forceinline__ void tally<Counters>(Counters &ct, int i,
 
 // Build the path of tuple (pixel, sample): sampler draws (sampling.rs:232-271),
 // camera ray (camera.rs:95-114), per-sample wavelength cache (refraction.rs:127-174).
-template <int U = 1>
+// X: the extension instantiation (biaxial materials keep their beta-ray coefficient,
+// or the ordinary one when the material has no third band set, where uniaxial ones
+// keep n_e - n_o, which no biaxial step reads).
+template <int U = 1, bool X = false>
 __device__ __forceinline__ void path_init(Path &P, const SceneConst &S, const SceneBuffers &B, uint32_t pixel,
                                           uint32_t sample, uint32_t tuple) {
     Draws dr = sample_draws(pixel, sample);
@@ -136,6 +139,11 @@ __device__ __forceinline__ void path_init(Path &P, const SceneConst &S, const Sc
         arr(P.a_o4, k) = ao;
         arr(P.a_e4, k) = ae;
         any = any || (ao != 0.0f) || (ae != 0.0f);
+        if (X && S.biaxial) {
+            const float ab = (S.absorbing && S.has_beta) ? band_sum(S.b_bands, S.n_b_bands, lam) : ao;
+            arr(P.ne_d4, k) = ab;
+            any = any || (ab != 0.0f);
+        }
     }
     // Every alpha exactly zero makes the Beer-Lambert factor exp_poly(-0) == 1.0 for
     // every channel, so skipping the absorption step is bit-identical.
@@ -394,25 +402,51 @@ __device__ __forceinline__ V3 shading_normal(const float4 *planes, uint32_t n, V
 
 // Per-channel pleochroic alpha of the current segment (channel_absorption_alphas,
 // raytracer/absorption.rs:175-216) against plane-of-incidence normal `s_axis`.
-template <int U>
+// The eigenmode pair of channel_absorption_alphas (raytracer/absorption.rs:175-196):
+// the hero indicatrix's (slow, fast) D directions for a biaxial material (X only),
+// else the uniaxial ordinary / extraordinary pair.
+template <bool X>
+__device__ __forceinline__ void absorption_eigenmodes(const Path &P, const SceneConst &S, V3 kk, V3 &ea, V3 &eb) {
+    if (X && S.biaxial) {
+        eigen_pair(S, make_ind(S, arr(P.n_o4, 0)), kk, ea, eb);
+    } else {
+        ea = ordinary_eigen(kk, ld3(S.c_axis));
+        eb = extraordinary_eigen_from(kk, ea);
+    }
+}
+// effective_pleochroic_alpha (optics/birefringence.rs:272-286) of channel k against the
+// tensor the wavelength cache built for it (uniaxial, or biaxial with a beta band set).
+template <bool X>
+__device__ __forceinline__ float channel_alpha(const Path &P, const SceneConst &S, int k, const Stokes &st, V3 e_hat,
+                                               V3 ea, V3 eb) {
+    const float a_o = arr(P.a_o4, k), a_e = arr(P.a_e4, k);
+    const float p = clampf(dop(st), 0.0f, 1.0f);
+    if (X && S.biaxial) {
+        const float a_b = arr(P.ne_d4, k);
+        const float a_pol = quad_form3(S, a_o, a_b, a_e, e_hat);
+        const float a_unp = midpoint(quad_form3(S, a_o, a_b, a_e, ea), quad_form3(S, a_o, a_b, a_e, eb));
+        return fmaf(p, a_pol - a_unp, a_unp);
+    }
+    const float a_pol = quad_form(S, a_o, a_e, e_hat);
+    const float a_unp = midpoint(quad_form(S, a_o, a_e, ea), quad_form(S, a_o, a_e, eb));
+    return fmaf(p, a_pol - a_unp, a_unp);
+}
+
+template <int U, bool X = false>
 __device__ __forceinline__ void segment_alphas(const Path &P, const SceneConst &S, V3 s_axis, V3 kk, float alpha[NCH]) {
     if (!(state_bits(P) & F_ABSORBING)) {
 #pragma unroll
         for (int k = 0; k < NCH; ++k) alpha[k] = 0.0f;
         return;
     }
-    const V3 ea = ordinary_eigen(kk, ld3(S.c_axis));
-    const V3 eb = extraordinary_eigen_from(kk, ea);
+    V3 ea, eb;
+    absorption_eigenmodes<X>(P, S, kk, ea, eb);
 #pragma unroll U
     for (int k = 0; k < NCH; ++k) {
         const float4 s4 = P.st[k];
         const Stokes st{s4.x, s4.y, s4.z, s4.w};
-        const float a_o = arr(P.a_o4, k), a_e = arr(P.a_e4, k);
         const V3 e_hat = electric_field_direction(st, s_axis, kk);
-        const float p = clampf(dop(st), 0.0f, 1.0f);
-        const float a_pol = quad_form(S, a_o, a_e, e_hat);
-        const float a_unp = midpoint(quad_form(S, a_o, a_e, ea), quad_form(S, a_o, a_e, eb));
-        alpha[k] = fmaf(p, a_pol - a_unp, a_unp);
+        alpha[k] = channel_alpha<X>(P, S, k, st, e_hat, ea, eb);
     }
 }
 
@@ -454,7 +488,7 @@ __device__ __noinline__ bool scatter_step(Path &P, const SceneConst &S, float t_
     const uint32_t seed = p_seed(P);
     const V3 kk = xyz(P.k_state);
     float alpha[NCH];
-    segment_alphas<U>(P, S, xyz(P.prev_tuple), kk, alpha);
+    segment_alphas<U, true>(P, S, xyz(P.prev_tuple), kk, alpha);
     const float sigma_s = S.sigma_s;
     const float sigma_t_hero = alpha[0] + sigma_s;  // the hero is channel 0
     const float omu = fmaxf(1.0f - rng_draw(seed, bounce, DISTANCE_SAMPLE_STREAM), 1e-7f);
@@ -495,11 +529,42 @@ __device__ __noinline__ bool scatter_step(Path &P, const SceneConst &S, float t_
     return false;
 }
 
+// hero_biaxial_wave_dirs + per_channel_biaxial_indices (refraction.rs:345-401) with the
+// medium choice of compute_bounce_refraction_geometry (:509-520): each channel's slow
+// (mode B) index at the hero's slow wave normal -- the ray's own inside the stone, the
+// resolved refracted one (resolve_entry_mode) outside -- or, for the fast mode inside
+// (use_a), its fast (mode A) index.
+static __device__ __noinline__ void biaxial_media(const Path &P, const SceneConst &S, V3 kk, V3 normal, float cos_i,
+                                                  bool inside, bool use_a, Event &E) {
+    const float n0 = arr(P.n_o4, 0);
+    const V3 dir = inside ? kk : resolve_entry_mode(S, make_ind(S, n0), kk, normal, cos_i, n0, true);
+#pragma unroll 1
+    for (int k = 0; k < NCH; ++k) {
+        float ns, nf;
+        wave_indices(S, make_ind(S, arr(P.n_o4, k)), dir, ns, nf);
+        arr(E.n_med4, k) = use_a ? nf : ns;
+    }
+}
+// The mode-A (fast) indices at the hero's resolved fast wave normal, for a fast-mode
+// biaxial entry (n_biax_a_ch, refraction.rs:381-401).
+static __device__ __noinline__ void biaxial_fast_entry(const Path &P, const SceneConst &S, V3 kk, V3 normal,
+                                                       float cos_i, Event &E) {
+    const float n0 = arr(P.n_o4, 0);
+    const V3 dir = resolve_entry_mode(S, make_ind(S, n0), kk, normal, cos_i, n0, false);
+#pragma unroll 1
+    for (int k = 0; k < NCH; ++k) {
+        float ns, nf;
+        wave_indices(S, make_ind(S, arr(P.n_o4, k)), dir, ns, nf);
+        arr(E.n_med4, k) = nf;
+    }
+}
+
 // One intersection and everything of the bounce up to the hero's event decision
 // (transport.rs:781-895, raytracer/absorption.rs:71-141, refraction.rs:428-547,
 // 1036-1060).  Returns EV_DONE on an escape (F_ESCAPED set, F_ALIVE cleared).
-// X: the instantiation that handles frosted facets and volume scattering (scenes
-// without either run the X = false code, which has neither branch).
+// X: the instantiation that handles frosted facets, volume scattering and biaxial
+// materials (scenes without any of them run the X = false code, which has none of
+// those branches).
 template <int U, class CT, bool R = false, bool X = false>
 __device__ __forceinline__ uint32_t step_hit(Path &P, const SceneConst &S, const Planes &PL, Event &E, CT &ct) {
     const uint32_t bits = state_bits(P);
@@ -548,9 +613,8 @@ __device__ __forceinline__ uint32_t step_hit(Path &P, const SceneConst &S, const
         normal = neg(normal);
         if ((bits & F_ABSORBING) && !extinguished) {
             tally(ct, C_ABSORB);
-            V3 c_axis = ld3(S.c_axis);
-            V3 ea = ordinary_eigen(kk, c_axis);
-            V3 eb = extraordinary_eigen_from(kk, ea);
+            V3 ea, eb;
+            absorption_eigenmodes<X>(P, S, kk, ea, eb);
             float scaled = t_hit * S.path_scale;
             // Every channel's alpha reads that channel's Stokes vector before it is
             // scaled, so computing and applying per channel is the reference's
@@ -559,12 +623,8 @@ __device__ __forceinline__ uint32_t step_hit(Path &P, const SceneConst &S, const
             for (int k = 0; k < NCH; ++k) {
                 float4 s4 = P.st[k];
                 Stokes s{s4.x, s4.y, s4.z, s4.w};
-                float a_o = arr(P.a_o4, k), a_e = arr(P.a_e4, k);
                 V3 e_hat = electric_field_direction(s, cur_plane, kk);
-                float p = clampf(dop(s), 0.0f, 1.0f);
-                float a_pol = quad_form(S, a_o, a_e, e_hat);
-                float a_unp = midpoint(quad_form(S, a_o, a_e, ea), quad_form(S, a_o, a_e, eb));
-                float alpha = fmaf(p, a_pol - a_unp, a_unp);
+                float alpha = channel_alpha<X>(P, S, k, s, e_hat, ea, eb);
                 Stokes r = scale(s, exp_poly(-alpha * scaled));
                 P.st[k] = make_float4(r.i, r.q, r.u, r.v);
             }
@@ -576,7 +636,10 @@ __device__ __forceinline__ uint32_t step_hit(Path &P, const SceneConst &S, const
     float cos_i = clampf(dot(neg(kk), normal), 0.0f, 1.0f);
     float one_m_c2 = fmaf(cos_i, -cos_i, 1.0f);
     float n_o_hero = arr(P.n_o4, 0);
-    if (aniso) {
+    if (X && S.biaxial) {
+        if (aniso) tally(ct, C_ANISO_BOUNCES);
+        biaxial_media(P, S, kk, normal, cos_i, inside, aniso && inside && !(bits & F_IS_E), E);
+    } else if (aniso) {
         tally(ct, C_ANISO_BOUNCES);
         float n_e_hero = n_o_hero + arr(P.ne_d4, 0);
         V3 c_axis = ld3(S.c_axis);
@@ -641,7 +704,13 @@ __device__ __forceinline__ uint32_t step_hit(Path &P, const SceneConst &S, const
     float ru = r_unpol(rs, rp);
     E.n_ru = make_float4(normal.x, normal.y, normal.z, ru);
     set_state_bits(P, bits & ~F_TIR);
-    return rng_draw(p_seed(P), bounce, FRESNEL_BRANCH_STREAM) < ru ? EV_REFLECT : EV_REFRACT;
+    const bool refract = !(rng_draw(p_seed(P), bounce, FRESNEL_BRANCH_STREAM) < ru);
+    // a biaxial entry in the fast mode (the split draw of apply_refract_bounce,
+    // refraction.rs:781-789) refracts with the mode-A indices
+    if (X && S.biaxial && refract && !inside && aniso &&
+        !(rng_draw(p_seed(P), bounce, BIREFRINGENT_SPLIT_STREAM) < 0.5f))
+        biaxial_fast_entry(P, S, kk, normal, cos_i, E);
+    return refract ? EV_REFRACT : EV_REFLECT;
 }
 
 // Direction / state update after an event, internal mode coupling and Russian
@@ -732,7 +801,7 @@ __device__ __noinline__ void frosted_bounce(Path &P, const SceneConst &S, V3 hp,
 
 // apply_tir_bounce (refraction.rs:599-637) and apply_partial_reflect_bounce
 // (refraction.rs:650-690) in one channel loop.
-template <int U, class CT>
+template <int U, class CT, bool X = false>
 __device__ __forceinline__ void step_reflect(Path &P, const SceneConst &S, const Event &E, CT &ct) {
     const uint32_t bits = state_bits(P);
     const bool inside = (bits & F_INSIDE) != 0;
@@ -768,8 +837,11 @@ __device__ __forceinline__ void step_reflect(Path &P, const SceneConst &S, const
         P.st[k] = make_float4(s.i, s.q, s.u, s.v);
     }
     V3 new_k = sub(kk, smul(2.0f * dot(kk, normal), normal));
+    // poynting_dir_for_mode (refraction.rs:564-582): both biaxial modes walk off
     V3 new_s = new_k;
-    if (inside && S.anisotropic && (bits & F_IS_E)) {
+    if (X && S.biaxial) {
+        if (inside && S.anisotropic) new_s = mode_poynting_dir(S, make_ind(S, arr(P.n_o4, 0)), new_k, (bits & F_IS_E) != 0);
+    } else if (inside && S.anisotropic && (bits & F_IS_E)) {
         float n_o_hero = arr(P.n_o4, 0);
         new_s = extraordinary_poynting_dir(new_k, ld3(S.c_axis), n_o_hero, n_o_hero + arr(P.ne_d4, 0));
     }
@@ -777,7 +849,7 @@ __device__ __forceinline__ void step_reflect(Path &P, const SceneConst &S, const
 }
 
 // apply_refract_bounce (refraction.rs:748-867) + apply_refract_channel (:883-1011)
-template <int U, class CT>
+template <int U, class CT, bool X = false>
 __device__ __forceinline__ void step_refract(Path &P, const SceneConst &S, const Event &E, CT &ct) {
     const uint32_t bits = state_bits(P);
     const uint32_t bounce = bits >> BOUNCE_SHIFT;
@@ -795,15 +867,19 @@ __device__ __forceinline__ void step_refract(Path &P, const SceneConst &S, const
     const bool entering_aniso = !inside && aniso;
     bool use_e = (bits & F_IS_E) != 0;
     if (entering_aniso) use_e = rng_draw(p_seed(P), bounce, BIREFRINGENT_SPLIT_STREAM) < 0.5f;
-    const bool ordinary_entry = entering_aniso && !use_e;
-    const bool extra_entry = entering_aniso && use_e;
+    // A biaxial entry (X only) refracts with the selected mode's indices, which step_hit
+    // left in n_med4, and both of its modes walk off (refraction.rs:791-806,929-950).
+    const bool biax_entry = X && S.biaxial && entering_aniso;
+    const bool ordinary_entry = entering_aniso && !use_e && !biax_entry;
+    const bool extra_entry = entering_aniso && use_e && !biax_entry;
     const float n2_dir = ordinary_entry ? n_o_hero : n2;
     const float eta_dir = n1 / n2_dir;
     const float s2d = fminf(eta_dir * eta_dir * one_m_c2, 1.0f);
     const float ctd = sqrtf(fmaxf(1.0f - s2d, 0.0f));
     const V3 refr = normalize(add(smul(eta_dir, kk), smul(fmaf(eta_dir, cos_i, -ctd), normal)));
     const V3 c_axis = ld3(S.c_axis);
-    const V3 final_dir = extra_entry ? extraordinary_poynting_dir(refr, c_axis, n_o_hero, n_e_hero) : refr;
+    V3 final_dir = extra_entry ? extraordinary_poynting_dir(refr, c_axis, n_o_hero, n_e_hero) : refr;
+    if (biax_entry) final_dir = mode_poynting_dir(S, make_ind(S, n_o_hero), refr, use_e);
     if (extra_entry) tally(ct, C_WALKOFF, 9);
     const float tinv = 1.0f / (1.0f - ru);
     const float TOL = 1.0f - 1e-6f;
@@ -823,6 +899,7 @@ __device__ __forceinline__ void step_refract(Path &P, const SceneConst &S, const
             ctk = sqrtf(fmaxf(1.0f - s2k, 0.0f));
             V3 rk = normalize(add(smul(ratio, kk), smul(fmaf(ratio, cos_i, -ctk), normal)));
             V3 fk = extra_entry ? extraordinary_poynting_dir(rk, c_axis, n_o_k, n_o_k + arr(P.ne_d4, k)) : rk;
+            if (biax_entry) fk = mode_poynting_dir(S, make_ind(S, n_o_k), rk, use_e);
             keep = dot(fk, final_dir) >= TOL;
         }
         if (keep) {
@@ -890,8 +967,8 @@ __device__ __forceinline__ V3 trace_path(Path &P, const SceneConst &S, const Sce
     while (state_bits(P) & F_ALIVE) {
         Event E;
         uint32_t ev = step_hit<1, CT, R, X>(P, S, PL, E, ct);
-        if (ev == EV_REFLECT) step_reflect<1>(P, S, E, ct);
-        else if (ev == EV_REFRACT) step_refract<1>(P, S, E, ct);
+        if (ev == EV_REFLECT) step_reflect<1, CT, X>(P, S, E, ct);
+        else if (ev == EV_REFRACT) step_refract<1, CT, X>(P, S, E, ct);
     }
     return path_finish<1>(P, S, B);
 }

@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(256) k_wf_regen(SceneConst S, SceneBuffers B, 
         const uint64_t t = t0 + i;
         uint32_t pixel, sample;
         tuple_coords(R, t, pixel, sample);
-        path_init<1>(W.pool[slot], S, B, pixel, sample, (uint32_t)t);
+        path_init<1, true>(W.pool[slot], S, B, pixel, sample, (uint32_t)t);
         wq_push(act, W.cnt + (cur ? W_ACT1 : W_ACT0), slot);
     }
 }
@@ -117,8 +117,8 @@ __global__ void __launch_bounds__(256) k_wf_event(SceneConst S, WaveBuffers W, u
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const uint32_t slot = q[i];
         Path &P = W.pool[slot];
-        if (REFRACT) step_refract<1>(P, S, W.events[slot], nc);
-        else step_reflect<1>(P, S, W.events[slot], nc);
+        if (REFRACT) step_refract<1, NoCounters, true>(P, S, W.events[slot], nc);
+        else step_reflect<1, NoCounters, true>(P, S, W.events[slot], nc);
         if (state_bits(P) & F_ALIVE) wq_push(act, W.cnt + (nxt ? W_ACT1 : W_ACT0), slot);
         else wq_push(W.q_finish, W.cnt + W_FIN, slot);
     }

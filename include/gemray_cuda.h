@@ -38,11 +38,13 @@ extern "C" {
 
 /* Status codes.  GR_DECLINED_* mirror GpuFrameError (renderer/gpu/frame.rs:196-210):
  * they mean "render this on the CPU tracer instead", exactly like a `false` from
- * GpuBackend::try_accumulate (renderer/gpu_backend.rs:160-193). */
+ * GpuBackend::try_accumulate (renderer/gpu_backend.rs:160-193).  Every environment
+ * kind and material kind of the reference's render path is handled on the device, so
+ * neither is returned at present; they stay part of the contract. */
 typedef enum gr_status {
     GR_OK = 0,
     GR_DECLINED_ENV = 1,      /* environment kind not handled on the device */
-    GR_DECLINED_MATERIAL = 2, /* biaxial indicatrix or trichroic beta-ray material: not handled on the device */
+    GR_DECLINED_MATERIAL = 2, /* material kind not handled on the device */
     GR_NO_DEVICE = 3,         /* no usable CUDA device (GpuAcquireError) */
     GR_EINVAL = 4,            /* bad argument (length mismatch, null pointer, limits) */
     GR_ENOMEM = 5,            /* device or pinned-host allocation failed */

@@ -20,6 +20,7 @@
 // Mat4::mul_vec4 is ((c0*x + c1*y) + c2*z) + c3*w per row.
 #pragma once
 
+#include <cfloat>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -498,6 +499,176 @@ static inline R effective_pleochroic_alpha(const Tensor3<R> &t, const V3<R> &e, 
 }
 
 // ---------------------------------------------------------------------------------
+// Biaxial indicatrix -- optics/birefringence.rs:133-170,349-839 (BiaxialIndicatrix),
+// optics/materials.rs:1508-1519 (GemMaterial::biaxial_indicatrix)
+// ---------------------------------------------------------------------------------
+// Principal indices n_alpha <= n_beta <= n_gamma along the frame (ax0, ax1, ax2) =
+// (stable_orthonormal_basis(c), c) -- the same frame as AbsorptionTensor3.
+template <class R> struct Indicatrix { R na, nb, ng; V3<R> ax0, ax1, ax2; };
+
+// biaxial_indicatrix (materials.rs:1508-1519) + from_gamma_axis (birefringence.rs:391-396):
+// n_beta = dispersion(lambda), n_alpha = n_beta - delta_beta_alpha, n_gamma = n_alpha + birefringence.
+template <class R> static inline Indicatrix<R> make_indicatrix(R n_beta, R d_beta_alpha, R bire, const V3<R> &c_axis) {
+    Indicatrix<R> I;
+    I.nb = n_beta;
+    I.na = n_beta - d_beta_alpha;
+    I.ng = I.na + bire;
+    const V3<R> g = c_axis.normalize_or_zero();
+    stable_orthonormal_basis(g, I.ax0, I.ax1);
+    I.ax2 = g;
+    return I;
+}
+// axes^T * v and axes * v (glam Mat3 mul_vec3: column sums, left to right)
+template <class R> static inline V3<R> ind_local(const Indicatrix<R> &I, const V3<R> &v) {
+    return V3<R>(I.ax0.dot(v), I.ax1.dot(v), I.ax2.dot(v));
+}
+template <class R> static inline V3<R> ind_world(const Indicatrix<R> &I, const V3<R> &v) {
+    return (I.ax0 * v.x + I.ax1 * v.y) + I.ax2 * v.z;
+}
+// cross_fma / dot_fma / canonicalize_eigenvector_sign (birefringence.rs:139-170)
+template <class R> static inline V3<R> cross_fma(const V3<R> &a, const V3<R> &b) {
+    return V3<R>(M<R>::fma(a.y, b.z, -(a.z * b.y)), M<R>::fma(a.z, b.x, -(a.x * b.z)), M<R>::fma(a.x, b.y, -(a.y * b.x)));
+}
+template <class R> static inline R dot_fma(const V3<R> &a, const V3<R> &b) {
+    return M<R>::fma(a.x, b.x, M<R>::fma(a.y, b.y, a.z * b.z));
+}
+template <class R> static inline V3<R> canonicalize_sign(const V3<R> &v) {
+    const R ax = std::fabs(v.x), ay = std::fabs(v.y), az = std::fabs(v.z);
+    const R largest = (ax >= ay && ax >= az) ? v.x : (ay >= az ? v.y : v.z);
+    return largest < R(0) ? -v : v;
+}
+// indices_are_degenerate (:508-511): |a - b| <= sqrt(f32::EPSILON) * max(|a|, |b|, 1)
+template <class R> static inline bool indices_degenerate(R a, R b) {
+    const R scale = rmax(rmax(std::fabs(a), std::fabs(b)), R(1));
+    return std::fabs(a - b) <= R(::sqrtf(FLT_EPSILON)) * scale;
+}
+// uniaxial_wave_indices (:494-498) -> (n_slow, n_fast)
+template <class R> static inline void uniaxial_wave_indices(const V3<R> &k, const V3<R> &c, R n_o, R n_e, R &ns, R &nf) {
+    const R theta = M<R>::acos(std::fabs(clampr(k.dot(c), R(-1), R(1))));
+    const R n_eff = effective_extraordinary_index(n_o, n_e, theta);
+    ns = rmax(n_o, n_eff);
+    nf = rmin(n_o, n_eff);
+}
+// wave_indices (:435-484): Fresnel's equation of wave normals -> (n_slow, n_fast)
+template <class R> static inline void wave_indices(const Indicatrix<R> &I, const V3<R> &wave_normal, R &ns, R &nf) {
+    const V3<R> k = wave_normal.normalize_or_zero();
+    const bool ab = indices_degenerate(I.na, I.nb);
+    const bool bg = indices_degenerate(I.nb, I.ng);
+    if (ab && bg) {
+        const R n = ((I.na + I.nb) + I.ng) / R(3);
+        ns = n;
+        nf = n;
+        return;
+    }
+    if (ab) { uniaxial_wave_indices(k, I.ax2, midpoint(I.na, I.nb), I.ng, ns, nf); return; }
+    if (bg) { uniaxial_wave_indices(k, I.ax0, midpoint(I.nb, I.ng), I.na, ns, nf); return; }
+    const V3<R> l = ind_local(I, k);
+    const R a2 = l.x * l.x, b2 = l.y * l.y, g2 = l.z * l.z;
+    const R b1 = R(1) / (I.na * I.na), b2c = R(1) / (I.nb * I.nb), b3 = R(1) / (I.ng * I.ng);
+    const R big_b = M<R>::fma(a2, b2c + b3, M<R>::fma(b2, b1 + b3, g2 * (b1 + b2c)));
+    const R big_c = M<R>::fma(a2, b2c * b3, M<R>::fma(b2, b1 * b3, g2 * b1 * b2c));
+    const R disc = M<R>::sqrt(rmax(M<R>::fma(big_b, big_b, R(-4) * big_c), R(0)));
+    const R x_lo = R(0.5f) * (big_b - disc);
+    const R x_hi = midpoint(big_b, disc);
+    ns = R(1) / M<R>::sqrt(rmax(x_lo, R(1e-12f)));
+    nf = R(1) / M<R>::sqrt(rmax(x_hi, R(1e-12f)));
+}
+// precise_root_near (:717-749): the root of the same quadratic nearest x, its
+// discriminant formed from direct differences of the principal 1/n^2
+template <class R> static inline R precise_root_near(const V3<R> &l, const R b[3], R x) {
+    const R a = l.x * l.x, bb = l.y * l.y, cc = l.z * l.z;
+    const R big_b = M<R>::fma(a, b[1] + b[2], M<R>::fma(bb, b[0] + b[2], cc * (b[0] + b[1])));
+    const R xdiff = b[0] - b[1];
+    const R ydiff = b[2] - b[0];
+    const R a_plus_c = a + cc;
+    const R a_plus_bb = a + bb;
+    const R two_a_minus_bc = R(2) * M<R>::fma(bb, -cc, a);
+    const R disc_sq = M<R>::fma(a_plus_c * a_plus_c, xdiff * xdiff,
+                                M<R>::fma(a_plus_bb * a_plus_bb, ydiff * ydiff, two_a_minus_bc * xdiff * ydiff));
+    const R disc = M<R>::sqrt(rmax(disc_sq, R(0)));
+    const R x_lo = R(0.5f) * (big_b - disc);
+    const R x_hi = midpoint(big_b, disc);
+    return std::fabs(x - x_lo) <= std::fabs(x - x_hi) ? x_lo : x_hi;
+}
+// eigenvector_world (:659-702): null vector of Gamma - x I (Gamma = P B P) as the
+// sign-aligned sum of its three row-pair cross products, in world space
+template <class R> static inline V3<R> eigenvector_world(const Indicatrix<R> &I, const V3<R> &l, const R b[3], R x_in,
+                                                         const V3<R> &k_hat) {
+    const R x = precise_root_near(l, b, x_in);
+    const R s = M<R>::fma(b[0], l.x * l.x, M<R>::fma(b[1], l.y * l.y, b[2] * l.z * l.z));
+    const R m00 = M<R>::fma(l.x * l.x, M<R>::fma(R(2), -b[0], s), b[0] - x);
+    const R m11 = M<R>::fma(l.y * l.y, M<R>::fma(R(2), -b[1], s), b[1] - x);
+    const R m22 = M<R>::fma(l.z * l.z, M<R>::fma(R(2), -b[2], s), b[2] - x);
+    const R m01 = l.x * l.y * (s - b[0] - b[1]);
+    const R m02 = l.x * l.z * (s - b[0] - b[2]);
+    const R m12 = l.y * l.z * (s - b[1] - b[2]);
+    const V3<R> row0(m00, m01, m02), row1(m01, m11, m12), row2(m02, m12, m22);
+    const V3<R> c01 = cross_fma(row0, row1), c02 = cross_fma(row0, row2), c12 = cross_fma(row1, row2);
+    const R sign02 = dot_fma(c01, c02) < R(0) ? R(-1) : R(1);
+    const R sign12 = dot_fma(c01, c12) < R(0) ? R(-1) : R(1);
+    const V3<R> v_local = (c01 + c02 * sign02) + c12 * sign12;
+    const V3<R> v_world = ind_world(I, v_local);
+    if (v_world.length_squared() > R(1e-12f)) return canonicalize_sign(v_world).normalize();
+    V3<R> t, bt;
+    stable_orthonormal_basis(k_hat, t, bt);
+    return t;
+}
+// eigen_polarizations (:542-554): D directions of the (slow, fast) modes
+template <class R> static inline void eigen_polarizations(const Indicatrix<R> &I, const V3<R> &wave_normal, V3<R> &d_slow,
+                                                          V3<R> &d_fast) {
+    const V3<R> k = wave_normal.normalize_or_zero();
+    const V3<R> l = ind_local(I, k);
+    const R b[3] = {R(1) / (I.na * I.na), R(1) / (I.nb * I.nb), R(1) / (I.ng * I.ng)};
+    R ns, nf;
+    wave_indices(I, wave_normal, ns, nf);
+    const R x_slow = R(1) / (ns * ns);
+    const R x_fast = R(1) / (nf * nf);
+    d_slow = eigenvector_world(I, l, b, x_slow, k);
+    d_fast = eigenvector_world(I, l, b, x_fast, k);
+}
+// d_to_e_direction (:760-768)
+template <class R> static inline V3<R> d_to_e_direction(const Indicatrix<R> &I, const V3<R> &d_hat) {
+    const V3<R> dl = ind_local(I, d_hat);
+    const V3<R> el(dl.x / (I.na * I.na), dl.y / (I.nb * I.nb), dl.z / (I.ng * I.ng));
+    return ind_world(I, el).normalize_or_zero();
+}
+// poynting_direction (:860-870): the component of k perpendicular to E
+template <class R> static inline V3<R> poynting_direction(const V3<R> &wave_normal, const V3<R> &e_field) {
+    const V3<R> k = wave_normal.normalize_or_zero();
+    const V3<R> e = e_field.normalize_or_zero();
+    const V3<R> perp = k - e * e.dot(k);
+    const R len2 = perp.length_squared();
+    if (len2 > R(1e-10f)) {
+        const R l = M<R>::sqrt(len2);
+        return V3<R>(perp.x / l, perp.y / l, perp.z / l);
+    }
+    return k;
+}
+// mode_poynting_dir (:831-836)
+template <class R> static inline V3<R> mode_poynting_dir(const Indicatrix<R> &I, const V3<R> &wave_normal, bool want_slow) {
+    V3<R> ds, df;
+    eigen_polarizations(I, wave_normal, ds, df);
+    return poynting_direction(wave_normal, d_to_e_direction(I, want_slow ? ds : df));
+}
+// resolve_entry_mode (:795-818): two fixed-point steps of the refracted wave normal
+template <class R> static inline V3<R> resolve_entry_mode(const Indicatrix<R> &I, const V3<R> &incident, const V3<R> &normal,
+                                                          R cos_i, R n_seed, bool want_slow) {
+    R n_guess = n_seed;
+    V3<R> wave_dir = incident;
+    for (int it = 0; it < 2; ++it) {
+        const R eta = R(1) / n_guess;
+        const R s2 = eta * eta * M<R>::fma(cos_i, -cos_i, R(1));
+        if (s2 > R(1)) break;
+        const R ct = M<R>::sqrt(rmax(R(1) - s2, R(0)));
+        wave_dir = (eta * incident + M<R>::fma(eta, cos_i, -ct) * normal).normalize();
+        R ns, nf;
+        wave_indices(I, wave_dir, ns, nf);
+        n_guess = want_slow ? ns : nf;
+    }
+    return wave_dir;
+}
+
+// ---------------------------------------------------------------------------------
 // a5. Polyhedron clip -- intersect.rs:93-132 + simd/slab.rs:101-152
 // ---------------------------------------------------------------------------------
 template <class R> struct Hit { bool hit; R t; V3<R> normal; int facet; };
@@ -814,8 +985,10 @@ template <class R> struct MaterialCtx {
     const gr_material *mat;
     const gr_material_ext *ext;
     bool anisotropic;
+    bool biaxial;  // biaxial_delta_beta_alpha.is_some() (refraction.rs:459)
     V3<R> c_axis;
     R bire;
+    R d_beta_alpha;
 };
 
 template <class R> static inline MaterialCtx<R> make_material(const gr_material *m, const gr_material_ext *ext) {
@@ -825,27 +998,30 @@ template <class R> static inline MaterialCtx<R> make_material(const gr_material 
     c.c_axis = V3<R>(R(m->dispersion.c_axis_and_birefringence[0]), R(m->dispersion.c_axis_and_birefringence[1]),
                      R(m->dispersion.c_axis_and_birefringence[2]));
     c.bire = R(m->dispersion.c_axis_and_birefringence[3]);
+    c.biaxial = m->dispersion.has_biaxial_delta != 0;
+    c.d_beta_alpha = R(m->dispersion.biaxial_delta_beta_alpha);
     // transport.rs:620-621
     c.anisotropic = m->crystal_system != GR_CRYSTAL_CUBIC && std::fabs(m->dispersion.c_axis_and_birefringence[3]) > 1e-4f;
     return c;
 }
 
-// The v1 device path handles polished facets of isotropic/uniaxial, non-scattering
-// materials; the others are declined (the reference's decline => CPU fallback
-// contract, renderer/gpu_backend.rs:27-44).
+// Every material kind of the reference's render path is handled (isotropic, uniaxial,
+// biaxial with or without a beta-ray band set; polished or frosted facets; volume
+// scattering); the decline status stays for malformed materials only
+// (renderer/gpu/frame.rs:680-693, GemMaterial::gpu_supported).
 static inline bool material_supported(const gr_material *m, const uint32_t *finishes, uint32_t n_planes) {
     (void)finishes;
     (void)n_planes;
-    if (m->dispersion.has_biaxial_delta) return false;
-    if (m->has_beta_ray) return false;
-    return true;
+    return m->o_ray_band_count <= GR_MAX_BANDS && m->e_ray_band_count <= GR_MAX_BANDS &&
+           m->beta_ray_band_count <= GR_MAX_BANDS;
 }
 
-// Per-sample wavelength cache (refraction.rs:127-174, uniaxial only).
+// Per-sample wavelength cache (build_ray_wavelength_cache, refraction.rs:127-174).
 template <class R> struct WaveCache {
     R n_o[8];
     R n_e_delta[8];  // n_e - n_o per channel (constant birefringence_delta unless extended)
     Tensor3<R> tensor[8];
+    Indicatrix<R> ind[8];  // biaxial materials: per-channel indicatrix (hero = channel 0)
     bool any_absorption;
 };
 
@@ -876,6 +1052,16 @@ static inline WaveCache<R> build_cache(const MaterialCtx<R> &mc, const R lam[8])
         }
         if (ao != R(0) || ae != R(0)) wc.any_absorption = true;
         wc.tensor[k] = tensor_uniaxial(ao, ae, mc.c_axis);
+        if (mc.biaxial) {
+            wc.ind[k] = make_indicatrix(wc.n_o[k], mc.d_beta_alpha, mc.bire, mc.c_axis);
+            // AbsorptionTensor3::biaxial(alpha_o, beta, alpha_e, c) (birefringence.rs:238-245):
+            // the uniaxial frame with the beta band set's coefficient on the second axis
+            if (m->has_beta_ray) {
+                const R ab = spectral_absorption(m->beta_ray_bands, m->beta_ray_band_count, lam[k]);
+                wc.tensor[k].alpha = V3<R>(ao, ab, ae);
+                if (ab != R(0)) wc.any_absorption = true;
+            }
+        }
     }
     return wc;
 }
@@ -890,9 +1076,10 @@ template <class R> static inline R tir_phase_delta(R n1k, R cos_i, R sin_i) {
 template <class R> struct Geo {
     R cos_i, sin_i, n_o_hero, n_e_hero, n1, n2, sin2_t;
     R n_o_ch[8], n1_ch[8], n2_ch[8], sin2_t_ch[8];
+    R n_biax_a_ch[8];  // biaxial: fast-mode index per channel at the hero's fast wave normal
 };
 
-// refraction.rs:428-547 (uniaxial / isotropic branch)
+// compute_bounce_refraction_geometry (refraction.rs:428-547)
 template <class R>
 static inline Geo<R> bounce_geometry(const MaterialCtx<R> &mc, const WaveCache<R> &wc, const V3<R> &normal,
                                      const V3<R> &k_hat, bool inside, bool is_e) {
@@ -902,7 +1089,7 @@ static inline Geo<R> bounce_geometry(const MaterialCtx<R> &mc, const WaveCache<R
     R n_o_seed = wc.n_o[0];
     // theta_c_for_bounce (refraction.rs:235-273)
     R theta;
-    if (!inside && mc.anisotropic) {
+    if (!inside && mc.anisotropic && !mc.biaxial) {
         R n_e_seed = n_o_seed + wc.n_e_delta[0];
         R n_guess = n_o_seed;
         theta = R(0);
@@ -928,7 +1115,29 @@ static inline Geo<R> bounce_geometry(const MaterialCtx<R> &mc, const WaveCache<R
     }
     g.n_o_hero = wc.n_o[0];
     g.n_e_hero = g.n_o_hero + wc.n_e_delta[0];
-    const R *n_med = (mc.anisotropic && inside && !is_e) ? g.n_o_ch : n_eff;
+    // hero_biaxial_wave_dirs + per_channel_biaxial_indices (refraction.rs:345-401): mode
+    // A (fast) and mode B (slow) indices at the hero's two wave normals -- the ray's own
+    // inside the stone, the refracted ones (resolve_entry_mode) on entry
+    R n_biax_b[8];
+    if (mc.biaxial) {
+        V3<R> dir_a = k_hat, dir_b = k_hat;
+        if (!inside) {
+            dir_a = resolve_entry_mode(wc.ind[0], k_hat, normal, g.cos_i, n_o_seed, false);
+            dir_b = resolve_entry_mode(wc.ind[0], k_hat, normal, g.cos_i, n_o_seed, true);
+        }
+        for (int k = 0; k < 8; ++k) {
+            R ns, nf;
+            wave_indices(wc.ind[k], dir_a, ns, nf);
+            g.n_biax_a_ch[k] = nf;
+            wave_indices(wc.ind[k], dir_b, ns, nf);
+            n_biax_b[k] = ns;
+        }
+    } else {
+        for (int k = 0; k < 8; ++k) { g.n_biax_a_ch[k] = R(0); n_biax_b[k] = R(0); }
+    }
+    const R *mode_a = mc.biaxial ? g.n_biax_a_ch : g.n_o_ch;
+    const R *mode_b = mc.biaxial ? n_biax_b : n_eff;
+    const R *n_med = (mc.anisotropic && inside && !is_e) ? mode_a : mode_b;
     R n_med_hero = n_med[0];
     g.n1 = inside ? n_med_hero : R(1);
     g.n2 = inside ? R(1) : n_med_hero;
@@ -945,12 +1154,28 @@ static inline Geo<R> bounce_geometry(const MaterialCtx<R> &mc, const WaveCache<R
     return g;
 }
 
-// refraction.rs:564-582 (uniaxial)
+// poynting_dir_for_mode (refraction.rs:564-582): biaxial modes both walk off
 template <class R>
-static inline V3<R> poynting_dir_for_mode(const MaterialCtx<R> &mc, const Geo<R> &g, const V3<R> &k, bool inside, bool is_e) {
+static inline V3<R> poynting_dir_for_mode(const MaterialCtx<R> &mc, const WaveCache<R> &wc, const Geo<R> &g,
+                                          const V3<R> &k, bool inside, bool is_e) {
     if (!inside || !mc.anisotropic) return k;
+    if (mc.biaxial) return mode_poynting_dir(wc.ind[0], k, is_e);
     if (is_e) return extraordinary_poynting_dir(k, mc.c_axis, g.n_o_hero, g.n_e_hero);
     return k;
+}
+
+// channel_absorption_alphas' eigenmode pair (raytracer/absorption.rs:175-196): the hero
+// indicatrix's (slow, fast) D directions for a biaxial material, else the uniaxial
+// ordinary / extraordinary pair
+template <class R>
+static inline void absorption_eigenmodes(const MaterialCtx<R> &mc, const WaveCache<R> &wc, const V3<R> &k, V3<R> &ea,
+                                         V3<R> &eb) {
+    if (mc.biaxial) {
+        eigen_polarizations(wc.ind[0], k, ea, eb);
+    } else {
+        ea = ordinary_eigen_polarization(k, mc.c_axis);
+        eb = extraordinary_eigen_polarization(k, mc.c_axis);
+    }
 }
 
 template <class R> static inline void fresnel_rs_rp(R n1k, R n2k, R cos_i, R cos_t, R &rs, R &rp) {
@@ -1054,8 +1279,8 @@ static inline V3<R> trace_spectral_ray(const Ray<float> &initial, const gr_plane
         // (which then replaces apply_absorption below).
         if (inside && mat->scattering_sigma_s > 0.0f) {
             const V3<R> s_axis = have_prev ? prev_plane : V3<R>();
-            const V3<R> ea = ordinary_eigen_polarization(cur_k, mc.c_axis);
-            const V3<R> eb = extraordinary_eigen_polarization(cur_k, mc.c_axis);
+            V3<R> ea, eb;
+            absorption_eigenmodes(mc, wc, cur_k, ea, eb);
             R alphas[8];
             for (int k = 0; k < 8; ++k) {
                 V3<R> e_hat = electric_field_direction(st[k], s_axis, cur_k);
@@ -1124,8 +1349,8 @@ static inline V3<R> trace_spectral_ray(const Ray<float> &initial, const gr_plane
         if (inside) {
             normal = -normal;
             if (mat->scattering_sigma_s <= 0.0f) {
-                V3<R> ea = ordinary_eigen_polarization(cur_k, mc.c_axis);
-                V3<R> eb = extraordinary_eigen_polarization(cur_k, mc.c_axis);
+                V3<R> ea, eb;
+                absorption_eigenmodes(mc, wc, cur_k, ea, eb);
                 R scaled = hit.t * R(mat->absorption_path_scale);
                 R alphas[8];
                 for (int k = 0; k < 8; ++k) {
@@ -1202,7 +1427,7 @@ static inline V3<R> trace_spectral_ray(const Ray<float> &initial, const gr_plane
                 }
             }
             new_k = cur_k - (R(2) * cur_k.dot(normal)) * normal;
-            new_s = poynting_dir_for_mode(mc, g, new_k, inside, is_e);
+            new_s = poynting_dir_for_mode(mc, wc, g, new_k, inside, is_e);
             if (log) { log->n_tir++; if (bounce < 64) log->events[bounce] = EV_TIR; }
         } else {
             // apply_partial_fresnel_bounce (refraction.rs:1036-1086)
@@ -1229,26 +1454,32 @@ static inline V3<R> trace_spectral_ray(const Ray<float> &initial, const gr_plane
                     st[k] = apply_matrix(st[k], mm).scale(R(1) / r_unpol);
                 }
                 new_k = cur_k - (R(2) * cur_k.dot(normal)) * normal;
-                new_s = poynting_dir_for_mode(mc, g, new_k, inside, is_e);
+                new_s = poynting_dir_for_mode(mc, wc, g, new_k, inside, is_e);
                 if (log) { log->n_reflect++; if (bounce < 64) log->events[bounce] = EV_REFLECT; }
             } else {
                 // apply_refract_bounce (refraction.rs:748-867)
                 bool entering_aniso = !inside && mc.anisotropic;
                 bool use_e = is_e;
                 if (entering_aniso) use_e = rng_draw(rng_seed, bounce, BIREFRINGENT_SPLIT_STREAM) < 0.5f;
-                R n2_dir = (entering_aniso && !use_e) ? g.n_o_hero : g.n2;
+                // biaxial entry: the selected mode's hero index, both modes walk off
+                const bool biax_entry = entering_aniso && mc.biaxial;
+                R n2_dir;
+                if (biax_entry) n2_dir = use_e ? g.n2 : g.n_biax_a_ch[0];
+                else n2_dir = (entering_aniso && !use_e) ? g.n_o_hero : g.n2;
                 R eta_dir = g.n1 / n2_dir;
                 R s2d = rmin(eta_dir * eta_dir * M<R>::fma(g.cos_i, -g.cos_i, R(1)), R(1));
                 R ctd = M<R>::sqrt(rmax(R(1) - s2d, R(0)));
                 V3<R> refr = (eta_dir * cur_k + M<R>::fma(eta_dir, g.cos_i, -ctd) * normal).normalize();
-                V3<R> final_dir = (entering_aniso && use_e)
-                                      ? extraordinary_poynting_dir(refr, mc.c_axis, g.n_o_hero, g.n_e_hero)
-                                      : refr;
+                V3<R> final_dir;
+                if (biax_entry) final_dir = mode_poynting_dir(wc.ind[0], refr, use_e);
+                else final_dir = (entering_aniso && use_e)
+                                     ? extraordinary_poynting_dir(refr, mc.c_axis, g.n_o_hero, g.n_e_hero)
+                                     : refr;
                 // apply_refract_channel (refraction.rs:883-1011)
                 const R TOL = R(1) - R(1e-6f);
                 for (int k = 0; k < 8; ++k) {
                     R n1k = g.n1_ch[k];
-                    R n2k = (entering_aniso && !use_e) ? g.n_o_ch[k] : g.n2_ch[k];
+                    R n2k = (entering_aniso && !use_e) ? (mc.biaxial ? g.n_biax_a_ch[k] : g.n_o_ch[k]) : g.n2_ch[k];
                     R ratio = n1k / n2k;
                     R s2k = (ratio * ratio) * M<R>::fma(g.cos_i, -g.cos_i, R(1));
                     if (s2k > R(1)) { st[k] = st[k].scale(R(0)); pdf[k] = R(0); continue; }
@@ -1256,7 +1487,9 @@ static inline V3<R> trace_spectral_ray(const Ray<float> &initial, const gr_plane
                     R eta_k = n1k / n2k;
                     V3<R> rk = (eta_k * cur_k + M<R>::fma(eta_k, g.cos_i, -ctk) * normal).normalize();
                     V3<R> fk = rk;
-                    if (entering_aniso && use_e) {
+                    if (biax_entry) {
+                        fk = mode_poynting_dir(wc.ind[k], rk, use_e);
+                    } else if (entering_aniso && use_e) {
                         R n_e_k = g.n_o_ch[k] + wc.n_e_delta[k];
                         fk = extraordinary_poynting_dir(rk, mc.c_axis, g.n_o_ch[k], n_e_k);
                     }

@@ -216,6 +216,49 @@ int gro_probe_grid(const gr_scene *sc, uint32_t grid, uint32_t spp, uint32_t sal
     return GR_OK;
 }
 
+// BiaxialIndicatrix entry points (optics/birefringence.rs:349-839) for the property
+// tests: an indicatrix from three principal indices and a frame given as columns
+// (ax0, ax1, ax2), or from a material at a wavelength (materials.rs:1508-1519).
+static Indicatrix<float> ind_from(float na, float nb, float ng, const float axes[9]) {
+    Indicatrix<float> I;
+    I.na = na; I.nb = nb; I.ng = ng;
+    I.ax0 = V3<float>(axes[0], axes[1], axes[2]);
+    I.ax1 = V3<float>(axes[3], axes[4], axes[5]);
+    I.ax2 = V3<float>(axes[6], axes[7], axes[8]);
+    return I;
+}
+
+void gro_biaxial_wave_indices(float na, float nb, float ng, const float axes[9], const float wn[3], float out[2]) {
+    wave_indices(ind_from(na, nb, ng, axes), V3<float>(wn[0], wn[1], wn[2]), out[0], out[1]);
+}
+
+void gro_biaxial_eigen(float na, float nb, float ng, const float axes[9], const float wn[3], float d_slow[3],
+                       float d_fast[3]) {
+    V3<float> s, f;
+    eigen_polarizations(ind_from(na, nb, ng, axes), V3<float>(wn[0], wn[1], wn[2]), s, f);
+    d_slow[0] = s.x; d_slow[1] = s.y; d_slow[2] = s.z;
+    d_fast[0] = f.x; d_fast[1] = f.y; d_fast[2] = f.z;
+}
+
+void gro_biaxial_poynting(float na, float nb, float ng, const float axes[9], const float wn[3], int want_slow,
+                          float out[3]) {
+    const V3<float> d = mode_poynting_dir(ind_from(na, nb, ng, axes), V3<float>(wn[0], wn[1], wn[2]), want_slow != 0);
+    out[0] = d.x; out[1] = d.y; out[2] = d.z;
+}
+
+int gro_material_indicatrix(const gr_material *m, float lambda_nm, float n_out[3], float axes_out[9]) {
+    if (!m || !m->dispersion.has_biaxial_delta) return -1;
+    const V3<float> c(m->dispersion.c_axis_and_birefringence[0], m->dispersion.c_axis_and_birefringence[1],
+                      m->dispersion.c_axis_and_birefringence[2]);
+    const Indicatrix<float> I = make_indicatrix<float>(dispersion_evaluate<float>(m->dispersion, lambda_nm),
+                                                       m->dispersion.biaxial_delta_beta_alpha,
+                                                       m->dispersion.c_axis_and_birefringence[3], c);
+    n_out[0] = I.na; n_out[1] = I.nb; n_out[2] = I.ng;
+    const V3<float> ax[3] = {I.ax0, I.ax1, I.ax2};
+    for (int i = 0; i < 3; ++i) { axes_out[3 * i] = ax[i].x; axes_out[3 * i + 1] = ax[i].y; axes_out[3 * i + 2] = ax[i].z; }
+    return 0;
+}
+
 // The two direction samplers of the frosted and scattering paths (scattering.rs:
 // 356-362 cosine_weighted_hemisphere, 428-443 sample_henyey_greenstein_direction).
 void gro_cosine_hemisphere(float u1, float u2, const float n[3], float out[3]) {

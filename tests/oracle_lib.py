@@ -82,6 +82,14 @@ def lib():
     L.gro_cosine_hemisphere.argtypes = [F, F, fp, fp]
     L.gro_sample_hg.restype = None
     L.gro_sample_hg.argtypes = [F, F, F, fp, fp]
+    L.gro_biaxial_wave_indices.restype = None
+    L.gro_biaxial_wave_indices.argtypes = [F, F, F, fp, fp, fp]
+    L.gro_biaxial_eigen.restype = None
+    L.gro_biaxial_eigen.argtypes = [F, F, F, fp, fp, fp, fp]
+    L.gro_biaxial_poynting.restype = None
+    L.gro_biaxial_poynting.argtypes = [F, F, F, fp, fp, C.c_int, fp]
+    L.gro_material_indicatrix.restype = C.c_int
+    L.gro_material_indicatrix.argtypes = [C.POINTER(abi.gr_material), F, fp, fp]
     L.gro_accumulate.restype = C.c_int
     L.gro_accumulate.argtypes = [sc, U, U, fp, C.c_int]
     L.gro_accumulate_f64.restype = C.c_int

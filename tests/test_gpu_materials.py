@@ -1,5 +1,7 @@
-"""Frosted facet finishes and Henyey-Greenstein volume scattering on the device
-(raytracer/scattering.rs:132-602), against the oracle.
+"""Frosted facet finishes, Henyey-Greenstein volume scattering
+(raytracer/scattering.rs:132-602) and biaxial materials (BiaxialIndicatrix,
+optics/birefringence.rs:349-839, with trichroic beta-ray absorption) on the device,
+against the oracle.
 
 Per sample the engine follows the oracle the way the polished path does: the new
 arithmetic (cosine-weighted and Henyey-Greenstein directions, free-flight distances
@@ -8,8 +10,7 @@ flips a Fresnel, distance or roulette decision through a libm ULP.  Scene-level
 properties from the reference's own tests hold on the device too: a bruted girdle
 makes the face-up studio view brighter (raytracer_tests.rs:2411-2460), and a
 lossless scattering medium in a uniform environment returns the environment's
-radiance (the white furnace).  Materials the device still declines keep the
-buffer untouched.
+radiance (the white furnace).  Every built-in material renders on the device.
 """
 from __future__ import annotations
 
@@ -60,6 +61,19 @@ def _cases():
                                               material=_scattering(S.custom_material(1.6, 0.01, 0.02, (0.3, 0.1, 0.5)),
                                                                    2.0, -0.3),
                                               cam=cam, max_bounces=16, env_mode=abi.GR_ENV_STUDIO),
+        "biaxial Alexandrite studio": S.Scene(width=24, height=24, planes=planes,
+                                              material=S.builtin_material("Alexandrite"), cam=cam, max_bounces=16),
+        "biaxial Topaz studio": S.Scene(width=24, height=24, planes=planes, material=S.builtin_material("Topaz"),
+                                        cam=cam, max_bounces=16, preset="Daylight"),
+        "biaxial Tanzanite latlong": S.Scene(width=24, height=24, planes=planes,
+                                             material=S.builtin_material("Tanzanite"), cam=cam, max_bounces=16,
+                                             env_mode=abi.GR_ENV_LATLONG, latlong=env),
+        "biaxial frosted Tanzanite": S.Scene(width=24, height=24, planes=planes,
+                                             material=S.builtin_material("Tanzanite"), cam=cam, max_bounces=16,
+                                             finishes=_girdle_finishes()),
+        "biaxial scattering Alexandrite": S.Scene(width=24, height=24, planes=planes,
+                                                  material=_scattering(S.builtin_material("Alexandrite"), 1.0, 0.5),
+                                                  cam=cam, max_bounces=16),
     }
 
 
@@ -73,8 +87,13 @@ def test_per_sample_matches_oracle(renderer, oracle, case):
     assert np.all(np.isfinite(gpu))
     rel = _rel(gpu, ref)
     # the polished path's bars: a lat-long lookup turns direction ULPs into radiance
-    # ULPs (0.9 tight there, as for polished lat-long scenes), elsewhere 0.98 / 1 %
+    # ULPs (0.9 tight there, as for polished lat-long scenes), elsewhere 0.98 / 1 %.
+    # In a scattering biaxial stone the HG directions carry CUDA's sincosf/logf ULPs
+    # into the eigenvector solve, whose sensitivity grows as 1/(mode gap): more
+    # samples land between 1e-5 and 1e-3 (measured 96-98 % tight), none more flip.
     tight = 0.9 if sc.env_mode == abi.GR_ENV_LATLONG else 0.98
+    if sc.material.dispersion.has_biaxial_delta and sc.material.scattering_sigma_s > 0:
+        tight = 0.95
     assert np.mean(rel <= 1e-5) >= tight, (case, np.mean(rel <= 1e-5))
     assert np.mean(rel > 1e-3) <= 0.01, (case, np.mean(rel > 1e-3))
 
@@ -105,6 +124,27 @@ def test_scattering_white_furnace(renderer, oracle):
         renderer.accumulate(sc, 0, 256, film)
         mean = film.astype(np.float64).sum(0) / (48 * 48 * 256)
         assert np.all(np.abs(mean - target) / target <= 0.02), (sigma_s, mean, target)
+
+
+def test_biaxial_white_furnace(renderer, oracle):
+    """A lossless biaxial stone (n_gamma - n_alpha = 0.03, n_beta - n_alpha = 0.01 /
+    0.02) in a uniform environment returns the environment's radiance; the oracle
+    measures +0.13 % at 64 bounces."""
+    l0 = 2.5
+    t = (C.c_float * 3)()
+    oracle.gro_furnace_target(l0, t)
+    target = np.array(t, np.float64)
+    for dba in (0.01, 0.02):
+        m = S.custom_material(1.5, 0.0, 0.03)
+        m.dispersion.has_biaxial_delta = 1
+        m.dispersion.biaxial_delta_beta_alpha = dba
+        sc = S.Scene(width=48, height=48, planes=S.standard_round_brilliant(), material=m,
+                     cam=S.camera(0.35, 0.28, 5.0, 18.0), max_bounces=64, env_mode=abi.GR_ENV_UNIFORM,
+                     uniform_rgb=(l0, l0, l0))
+        film = np.zeros((48 * 48, 3), np.float32)
+        renderer.accumulate(sc, 0, 256, film)
+        mean = film.astype(np.float64).sum(0) / (48 * 48 * 256)
+        assert np.all(np.abs(mean - target) / target <= 0.01), (dba, mean, target)
 
 
 def test_default_off_extras_bit_identical(renderer):
@@ -140,13 +180,13 @@ def test_batch_with_frosted_and_scattering_scenes(engine_lib, flags):
                   S.Scene(width=20, height=12, planes=S.standard_round_brilliant(),
                           material=S.builtin_material("Sapphire"), cam=S.camera(0.35, 0.28, 5.0, 18.0),
                           max_bounces=16),
-                  cases["scattering tinted uniaxial"]]
+                  cases["scattering tinted uniaxial"], cases["biaxial Alexandrite studio"]]
         ids = []
         for sc in scenes:
             sid = C.c_uint64()
             assert lib.gr_scene_upload(h, C.byref(sc.c_scene()), C.byref(sid)) == abi.GR_OK
             ids.append(sid.value)
-        spps = [12, 5, 9, 16]
+        spps = [12, 5, 9, 16, 7]
         alone = [torch.zeros((sc.width * sc.height, 3), dtype=torch.float32, device="cuda") for sc in scenes]
         batched = [torch.zeros_like(f) for f in alone]
         torch.cuda.synchronize()
@@ -168,12 +208,14 @@ def test_batch_with_frosted_and_scattering_scenes(engine_lib, flags):
         assert lib.gr_destroy(h) == abi.GR_OK
 
 
-def test_still_declined_materials_leave_buffer_untouched(renderer):
-    from gemray_studio_b200.backend import UnsupportedMaterial
-    for name in ("Alexandrite", "Tanzanite"):
-        sc = S.Scene(width=8, height=8, planes=S.standard_round_brilliant(), material=S.builtin_material(name),
-                     cam=S.camera(0.35, 0.28, 5.0, 18.0), max_bounces=8)
-        acc = np.full((64, 3), 7.0, np.float32)
-        with pytest.raises(UnsupportedMaterial):
-            renderer.accumulate(sc, 0, 4, acc)
-        assert np.all(acc == 7.0)
+def test_every_builtin_material_renders(renderer):
+    """No built-in material is declined (the reference's GemMaterial::gpu_supported is
+    true for all of them, renderer/gpu/frame.rs:680-693); every film is finite and
+    adds into the caller's buffer."""
+    for name in S.BUILTIN_MATERIALS:
+        sc = S.Scene(width=12, height=12, planes=S.standard_round_brilliant(), material=S.builtin_material(name),
+                     cam=S.camera(0.35, 0.28, 5.0, 18.0), max_bounces=12)
+        acc = np.full((144, 3), 1.0, np.float32)
+        renderer.accumulate(sc, 0, 16, acc)
+        # (a von Kries-adapted XYZ can dip below zero for saturated spectra)
+        assert np.all(np.isfinite(acc)) and np.any(acc != 1.0), name

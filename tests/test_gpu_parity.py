@@ -139,14 +139,15 @@ def test_kahan_film_close_to_plain(renderer):
     assert np.allclose(a, b, rtol=1e-5, atol=1e-6)
 
 
-def test_declined_material_leaves_accum_untouched(renderer):
-    sc = srb_scene("Tanzanite", width=8, height=8)  # biaxial
+def test_failed_call_leaves_accum_untouched(renderer):
+    sc = srb_scene("Tanzanite", width=8, height=8)
+    sc.env_mode = 9  # no such environment kind
     acc = np.full((64, 3), 7.0, np.float32)
     from gemray_studio_b200 import GpuBackend
     b = GpuBackend(renderer)
     assert b.try_accumulate(sc, 0, 4, acc) is False
     assert np.all(acc == 7.0)
-    assert "biaxial" in (b.last_error or "")
+    assert "environment" in (b.last_error or "")
 
 
 def test_empty_frame_and_zero_spp_are_noops(renderer):

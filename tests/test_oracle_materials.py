@@ -162,10 +162,3 @@ def test_scattering_changes_face_up_y(oracle):
     clear = _probe(oracle, S.Scene(14, 14, PLANES, d, CAM), 14, 96, 0x0BADF00D, 12)
     hazy = _probe(oracle, S.Scene(14, 14, PLANES, _scattering(d, 1.5, 0.3), CAM), 14, 96, 0x0BADF00D, 12)
     assert abs(hazy[1] - clear[1]) / clear[1] > 0.01, (clear[1], hazy[1])
-
-
-def test_biaxial_and_beta_ray_still_declined(oracle):
-    for name in ("Alexandrite", "Topaz", "Tanzanite"):
-        out = (C.c_float * 3)()
-        sc = S.Scene(4, 4, PLANES, S.builtin_material(name), CAM)
-        assert oracle.gro_probe_grid(C.byref(sc.c_scene()), 4, 1, 0, 8, out) == abi.GR_DECLINED_MATERIAL

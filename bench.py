@@ -263,6 +263,31 @@ def hbm_view(tuples_per_launch: float, ms_per_launch: float):
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if peak else None}
 
 
+def stream_view(r, sid: int, sc, first: int, spp: int, cadence_ms: float = 50.0) -> dict:
+    """One frame streamed as FRAME deltas (gr_stream_*: adaptive sub-batches toward
+    100 ms of device time, starting at 1 sample), drained on a fixed host cadence; host
+    wall clock from open to the last drain, and the time each drain took (a 24.9 MB
+    device-to-pageable-host copy for c2)."""
+    from gemray_studio_b200.stream import FrameStream
+    take_ms, frames = [], 0
+    t0 = time.perf_counter()
+    with FrameStream(r, sid, sc.width, sc.height, first, spp) as fs:
+        while True:
+            time.sleep(cadence_ms / 1e3)
+            _done, state = fs.status()
+            a = time.perf_counter()
+            d = fs.take()
+            take_ms.append((time.perf_counter() - a) * 1e3)
+            frames += d is not None
+            if state != "running":
+                break
+        wall = time.perf_counter() - t0
+    n = sc.width * sc.height * spp
+    return {"path_samples_per_s": n / wall, "frames": frames, "cadence_ms": cadence_ms,
+            "drain_ms_p50": float(np.percentile(take_ms, 50)), "drain_ms_max": float(max(take_ms)),
+            "how": "gr_stream_open .. last gr_stream_take, host wall clock, one frame of the workload"}
+
+
 def run_engine(args):
     world, rank, local = dist_setup()
     import torch
@@ -354,6 +379,8 @@ def run_engine(args):
     mvals = M.evaluate_poses(r, sc.planes, sc.material, poses)
     metrics_ms = (time.perf_counter() - t1) * 1e3
 
+    fstream = stream_view(r, sid.value, sc, base + (args.warmup + args.steps) * spp, spp) if world == 1 else None
+
     trace_ms_per_launch = tr.value / max(1, ntr.value)
     frames = args.steps
     flops_per_frame = model.flops_per_sample * samples_per_step
@@ -384,6 +411,7 @@ def run_engine(args):
                                  "brilliance_pct": [round(float(v), 3) for v in mvals[:, 0]],
                                  "fire_index": [round(float(v), 3) for v in mvals[:, 1]],
                                  "scintillation_pct": [round(float(v), 3) for v in mvals[:, 2]]},
+            "frame_stream": fstream,
             "gpu_launches": int(ntr.value + nfo.value),  # this library's trace + fold launches
             "clocks": clk,
             "device": r.adapter_label(),

@@ -133,6 +133,14 @@ class gr_request_status(C.Structure):
                 ("queued_ms", C.c_double), ("latency_ms", C.c_double)]
 
 
+class gr_stream_opts(C.Structure):
+    _fields_ = [("target_ms", C.c_uint32), ("first_batch", C.c_uint32), ("fixed_batch", C.c_uint32),
+                ("reserved", C.c_uint32)]
+
+
+GR_STREAM_RUNNING, GR_STREAM_FINISHED, GR_STREAM_CANCELLED, GR_STREAM_FAILED = 0, 1, 2, 3
+
+
 class gr_environment(C.Structure):
     _fields_ = [
         ("mode", C.c_uint32), ("uniform_rgb", C.c_float * 3),
@@ -224,6 +232,17 @@ EXPORTS = [
     ("gr_request_film", C.c_int, [_ctx_p, C.c_uint64, C.POINTER(C.c_float)]),
     ("gr_request_metrics", C.c_int, [_ctx_p, C.c_uint64, C.POINTER(gr_metrics_out)]),
     ("gr_request_release", C.c_int, [_ctx_p, C.c_uint64]),
+    ("gr_stream_open", C.c_int, [_ctx_p, C.c_uint64, C.c_uint32, C.c_uint32, C.POINTER(gr_stream_opts),
+                                 C.POINTER(C.c_uint64)]),
+    ("gr_stream_take", C.c_int, [_ctx_p, C.c_uint64, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                 C.POINTER(C.c_float)]),
+    ("gr_stream_status", C.c_int, [_ctx_p, C.c_uint64, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                   C.POINTER(C.c_int)]),
+    ("gr_stream_total", C.c_int, [_ctx_p, C.c_uint64, C.POINTER(C.c_float)]),
+    ("gr_stream_preview", C.c_int, [_ctx_p, C.c_uint64, C.c_uint32, C.c_uint32, C.POINTER(C.c_float)]),
+    ("gr_stream_cancel", C.c_int, [_ctx_p, C.c_uint64]),
+    ("gr_stream_close", C.c_int, [_ctx_p, C.c_uint64]),
+    ("gr_next_batch_size", C.c_uint32, [C.c_uint32, C.c_double, C.c_double]),
     ("gr_timing_enable", C.c_int, [_ctx_p, C.c_uint32]),
     ("gr_timing_read", C.c_int, [_ctx_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_uint64),
                                  C.POINTER(C.c_uint64)]),

@@ -31,7 +31,10 @@ struct ResidentScene {
     SceneConst S;
     grh::DeviceBuffer planes, map, ext;
     uint64_t bytes = 0;
+    uint32_t users = 0;  // open frame streams rendering this scene (gr_stream.cu)
 };
+
+struct FrameStream;  // gr_stream.cu
 
 struct ServeState;  // gr_serve.cu
 
@@ -76,6 +79,9 @@ struct gr_ctx {
     ServeState *serve = nullptr;
     std::map<uint64_t, ResidentScene *> scenes;
     uint64_t next_scene_id = 1;
+    // gr_stream_* frame-delta streams (gr_stream.cu)
+    std::map<uint64_t, FrameStream *> streams;
+    uint64_t next_stream_id = 1;
     uint64_t resident_bytes = 0;
 };
 
@@ -98,4 +104,18 @@ gr_status batch_enqueue(gr_ctx *ctx, const BatchItem *items, uint32_t n_items, u
 namespace grh {
 // Stops the request loop and frees its requests; the caller holds no lock.
 void serve_shutdown(gr_ctx *ctx);
+// Cancels, joins and frees every frame stream; the caller holds no lock.
+void streams_shutdown(gr_ctx *ctx);
+}  // namespace grh
+
+namespace grd {
+struct LaunchRange;
+}
+namespace grh {
+// Tuples [0, R.n_tuples) of one chunk traced into xyz on `stream` with kernel `mode`
+// (gr_host.cu), and the ordered per-pixel fold of n_pixels pixels into film.
+gr_status launch_trace(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuffers &B, const grd::LaunchRange &R,
+                       float *xyz, cudaStream_t stream, int mode);
+gr_status launch_fold(const float *xyz, uint32_t n_pixels, uint32_t spp, uint32_t first_pixel, float *film,
+                      uint32_t kahan, cudaStream_t stream);
 }  // namespace grh

@@ -586,6 +586,7 @@ gr_status gr_create(gr_ctx **out, const gr_create_opts *opts) {
 gr_status gr_destroy(gr_ctx *ctx) {
     if (!ctx) return GR_OK;
     grh::serve_shutdown(ctx);  // joins the request loop, which takes ctx->mu itself
+    grh::streams_shutdown(ctx);
     {
         std::lock_guard<std::mutex> lk(ctx->mu);
         cudaSetDevice(ctx->device);
@@ -815,6 +816,9 @@ gr_status gr_scene_release(gr_ctx *ctx, uint64_t id) {
     std::lock_guard<std::mutex> lk(ctx->mu);
     auto it = ctx->scenes.find(id);
     if (it == ctx->scenes.end()) return fail(GR_ENOTFOUND, "unknown scene id %llu", (unsigned long long)id);
+    if (it->second->users)
+        return fail(GR_EBUSY, "scene %llu is rendered by %u open frame stream(s)", (unsigned long long)id,
+                    it->second->users);
     GR_CUDA(cudaSetDevice(ctx->device));
     GR_CUDA(cudaStreamSynchronize(ctx->stream));
     ResidentScene *rs = it->second;

@@ -461,6 +461,64 @@ gr_status gr_request_release(gr_ctx *ctx, uint64_t request_id);
 gr_status gr_render_resident_static(gr_ctx *ctx, uint64_t scene_id, uint32_t sample_offset, uint32_t spp,
                                     float *film_device, void *stream);
 
+/* ---- frame-delta streaming (the worker's tracer / emitter split) ------------------ */
+
+/* One render request streamed as FRAME deltas, replacing the worker's stream emitter
+ * around the render path (apps/gemray-worker/src/stream_emit/: tracer.rs:64-117
+ * run_tracer, emitter.rs:46-96 PendingDelta, sizing.rs:22-30 next_batch_size,
+ * downsample.rs:17-53 downsample_preview; apps/gemray-worker/docs/architecture.md:
+ * 33-129).  gr_stream_open starts a tracer thread that renders samples
+ * [first_sample, first_sample + samples) of a resident scene in sub-batches, each
+ * sized from the previous one's device time toward target_ms (x4 growth at most,
+ * never 0), starting at first_batch samples; every sub-batch is traced into a zeroed
+ * film (one per-pixel sum in sample order, the film a render_core::
+ * trace_samples_with_gpu call returns) and then folded into the pending delta (copied
+ * when the delta is empty, else added) and into the running total (added).  The
+ * caller drains the delta on its own cadence with gr_stream_take: the payload is the
+ * radiance wire format itself (W*H*3 little-endian f32 = W*H*12 bytes,
+ * crates/gemray-net/src/radiance/mod.rs:26-67) and its contiguous sample range.
+ * Drains never wait for a sub-batch in progress: the tracer folds into one of two
+ * delta buffers while the other is copied out.  Cancellation (gr_stream_cancel) is
+ * observed between sub-batches; the pending delta is then discarded.  fixed_batch != 0
+ * replaces the adaptive sizing by sub-batches of exactly that many samples (the last
+ * one shorter).  A stream keeps its scene resident: gr_scene_release returns
+ * GR_EBUSY until the stream is closed.  Calls on one stream are thread-safe, except
+ * that none may overlap its gr_stream_close. */
+typedef struct gr_stream_opts {
+    uint32_t target_ms;   /* sub-batch device-time target; 0 = 100 (sizing.rs:7) */
+    uint32_t first_batch; /* first sub-batch in samples; 0 = 1 (tracer.rs:82) */
+    uint32_t fixed_batch; /* != 0: every sub-batch has this many samples */
+    uint32_t reserved;
+} gr_stream_opts;
+
+typedef enum gr_stream_state {
+    GR_STREAM_RUNNING = 0,
+    GR_STREAM_FINISHED = 1,  /* every sample traced and folded */
+    GR_STREAM_CANCELLED = 2, /* stopped between sub-batches by gr_stream_cancel */
+    GR_STREAM_FAILED = 3     /* a CUDA error stopped the tracer; see gr_stream_status */
+} gr_stream_state;
+
+gr_status gr_stream_open(gr_ctx *ctx, uint64_t scene_id, uint32_t first_sample, uint32_t samples,
+                         const gr_stream_opts *opts /* NULL = defaults */, uint64_t *out_stream);
+/* The pending delta (PendingDelta::take): writes W*H*3 floats to xyz_host and its
+ * range; *samples = 0 (and nothing written) when nothing is pending or the stream was
+ * cancelled. */
+gr_status gr_stream_take(gr_ctx *ctx, uint64_t stream, uint32_t *first_sample, uint32_t *samples, float *xyz_host);
+/* samples folded so far, the gr_stream_state, and the tracer's error (GR_OK unless
+ * FAILED). */
+gr_status gr_stream_status(gr_ctx *ctx, uint64_t stream, uint32_t *samples_done, uint32_t *state,
+                           gr_status *tracer_error);
+/* The running total (W*H*3 floats), as of the last folded sub-batch. */
+gr_status gr_stream_total(gr_ctx *ctx, uint64_t stream, float *xyz_host);
+/* downsample_preview of the running total to tw x th (box mean, tw/th 0 -> 1). */
+gr_status gr_stream_preview(gr_ctx *ctx, uint64_t stream, uint32_t tw, uint32_t th, float *xyz_host);
+gr_status gr_stream_cancel(gr_ctx *ctx, uint64_t stream);
+/* Stops the tracer (as gr_stream_cancel), joins it and frees the stream. */
+gr_status gr_stream_close(gr_ctx *ctx, uint64_t stream);
+/* The sizing rule (sizing.rs:22-30): prev * target / elapsed, clamped to
+ * [1, max(prev * 4, 1)] (u32 saturating), rounded; elapsed 0 -> max(prev * 4, 1). */
+uint32_t gr_next_batch_size(uint32_t prev, double elapsed_ms, double target_ms);
+
 /* ---- engine controls ---------------------------------------------------------- */
 
 /* Transport kernel selection.  PLAIN (default): one thread per (pixel, sample)

@@ -216,6 +216,42 @@ int gro_probe_grid(const gr_scene *sc, uint32_t grid, uint32_t spp, uint32_t sal
     return GR_OK;
 }
 
+// downsample_preview (apps/gemray-worker/src/stream_emit/downsample.rs:17-53): the box
+// mean of the running total over each preview pixel's source block, summed row by row
+// from zero in f32 and divided by the count as f32.
+void gro_downsample_preview(const float *src, uint32_t w, uint32_t h, uint32_t tw, uint32_t th, float *out) {
+    const size_t TW = tw ? tw : 1, TH = th ? th : 1;
+    for (size_t i = 0; i < 3 * TW * TH; ++i) out[i] = 0.0f;
+    if (w == 0 || h == 0) return;
+    for (size_t oy = 0; oy < TH; ++oy) {
+        const size_t y0 = oy * h / TH;
+        size_t y1 = (oy + 1) * h / TH;
+        if (y1 < y0 + 1) y1 = y0 + 1;
+        if (y1 > h) y1 = h;
+        for (size_t ox = 0; ox < TW; ++ox) {
+            const size_t x0 = ox * w / TW;
+            size_t x1 = (ox + 1) * w / TW;
+            if (x1 < x0 + 1) x1 = x0 + 1;
+            if (x1 > w) x1 = w;
+            float s[3] = {0.0f, 0.0f, 0.0f};
+            uint32_t count = 0;
+            for (size_t y = y0; y < y1; ++y)
+                for (size_t x = x0; x < x1; ++x) {
+                    const float *p = src + 3 * (y * w + x);
+                    s[0] = s[0] + p[0];
+                    s[1] = s[1] + p[1];
+                    s[2] = s[2] + p[2];
+                    ++count;
+                }
+            float *o = out + 3 * (oy * TW + ox);
+            if (count) {
+                const float c = (float)count;
+                o[0] = s[0] / c; o[1] = s[1] / c; o[2] = s[2] / c;
+            }
+        }
+    }
+}
+
 // BiaxialIndicatrix entry points (optics/birefringence.rs:349-839) for the property
 // tests: an indicatrix from three principal indices and a frame given as columns
 // (ax0, ax1, ax2), or from a material at a wavelength (materials.rs:1508-1519).

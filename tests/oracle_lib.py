@@ -90,6 +90,8 @@ def lib():
     L.gro_biaxial_poynting.argtypes = [F, F, F, fp, fp, C.c_int, fp]
     L.gro_material_indicatrix.restype = C.c_int
     L.gro_material_indicatrix.argtypes = [C.POINTER(abi.gr_material), F, fp, fp]
+    L.gro_downsample_preview.restype = None
+    L.gro_downsample_preview.argtypes = [fp, U, U, U, U, fp]
     L.gro_accumulate.restype = C.c_int
     L.gro_accumulate.argtypes = [sc, U, U, fp, C.c_int]
     L.gro_accumulate_f64.restype = C.c_int

@@ -288,6 +288,67 @@ def stream_view(r, sid: int, sc, first: int, spp: int, cadence_ms: float = 50.0)
             "how": "gr_stream_open .. last gr_stream_take, host wall clock, one frame of the workload"}
 
 
+def denoise_view(r, sc, film, count: int, stream, reps: int = 5) -> dict:
+    """The display path of a progressive render on the device: guide pass
+    (gr_guide_buffers_device) and denoise + tone map of the frame's running sum
+    (gr_denoise_tonemap_device, 5 A-Trous passes), CUDA events on the context stream,
+    mean of `reps` after one warm-up; plus the oracle's single-threaded filter on a
+    crop of the frame, scaled by area (the reference filters on the CPU)."""
+    import torch
+    from gemray_studio_b200 import abi
+    lib, ctx = r.lib, r.ctx
+    n = sc.width * sc.height
+    with torch.cuda.stream(stream):
+        depth = torch.empty(n, dtype=torch.float32, device="cuda")
+        normal = torch.empty((n, 3), dtype=torch.float32, device="cuda")
+        facet = torch.empty(n, dtype=torch.int32, device="cuda")
+        rgba = torch.empty((n, 4), dtype=torch.uint8, device="cuda")
+
+    def guide():
+        assert lib.gr_guide_buffers_device(ctx, C.byref(sc.c_scene()), depth.data_ptr(), normal.data_ptr(),
+                                           facet.data_ptr(), None) == abi.GR_OK
+
+    def dn():
+        assert lib.gr_denoise_tonemap_device(ctx, film.data_ptr(), count, depth.data_ptr(), normal.data_ptr(),
+                                             facet.data_ptr(), sc.width, sc.height, None, rgba.data_ptr(),
+                                             None) == abi.GR_OK
+
+    out = {}
+    for name, fn in (("guide_ms", guide), ("denoise_tonemap_ms", dn)):
+        fn()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        out[name] = a.elapsed_time(b) / reps
+    # oracle filter (one thread) on a 480x270 crop of the averaged frame and its guides
+    try:
+        import sys
+        sys.path.insert(0, str(Path(__file__).resolve().parent / "tests"))
+        import oracle_lib
+        o = oracle_lib.lib()
+        cw, ch = min(480, sc.width), min(270, sc.height)
+        avg = (film.float() * (1.0 / count)).cpu().numpy().reshape(sc.height, sc.width, 3)[:ch, :cw].copy()
+        d = depth.cpu().numpy().reshape(sc.height, sc.width)[:ch, :cw].copy()
+        nrm = normal.cpu().numpy().reshape(sc.height, sc.width, 3)[:ch, :cw].copy()
+        fc = facet.cpu().numpy().reshape(sc.height, sc.width)[:ch, :cw].copy()
+        res = np.empty_like(avg)
+        fp, ip = C.POINTER(C.c_float), C.POINTER(C.c_int32)
+        t0 = time.perf_counter()
+        o.gro_atrous_denoise(avg.ctypes.data_as(fp), d.ctypes.data_as(fp), nrm.ctypes.data_as(fp),
+                             fc.ctypes.data_as(ip), cw, ch, count, 5, 0.35, 0.1, 64.0, 4.0, 0.02, res.ctypes.data_as(fp))
+        out["cpu_oracle_ms_full_frame"] = (time.perf_counter() - t0) * 1e3 * (n / (cw * ch))
+        out["cpu_oracle_how"] = f"oracle A-Trous, 1 thread, {cw}x{ch} crop scaled by area"
+    except Exception as e:  # the oracle is optional on the bench host
+        out["cpu_oracle_ms_full_frame"] = None
+        out["cpu_oracle_how"] = f"unavailable: {e}"
+    out["pixels"] = n
+    out["passes"] = 5
+    return out
+
+
 def run_engine(args):
     world, rank, local = dist_setup()
     import torch
@@ -380,6 +441,7 @@ def run_engine(args):
     metrics_ms = (time.perf_counter() - t1) * 1e3
 
     fstream = stream_view(r, sid.value, sc, base + (args.warmup + args.steps) * spp, spp) if world == 1 else None
+    dnv = denoise_view(r, sc, film, (args.warmup + args.steps) * spp, stream) if world == 1 else None
 
     trace_ms_per_launch = tr.value / max(1, ntr.value)
     frames = args.steps
@@ -412,6 +474,7 @@ def run_engine(args):
                                  "fire_index": [round(float(v), 3) for v in mvals[:, 1]],
                                  "scintillation_pct": [round(float(v), 3) for v in mvals[:, 2]]},
             "frame_stream": fstream,
+            "denoise": dnv,
             "gpu_launches": int(ntr.value + nfo.value),  # this library's trace + fold launches
             "clocks": clk,
             "device": r.adapter_label(),

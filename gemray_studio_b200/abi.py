@@ -141,6 +141,12 @@ class gr_stream_opts(C.Structure):
 GR_STREAM_RUNNING, GR_STREAM_FINISHED, GR_STREAM_CANCELLED, GR_STREAM_FAILED = 0, 1, 2, 3
 
 
+class gr_atrous_params(C.Structure):
+    _fields_ = [("num_passes", C.c_uint32), ("sigma_color", C.c_float), ("sigma_depth", C.c_float),
+                ("normal_power", C.c_float), ("taper_reference_spp", C.c_float),
+                ("taper_identity_epsilon", C.c_float)]
+
+
 class gr_environment(C.Structure):
     _fields_ = [
         ("mode", C.c_uint32), ("uniform_rgb", C.c_float * 3),
@@ -243,6 +249,19 @@ EXPORTS = [
     ("gr_stream_cancel", C.c_int, [_ctx_p, C.c_uint64]),
     ("gr_stream_close", C.c_int, [_ctx_p, C.c_uint64]),
     ("gr_next_batch_size", C.c_uint32, [C.c_uint32, C.c_double, C.c_double]),
+    ("gr_guide_buffers", C.c_int, [_ctx_p, C.POINTER(gr_scene), C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                   C.POINTER(C.c_int32)]),
+    ("gr_guide_buffers_device", C.c_int, [_ctx_p, C.POINTER(gr_scene), C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_void_p]),
+    ("gr_atrous_denoise", C.c_int, [_ctx_p, C.POINTER(C.c_float), C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                    C.POINTER(C.c_int32), C.c_uint32, C.c_uint32, C.c_uint32,
+                                    C.POINTER(gr_atrous_params), C.POINTER(C.c_float)]),
+    ("gr_atrous_denoise_device", C.c_int, [_ctx_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                           C.c_uint32, C.c_uint32, C.POINTER(gr_atrous_params), C.c_void_p,
+                                           C.c_void_p]),
+    ("gr_denoise_tonemap_device", C.c_int, [_ctx_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p,
+                                            C.c_uint32, C.c_uint32, C.POINTER(gr_atrous_params), C.c_void_p,
+                                            C.c_void_p]),
     ("gr_timing_enable", C.c_int, [_ctx_p, C.c_uint32]),
     ("gr_timing_read", C.c_int, [_ctx_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_uint64),
                                  C.POINTER(C.c_uint64)]),

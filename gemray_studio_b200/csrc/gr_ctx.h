@@ -82,6 +82,9 @@ struct gr_ctx {
     // gr_stream_* frame-delta streams (gr_stream.cu)
     std::map<uint64_t, FrameStream *> streams;
     uint64_t next_stream_id = 1;
+    // guide pass and A-Trous scratch (gr_denoise.cu)
+    grh::DeviceBuffer dn_a, dn_b, dn_n, dn_g, dn_in, dn_out, dn_planes;
+    cudaEvent_t dn_ev = nullptr;
     uint64_t resident_bytes = 0;
 };
 

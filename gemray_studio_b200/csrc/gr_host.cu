@@ -599,6 +599,10 @@ gr_status gr_destroy(gr_ctx *ctx) {
         ctx->counter.release();
         ctx->rgba.release();
         ctx->metrics.release();
+        for (grh::DeviceBuffer *b : {&ctx->dn_a, &ctx->dn_b, &ctx->dn_n, &ctx->dn_g, &ctx->dn_in, &ctx->dn_out,
+                                     &ctx->dn_planes})
+            b->release();
+        if (ctx->dn_ev) cudaEventDestroy(ctx->dn_ev);
         for (int k = 0; k < gr_ctx::kStageSlots; ++k) {
             if (ctx->stage_host[k]) cudaFreeHost(ctx->stage_host[k]);
             if (ctx->stage_ev[k]) cudaEventDestroy(ctx->stage_ev[k]);

@@ -519,6 +519,46 @@ gr_status gr_stream_close(gr_ctx *ctx, uint64_t stream);
  * [1, max(prev * 4, 1)] (u32 saturating), rounded; elapsed 0 -> max(prev * 4, 1). */
 uint32_t gr_next_batch_size(uint32_t prev, double elapsed_ms, double target_ms);
 
+/* ---- denoiser: guide pass and edge-avoiding A-Trous ------------------------------- */
+
+/* = AtrousParams (crates/gemray/src/renderer/denoise/mod.rs:188-230); a NULL params
+ * pointer means AtrousParams::default(): 5 passes, sigma_color 0.35, sigma_depth 0.1,
+ * normal_power 64, taper_reference_spp 4, taper_identity_epsilon 0.02. */
+typedef struct gr_atrous_params {
+    uint32_t num_passes; /* clamped to [1, 8]; pass k dilates the 5x5 B3 kernel by 2^k */
+    float sigma_color;   /* scaled by the taper 1 / sqrt(1 + spp / taper_reference_spp) */
+    float sigma_depth;
+    float normal_power;
+    float taper_reference_spp;
+    float taper_identity_epsilon; /* taper below this: the output is the input, bit for bit */
+} gr_atrous_params;
+
+/* The guide pass (apps/diagram-gui/src/bridge/guide_pass.rs, generate_guide_buffers):
+ * for each pixel the primary ray through the pixel's corner (zero jitter) against the
+ * scene's planes -- depth = hit t, normal = the hit plane's normal, facet_id = its
+ * index, or (1e6, 0, -1) on a miss.  Reads only the scene's camera, width, height and
+ * planes.  Host outputs (W*H, W*H*3, W*H), or device outputs ordered on `stream`. */
+gr_status gr_guide_buffers(gr_ctx *ctx, const gr_scene *scene, float *depth, float *normal, int32_t *facet_id);
+gr_status gr_guide_buffers_device(gr_ctx *ctx, const gr_scene *scene, float *depth, float *normal,
+                                  int32_t *facet_id, void *stream);
+
+/* AtrousDenoiser::denoise_into (denoise/mod.rs:560-684): `color` is the averaged XYZ
+ * image (W*H*3), guides as produced by the guide pass, spp the sample count behind
+ * the average; out (W*H*3) must not alias color.  Host or device buffers. */
+gr_status gr_atrous_denoise(gr_ctx *ctx, const float *color, const float *depth, const float *normal,
+                            const int32_t *facet_id, uint32_t width, uint32_t height, uint32_t spp,
+                            const gr_atrous_params *params, float *out);
+gr_status gr_atrous_denoise_device(gr_ctx *ctx, const float *color, const float *depth, const float *normal,
+                                   const int32_t *facet_id, uint32_t width, uint32_t height, uint32_t spp,
+                                   const gr_atrous_params *params, float *out, void *stream);
+
+/* denoise_and_tonemap_frame (apps/diagram-gui/src/bridge/render_thread/denoise.rs):
+ * the running-sum film scaled by 1 / sample_count, denoised with spp = sample_count,
+ * tone-mapped at scale 1 to RGBA8 (W*H*4) -- all on the device. */
+gr_status gr_denoise_tonemap_device(gr_ctx *ctx, const float *film, uint32_t sample_count, const float *depth,
+                                    const float *normal, const int32_t *facet_id, uint32_t width, uint32_t height,
+                                    const gr_atrous_params *params, void *rgba, void *stream);
+
 /* ---- engine controls ---------------------------------------------------------- */
 
 /* Transport kernel selection.  PLAIN (default): one thread per (pixel, sample)

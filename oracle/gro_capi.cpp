@@ -252,6 +252,126 @@ void gro_downsample_preview(const float *src, uint32_t w, uint32_t h, uint32_t t
     }
 }
 
+// The denoiser's guide pass (apps/diagram-gui/src/bridge/guide_pass.rs:
+// generate_guide_buffers): per pixel the primary ray through the pixel's corner
+// (generate_ray with zero jitter) against the stone -- t, the hit plane's normal and
+// its index, or (1e6, 0, -1) on a miss.
+void gro_guide_buffers(const gr_scene *sc, float *depth, float *normal, int32_t *facet) {
+    const float w = (float)sc->width, h = (float)sc->height;
+    for (uint32_t y = 0; y < sc->height; ++y)
+        for (uint32_t x = 0; x < sc->width; ++x) {
+            const size_t i = (size_t)y * sc->width + x;
+            const Ray<float> ray = generate_ray(sc->camera, (float)x, (float)y, w, h, 0.0f, 0.0f);
+            const Hit<float> hit = intersect_polyhedron<float>(ray, sc->planes, sc->n_planes);
+            depth[i] = hit.hit ? hit.t : 1.0e6f;
+            normal[3 * i + 0] = hit.hit ? hit.normal.x : 0.0f;
+            normal[3 * i + 1] = hit.hit ? hit.normal.y : 0.0f;
+            normal[3 * i + 2] = hit.hit ? hit.normal.z : 0.0f;
+            facet[i] = hit.hit ? hit.facet : -1;
+        }
+}
+
+// Edge-avoiding A-Trous denoiser (crates/gemray/src/renderer/denoise/mod.rs:154-690),
+// single-threaded (the reference's result is thread-count invariant): taper of the
+// colour sigma with spp, identity copy below the taper epsilon, 1..8 passes of the
+// dilated 5x5 B3 kernel gated by facet id, normal cosine power, depth and colour.
+namespace atrous {
+static inline float sanitize(float v) { return std::isfinite(v) ? v : 0.0f; }
+static inline float cos_pow(float base, float power) {  // :294-311
+    if (power >= 0.0f && power == std::floor(power) && power <= 4294967295.0f) {
+        const uint32_t ip = (uint32_t)power;
+        if (ip != 0 && (ip & (ip - 1)) == 0) {
+            float v = base;
+            for (uint32_t k = ip; k > 1; k >>= 1) v *= v;
+            return v;
+        }
+    }
+    return ::powf(base, power);
+}
+}  // namespace atrous
+
+float gro_taper_strength(uint32_t spp, float n0_in) {  // :244-250
+    const float n0 = rmax(n0_in, 1.0e-8f);
+    return 1.0f / ::sqrtf(1.0f + (float)spp / n0);
+}
+
+float gro_cos_pow(float base, float power) { return atrous::cos_pow(base, power); }
+
+void gro_atrous_denoise(const float *color, const float *depth, const float *normal, const int32_t *facet, uint32_t w,
+                        uint32_t h, uint32_t spp, uint32_t num_passes_in, float sigma_color, float sigma_depth_in,
+                        float normal_power, float taper_ref, float taper_eps, float *out) {
+    using namespace atrous;
+    const size_t len = (size_t)w * h;
+    if (len == 0) return;
+    const float taper = gro_taper_strength(spp, taper_ref);
+    const uint32_t num_passes = num_passes_in < 1 ? 1 : (num_passes_in > 8 ? 8 : num_passes_in);
+    if (taper < taper_eps) {
+        std::memcpy(out, color, len * 3 * sizeof(float));
+        return;
+    }
+    const float sce = rmax(sigma_color * taper, 0.0f);
+    std::vector<float> ping(color, color + 3 * len), pong(3 * len), nn(3 * len);
+    for (size_t i = 0; i < len; ++i) {  // unit_normal_or_zero (:268-276)
+        const V3<float> n(sanitize(normal[3 * i]), sanitize(normal[3 * i + 1]), sanitize(normal[3 * i + 2]));
+        const float l = ::sqrtf(n.dot(n));
+        const bool z = l <= 1.0e-8f;
+        nn[3 * i + 0] = z ? 0.0f : n.x / l;
+        nn[3 * i + 1] = z ? 0.0f : n.y / l;
+        nn[3 * i + 2] = z ? 0.0f : n.z / l;
+    }
+    const float sd = rmax(sigma_depth_in, 1.0e-8f);
+    const float scs = rmax(sce * sce, 1.0e-8f);
+    const float nisd = -1.0f / sd;
+    const float nits = -1.0f / (2.0f * scs);
+    const float np = rmax(normal_power, 0.0f);
+    static const float B3[5] = {1.0f / 16.0f, 1.0f / 4.0f, 3.0f / 8.0f, 1.0f / 4.0f, 1.0f / 16.0f};
+    for (uint32_t pass = 0; pass < num_passes; ++pass) {
+        const int64_t stride = (int64_t)1 << pass;
+        for (int64_t y = 0; y < (int64_t)h; ++y)
+            for (int64_t x = 0; x < (int64_t)w; ++x) {  // atrous_pixel (:383-444)
+                const size_t c = (size_t)y * w + x;
+                const V3<float> cc(ping[3 * c], ping[3 * c + 1], ping[3 * c + 2]);
+                const V3<float> cn(nn[3 * c], nn[3 * c + 1], nn[3 * c + 2]);
+                const bool cn_zero = cn.x == 0.0f && cn.y == 0.0f && cn.z == 0.0f;
+                const float cdep = sanitize(depth[c]);
+                V3<float> sum(0.0f, 0.0f, 0.0f);
+                float wsum = 0.0f;
+                for (int ky = 0; ky < 5; ++ky) {
+                    const int64_t sy = y + (ky - 2) * stride;
+                    if (sy < 0 || sy >= (int64_t)h) continue;
+                    for (int kx = 0; kx < 5; ++kx) {
+                        const int64_t sx = x + (kx - 2) * stride;
+                        if (sx < 0 || sx >= (int64_t)w) continue;
+                        const size_t q = (size_t)sy * w + sx;
+                        const float kw = B3[ky] * B3[kx];
+                        const float wf = facet[c] == facet[q] ? 1.0f : 0.0f;
+                        if (wf == 0.0f) continue;
+                        const V3<float> qn(nn[3 * q], nn[3 * q + 1], nn[3 * q + 2]);
+                        float wn = 1.0f;
+                        if (!cn_zero && !(qn.x == 0.0f && qn.y == 0.0f && qn.z == 0.0f))
+                            wn = cos_pow(rmax(clampr(cn.dot(qn), -1.0f, 1.0f), 0.0f), np);
+                        const float wd = ::expf(std::fabs(cdep - sanitize(depth[q])) * nisd);
+                        const V3<float> qc(ping[3 * q], ping[3 * q + 1], ping[3 * q + 2]);
+                        const V3<float> dc(sanitize(cc.x) - sanitize(qc.x), sanitize(cc.y) - sanitize(qc.y),
+                                           sanitize(cc.z) - sanitize(qc.z));
+                        const float wc = ::expf(dc.dot(dc) * nits);
+                        const float wgt = (((kw * wf) * wn) * wd) * wc;
+                        sum = sum + qc * wgt;
+                        wsum = wsum + wgt;
+                    }
+                }
+                float *o = &pong[3 * c];
+                if (wsum > 1.0e-8f) {
+                    o[0] = sum.x / wsum; o[1] = sum.y / wsum; o[2] = sum.z / wsum;
+                } else {
+                    o[0] = cc.x; o[1] = cc.y; o[2] = cc.z;
+                }
+            }
+        ping.swap(pong);
+    }
+    std::memcpy(out, ping.data(), len * 3 * sizeof(float));
+}
+
 // BiaxialIndicatrix entry points (optics/birefringence.rs:349-839) for the property
 // tests: an indicatrix from three principal indices and a frame given as columns
 // (ax0, ax1, ax2), or from a material at a wavelength (materials.rs:1508-1519).

@@ -92,6 +92,14 @@ def lib():
     L.gro_material_indicatrix.argtypes = [C.POINTER(abi.gr_material), F, fp, fp]
     L.gro_downsample_preview.restype = None
     L.gro_downsample_preview.argtypes = [fp, U, U, U, U, fp]
+    L.gro_guide_buffers.restype = None
+    L.gro_guide_buffers.argtypes = [sc, fp, fp, C.POINTER(C.c_int32)]
+    L.gro_taper_strength.restype = F
+    L.gro_taper_strength.argtypes = [U, F]
+    L.gro_cos_pow.restype = F
+    L.gro_cos_pow.argtypes = [F, F]
+    L.gro_atrous_denoise.restype = None
+    L.gro_atrous_denoise.argtypes = [fp, fp, fp, C.POINTER(C.c_int32), U, U, U, U, F, F, F, F, F, fp]
     L.gro_accumulate.restype = C.c_int
     L.gro_accumulate.argtypes = [sc, U, U, fp, C.c_int]
     L.gro_accumulate_f64.restype = C.c_int

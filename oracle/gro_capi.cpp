@@ -372,6 +372,15 @@ void gro_atrous_denoise(const float *color, const float *depth, const float *nor
     std::memcpy(out, ping.data(), len * 3 * sizeof(float));
 }
 
+// shading_normal_near_edge (optics/raytracer/intersect.rs:196-229), for the edge
+// rounding unit tests.
+void gro_shading_normal(const gr_plane *planes, uint32_t n, const float hp[3], int hit_idx, const float hn[3],
+                        float radius, float out[3]) {
+    const V3<float> r = shading_normal_near_edge<float>(planes, n, V3<float>(hp[0], hp[1], hp[2]), hit_idx,
+                                                        V3<float>(hn[0], hn[1], hn[2]), radius);
+    out[0] = r.x; out[1] = r.y; out[2] = r.z;
+}
+
 // BiaxialIndicatrix entry points (optics/birefringence.rs:349-839) for the property
 // tests: an indicatrix from three principal indices and a frame given as columns
 // (ax0, ax1, ax2), or from a material at a wavelength (materials.rs:1508-1519).

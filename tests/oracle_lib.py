@@ -100,6 +100,8 @@ def lib():
     L.gro_cos_pow.argtypes = [F, F]
     L.gro_atrous_denoise.restype = None
     L.gro_atrous_denoise.argtypes = [fp, fp, fp, C.POINTER(C.c_int32), U, U, U, U, F, F, F, F, F, fp]
+    L.gro_shading_normal.restype = None
+    L.gro_shading_normal.argtypes = [C.POINTER(abi.gr_plane), U, fp, C.c_int, fp, F, fp]
     L.gro_accumulate.restype = C.c_int
     L.gro_accumulate.argtypes = [sc, U, U, fp, C.c_int]
     L.gro_accumulate_f64.restype = C.c_int

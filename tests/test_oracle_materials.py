@@ -162,3 +162,58 @@ def test_scattering_changes_face_up_y(oracle):
     clear = _probe(oracle, S.Scene(14, 14, PLANES, d, CAM), 14, 96, 0x0BADF00D, 12)
     hazy = _probe(oracle, S.Scene(14, 14, PLANES, _scattering(d, 1.5, 0.3), CAM), 14, 96, 0x0BADF00D, 12)
     assert abs(hazy[1] - clear[1]) / clear[1] > 0.01, (clear[1], hazy[1])
+
+
+# ---- edge rounding (optics/raytracer/intersect.rs:196-229 and its tests :312-600) ----
+
+def _corner_planes():
+    return (abi.gr_plane * 2)(abi.gr_plane((0.0, 1.0, 0.0), 0.0), abi.gr_plane((1.0, 0.0, 0.0), 0.0))
+
+
+def _shade(oracle, hp, idx, hn, radius):
+    out = (C.c_float * 3)()
+    oracle.gro_shading_normal(_corner_planes(), 2, (C.c_float * 3)(*hp), idx, (C.c_float * 3)(*hn), radius, out)
+    return np.array(out, np.float32)
+
+
+def test_edge_rounding_unit_properties(oracle):
+    up, right = (0.0, 1.0, 0.0), (1.0, 0.0, 0.0)
+    for r in (0.0, -1.0, -0.001):  # disabled: the flat normal, unchanged
+        assert _shade(oracle, (0, 0, 5), 0, up, r).tolist() == [0.0, 1.0, 0.0]
+    a, b = _shade(oracle, (0, 0, 5), 0, up, 1.0), _shade(oracle, (0, 0, 5), 1, right, 1.0)
+    bis = np.array([1, 1, 0], np.float32) / np.float32(np.sqrt(2))
+    assert np.linalg.norm(a - b) < 1e-5 and np.linalg.norm(a - bis) < 1e-5  # continuous; the bisector at the edge
+    assert _shade(oracle, (-10, 0, 5), 0, up, 1.0).tolist() == [0.0, 1.0, 0.0]  # interior stays flat
+    t = np.float32(0.5)
+    st = t * t * np.float32(3.0 - 2.0 * 0.5)
+    exp = np.array(up, np.float32) * (1 - st) + bis * st
+    exp /= np.linalg.norm(exp)
+    assert np.linalg.norm(_shade(oracle, (-0.5, 0, 5), 0, up, 1.0) - exp) < 1e-5  # the smoothstep blend
+
+
+def _rounded(m: abi.gr_material, radius: float) -> abi.gr_material:
+    m = abi.gr_material.from_buffer_copy(m)
+    m.edge_rounding_radius = radius
+    return m
+
+
+def test_edge_rounding_default_off_bit_identical(oracle):
+    d = S.builtin_material("Diamond")
+    env = dict(preset="Daylight", exposure=1.0, light_yaw=0.4, light_pitch=0.35)
+    a = _probe(oracle, S.Scene(6, 6, PLANES, d, CAM, **env), 6, 4, 0x2468ACE0, 10)
+    b = _probe(oracle, S.Scene(6, 6, PLANES, _rounded(d, 0.0), CAM, **env), 6, 4, 0x2468ACE0, 10)
+    assert a.tobytes() == b.tobytes()
+
+
+def test_edge_rounding_changes_face_up_y(oracle):
+    d = S.builtin_material("Diamond")
+    sharp = _probe(oracle, S.Scene(16, 16, PLANES, d, CAM), 16, 128, 0xF00DCAFE, 12)
+    rounded = _probe(oracle, S.Scene(16, 16, PLANES, _rounded(d, 0.02), CAM), 16, 128, 0xF00DCAFE, 12)
+    assert abs(rounded[1] - sharp[1]) / sharp[1] > 0.005, (sharp[1], rounded[1])
+
+
+def test_edge_rounding_white_furnace(oracle):
+    m = _rounded(S.custom_material(1.5, 0.0, 0.0), 0.03)
+    mean = _probe(oracle, S.Scene(12, 12, PLANES, m, CAM, **UNIFORM), 12, 96, 0xABAD1DEA, 16)
+    err = np.abs(mean - _target(oracle)) / _target(oracle)
+    assert np.all(err <= 0.06), err

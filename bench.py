@@ -239,10 +239,11 @@ def run_reference(args):
 
 
 def traffic_per_launch(tuples_per_launch: float):
-    """DRAM bytes (read + write) of one k_trace_plain launch: the per-tuple traffic of
-    the committed ncu capture (profiles/k_trace_plain_traffic.json) times the tuples
-    one launch processes, or None without a capture."""
-    p = ROOT / "profiles" / "k_trace_plain_traffic.json"
+    """DRAM bytes (read + write) of one transport launch (the staged kernels' three
+    stages): the per-tuple traffic of the committed ncu capture
+    (profiles/k_trace_staged_traffic.json) times the tuples one launch processes, or
+    None without a capture."""
+    p = ROOT / "profiles" / "k_trace_staged_traffic.json"
     if not p.exists():
         return None
     per_tuple = json.loads(p.read_text())["dram_bytes_per_tuple"]
@@ -458,7 +459,7 @@ def run_engine(args):
             "config": workload_config(args.workload, w, f"sample-range shards x{world}" if world > 1 else "single GPU"),
             "e2e": {"value": e2e_value, "unit": "path-samples/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
-            "roofline": {"bound": "fp32", "kernel": "k_trace_plain", "achieved": achieved, "peak": fp32_peak,
+            "roofline": {"bound": "fp32", "kernel": "k_trace_stage1 + k_trace_stage2 x2 (staged transport)", "achieved": achieved, "peak": fp32_peak,
                          "unit": "TFLOP/s", "frac": achieved / fp32_peak,
                          "traffic": traffic_per_launch(samples_per_step / max(1, ntr.value / frames)),
                          "hbm_view": hbm_view(samples_per_step / max(1, ntr.value / frames),

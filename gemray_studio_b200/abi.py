@@ -53,6 +53,7 @@ GR_EVENT_COUNT = len(EVENT_NAMES)
 GR_KERNEL_PLAIN = 0
 GR_KERNEL_WAVEFRONT = 1
 GR_KERNEL_REGEN = 2
+GR_KERNEL_STAGED = 3
 GR_STATIC_SCRATCH_BYTES = 16 << 20
 GR_STATIC_SCRATCH_TUPLES = GR_STATIC_SCRATCH_BYTES // 12
 

@@ -54,10 +54,12 @@ struct gr_ctx {
     uint64_t serve_budget = 60ull << 30;
     int sm_count = 0;
     grh::DeviceBuffer xyz, film, planes, map, ext, counter, rgba, metrics;
-    int kernel_mode = GR_KERNEL_PLAIN;
+    int kernel_mode = GR_KERNEL_STAGED;
     // wavefront engine pool (gr_wavefront.cuh)
     uint32_t wave_cap = 1u << 18;
     grh::DeviceBuffer wf_pool, wf_events, wf_queues, wf_cnt;
+    // staged kernels' park buffer (count word, then parked path records)
+    grh::DeviceBuffer park;
     uint32_t *wf_done_host = nullptr;
     // Optional per-launch timing of the trace and fold kernels (CUDA events on the
     // launch stream); read back by gr_timing_read.
@@ -117,8 +119,9 @@ struct LaunchRange;
 namespace grh {
 // Tuples [0, R.n_tuples) of one chunk traced into xyz on `stream` with kernel `mode`
 // (gr_host.cu), and the ordered per-pixel fold of n_pixels pixels into film.
+// STAGED mode parks paths in `park` (the context's buffer when NULL).
 gr_status launch_trace(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuffers &B, const grd::LaunchRange &R,
-                       float *xyz, cudaStream_t stream, int mode);
+                       float *xyz, cudaStream_t stream, int mode, grh::DeviceBuffer *park = nullptr);
 gr_status launch_fold(const float *xyz, uint32_t n_pixels, uint32_t spp, uint32_t first_pixel, float *film,
                       uint32_t kahan, cudaStream_t stream);
 }  // namespace grh

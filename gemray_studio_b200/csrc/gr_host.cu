@@ -421,7 +421,7 @@ gr_status launch_wavefront(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuf
 
 // Trace tuples [0, R.n_tuples) of one chunk into xyz (device).
 gr_status launch_trace(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuffers &B, const grd::LaunchRange &R,
-                       float *xyz, cudaStream_t stream, int mode) {
+                       float *xyz, cudaStream_t stream, int mode, grh::DeviceBuffer *park_buf) {
     if (R.n_tuples == 0) return GR_OK;
     size_t smem = grd::planes_smem_bytes(S.n_planes);
     const bool extras = grd::needs_extras(S);
@@ -443,6 +443,44 @@ gr_status launch_trace(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuffers
         else
             grd::k_trace_plain<grd::NoCounters><<<(unsigned)plain_blocks, grd::TRACE_THREADS, smem, stream>>>(S, B, R, xyz,
                                                                                                            nullptr);
+        GR_CUDA(cudaGetLastError());
+        return GR_OK;
+    }
+    if (mode == GR_KERNEL_STAGED) {
+        // park buffers: stage 1 parks up to 1/8 of the launch's paths (at most 4 GiB),
+        // stage 2 up to 1/4 of that; overflowing paths finish where they are
+        uint64_t cap1 = (R.n_tuples + 7) / 8;
+        const uint64_t max_cap = (4ull << 30) / sizeof(grd::Path);
+        if (cap1 > max_cap) cap1 = max_cap;
+        if (cap1 < 1024) cap1 = 1024;
+        const uint64_t cap2 = GR_STAGE_CAP2 == 0xFFFFFFFFu ? 0 : (cap1 + 3) / 4;
+        grh::DeviceBuffer &pk = park_buf ? *park_buf : ctx->park;
+        gr_status st = pk.reserve((size_t)(cap1 + cap2) * sizeof(grd::Path) + 256);
+        if (st != GR_OK) return st;
+        unsigned int *counts = (unsigned int *)pk.ptr;
+        grd::Path *park1 = (grd::Path *)((char *)pk.ptr + 256);
+        grd::Path *park2 = park1 + cap1;
+        GR_CUDA(cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned int), stream));
+        const grd::ParkOut out1{park1, (uint32_t)cap1, counts};
+        const grd::ParkOut out2{park2, (uint32_t)cap2, counts + 1};
+        const grd::ParkOut none{nullptr, 0, nullptr};
+        const unsigned b2 = (unsigned)((cap1 + grd::TRACE_THREADS - 1) / grd::TRACE_THREADS);
+        const unsigned b3 = (unsigned)((cap2 + grd::TRACE_THREADS - 1) / grd::TRACE_THREADS);
+        if (extras) {
+            grd::k_trace_stage1<true><<<(unsigned)plain_blocks, grd::TRACE_THREADS, smem, stream>>>(S, B, R, xyz, out1);
+            grd::k_trace_stage2<true><<<b2, grd::TRACE_THREADS, smem, stream>>>(S, B, park1, (uint32_t)cap1, counts,
+                                                                                GR_STAGE_CAP2, out2, xyz);
+            if (cap2)
+                grd::k_trace_stage2<true><<<b3, grd::TRACE_THREADS, smem, stream>>>(S, B, park2, (uint32_t)cap2,
+                                                                                    counts + 1, 0xFFFFFFFFu, none, xyz);
+        } else {
+            grd::k_trace_stage1<false><<<(unsigned)plain_blocks, grd::TRACE_THREADS, smem, stream>>>(S, B, R, xyz, out1);
+            grd::k_trace_stage2<false><<<b2, grd::TRACE_THREADS, smem, stream>>>(S, B, park1, (uint32_t)cap1, counts,
+                                                                                 GR_STAGE_CAP2, out2, xyz);
+            if (cap2)
+                grd::k_trace_stage2<false><<<b3, grd::TRACE_THREADS, smem, stream>>>(S, B, park2, (uint32_t)cap2,
+                                                                                     counts + 1, 0xFFFFFFFFu, none, xyz);
+        }
         GR_CUDA(cudaGetLastError());
         return GR_OK;
     }
@@ -507,7 +545,9 @@ gr_status render_into(gr_ctx *ctx, const gr_scene *sc, const SceneConst &S, cons
         st = launch_trace(ctx, S, B, R, (float *)ctx->xyz.ptr, stream, ctx->kernel_mode);
         if (st != GR_OK) return st;
         if (tev) cudaEventRecord(tev[1], stream);
-        ctx->trace_launches++;
+        // kernel launches of one trace: stage 1, 2 and 3 in STAGED mode
+        ctx->trace_launches += (ctx->kernel_mode == GR_KERNEL_STAGED && S.max_bounces > 0 &&
+                                !(S.flags & GR_FLAG_FP64_RESOLVE)) ? 3 : 1;
         cudaEvent_t *fev = timing_slot(ctx, ctx->fold_ev, ctx->fold_used);
         if (fev) cudaEventRecord(fev[0], stream);
         st = launch_fold((const float *)ctx->xyz.ptr, (uint32_t)np, spp, (uint32_t)first, film_dev,
@@ -599,6 +639,7 @@ gr_status gr_destroy(gr_ctx *ctx) {
         ctx->counter.release();
         ctx->rgba.release();
         ctx->metrics.release();
+        ctx->park.release();
         for (grh::DeviceBuffer *b : {&ctx->dn_a, &ctx->dn_b, &ctx->dn_n, &ctx->dn_g, &ctx->dn_in, &ctx->dn_out,
                                      &ctx->dn_planes})
             b->release();
@@ -1041,7 +1082,8 @@ gr_status gr_angular_profile(gr_ctx *ctx, const gr_plane *planes, uint32_t n_pla
 
 gr_status gr_set_kernel(gr_ctx *ctx, uint32_t kernel) {
     if (!ctx) return fail(GR_EINVAL, "ctx is NULL");
-    if (kernel != GR_KERNEL_PLAIN && kernel != GR_KERNEL_WAVEFRONT && kernel != GR_KERNEL_REGEN)
+    if (kernel != GR_KERNEL_PLAIN && kernel != GR_KERNEL_WAVEFRONT && kernel != GR_KERNEL_REGEN &&
+        kernel != GR_KERNEL_STAGED)
         return fail(GR_EINVAL, "unknown kernel %u", kernel);
     std::lock_guard<std::mutex> lk(ctx->mu);
     ctx->kernel_mode = (int)kernel;

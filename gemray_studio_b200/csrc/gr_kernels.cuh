@@ -45,6 +45,111 @@ __global__ void __launch_bounds__(TRACE_THREADS, GR_TRACE_MIN_BLOCKS) k_trace_pl
     }
 }
 
+// Staged kernels.  Within a warp path lengths differ widely (on the c2 brilliant the
+// warp's longest path averages ~2.6x the mean), so a warp spends most of its bounce
+// iterations on a few long paths with the other lanes idle.  Stage 1 runs every path
+// for at most GR_STAGE_CAP bounces; a path still alive then is parked -- its record
+// copied to a park buffer in warp-aggregated slots -- and a continuation stage
+// resumes the parked paths, now packed densely, one per thread, again up to a cap
+// (GR_STAGE_CAP2) with its own park buffer for a final, uncapped stage.  A path whose
+// slot would overflow a park buffer simply continues in place.  Each path runs the
+// same functions in the same order as in the plain kernel, so every XYZ is
+// bit-identical; only the schedule differs.
+#ifndef GR_STAGE_CAP
+#define GR_STAGE_CAP 12
+#endif
+#ifndef GR_STAGE_CAP2
+#define GR_STAGE_CAP2 20
+#endif
+
+struct ParkOut {
+    Path *park;
+    uint32_t cap;
+    unsigned int *count;
+};
+
+// Bounces P up to `cap` (absolute bounce index), then parks it in `out` if still alive
+// and a slot is free; returns true when parked.  A path that cannot be parked is run
+// to its end.  Every lane of the warp must call this (the slot ballot), `active`
+// false for lanes without a path.
+template <bool EXTRAS>
+__device__ __forceinline__ bool run_or_park(Path &P, const SceneConst &S, const Planes &PL, bool active, uint32_t cap,
+                                            const ParkOut &out) {
+    NoCounters nc;
+    const uint32_t lane = threadIdx.x & 31u;
+    for (int round = 0; round < 2; ++round) {
+        if (active) {
+            while ((state_bits(P) & F_ALIVE) && p_bounce(P) < cap) {
+                Event E;
+                const uint32_t ev = step_hit<1, NoCounters, false, EXTRAS>(P, S, PL, E, nc);
+                if (ev == EV_REFLECT) step_reflect<1, NoCounters, EXTRAS>(P, S, E, nc);
+                else if (ev == EV_REFRACT) step_refract<1, NoCounters, EXTRAS>(P, S, E, nc);
+            }
+        }
+        if (round == 1 || out.cap == 0) break;
+        const bool want = active && (state_bits(P) & F_ALIVE);
+        const uint32_t mask = __ballot_sync(0xffffffffu, want);
+        if (mask == 0u) break;
+        uint32_t base = 0;
+        const uint32_t leader = __ffs(mask) - 1;
+        if (lane == leader) base = atomicAdd(out.count, (unsigned)__popc(mask));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (want) {
+            const uint32_t slot = base + __popc(mask & ((1u << lane) - 1u));
+            if (slot < out.cap) {
+                out.park[slot] = P;
+                return true;
+            }
+        }
+        cap = 0xFFFFFFFFu;  // park buffer full: finish in place
+    }
+    return false;
+}
+
+template <bool EXTRAS>
+__global__ void __launch_bounds__(TRACE_THREADS, GR_TRACE_MIN_BLOCKS) k_trace_stage1(SceneConst S, SceneBuffers B,
+                                                                                     LaunchRange R,
+                                                                                     float *__restrict__ xyz,
+                                                                                     ParkOut out) {
+    extern __shared__ float4 s_planes[];
+    const Planes PL = stage_plane_set(s_planes, B.planes, S.n_planes);
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = t < R.n_tuples;
+    Path P;
+    if (active) {
+        uint32_t pixel, sample;
+        tuple_coords(R, t, pixel, sample);
+        path_init<1, EXTRAS>(P, S, B, pixel, sample, (uint32_t)t);
+    }
+    if (run_or_park<EXTRAS>(P, S, PL, active, GR_STAGE_CAP, out) || !active) return;
+    const V3 c = path_finish<1>(P, S, B);
+    xyz[3 * t + 0] = c.x;
+    xyz[3 * t + 1] = c.y;
+    xyz[3 * t + 2] = c.z;
+}
+
+// Continuation: parked paths [0, min(*count_in, cap_in)) resumed one per thread, up to
+// `bounce_cap`, survivors parked in `out` (out.cap 0: run to the end).
+template <bool EXTRAS>
+__global__ void __launch_bounds__(TRACE_THREADS, GR_TRACE_MIN_BLOCKS) k_trace_stage2(
+    SceneConst S, SceneBuffers B, const Path *__restrict__ park_in, uint32_t cap_in,
+    const unsigned int *__restrict__ count_in, uint32_t bounce_cap, ParkOut out, float *__restrict__ xyz) {
+    const uint32_t n = min((uint32_t)*count_in, cap_in);
+    if ((uint64_t)blockIdx.x * blockDim.x >= n) return;  // whole block past the parked paths
+    extern __shared__ float4 s_planes[];
+    const Planes PL = stage_plane_set(s_planes, B.planes, S.n_planes);
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = i < n;
+    Path P;
+    if (active) P = park_in[i];
+    if (run_or_park<EXTRAS>(P, S, PL, active, bounce_cap, out) || !active) return;
+    const V3 c = path_finish<1>(P, S, B);
+    const uint64_t t = p_tuple(P);
+    xyz[3 * t + 0] = c.x;
+    xyz[3 * t + 1] = c.y;
+    xyz[3 * t + 2] = c.z;
+}
+
 // Path-regeneration kernel.  Path lengths within a warp vary widely (on a brilliant
 // the mean is ~3.7 bounces but the warp's longest path averages ~12), so a warp
 // that runs each lane's path to its end idles most lanes most of the time.  Here

@@ -102,7 +102,7 @@ struct FrameStream {
     cudaStream_t main = nullptr, side = nullptr;
     cudaEvent_t folded = nullptr, drained = nullptr, t0 = nullptr, t1 = nullptr;
     bool drained_recorded = false;
-    grh::DeviceBuffer scratch, batch, pending[2], total, preview;
+    grh::DeviceBuffer scratch, batch, pending[2], total, preview, park;
     std::mutex mu;       // tracer <-> drains: cur, empty, range, progress, state
     std::mutex emit_mu;  // serialises the drains (take / total / preview) of this stream
     int cur = 0;
@@ -145,7 +145,8 @@ gr_status trace_subbatch(FrameStream *fs, uint32_t bfirst, uint32_t n) {
         R.sample_offset = bfirst;
         R.spp = n;
         R.n_tuples = np * n;
-        st = grh::launch_trace(fs->ctx, fs->S, fs->B, R, (float *)fs->scratch.ptr, fs->main, GR_KERNEL_PLAIN);
+        st = grh::launch_trace(fs->ctx, fs->S, fs->B, R, (float *)fs->scratch.ptr, fs->main, GR_KERNEL_STAGED,
+                               &fs->park);
         if (st != GR_OK) return st;
         st = grh::launch_fold((const float *)fs->scratch.ptr, (uint32_t)np, n, (uint32_t)p0, (float *)fs->batch.ptr,
                               (fs->S.flags & GR_FLAG_KAHAN_FILM) ? 1u : 0u, fs->main);
@@ -257,6 +258,7 @@ void destroy_stream(FrameStream *fs) {
     fs->pending[1].release();
     fs->total.release();
     fs->preview.release();
+    fs->park.release();
     for (cudaEvent_t ev : {fs->folded, fs->drained, fs->t0, fs->t1})
         if (ev) cudaEventDestroy(ev);
     if (fs->main) cudaStreamDestroy(fs->main);

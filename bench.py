@@ -579,7 +579,7 @@ def run_batch(args):
                                f" px square, spp 32-512, Kahan films, one gr_render_batch call per step (CUDA graph)",
                    "path_samples_per_step": tuples, "scale": s, "l2": "flushed between steps (256 MiB device write)"},
         "serial_plain": {"value": tuples / (ms_serial * 1e-3), "ms_per_step": ms_serial,
-                         "how": "the same 64 renders, one gr_render_resident call (plain kernel) per stone"},
+                         "how": "the same 64 renders, one gr_render_resident call (single-scene staged kernels) per stone"},
         "batched_over_serial": ms_serial / ms_batch,
         "e2e": {"value": tuples / (ms_e2e * 1e-3), "unit": "path-samples/s", "h2d_bytes_per_step": film_bytes,
                 "d2h_bytes_per_step": film_bytes},
@@ -693,7 +693,7 @@ def run_serve(args):
         "serial_plain": {"value": render_tuples / rep_span, "p50": float(np.percentile(lat_rep, 50)),
                          "p99": float(np.percentile(lat_rep, 99)),
                          "how": "the same arrival schedule replayed in real time through a serial server: each "
-                                "request rendered alone with gr_render_resident (plain kernel) in arrival order"},
+                                "request rendered alone with gr_render_resident (single-scene staged kernels) in arrival order"},
         "serial_plain_model": {"value": render_tuples / (ser_span * 1e-3), "p50": float(np.percentile(lat_ser, 50)),
                                "p99": float(np.percentile(lat_ser, 99)),
                                "how": "FIFO queue model from device-timed service times alone (no host cost)"},

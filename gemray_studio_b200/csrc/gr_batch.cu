@@ -9,6 +9,10 @@
 // and the per-pixel fold order are those of the single-scene kernels: every film is
 // bit-identical to rendering its item alone with gr_render_resident.
 //
+// Launches are staged like the single-scene renders (gr_stage.cuh): k_trace_batch runs
+// paths up to the stage cap and parks the survivors in their segment's park region,
+// k_trace_batch_cont finishes them, one block per 128 parked paths of one segment.
+//
 // With GR_BATCH_GRAPH the launch sequence is captured once as a CUDA graph and
 // replayed whenever the same batch shape recurs (same scenes, films, spp, frame sizes
 // and tables); only the device tables, which carry the sample offsets, are uploaded
@@ -33,6 +37,7 @@ struct Launch {
     uint64_t blocks, warps;
     uint32_t max_planes;
     bool extras;  // a segment's scene has frosted facets, scattering or a biaxial material
+    uint64_t park_paths, park_blocks;  // park slots over the launch's segments, continuation blocks
 };
 
 struct Plan {
@@ -40,19 +45,50 @@ struct Plan {
     std::vector<grd::BatchSegment> segs;
     std::vector<Launch> launches;
     uint64_t max_tuples = 0;  // scratch tuples one launch needs
+    uint64_t max_park = 0;    // park slots one launch needs
+    uint32_t max_segs = 0;    // segments of the largest launch (park slot counters)
 };
+
+// Park slots per launch: 1/16 of its tuples (paths alive after the stage cap are a few
+// percent on the stones measured), at most 4 GiB of records; a segment whose region
+// fills up finishes the rest of its paths in stage 1.
+constexpr uint64_t kBatchParkLimit = (4ull << 30) / sizeof(grd::Path);
+
+void place_park(Plan &P, Launch &L) {
+    uint64_t tuples = 0;
+    for (uint32_t i = 0; i < L.seg_count; ++i) tuples += P.segs[L.seg_first + i].R.n_tuples;
+    const double scale = std::min(1.0 / 16.0, (double)kBatchParkLimit / (double)std::max<uint64_t>(tuples, 1));
+    uint64_t off = 0, blocks = 0;
+    for (uint32_t i = 0; i < L.seg_count; ++i) {
+        grd::BatchSegment &g = P.segs[L.seg_first + i];
+        uint64_t cap = (uint64_t)((double)g.R.n_tuples * scale) + 32;
+        if (cap > g.R.n_tuples) cap = g.R.n_tuples;
+        g.park_cap = (uint32_t)cap;
+        g.park_off = off;
+        g.park_block_begin = blocks;
+        off += cap;
+        blocks += (cap + grd::TRACE_THREADS - 1) / grd::TRACE_THREADS;
+    }
+    L.park_paths = off;
+    L.park_blocks = blocks;
+    P.max_park = std::max(P.max_park, off);
+    P.max_segs = std::max(P.max_segs, L.seg_count);
+}
 
 // Cuts the items into launches of at most `budget` tuples (a pixel whose spp alone
 // exceeds the budget gets a launch of its own).  xyz pointers are offsets from 0
 // until the scratch is placed.
 gr_status make_plan(gr_ctx *ctx, const grh::BatchItem *items, uint32_t n_items, uint64_t budget, Plan &P) {
     std::unordered_map<uint64_t, uint32_t> slot_of;
-    Launch cur{0, 0, 0, 0, 0, false};
+    Launch cur{0, 0, 0, 0, 0, false, 0, 0};
     uint64_t used = 0;
     auto close = [&]() {
-        if (cur.seg_count) P.launches.push_back(cur);
+        if (cur.seg_count) {
+            place_park(P, cur);
+            P.launches.push_back(cur);
+        }
         P.max_tuples = std::max(P.max_tuples, used);
-        cur = Launch{(uint32_t)P.segs.size(), 0, 0, 0, 0, false};
+        cur = Launch{(uint32_t)P.segs.size(), 0, 0, 0, 0, false, 0, 0};
         used = 0;
     };
     for (uint32_t i = 0; i < n_items; ++i) {
@@ -130,14 +166,24 @@ size_t grown(size_t cap, size_t need, size_t limit) {
     return want;
 }
 
-gr_status launch_plan(const Plan &P, const grd::SceneSlot *slots, const grd::BatchSegment *segs, cudaStream_t s) {
+gr_status launch_plan(const Plan &P, const grd::SceneSlot *slots, const grd::BatchSegment *segs, void *park_buf,
+                      cudaStream_t s) {
+    unsigned int *counts = (unsigned int *)park_buf;
+    grd::Path *park = (grd::Path *)((char *)park_buf + (((size_t)P.max_segs * sizeof(unsigned int) + 255) & ~(size_t)255));
     for (const Launch &L : P.launches) {
-        if (L.extras)
-            grd::k_trace_batch<true><<<(unsigned)L.blocks, grd::TRACE_THREADS, grd::planes_smem_bytes(L.max_planes), s>>>(
-                slots, segs + L.seg_first, L.seg_count);
-        else
-            grd::k_trace_batch<false><<<(unsigned)L.blocks, grd::TRACE_THREADS, grd::planes_smem_bytes(L.max_planes), s>>>(
-                slots, segs + L.seg_first, L.seg_count);
+        const size_t smem = grd::planes_smem_bytes(L.max_planes);
+        GR_CUDA(cudaMemsetAsync(counts, 0, (size_t)L.seg_count * sizeof(unsigned int), s));
+        if (L.extras) {
+            grd::k_trace_batch<true><<<(unsigned)L.blocks, grd::TRACE_THREADS, smem, s>>>(slots, segs + L.seg_first,
+                                                                                          L.seg_count, park, counts);
+            grd::k_trace_batch_cont<true><<<(unsigned)L.park_blocks, grd::TRACE_THREADS, smem, s>>>(
+                slots, segs + L.seg_first, L.seg_count, park, counts);
+        } else {
+            grd::k_trace_batch<false><<<(unsigned)L.blocks, grd::TRACE_THREADS, smem, s>>>(slots, segs + L.seg_first,
+                                                                                           L.seg_count, park, counts);
+            grd::k_trace_batch_cont<false><<<(unsigned)L.park_blocks, grd::TRACE_THREADS, smem, s>>>(
+                slots, segs + L.seg_first, L.seg_count, park, counts);
+        }
         const unsigned T = 256;
         grd::k_fold_batch<<<(unsigned)((L.warps * 32 + T - 1) / T), T, 0, s>>>(segs + L.seg_first, L.seg_count);
     }
@@ -146,10 +192,12 @@ gr_status launch_plan(const Plan &P, const grd::SceneSlot *slots, const grd::Bat
 }
 
 // The shape a captured graph is valid for: everything but the sample offsets.
-std::vector<uint64_t> graph_key(const Plan &P, const void *tables, const void *xyz) {
+std::vector<uint64_t> graph_key(const Plan &P, const void *tables, const void *xyz, const void *park) {
     std::vector<uint64_t> k;
     k.push_back((uint64_t)(uintptr_t)tables);
     k.push_back((uint64_t)(uintptr_t)xyz);
+    k.push_back((uint64_t)(uintptr_t)park);
+    k.push_back(P.max_segs);
     k.push_back(P.slots.size());
     for (const grd::BatchSegment &g : P.segs) {
         k.push_back((uint64_t)(uintptr_t)g.film);
@@ -180,6 +228,10 @@ gr_status batch_enqueue(gr_ctx *ctx, const BatchItem *items, uint32_t n_items, u
     const size_t seg_bytes = P.segs.size() * sizeof(grd::BatchSegment);
     st = ctx->batch_tables.reserve(grown(ctx->batch_tables.cap, slot_bytes + seg_bytes, SIZE_MAX));
     if (st != GR_OK) return st;
+    const size_t park_bytes = (((size_t)P.max_segs * sizeof(unsigned int) + 255) & ~(size_t)255) +
+                              (size_t)P.max_park * sizeof(grd::Path);
+    st = ctx->batch_park.reserve(grown(ctx->batch_park.cap, park_bytes, SIZE_MAX));
+    if (st != GR_OK) return st;
     float *xyz = (float *)ctx->xyz.ptr;
     for (grd::BatchSegment &g : P.segs) g.xyz = xyz + ((uintptr_t)g.xyz) / sizeof(float);
     grd::SceneSlot *d_slots = (grd::SceneSlot *)ctx->batch_tables.ptr;
@@ -205,16 +257,16 @@ gr_status batch_enqueue(gr_ctx *ctx, const BatchItem *items, uint32_t n_items, u
     GR_CUDA(cudaMemcpyAsync(ctx->batch_tables.ptr, h, slot_bytes + seg_bytes, cudaMemcpyHostToDevice, s));
     GR_CUDA(cudaEventRecord(ctx->stage_ev[k], s));
 
-    if (!(flags & GR_BATCH_GRAPH)) return launch_plan(P, d_slots, d_segs, s);
+    if (!(flags & GR_BATCH_GRAPH)) return launch_plan(P, d_slots, d_segs, ctx->batch_park.ptr, s);
 
-    const std::vector<uint64_t> key = graph_key(P, ctx->batch_tables.ptr, ctx->xyz.ptr);
+    const std::vector<uint64_t> key = graph_key(P, ctx->batch_tables.ptr, ctx->xyz.ptr, ctx->batch_park.ptr);
     cudaGraphExec_t exec = nullptr;
     for (const BatchGraph &g : ctx->batch_graphs)
         if (g.key == key) exec = g.exec;
     if (!exec) {
         cudaGraph_t graph = nullptr;
         GR_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-        st = launch_plan(P, d_slots, d_segs, s);
+        st = launch_plan(P, d_slots, d_segs, ctx->batch_park.ptr, s);
         cudaError_t e = cudaStreamEndCapture(s, &graph);
         if (st != GR_OK) {
             if (graph) cudaGraphDestroy(graph);

@@ -2,7 +2,7 @@
 // environment and film) in one grid.  Included by gr_batch.cu only.
 #pragma once
 
-#include "gr_launch.cuh"
+#include "gr_stage.cuh"
 
 namespace grd {
 
@@ -27,59 +27,103 @@ struct BatchSegment {
     uint32_t scene;        // index into the SceneSlot table
     uint32_t kahan;
     uint32_t cont;         // fold_pixel continue mode
-    uint32_t pad;
+    uint32_t park_cap;     // park slots of this segment (paths alive after the stage cap)
+    uint64_t park_off;     // first park slot of this segment in the launch's park buffer
+    uint64_t park_block_begin;  // first continuation block of the segment
 };
 
-template <bool BY_WARP>
+// KEY 0: trace blocks, 1: fold warps, 2: continuation blocks.
+template <int KEY>
 __device__ __forceinline__ uint32_t find_segment(const BatchSegment *__restrict__ segs, uint32_t n, uint64_t key) {
     uint32_t lo = 0, hi = n;  // last segment whose begin <= key
     while (hi - lo > 1) {
         const uint32_t mid = (lo + hi) >> 1;
-        const uint64_t b = BY_WARP ? segs[mid].warp_begin : segs[mid].block_begin;
+        const uint64_t b = KEY == 1 ? segs[mid].warp_begin : (KEY == 2 ? segs[mid].park_block_begin : segs[mid].block_begin);
         if (b <= key) lo = mid;
         else hi = mid;
     }
     return lo;
 }
 
-// EXTRAS: the variant for launches holding a scene with frosted facets or scattering.
+__device__ __forceinline__ void load_slot(SceneSlot &dst_slot, const SceneSlot *__restrict__ src_slot) {
+    const uint32_t *src = reinterpret_cast<const uint32_t *>(src_slot);
+    uint32_t *dst = reinterpret_cast<uint32_t *>(&dst_slot);
+    for (uint32_t i = threadIdx.x; i < sizeof(SceneSlot) / 4; i += blockDim.x) dst[i] = src[i];
+}
+
+// Stage 1 of a batched launch (the staged scheme of the single-scene kernels): paths
+// run up to GR_STAGE_CAP bounces; survivors are parked in their segment's park region
+// (`park`, slot counters `counts` per segment of the launch) for k_trace_batch_cont.
+// EXTRAS: the variant for launches holding a scene with frosted facets, scattering or
+// a biaxial material.
 template <bool EXTRAS>
 __global__ void __launch_bounds__(TRACE_THREADS, GR_TRACE_MIN_BLOCKS)
-    k_trace_batch(const SceneSlot *__restrict__ slots, const BatchSegment *__restrict__ segs, uint32_t n_segs) {
+    k_trace_batch(const SceneSlot *__restrict__ slots, const BatchSegment *__restrict__ segs, uint32_t n_segs,
+                  Path *__restrict__ park, unsigned int *__restrict__ counts) {
     __shared__ SceneSlot s_slot;
     __shared__ uint32_t s_seg;
     extern __shared__ float4 s_planes[];
-    if (threadIdx.x == 0) s_seg = find_segment<false>(segs, n_segs, blockIdx.x);
+    if (threadIdx.x == 0) s_seg = find_segment<0>(segs, n_segs, blockIdx.x);
     __syncthreads();
     const BatchSegment &G = segs[s_seg];
-    {
-        const uint32_t *src = reinterpret_cast<const uint32_t *>(slots + G.scene);
-        uint32_t *dst = reinterpret_cast<uint32_t *>(&s_slot);
-        for (uint32_t i = threadIdx.x; i < sizeof(SceneSlot) / 4; i += blockDim.x) dst[i] = src[i];
-    }
+    load_slot(s_slot, slots + G.scene);
     __syncthreads();
     const SceneConst &S = s_slot.S;
     const SceneBuffers &B = s_slot.B;
     const Planes PL = stage_plane_set(s_planes, B.planes, S.n_planes);
     const LaunchRange R = G.R;
     const uint64_t t = (uint64_t)(blockIdx.x - G.block_begin) * blockDim.x + threadIdx.x;
-    if (t < R.n_tuples) {
+    const bool active = t < R.n_tuples;
+    Path P;
+    if (active) {
         uint32_t pixel, sample;
         tuple_coords(R, t, pixel, sample);
-        Path P;
         path_init<1, EXTRAS>(P, S, B, pixel, sample, (uint32_t)t);
-        NoCounters nc;
-        const V3 c = trace_path<NoCounters, false, EXTRAS>(P, S, B, PL, nc);
-        float *xyz = G.xyz;
-        xyz[3 * t + 0] = c.x;
-        xyz[3 * t + 1] = c.y;
-        xyz[3 * t + 2] = c.z;
     }
+    const ParkOut out{park + G.park_off, G.park_cap, counts + s_seg};
+    if (run_or_park<EXTRAS>(P, S, PL, active, GR_STAGE_CAP, out) || !active) return;
+    const V3 c = path_finish<1>(P, S, B);
+    float *xyz = G.xyz;
+    xyz[3 * t + 0] = c.x;
+    xyz[3 * t + 1] = c.y;
+    xyz[3 * t + 2] = c.z;
+}
+
+// Stage 2: each block resumes up to 128 parked paths of one segment (its scene in
+// shared memory, as in stage 1) and runs them to their end.
+template <bool EXTRAS>
+__global__ void __launch_bounds__(TRACE_THREADS, GR_TRACE_MIN_BLOCKS)
+    k_trace_batch_cont(const SceneSlot *__restrict__ slots, const BatchSegment *__restrict__ segs, uint32_t n_segs,
+                       const Path *__restrict__ park, const unsigned int *__restrict__ counts) {
+    __shared__ SceneSlot s_slot;
+    __shared__ uint32_t s_seg;
+    extern __shared__ float4 s_planes[];
+    if (threadIdx.x == 0) s_seg = find_segment<2>(segs, n_segs, blockIdx.x);
+    __syncthreads();
+    const BatchSegment &G = segs[s_seg];
+    const uint32_t n = min((uint32_t)counts[s_seg], G.park_cap);
+    const uint64_t j0 = (uint64_t)(blockIdx.x - G.park_block_begin) * blockDim.x;
+    if (j0 >= n) return;  // block-uniform: no thread of this block reaches a barrier
+    load_slot(s_slot, slots + G.scene);
+    __syncthreads();
+    const SceneConst &S = s_slot.S;
+    const SceneBuffers &B = s_slot.B;
+    const Planes PL = stage_plane_set(s_planes, B.planes, S.n_planes);
+    const uint64_t i = j0 + threadIdx.x;
+    if (i >= n) return;
+    Path P = park[G.park_off + i];
+    NoCounters nc;
+    const V3 c = trace_path<NoCounters, false, EXTRAS>(P, S, B, PL, nc);
+    const uint64_t t = p_tuple(P);
+    float *xyz = G.xyz;
+    xyz[3 * t + 0] = c.x;
+    xyz[3 * t + 1] = c.y;
+    xyz[3 * t + 2] = c.z;
 }
 
 __global__ void k_fold_batch(const BatchSegment *__restrict__ segs, uint32_t n_segs) {
     const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const BatchSegment &G = segs[find_segment<true>(segs, n_segs, warp)];
+    const BatchSegment &G = segs[find_segment<1>(segs, n_segs, warp)];
     const uint64_t px = warp - G.warp_begin;
     if (px >= G.R.n_pixels) return;  // the grid's last warps past the final segment
     fold_pixel(G.xyz, px, G.R.spp, G.R.first_pixel + (uint32_t)px, G.film, G.kahan, G.cont, G.comp);

@@ -70,7 +70,7 @@ struct gr_ctx {
     // gr_render_batch: scene-slot + segment tables, captured launch sequences, and a
     // ring of pinned host staging buffers for the table uploads (a pageable source
     // would make each upload wait for the previous batch to reach its copy)
-    grh::DeviceBuffer batch_tables;
+    grh::DeviceBuffer batch_tables, batch_park;  // segment tables; staged park records + slot counters
     static constexpr int kStageSlots = 4;
     void *stage_host[kStageSlots] = {};
     size_t stage_cap[kStageSlots] = {};

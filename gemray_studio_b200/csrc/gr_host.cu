@@ -651,6 +651,7 @@ gr_status gr_destroy(gr_ctx *ctx) {
         for (BatchGraph &g : ctx->batch_graphs) cudaGraphExecDestroy(g.exec);
         ctx->batch_graphs.clear();
         ctx->batch_tables.release();
+        ctx->batch_park.release();
         ctx->wf_pool.release();
         ctx->wf_events.release();
         ctx->wf_queues.release();

@@ -62,9 +62,15 @@ def make_scene(name: str):
     planes = S.round_brilliant_57() if w["stone"] == "rb57" else S.emerald_cut_49()
     env_mode = {"uniform": abi.GR_ENV_UNIFORM, "latlong": abi.GR_ENV_LATLONG, "studio": abi.GR_ENV_STUDIO}[w["env"]]
     latlong = S.gaussian_blob_latlong(2048, 1024, 12, seed=0) if w["env"] == "latlong" else None
-    mat = S.builtin_material("Diamond") if w["stone"] == "rb57" else S.builtin_material("Emerald")
+    ext = None
+    if w["stone"] == "rb57":
+        mat = S.builtin_material("Diamond")
+    else:  # the emerald's uniaxial, dichroic material with a wavelength-dependent birefringence
+        from gemray_studio_b200 import workloads as W
+        mat, ext = W.birefringent_emerald_material()
     sc = S.Scene(width=w["width"], height=w["height"], planes=planes, material=mat, cam=S.camera(0.35, 0.28, 5.0, 18.0),
-                 max_bounces=w["max_bounces"], env_mode=env_mode, latlong=latlong, uniform_rgb=(1.0, 1.0, 1.0))
+                 max_bounces=w["max_bounces"], env_mode=env_mode, latlong=latlong, uniform_rgb=(1.0, 1.0, 1.0),
+                 ext=ext)
     return sc, w
 
 
@@ -74,7 +80,9 @@ def workload_config(name: str, w: dict, parallelism: str) -> dict:
     return {"workload": f"{name}: {stone}, {w['width']}x{w['height']}, {w['spp']} spp, max depth {w['max_bounces']}, "
                         f"{w['env']} environment",
             "width": w["width"], "height": w["height"], "spp": w["spp"], "max_bounces": w["max_bounces"],
-            "environment": w["env"], "material": "Diamond" if w["stone"] == "rb57" else "Emerald",
+            "environment": w["env"], "material": "Diamond" if w["stone"] == "rb57" else
+            "uniaxial Cauchy n_o 1.640+0.0042/l^2, n_e 1.620+0.0040/l^2 (wavelength-dependent birefringence), "
+            "dichroic absorption tables, random c-axis",
             "path_samples_per_step": w["width"] * w["height"] * w["spp"], "parallelism": parallelism,
             "l2": "flushed between steps (256 MiB device write)"}
 

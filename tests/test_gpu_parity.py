@@ -183,3 +183,38 @@ def test_tonemap_matches_oracle(renderer, oracle):
     diff = np.abs(got.astype(int) - ref.astype(int))
     assert diff.max() <= 1
     assert np.mean(diff == 0) > 0.999
+
+
+def test_staged_kernels_bit_identical_when_park_buffers_overflow(engine_lib):
+    """A light-trapping stone (n = 3.5): ~16% of paths outlive the first stage cap and
+    ~11% the second, more than the park buffers hold (1/8 and 1/32 of a launch's
+    tuples; 1/16 per batched segment), so the in-place completion path runs in every
+    stage.  Films stay bit-identical to the plain kernel's, single-scene and batched."""
+    import ctypes as C
+
+    import torch
+
+    from gemray_studio_b200 import GpuFrameRenderer
+    sc = S.Scene(width=40, height=32, planes=S.standard_round_brilliant(), material=S.custom_material(3.5, 0.0, 0.0),
+                 cam=S.camera(0.35, 0.28, 3.0, 18.0), max_bounces=64, env_mode=abi.GR_ENV_UNIFORM)
+    films = {}
+    for kernel in (abi.GR_KERNEL_PLAIN, abi.GR_KERNEL_STAGED):
+        r = GpuFrameRenderer(kernel=kernel)
+        acc = np.zeros((sc.width * sc.height, 3), np.float32)
+        r.accumulate(sc, 0, 64, acc)
+        films[kernel] = acc
+        if kernel == abi.GR_KERNEL_STAGED:
+            sid = C.c_uint64()
+            assert r.lib.gr_scene_upload(r.ctx, C.byref(sc.c_scene()), C.byref(sid)) == abi.GR_OK
+            f = torch.zeros((sc.width * sc.height, 3), dtype=torch.float32, device="cuda")
+            items = (abi.gr_batch_item * 1)(abi.gr_batch_item(sid.value, f.data_ptr(), 0, 64))
+            torch.cuda.synchronize()
+            assert r.lib.gr_render_batch(r.ctx, items, 1, 0, None) == abi.GR_OK
+            r.synchronize()
+            films["batch"] = f.cpu().numpy()
+            del f
+            r.lib.gr_scene_release(r.ctx, sid.value)
+        r.close()
+    ref = films[abi.GR_KERNEL_PLAIN].view(np.uint32)
+    assert np.array_equal(films[abi.GR_KERNEL_STAGED].view(np.uint32), ref)
+    assert np.array_equal(films["batch"].view(np.uint32), ref)

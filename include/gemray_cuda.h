@@ -17,6 +17,12 @@
  *     `GpuFacetPlane`, `GpuAbsorptionBand` and `GpuGemMaterial`
  *     (crates/gemray/src/geometry/plane.rs:6-9, renderer/buffers.rs:148-165,236-299),
  *     so a Rust caller can pass `bytemuck::bytes_of(&GpuGemMaterial::encode(m))`.
+ *   - Calls on one context are serialised by its mutex, and its device scratch (the
+ *     per-tuple XYZ chunk, the staged kernels' park records, batch tables) is reused
+ *     call after call in stream order.  Work a caller queues on its own streams must
+ *     therefore be ordered with the context's other work on the device (one stream,
+ *     or events).  The request loop queues on the context stream; frame streams own
+ *     their scratch and streams.
  */
 #ifndef GEMRAY_CUDA_H
 #define GEMRAY_CUDA_H

@@ -27,6 +27,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <string>
 #include <thread>
 
 #include "gr_ctx.h"
@@ -111,6 +112,7 @@ struct FrameStream {
     uint32_t samples_done = 0;
     uint32_t state = GR_STREAM_RUNNING;
     gr_status error = GR_OK;
+    std::string error_msg;  // the tracer thread's message (error strings are per thread)
     bool discarded = false;  // cancelled: pending deltas are dropped, not drained
     std::atomic<bool> cancel{false};
     std::thread tracer;
@@ -123,6 +125,7 @@ constexpr size_t kStreamScratchBudget = 256ull << 20;  // per-stream XYZ scratch
 gr_status stream_fail(FrameStream *fs, gr_status st) {
     std::lock_guard<std::mutex> lk(fs->mu);
     fs->error = st;
+    fs->error_msg = gr_last_error_string();
     fs->state = GR_STREAM_FAILED;
     return st;
 }
@@ -204,6 +207,7 @@ void tracer_main(FrameStream *fs) {
             if (e == cudaSuccess) e = cudaEventRecord(fs->folded, fs->main);
             if (e != cudaSuccess) {
                 fs->error = fail(GR_ECUDA, "stream fold failed: %s", cudaGetErrorString(e));
+                fs->error_msg = gr_last_error_string();
                 fs->state = GR_STREAM_FAILED;
                 return;
             }
@@ -224,6 +228,7 @@ void tracer_main(FrameStream *fs) {
     std::lock_guard<std::mutex> lk(fs->mu);
     if (e != cudaSuccess) {
         fs->error = fail(GR_ECUDA, "stream fold failed: %s", cudaGetErrorString(e));
+        fs->error_msg = gr_last_error_string();
         fs->state = GR_STREAM_FAILED;
     } else {
         fs->state = produced < fs->samples ? GR_STREAM_CANCELLED : GR_STREAM_FINISHED;
@@ -391,6 +396,8 @@ gr_status gr_stream_status(gr_ctx *ctx, uint64_t stream, uint32_t *samples_done,
     if (samples_done) *samples_done = fs->samples_done;
     if (state) *state = fs->state;
     if (tracer_error) *tracer_error = fs->error;
+    // make the tracer's message readable from this thread's gr_last_error_string()
+    if (fs->state == GR_STREAM_FAILED) fail(fs->error, "stream tracer: %s", fs->error_msg.c_str());
     return GR_OK;
 }
 

@@ -29,7 +29,7 @@ constexpr int NCH = 8;
 #define GR_ROT_UNROLL 8
 #endif
 #ifndef GR_RR_UNROLL
-#define GR_RR_UNROLL 8
+#define GR_RR_UNROLL 4  // measured on the c2 frame: 4 beats 8 / 2 / 1 by 1-3% (code layout)
 #endif
 constexpr int ROT_UNROLL = GR_ROT_UNROLL;
 constexpr int RR_UNROLL = GR_RR_UNROLL;

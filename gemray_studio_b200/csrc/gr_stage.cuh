@@ -23,6 +23,11 @@ namespace grd {
 #define GR_STAGE_CAP2 20
 #endif
 
+// Unroll factor of the per-channel loops in the staged kernels' bounce stages.
+#ifndef GR_STEP_UNROLL
+#define GR_STEP_UNROLL 1
+#endif
+
 struct ParkOut {
     Path *park;
     uint32_t cap;
@@ -42,9 +47,9 @@ __device__ __forceinline__ bool run_or_park(Path &P, const SceneConst &S, const 
         if (active) {
             while ((state_bits(P) & F_ALIVE) && p_bounce(P) < cap) {
                 Event E;
-                const uint32_t ev = step_hit<1, NoCounters, false, EXTRAS>(P, S, PL, E, nc);
-                if (ev == EV_REFLECT) step_reflect<1, NoCounters, EXTRAS>(P, S, E, nc);
-                else if (ev == EV_REFRACT) step_refract<1, NoCounters, EXTRAS>(P, S, E, nc);
+                const uint32_t ev = step_hit<GR_STEP_UNROLL, NoCounters, false, EXTRAS>(P, S, PL, E, nc);
+                if (ev == EV_REFLECT) step_reflect<GR_STEP_UNROLL, NoCounters, EXTRAS>(P, S, E, nc);
+                else if (ev == EV_REFRACT) step_refract<GR_STEP_UNROLL, NoCounters, EXTRAS>(P, S, E, nc);
             }
         }
         if (round == 1 || out.cap == 0) break;

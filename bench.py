@@ -511,7 +511,7 @@ def _flush_l2(flush, i, stream):
 def run_batch(args):
     """C4: 64 random stones (17-145 planes, six materials, Kahan films) rendered by
     one batched call per step (gr_render_batch, CUDA-graph replay) against the same
-    renders issued one scene at a time with gr_render_resident (the plain kernel)."""
+    renders issued one scene at a time with gr_render_resident (single-scene kernels)."""
     import torch
 
     from gemray_studio_b200 import GpuFrameRenderer, abi, build
@@ -604,7 +604,7 @@ def run_batch(args):
 def run_serve(args):
     """C5: Poisson render requests (plus 10% metric-only 64-tilt sweeps) over random
     stones through the request loop (gr_submit / gr_wait), against a FIFO server that
-    renders each request alone with the plain kernel (its measured service times)."""
+    renders each request alone with gr_render_resident, one scene per call (its measured service times)."""
     import torch
 
     from gemray_studio_b200 import abi, build, metrics as M
@@ -643,7 +643,7 @@ def run_serve(args):
     render_tuples = sum(stones[q.stone].scene.width * stones[q.stone].scene.height * q.spp for q in reqs
                         if not q.is_metrics)
     lat = np.array([s.latency_ms for s in stats])
-    # serial plain-kernel server: each request alone, in arrival order, one at a time
+    # serial unbatched server: each request alone, in arrival order, one at a time
     lib, ctx = srv.lib, srv.ctx
     stream = torch.cuda.ExternalStream(lib.gr_stream(ctx))
     films = {}
@@ -673,7 +673,7 @@ def run_serve(args):
     lat_ser = np.array(lat_ser)
     ser_span = max(finish, reqs[-1].arrival_s * 1e3) if reqs else 1.0
     # the same arrival schedule replayed in real time through a serial server: each
-    # request rendered alone, in arrival order, with the plain kernel
+    # request rendered alone, in arrival order, with the single-scene kernels
     lat_rep = []
     t0r = time.perf_counter()
     for q in reqs:

@@ -13,7 +13,9 @@
 //   * retirement -- when a tick's event completes its slices count as folded;
 //     a render is DONE when all its samples are; cancellation takes effect between
 //     slices;
-//   * metric requests (pose sweeps) run between ticks on the same stream.
+//   * metric requests (pose sweeps) skip admission (they hold no film): a second
+//     thread runs them in arrival order on its own high-priority stream, beside the
+//     tick in flight, so a sweep neither waits for a tick nor holds one up.
 // Slices fold in continue mode (fold_pixel): each slice carries the pixel's running
 // sum on from the film (and the Kahan compensation from a side buffer), and a request
 // starts on a zero film, so its film is one sequential per-pixel sum over all of its
@@ -41,11 +43,15 @@ using Clock = std::chrono::steady_clock;
 
 // A request's film (or Kahan compensation) from the stream-ordered allocator: taking
 // and returning it never synchronises the device, so admissions and releases do not
-// stall the ticks in flight.
+// stall the ticks in flight.  Films come from the serve loop's own pool, which keeps
+// the memory it has mapped (release threshold = the serve budget): the default pool
+// gives its free memory back at every synchronisation, and mapping it again on the
+// next admission was measured at 10-380 ms on B200 -- time the worker, which admits
+// under the serve lock, spent stalled with the ticks and every submitter behind it.
 struct StreamBuffer {
     void *ptr = nullptr;
-    cudaError_t alloc(size_t bytes, cudaStream_t s) {
-        cudaError_t e = cudaMallocAsync(&ptr, bytes, s);
+    cudaError_t alloc(size_t bytes, cudaStream_t s, cudaMemPool_t pool) {
+        cudaError_t e = pool ? cudaMallocFromPoolAsync(&ptr, bytes, pool, s) : cudaMallocAsync(&ptr, bytes, s);
         if (e != cudaSuccess) {
             ptr = nullptr;
             return e;
@@ -78,11 +84,26 @@ struct Request {
 
 // Path-samples one tick carries: ~10-30 ms of transport on B200, the latency quantum
 // of the request loop (a new arrival joins the tick after the one in flight).
-constexpr uint64_t kTickTuples = 8ull << 20;
+#ifndef GR_SERVE_TICK_MTUPLES
+#define GR_SERVE_TICK_MTUPLES 8
+#endif
+constexpr uint64_t kTickTuples = (uint64_t)GR_SERVE_TICK_MTUPLES << 20;
+// Slice order within a tick: 0 = arrival order, 1 = least remaining work first.
+#ifndef GR_SERVE_ORDER
+#define GR_SERVE_ORDER 0
+#endif
+// 1: while several renders are active none takes more than half of a tick.
+#ifndef GR_SERVE_HALF_CAP
+#define GR_SERVE_HALF_CAP 1
+#endif
 // Ticks queued on the device at once.  One: the host plans the next tick in ~0.1 ms,
 // so a second tick in flight buys no throughput and would make an arrival wait
 // behind two ticks instead of one.
 constexpr size_t kTicksInFlight = 1;
+// Film pool memory mapped when the serve loop starts (at most the serve budget), so
+// admissions map no memory until the live films pass it (~2,800 films of 384^2
+// pixels with Kahan compensation); growing the pool was measured at up to ~0.5 s.
+constexpr uint64_t kFilmPoolReserve = 4ull << 30;
 
 struct Tick {
     cudaEvent_t ev = nullptr;
@@ -97,16 +118,18 @@ double ms_between(Clock::time_point a, Clock::time_point b) {
 
 struct ServeState {
     std::mutex mu;
-    cudaStream_t metrics_stream = nullptr;  // metric sweeps run beside the ticks
+    cudaStream_t metrics_stream = nullptr;  // metric sweeps, beside the ticks
+    cudaMemPool_t film_pool = nullptr;      // request films (null: the device's default pool)
     grh::DeviceBuffer metrics_scratch;
-    std::condition_variable cv_work, cv_done;
+    std::condition_variable cv_work, cv_done, cv_metrics;
     std::unordered_map<uint64_t, Request *> reqs;
-    std::deque<uint64_t> queue;   // admission order
+    std::deque<uint64_t> queue;   // renders, admission order
+    std::deque<uint64_t> metric_queue;  // metric sweeps, arrival order
     std::vector<uint64_t> running;
     uint64_t next_id = 1;
     uint64_t film_bytes = 0;      // films of admitted requests
     bool stop = false;
-    std::thread worker;
+    std::thread worker, metrics_worker;
 };
 
 namespace {
@@ -128,13 +151,6 @@ void admit(gr_ctx *ctx, ServeState &sv, uint64_t resident_bytes) {
             finish(sv, q, GR_REQ_CANCELLED);
             continue;
         }
-        if (q->r.kind == GR_REQ_METRICS) {
-            sv.queue.pop_front();
-            q->state = GR_REQ_RUNNING;
-            q->t_admit = Clock::now();
-            sv.running.push_back(q->id);
-            continue;
-        }
         if (resident_bytes + q->film_bytes > ctx->serve_budget) {  // can never fit, even with no other film
             sv.queue.pop_front();
             finish(sv, q, GR_REQ_FAILED, GR_EBUSY);
@@ -142,7 +158,8 @@ void admit(gr_ctx *ctx, ServeState &sv, uint64_t resident_bytes) {
         }
         if (resident_bytes + sv.film_bytes + q->film_bytes > ctx->serve_budget) break;  // wait for releases
         const size_t fb = (size_t)q->n_px * 3 * sizeof(float);
-        if (q->film.alloc(fb, ctx->stream) != cudaSuccess || (q->kahan && q->comp.alloc(fb, ctx->stream) != cudaSuccess)) {
+        if (q->film.alloc(fb, ctx->stream, sv.film_pool) != cudaSuccess ||
+            (q->kahan && q->comp.alloc(fb, ctx->stream, sv.film_pool) != cudaSuccess)) {
             sv.queue.pop_front();
             q->film.release(ctx->stream);
             q->comp.release(ctx->stream);
@@ -183,17 +200,12 @@ void worker_main(gr_ctx *ctx, ServeState *sv) {
         }
         std::vector<grh::BatchItem> items;
         std::vector<std::pair<uint64_t, uint32_t>> slices;
-        std::vector<Request *> metric_jobs;
         {
             std::unique_lock<std::mutex> lk(sv->mu);
             // 2. completions and cancellations of running requests
             std::vector<uint64_t> keep;
             for (uint64_t id : sv->running) {
                 Request *q = sv->reqs[id];
-                if (q->r.kind == GR_REQ_METRICS && q->cancel) {
-                    finish(*sv, q, GR_REQ_CANCELLED);
-                    continue;
-                }
                 if (q->r.kind == GR_REQ_RENDER && q->in_flight == 0 && (q->cancel || q->done >= q->r.spp)) {
                     finish(*sv, q, q->done >= q->r.spp ? GR_REQ_DONE : GR_REQ_CANCELLED);
                     continue;
@@ -213,14 +225,18 @@ void worker_main(gr_ctx *ctx, ServeState *sv) {
                 Request *q = sv->reqs[id];
                 n_active += q->r.kind == GR_REQ_RENDER && !q->cancel && q->issued < q->r.spp;
             }
-            const uint64_t cap = n_active > 1 ? kTickTuples / 2 : kTickTuples;
+            const uint64_t cap = GR_SERVE_HALF_CAP && n_active > 1 ? kTickTuples / 2 : kTickTuples;
             uint64_t budget = kTickTuples;
-            for (uint64_t id : sv->running) {
+            std::vector<uint64_t> order(sv->running);
+            if (GR_SERVE_ORDER == 1) {
+                auto left = [&](uint64_t id) {
+                    const Request *q = sv->reqs[id];
+                    return q->r.kind == GR_REQ_RENDER ? (uint64_t)(q->r.spp - q->issued) * q->n_px : 0;
+                };
+                std::stable_sort(order.begin(), order.end(), [&](uint64_t a, uint64_t b) { return left(a) < left(b); });
+            }
+            for (uint64_t id : order) {
                 Request *q = sv->reqs[id];
-                if (q->r.kind == GR_REQ_METRICS) {
-                    if (q->state == GR_REQ_RUNNING && !q->cancel) metric_jobs.push_back(q);
-                    continue;
-                }
                 if (q->cancel || q->issued >= q->r.spp) continue;
                 const uint64_t px = std::max<uint64_t>(1, q->n_px);
                 uint64_t want = std::min(budget, cap) / px;
@@ -238,7 +254,7 @@ void worker_main(gr_ctx *ctx, ServeState *sv) {
                 q->issued += slice;
                 q->in_flight += slice;
             }
-            if (items.empty() && metric_jobs.empty()) {
+            if (items.empty()) {
                 if (flight.empty()) {
                     if (sv->stop) break;
                     sv->cv_work.wait_for(lk, std::chrono::milliseconds(20));
@@ -251,20 +267,7 @@ void worker_main(gr_ctx *ctx, ServeState *sv) {
                 continue;
             }
         }
-        // 5. metric sweeps between ticks
-        for (Request *q : metric_jobs) {
-            // its own stream and scratch: no context lock, and the ticks in flight keep running
-            const gr_status st = grh::metrics_device(q->planes.data(), (uint32_t)q->planes.size(), &q->material,
-                                                     q->poses.data(), (uint32_t)q->poses.size(), q->metrics.data(),
-                                                     q->r.flags, sv->metrics_stream, sv->metrics_scratch);
-            std::lock_guard<std::mutex> lk(sv->mu);
-            std::vector<uint64_t> keep;
-            for (uint64_t id : sv->running)
-                if (id != q->id) keep.push_back(id);
-            sv->running.swap(keep);
-            finish(*sv, q, st == GR_OK ? GR_REQ_DONE : GR_REQ_FAILED, st);
-        }
-        // 6. launch the tick
+        // 5. launch the tick
         if (!items.empty()) {
             Tick t;
             t.slices = slices;
@@ -310,13 +313,55 @@ void worker_main(gr_ctx *ctx, ServeState *sv) {
         if (e) cudaEventDestroy(e);
 }
 
+// Metric sweeps, one at a time in arrival order (no context lock: own stream and scratch).
+void metrics_main(gr_ctx *ctx, ServeState *sv) {
+    cudaSetDevice(ctx->device);
+    for (;;) {
+        Request *q;
+        {
+            std::unique_lock<std::mutex> lk(sv->mu);
+            sv->cv_metrics.wait(lk, [&] { return sv->stop || !sv->metric_queue.empty(); });
+            if (sv->metric_queue.empty()) return;  // stopping, nothing left
+            q = sv->reqs[sv->metric_queue.front()];
+            sv->metric_queue.pop_front();
+            if (q->cancel) {
+                finish(*sv, q, GR_REQ_CANCELLED);
+                continue;
+            }
+        }
+        const gr_status st = grh::metrics_device(q->planes.data(), (uint32_t)q->planes.size(), &q->material,
+                                                 q->poses.data(), (uint32_t)q->poses.size(), q->metrics.data(),
+                                                 q->r.flags, sv->metrics_stream, sv->metrics_scratch);
+        std::lock_guard<std::mutex> lk(sv->mu);
+        finish(*sv, q, st == GR_OK ? GR_REQ_DONE : GR_REQ_FAILED, st);
+    }
+}
+
 ServeState *serve_state(gr_ctx *ctx) {
     std::lock_guard<std::mutex> lk(ctx->mu);
     if (!ctx->serve) {
         ctx->serve = new ServeState();
         cudaSetDevice(ctx->device);
-        cudaStreamCreateWithFlags(&ctx->serve->metrics_stream, cudaStreamNonBlocking);
+        int lo = 0, hi = 0;  // the numerically lowest priority is the highest
+        cudaDeviceGetStreamPriorityRange(&lo, &hi);
+        cudaStreamCreateWithPriority(&ctx->serve->metrics_stream, cudaStreamNonBlocking, hi);
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = ctx->device;
+        cudaMemPool_t pool = nullptr;
+        if (cudaMemPoolCreate(&pool, &props) == cudaSuccess) {
+            uint64_t keep = ctx->serve_budget;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+            void *p = nullptr;
+            if (cudaMallocFromPoolAsync(&p, std::min<uint64_t>(kFilmPoolReserve, ctx->serve_budget), pool,
+                                        ctx->stream) == cudaSuccess)
+                cudaFreeAsync(p, ctx->stream);  // mapped now, kept by the pool
+            ctx->serve->film_pool = pool;
+        }
+        cudaGetLastError();  // a pool that could not be set up leaves films on the default pool
         ctx->serve->worker = std::thread(worker_main, ctx, ctx->serve);
+        ctx->serve->metrics_worker = std::thread(metrics_main, ctx, ctx->serve);
     }
     return ctx->serve;
 }
@@ -347,7 +392,9 @@ void serve_shutdown(gr_ctx *ctx) {
         for (auto &kv : sv->reqs) kv.second->cancel = true;
     }
     sv->cv_work.notify_all();
+    sv->cv_metrics.notify_all();
     if (sv->worker.joinable()) sv->worker.join();
+    if (sv->metrics_worker.joinable()) sv->metrics_worker.join();
     cudaSetDevice(ctx->device);
     for (auto &kv : sv->reqs) {
         kv.second->film.release(ctx->stream);
@@ -355,6 +402,7 @@ void serve_shutdown(gr_ctx *ctx) {
         delete kv.second;
     }
     cudaStreamSynchronize(ctx->stream);  // stream-ordered frees above complete
+    if (sv->film_pool) cudaMemPoolDestroy(sv->film_pool);
     sv->metrics_scratch.release();
     if (sv->metrics_stream) cudaStreamDestroy(sv->metrics_stream);
     delete sv;
@@ -366,6 +414,7 @@ extern "C" {
 
 gr_status gr_submit(gr_ctx *ctx, const gr_request *req, uint64_t *request_id) {
     if (!ctx || !req || !request_id) return fail(GR_EINVAL, "NULL argument");
+    const Clock::time_point t_entry = Clock::now();  // latency counts any wait for the locks below
     Request *q = new Request();
     q->r = *req;
     if (req->kind == GR_REQ_RENDER) {
@@ -398,7 +447,7 @@ gr_status gr_submit(gr_ctx *ctx, const gr_request *req, uint64_t *request_id) {
     {
         std::lock_guard<std::mutex> lk(sv->mu);
         q->id = sv->next_id++;
-        q->t_submit = Clock::now();
+        q->t_submit = t_entry;
         if (q->r.kind == GR_REQ_METRICS && q->r.n_planes == 0) {
             for (auto &m : q->metrics) m = gr_metrics_out{85.0f, 25.0f, 75.0f, 5.0f, 5.0f};  // color/metrics.rs:1090-1103
             q->t_admit = q->t_submit;
@@ -406,13 +455,20 @@ gr_status gr_submit(gr_ctx *ctx, const gr_request *req, uint64_t *request_id) {
         } else if (q->r.kind == GR_REQ_RENDER && q->r.spp == 0) {
             q->t_admit = q->t_submit;
             finish(*sv, q, GR_REQ_DONE);
+        } else if (q->r.kind == GR_REQ_METRICS) {
+            q->state = GR_REQ_RUNNING;
+            q->t_admit = q->t_submit;
+            sv->metric_queue.push_back(q->id);
         } else {
             sv->queue.push_back(q->id);
         }
         sv->reqs[q->id] = q;
         *request_id = q->id;
     }
-    sv->cv_work.notify_all();
+    if (q->r.kind == GR_REQ_METRICS)
+        sv->cv_metrics.notify_all();
+    else
+        sv->cv_work.notify_all();
     return GR_OK;
 }
 

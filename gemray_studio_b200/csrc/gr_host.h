@@ -25,6 +25,8 @@ gr_status tonemap_device(const float *xyz_dev, float scale, uint32_t n, void *rg
 gr_status metrics_device(const gr_plane *planes, uint32_t n_planes, const gr_material *m, const gr_pose *poses,
                          uint32_t n_poses, gr_metrics_out *out, uint32_t flags, struct CUstream_st *s,
                          DeviceBuffer &scratch);
+// Device scratch bytes metrics_device needs (a scratch at least this large never grows).
+size_t metrics_scratch_bytes(uint32_t n_planes, uint32_t n_poses);
 
 // The fixed scratch of gr_render_resident_static (gr_static.cu): its address on
 // `device` (the current device), looked up once per device.  Returns a cudaError_t.

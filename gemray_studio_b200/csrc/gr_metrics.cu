@@ -303,6 +303,24 @@ float host_dispersion(const gr_dispersion &d, float lambda_nm) {  // optics/disp
 namespace grh {
 void studio_rig(float yaw, float pitch, float key[3], float fill[3], float ring[16][3]);
 
+namespace {
+struct MetricsLayout {
+    size_t pose_bytes, plane_bytes, sample_bytes, out_bytes;
+    size_t total() const { return pose_bytes + plane_bytes + sample_bytes + out_bytes; }
+};
+MetricsLayout metrics_layout(uint32_t n_planes, uint32_t n_poses) {
+    const size_t per_pose = (size_t)grd::MGRID * grd::MGRID * grd::MSLOTS;
+    MetricsLayout L;
+    L.pose_bytes = ((n_poses * sizeof(grd::PoseConst)) + 255) & ~(size_t)255;
+    L.plane_bytes = (((size_t)(n_planes ? n_planes : 1) * sizeof(float4)) + 255) & ~(size_t)255;
+    L.sample_bytes = ((n_poses * per_pose * sizeof(grd::MetricSample)) + 255) & ~(size_t)255;
+    L.out_bytes = n_poses * sizeof(gr_metrics_out);
+    return L;
+}
+}  // namespace
+
+size_t metrics_scratch_bytes(uint32_t n_planes, uint32_t n_poses) { return metrics_layout(n_planes, n_poses).total(); }
+
 gr_status metrics_device(const gr_plane *planes, uint32_t n_planes, const gr_material *m, const gr_pose *poses,
                          uint32_t n_poses, gr_metrics_out *out, uint32_t flags, cudaStream_t stream, DeviceBuffer &scratch) {
     std::vector<grd::PoseConst> pc(n_poses);
@@ -324,11 +342,10 @@ gr_status metrics_device(const gr_plane *planes, uint32_t n_planes, const gr_mat
         P.nc = nc;
     }
     const size_t per_pose = (size_t)grd::MGRID * grd::MGRID * grd::MSLOTS;
-    const size_t pose_bytes = ((n_poses * sizeof(grd::PoseConst)) + 255) & ~(size_t)255;
-    const size_t plane_bytes = (((size_t)(n_planes ? n_planes : 1) * sizeof(float4)) + 255) & ~(size_t)255;
-    const size_t sample_bytes = ((n_poses * per_pose * sizeof(grd::MetricSample)) + 255) & ~(size_t)255;
-    const size_t out_bytes = n_poses * sizeof(gr_metrics_out);
-    gr_status st = scratch.reserve(pose_bytes + plane_bytes + sample_bytes + out_bytes);
+    const MetricsLayout L = metrics_layout(n_planes, n_poses);
+    const size_t pose_bytes = L.pose_bytes, plane_bytes = L.plane_bytes, sample_bytes = L.sample_bytes,
+                 out_bytes = L.out_bytes;
+    gr_status st = scratch.reserve(L.total());
     if (st != GR_OK) return st;
     char *base = (char *)scratch.ptr;
     grd::PoseConst *d_pose = (grd::PoseConst *)base;

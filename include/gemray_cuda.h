@@ -424,7 +424,8 @@ typedef struct gr_request_status {
  * apps/gemray-worker/src/render_core/mod.rs).  A worker thread admits requests in
  * arrival order while their film (W*H*3 f32) fits the context's serve budget next to
  * the resident scenes and unreleased films, and advances every running render by one
- * slice per tick in a shared batched launch.  Slices continue each pixel's running
+ * slice per tick in a shared batched launch; metric requests hold no film and run on
+ * a second worker thread in arrival order, beside the renders.  Slices continue each pixel's running
  * sum, so a film is bit-identical to one gr_render_resident call over the same sample
  * range on a zero film -- for any slicing, alone or in any mix. */
 gr_status gr_submit(gr_ctx *ctx, const gr_request *request, uint64_t *request_id);

@@ -76,6 +76,38 @@ def test_results_identical_alone_and_in_mix(engine_lib):
         srv.close()
 
 
+def test_metric_sweeps_run_beside_a_long_render(engine_lib):
+    """Metric sweeps skip render admission and run on their own worker: submitted
+    behind a render of ~270 M samples they finish while it is still running, each
+    bit-identical to gr_optical_metrics, and stones with more planes than any swept
+    before (a larger sweep scratch) change nothing."""
+    srv = RenderServer()
+    try:
+        sc = S.Scene(width=256, height=256, planes=S.round_brilliant_57(), material=S.builtin_material("Diamond"),
+                     cam=S.camera(0.35, 0.28, 5.0, 18.0), max_bounces=32, env_mode=abi.GR_ENV_UNIFORM)
+        sid = srv.upload(sc)
+        long = srv.submit_render(sid, 0, 4096)
+        rng = np.random.default_rng(21)
+        stones = sorted((S.random_polyhedron(rng) for _ in range(4)), key=len)
+        assert len(stones[0]) < len(stones[-1])
+        mat = S.builtin_material("Spinel")
+        poses = np.array([[0.1 * k, 0.45, 0.85, 0.95] for k in range(16)], np.float32)
+        sweeps = [(planes, srv.submit_metrics(planes, mat, poses)) for planes in stones]
+        for _planes, mid in sweeps:
+            assert srv.wait(mid).state == "done"
+        st = srv.poll(long)
+        assert st.state in ("queued", "running") and st.samples_done < 4096
+        srv.cancel(long)
+        assert srv.wait(long).state == "cancelled"
+        for planes, mid in sweeps:  # references after the render: they share its stream
+            ref = M.evaluate_poses(srv.r, planes, mat, poses)
+            assert np.array_equal(srv.metrics(mid).view(np.uint32), ref.view(np.uint32))
+            srv.release(mid)
+        srv.release(long)
+    finally:
+        srv.close()
+
+
 def test_cancel_between_slices(engine_lib):
     srv = RenderServer()
     try:

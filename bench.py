@@ -562,6 +562,10 @@ def run_batch(args):
     with ClockSampler(0) as clocks:
         ms_serial = timed(serial, 0)
         ms_batch = timed(batched, 1000)
+        # the same serial renders with the plain one-thread-per-tuple kernel
+        assert lib.gr_set_kernel(ctx, abi.GR_KERNEL_PLAIN) == abi.GR_OK
+        ms_plain = timed(serial, 3000)
+        assert lib.gr_set_kernel(ctx, abi.GR_KERNEL_STAGED) == abi.GR_OK
     # e2e: films from pinned host memory in, batched render, films back out
     host = [torch.zeros(f.shape, dtype=torch.float32).pin_memory() for f in films]
     e_evs = []
@@ -592,6 +596,10 @@ def run_batch(args):
         "serial_plain": {"value": tuples / (ms_serial * 1e-3), "ms_per_step": ms_serial,
                          "how": "the same 64 renders, one gr_render_resident call (single-scene staged kernels) per stone"},
         "batched_over_serial": ms_serial / ms_batch,
+        "serial_plain_kernel": {"value": tuples / (ms_plain * 1e-3), "ms_per_step": ms_plain,
+                                "how": "the same 64 renders, one gr_render_resident call per stone with "
+                                       "GR_KERNEL_PLAIN (one thread per tuple, no staging)"},
+        "batched_over_plain_kernel": ms_plain / ms_batch,
         "e2e": {"value": tuples / (ms_e2e * 1e-3), "unit": "path-samples/s", "h2d_bytes_per_step": film_bytes,
                 "d2h_bytes_per_step": film_bytes},
         "clocks": clocks.summary(), "device": r.adapter_label(),

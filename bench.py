@@ -565,7 +565,7 @@ def run_batch(args):
         # the same serial renders with the plain one-thread-per-tuple kernel
         assert lib.gr_set_kernel(ctx, abi.GR_KERNEL_PLAIN) == abi.GR_OK
         ms_plain = timed(serial, 3000)
-        assert lib.gr_set_kernel(ctx, abi.GR_KERNEL_STAGED) == abi.GR_OK
+        assert lib.gr_set_kernel(ctx, abi.GR_KERNEL_AUTO) == abi.GR_OK
     # e2e: films from pinned host memory in, batched render, films back out
     host = [torch.zeros(f.shape, dtype=torch.float32).pin_memory() for f in films]
     e_evs = []
@@ -594,7 +594,8 @@ def run_batch(args):
                                f" px square, spp 32-512, Kahan films, one gr_render_batch call per step (CUDA graph)",
                    "path_samples_per_step": tuples, "scale": s, "l2": "flushed between steps (256 MiB device write)"},
         "serial_plain": {"value": tuples / (ms_serial * 1e-3), "ms_per_step": ms_serial,
-                         "how": "the same 64 renders, one gr_render_resident call (single-scene staged kernels) per stone"},
+                         "how": "the same 64 renders, one gr_render_resident call per stone (default kernel choice: "
+                                "staged from 2^19 tuples per launch, plain below)"},
         "batched_over_serial": ms_serial / ms_batch,
         "serial_plain_kernel": {"value": tuples / (ms_plain * 1e-3), "ms_per_step": ms_plain,
                                 "how": "the same 64 renders, one gr_render_resident call per stone with "

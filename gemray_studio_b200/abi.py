@@ -54,6 +54,8 @@ GR_KERNEL_PLAIN = 0
 GR_KERNEL_WAVEFRONT = 1
 GR_KERNEL_REGEN = 2
 GR_KERNEL_STAGED = 3
+GR_KERNEL_AUTO = 4
+GR_AUTO_STAGED_MIN_TUPLES = 1 << 19
 GR_STATIC_SCRATCH_BYTES = 16 << 20
 GR_STATIC_SCRATCH_TUPLES = GR_STATIC_SCRATCH_BYTES // 12
 

@@ -54,7 +54,7 @@ struct gr_ctx {
     uint64_t serve_budget = 60ull << 30;
     int sm_count = 0;
     grh::DeviceBuffer xyz, film, planes, map, ext, counter, rgba, metrics;
-    int kernel_mode = GR_KERNEL_STAGED;
+    int kernel_mode = GR_KERNEL_AUTO;
     // wavefront engine pool (gr_wavefront.cuh)
     uint32_t wave_cap = 1u << 18;
     grh::DeviceBuffer wf_pool, wf_events, wf_queues, wf_cnt;
@@ -122,6 +122,10 @@ namespace grh {
 // STAGED mode parks paths in `park` (the context's buffer when NULL).
 gr_status launch_trace(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuffers &B, const grd::LaunchRange &R,
                        float *xyz, cudaStream_t stream, int mode, grh::DeviceBuffer *park = nullptr);
+// The kernel a launch of n_tuples tuples runs in `mode` (AUTO resolved by size), and
+// how many kernel launches that trace makes.
+int resolve_kernel(int mode, uint64_t n_tuples);
+int trace_kernel_launches(int mode, const SceneConst &S, uint64_t n_tuples);
 gr_status launch_fold(const float *xyz, uint32_t n_pixels, uint32_t spp, uint32_t first_pixel, float *film,
                       uint32_t kahan, cudaStream_t stream);
 }  // namespace grh

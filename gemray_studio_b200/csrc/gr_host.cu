@@ -419,10 +419,22 @@ gr_status launch_wavefront(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuf
     return GR_OK;
 }
 
+int resolve_kernel(int mode, uint64_t n_tuples) {
+    if (mode != GR_KERNEL_AUTO) return mode;
+    return n_tuples < GR_AUTO_STAGED_MIN_TUPLES ? GR_KERNEL_PLAIN : GR_KERNEL_STAGED;
+}
+
+int trace_kernel_launches(int mode, const SceneConst &S, uint64_t n_tuples) {
+    const bool staged = resolve_kernel(mode, n_tuples) == GR_KERNEL_STAGED && S.max_bounces > 0 &&
+                        !(S.flags & GR_FLAG_FP64_RESOLVE);
+    return staged ? 3 : 1;  // stages 1, 2 and 3
+}
+
 // Trace tuples [0, R.n_tuples) of one chunk into xyz (device).
 gr_status launch_trace(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuffers &B, const grd::LaunchRange &R,
                        float *xyz, cudaStream_t stream, int mode, grh::DeviceBuffer *park_buf) {
     if (R.n_tuples == 0) return GR_OK;
+    mode = resolve_kernel(mode, R.n_tuples);
     size_t smem = grd::planes_smem_bytes(S.n_planes);
     const bool extras = grd::needs_extras(S);
     const uint64_t plain_blocks = (R.n_tuples + grd::TRACE_THREADS - 1) / grd::TRACE_THREADS;
@@ -545,9 +557,7 @@ gr_status render_into(gr_ctx *ctx, const gr_scene *sc, const SceneConst &S, cons
         st = launch_trace(ctx, S, B, R, (float *)ctx->xyz.ptr, stream, ctx->kernel_mode);
         if (st != GR_OK) return st;
         if (tev) cudaEventRecord(tev[1], stream);
-        // kernel launches of one trace: stage 1, 2 and 3 in STAGED mode
-        ctx->trace_launches += (ctx->kernel_mode == GR_KERNEL_STAGED && S.max_bounces > 0 &&
-                                !(S.flags & GR_FLAG_FP64_RESOLVE)) ? 3 : 1;
+        ctx->trace_launches += trace_kernel_launches(ctx->kernel_mode, S, R.n_tuples);
         cudaEvent_t *fev = timing_slot(ctx, ctx->fold_ev, ctx->fold_used);
         if (fev) cudaEventRecord(fev[0], stream);
         st = launch_fold((const float *)ctx->xyz.ptr, (uint32_t)np, spp, (uint32_t)first, film_dev,
@@ -1084,7 +1094,7 @@ gr_status gr_angular_profile(gr_ctx *ctx, const gr_plane *planes, uint32_t n_pla
 gr_status gr_set_kernel(gr_ctx *ctx, uint32_t kernel) {
     if (!ctx) return fail(GR_EINVAL, "ctx is NULL");
     if (kernel != GR_KERNEL_PLAIN && kernel != GR_KERNEL_WAVEFRONT && kernel != GR_KERNEL_REGEN &&
-        kernel != GR_KERNEL_STAGED)
+        kernel != GR_KERNEL_STAGED && kernel != GR_KERNEL_AUTO)
         return fail(GR_EINVAL, "unknown kernel %u", kernel);
     std::lock_guard<std::mutex> lk(ctx->mu);
     ctx->kernel_mode = (int)kernel;

@@ -148,7 +148,7 @@ gr_status trace_subbatch(FrameStream *fs, uint32_t bfirst, uint32_t n) {
         R.sample_offset = bfirst;
         R.spp = n;
         R.n_tuples = np * n;
-        st = grh::launch_trace(fs->ctx, fs->S, fs->B, R, (float *)fs->scratch.ptr, fs->main, GR_KERNEL_STAGED,
+        st = grh::launch_trace(fs->ctx, fs->S, fs->B, R, (float *)fs->scratch.ptr, fs->main, GR_KERNEL_AUTO,
                                &fs->park);
         if (st != GR_OK) return st;
         st = grh::launch_fold((const float *)fs->scratch.ptr, (uint32_t)np, n, (uint32_t)p0, (float *)fs->batch.ptr,

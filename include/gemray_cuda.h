@@ -573,15 +573,20 @@ gr_status gr_denoise_tonemap_device(gr_ctx *ctx, const float *film, uint32_t sam
  * records advanced by per-stage kernels over compacted event queues (about 3x slower
  * on B200: each bounce moves ~1 KB of record traffic).  REGEN: path regeneration,
  * each warp owns a run of consecutive tuples and lanes whose path has ended start the
- * next ones while the rest of the warp keeps bouncing.  STAGED (default): PLAIN's
- * launch shape with paths capped at 12 bounces; the ones still alive are parked and
- * resumed, packed densely, by a second kernel (capped at 20, then a third), so warps
- * stop waiting on a few long paths (+20% on the c2 frame).  Results are identical
- * (same arithmetic per path). */
+ * next ones while the rest of the warp keeps bouncing.  STAGED: PLAIN's launch shape
+ * with paths capped at 12 bounces; the ones still alive are parked and resumed, packed
+ * densely, by a second kernel (capped at 20, then a third), so warps stop waiting on
+ * a few long paths (+24-28% from 4 M tuples per launch up, e.g. the c2 frame).  AUTO
+ * (default): STAGED for launches of at least GR_AUTO_STAGED_MIN_TUPLES tuples, PLAIN
+ * below, where STAGED's extra launches and tails cost more than they save (measured
+ * on B200: PLAIN 1.2x faster at 0.26 M tuples, STAGED 1.09x faster at 1.05 M).
+ * Results are identical (same arithmetic per path). */
 #define GR_KERNEL_PLAIN 0u
 #define GR_KERNEL_WAVEFRONT 1u
 #define GR_KERNEL_REGEN 2u
 #define GR_KERNEL_STAGED 3u
+#define GR_KERNEL_AUTO 4u
+#define GR_AUTO_STAGED_MIN_TUPLES (1u << 19)
 gr_status gr_set_kernel(gr_ctx *ctx, uint32_t kernel);
 
 /* Per-launch timing: while enabled, every trace and film-fold launch is bracketed by

@@ -185,6 +185,32 @@ def test_tonemap_matches_oracle(renderer, oracle):
     assert np.mean(diff == 0) > 0.999
 
 
+def test_auto_kernel_picks_by_launch_size(engine_lib):
+    """GR_KERNEL_AUTO (the default) runs the plain kernel for launches under
+    GR_AUTO_STAGED_MIN_TUPLES tuples and the three staged kernels from there up: the
+    films are bit-identical to both explicit modes' and the launch counts show the
+    choice."""
+    from gemray_studio_b200 import GpuFrameRenderer
+    sc = srb_scene("Sapphire", width=128, height=128, max_bounces=24)
+    n_px = sc.width * sc.height
+    for spp, launches in ((abi.GR_AUTO_STAGED_MIN_TUPLES // n_px // 2, 1), (abi.GR_AUTO_STAGED_MIN_TUPLES // n_px, 3)):
+        films = {}
+        for kernel in (abi.GR_KERNEL_AUTO, abi.GR_KERNEL_PLAIN, abi.GR_KERNEL_STAGED):
+            r = GpuFrameRenderer(kernel=kernel)
+            assert r.lib.gr_timing_enable(r.ctx, 1) == abi.GR_OK
+            acc = np.zeros((n_px, 3), np.float32)
+            r.accumulate(sc, 3, spp, acc)
+            tr, fo, n_tr, n_fo = C.c_double(), C.c_double(), C.c_uint64(), C.c_uint64()
+            assert r.lib.gr_timing_read(r.ctx, C.byref(tr), C.byref(fo), C.byref(n_tr), C.byref(n_fo)) == abi.GR_OK
+            if kernel == abi.GR_KERNEL_AUTO:
+                assert n_tr.value == launches, (spp, n_tr.value)
+            films[kernel] = acc
+            r.close()
+        ref = films[abi.GR_KERNEL_PLAIN].view(np.uint32)
+        assert np.array_equal(films[abi.GR_KERNEL_AUTO].view(np.uint32), ref)
+        assert np.array_equal(films[abi.GR_KERNEL_STAGED].view(np.uint32), ref)
+
+
 def test_staged_kernels_bit_identical_when_park_buffers_overflow(engine_lib):
     """A light-trapping stone (n = 3.5): ~16% of paths outlive the first stage cap and
     ~11% the second, more than the park buffers hold (1/8 and 1/32 of a launch's

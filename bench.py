@@ -419,6 +419,8 @@ def run_engine(args):
         torch.cuda.synchronize()
         barrier(world)
     step_ms = sum(a.elapsed_time(b) for a, b in evs)
+    cap1, cap2 = C.c_uint32(), C.c_uint32()  # the scene's stage caps (chosen during the warm-up calls)
+    assert lib.gr_scene_stage_caps(ctx, sid.value, C.byref(cap1), C.byref(cap2)) == abi.GR_OK
     tr, fo, ntr, nfo = C.c_double(), C.c_double(), C.c_uint64(), C.c_uint64()
     lib.gr_timing_read(ctx, C.byref(tr), C.byref(fo), C.byref(ntr), C.byref(nfo))
     lib.gr_timing_enable(ctx, 0)
@@ -479,7 +481,8 @@ def run_engine(args):
                          "flops_per_sample": model.flops_per_sample,
                          "sfu_ops_per_sample": model.sfu / max(1, model.paths),
                          "kernel_ms_per_step": tr.value / frames, "fold_ms_per_step": fo.value / frames,
-                         "launches_per_step": (ntr.value + nfo.value) / frames},
+                         "launches_per_step": (ntr.value + nfo.value) / frames,
+                         "stage_caps": [cap1.value, cap2.value]},
             "events_per_sample": {k: v / max(1, tallies["paths"]) for k, v in tallies.items() if k != "paths"},
             "metrics_16_tilts": {"ms": metrics_ms, "how": "gr_optical_metrics, one device batch, host wall clock",
                                  "brilliance_pct": [round(float(v), 3) for v in mvals[:, 0]],

@@ -27,11 +27,36 @@ gr_status fail(gr_status st, const char *fmt, ...);
         if (e_ != cudaSuccess) return grh::fail(GR_ECUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
     } while (0)
 
+// Bounce caps of the staged kernels' first two stages; {0, 0} = the built-in pair.
+struct StageCaps {
+    uint32_t first = 0, second = 0;
+};
+
+// The stage caps a resident scene's staged renders use.  Every cap pair gives the same
+// films, but the fastest depends on the stone's path lengths, so from the scene's
+// second staged gr_render_resident call on, one call with each candidate pair is timed
+// on the device (the whole call: its chunks cover different parts of the image) and
+// the pair with the least time per tuple is kept (gr_host.cu, kStageCapCandidates).
+struct StageCapTune {
+    static constexpr int kCandidates = 2;
+    int best = -1;              // chosen candidate, -1 while measuring
+    uint32_t staged_calls = 0;  // staged calls seen
+    bool issued[kCandidates] = {};
+    float ms_per_mtuple[kCandidates] = {};
+    struct Trial {
+        cudaEvent_t start = nullptr, stop = nullptr;
+        int candidate = 0;
+        uint64_t tuples = 0;
+        bool done = false;
+    } trial[kCandidates];
+};
+
 struct ResidentScene {
     SceneConst S;
     grh::DeviceBuffer planes, map, ext;
     uint64_t bytes = 0;
     uint32_t users = 0;  // open frame streams rendering this scene (gr_stream.cu)
+    StageCapTune tune;
 };
 
 struct FrameStream;  // gr_stream.cu
@@ -121,7 +146,8 @@ namespace grh {
 // (gr_host.cu), and the ordered per-pixel fold of n_pixels pixels into film.
 // STAGED mode parks paths in `park` (the context's buffer when NULL).
 gr_status launch_trace(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuffers &B, const grd::LaunchRange &R,
-                       float *xyz, cudaStream_t stream, int mode, grh::DeviceBuffer *park = nullptr);
+                       float *xyz, cudaStream_t stream, int mode, grh::DeviceBuffer *park = nullptr,
+                       StageCaps caps = StageCaps{});
 // The kernel a launch of n_tuples tuples runs in `mode` (AUTO resolved by size), and
 // how many kernel launches that trace makes.
 int resolve_kernel(int mode, uint64_t n_tuples);

@@ -432,7 +432,8 @@ int trace_kernel_launches(int mode, const SceneConst &S, uint64_t n_tuples) {
 
 // Trace tuples [0, R.n_tuples) of one chunk into xyz (device).
 gr_status launch_trace(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuffers &B, const grd::LaunchRange &R,
-                       float *xyz, cudaStream_t stream, int mode, grh::DeviceBuffer *park_buf) {
+                       float *xyz, cudaStream_t stream, int mode, grh::DeviceBuffer *park_buf, StageCaps caps) {
+    if (caps.first == 0) caps = StageCaps{GR_STAGE_CAP, GR_STAGE_CAP2};
     if (R.n_tuples == 0) return GR_OK;
     mode = resolve_kernel(mode, R.n_tuples);
     size_t smem = grd::planes_smem_bytes(S.n_planes);
@@ -465,7 +466,7 @@ gr_status launch_trace(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuffers
         const uint64_t max_cap = (4ull << 30) / sizeof(grd::Path);
         if (cap1 > max_cap) cap1 = max_cap;
         if (cap1 < 1024) cap1 = 1024;
-        const uint64_t cap2 = GR_STAGE_CAP2 == 0xFFFFFFFFu ? 0 : (cap1 + 3) / 4;
+        const uint64_t cap2 = caps.second == 0xFFFFFFFFu ? 0 : (cap1 + 3) / 4;
         grh::DeviceBuffer &pk = park_buf ? *park_buf : ctx->park;
         gr_status st = pk.reserve((size_t)(cap1 + cap2) * sizeof(grd::Path) + 256);
         if (st != GR_OK) return st;
@@ -479,16 +480,18 @@ gr_status launch_trace(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuffers
         const unsigned b2 = (unsigned)((cap1 + grd::TRACE_THREADS - 1) / grd::TRACE_THREADS);
         const unsigned b3 = (unsigned)((cap2 + grd::TRACE_THREADS - 1) / grd::TRACE_THREADS);
         if (extras) {
-            grd::k_trace_stage1<true><<<(unsigned)plain_blocks, grd::TRACE_THREADS, smem, stream>>>(S, B, R, xyz, out1);
+            grd::k_trace_stage1<true><<<(unsigned)plain_blocks, grd::TRACE_THREADS, smem, stream>>>(S, B, R, xyz, out1,
+                                                                                                  caps.first);
             grd::k_trace_stage2<true><<<b2, grd::TRACE_THREADS, smem, stream>>>(S, B, park1, (uint32_t)cap1, counts,
-                                                                                GR_STAGE_CAP2, out2, xyz);
+                                                                                caps.second, out2, xyz);
             if (cap2)
                 grd::k_trace_stage2<true><<<b3, grd::TRACE_THREADS, smem, stream>>>(S, B, park2, (uint32_t)cap2,
                                                                                     counts + 1, 0xFFFFFFFFu, none, xyz);
         } else {
-            grd::k_trace_stage1<false><<<(unsigned)plain_blocks, grd::TRACE_THREADS, smem, stream>>>(S, B, R, xyz, out1);
+            grd::k_trace_stage1<false><<<(unsigned)plain_blocks, grd::TRACE_THREADS, smem, stream>>>(S, B, R, xyz, out1,
+                                                                                                   caps.first);
             grd::k_trace_stage2<false><<<b2, grd::TRACE_THREADS, smem, stream>>>(S, B, park1, (uint32_t)cap1, counts,
-                                                                                 GR_STAGE_CAP2, out2, xyz);
+                                                                                 caps.second, out2, xyz);
             if (cap2)
                 grd::k_trace_stage2<false><<<b3, grd::TRACE_THREADS, smem, stream>>>(S, B, park2, (uint32_t)cap2,
                                                                                      counts + 1, 0xFFFFFFFFu, none, xyz);
@@ -535,7 +538,8 @@ cudaEvent_t *timing_slot(gr_ctx *ctx, std::vector<std::pair<cudaEvent_t, cudaEve
 // [sample_offset, sample_offset + spp) samples chunk by chunk and add each pixel's
 // folded sum into film_dev.
 gr_status render_into(gr_ctx *ctx, const gr_scene *sc, const SceneConst &S, const grd::SceneBuffers &B,
-                      uint32_t sample_offset, uint32_t spp, float *film_dev, cudaStream_t stream) {
+                      uint32_t sample_offset, uint32_t spp, float *film_dev, cudaStream_t stream,
+                      StageCaps caps = StageCaps{}) {
     const uint64_t n_pixels = (uint64_t)sc->width * sc->height;
     uint64_t budget_tuples = ctx->chunk_budget / (3 * sizeof(float));
     if (budget_tuples > 0xFFFFFFFFull) budget_tuples = 0xFFFFFFFFull;  // tuple ids are u32 within a launch
@@ -554,7 +558,7 @@ gr_status render_into(gr_ctx *ctx, const gr_scene *sc, const SceneConst &S, cons
         R.n_tuples = np * spp;
         cudaEvent_t *tev = timing_slot(ctx, ctx->trace_ev, ctx->trace_used);
         if (tev) cudaEventRecord(tev[0], stream);
-        st = launch_trace(ctx, S, B, R, (float *)ctx->xyz.ptr, stream, ctx->kernel_mode);
+        st = launch_trace(ctx, S, B, R, (float *)ctx->xyz.ptr, stream, ctx->kernel_mode, nullptr, caps);
         if (st != GR_OK) return st;
         if (tev) cudaEventRecord(tev[1], stream);
         ctx->trace_launches += trace_kernel_launches(ctx->kernel_mode, S, R.n_tuples);
@@ -576,6 +580,37 @@ gr_status prepare(gr_ctx *ctx, const gr_scene *sc, SceneConst &S, grd::SceneBuff
     return upload_scene(ctx, sc, S, B);
 }
 
+// Stage-cap pairs a resident scene chooses between (StageCapTune): the pair measured
+// best on the c2 brilliant (long, TIR-trapped diamond paths) and the one measured best
+// on the c3 emerald (n ~ 1.6, shorter paths; 3.9% faster there).
+constexpr StageCaps kStageCapCandidates[StageCapTune::kCandidates] = {{12, 20}, {8, 16}};
+
+// Reads the trials whose events have completed; chooses once every candidate has one.
+void tune_harvest(StageCapTune &T) {
+    bool all = true;
+    for (auto &tr : T.trial) {
+        if (tr.start && !tr.done && cudaEventQuery(tr.stop) == cudaSuccess) {
+            float ms = 0.0f;
+            if (cudaEventElapsedTime(&ms, tr.start, tr.stop) == cudaSuccess && tr.tuples)
+                T.ms_per_mtuple[tr.candidate] = ms / (float)((double)tr.tuples * 1e-6);
+            tr.done = true;
+        }
+        all = all && tr.done;
+    }
+    cudaGetLastError();  // a query of an unfinished event is not an error to keep
+    if (!all) return;
+    T.best = 0;
+    for (int c = 1; c < StageCapTune::kCandidates; ++c)
+        if (T.ms_per_mtuple[c] < T.ms_per_mtuple[T.best]) T.best = c;
+}
+
+void tune_release(StageCapTune &T) {
+    for (auto &tr : T.trial) {
+        if (tr.start) cudaEventDestroy(tr.start);
+        if (tr.stop) cudaEventDestroy(tr.stop);
+        tr.start = tr.stop = nullptr;
+    }
+}
 }  // namespace grh
 
 // ---------------------------------------------------------------------------------
@@ -670,6 +705,7 @@ gr_status gr_destroy(gr_ctx *ctx) {
         for (auto &p : ctx->trace_ev) { cudaEventDestroy(p.first); cudaEventDestroy(p.second); }
         for (auto &p : ctx->fold_ev) { cudaEventDestroy(p.first); cudaEventDestroy(p.second); }
         for (auto &kv : ctx->scenes) {
+            grh::tune_release(kv.second->tune);
             kv.second->planes.release();
             kv.second->map.release();
             kv.second->ext.release();
@@ -879,6 +915,7 @@ gr_status gr_scene_release(gr_ctx *ctx, uint64_t id) {
     GR_CUDA(cudaStreamSynchronize(ctx->stream));
     ResidentScene *rs = it->second;
     ctx->resident_bytes -= rs->bytes;
+    grh::tune_release(rs->tune);
     rs->planes.release();
     rs->map.release();
     rs->ext.release();
@@ -886,6 +923,7 @@ gr_status gr_scene_release(gr_ctx *ctx, uint64_t id) {
     ctx->scenes.erase(it);
     return GR_OK;
 }
+
 
 gr_status gr_render_resident(gr_ctx *ctx, uint64_t id, uint32_t sample_offset, uint32_t spp, float *film_dev,
                              void *stream) {
@@ -903,7 +941,49 @@ gr_status gr_render_resident(gr_ctx *ctx, uint64_t id, uint32_t sample_offset, u
     std::memset(&shape, 0, sizeof(shape));
     shape.width = rs->S.width;
     shape.height = rs->S.height;
-    return grh::render_into(ctx, &shape, rs->S, resident_buffers(rs), sample_offset, spp, film_dev, s);
+    // stage caps: the chosen pair, or a timed trial of the next unmeasured candidate
+    StageCapTune &T = rs->tune;
+    const uint64_t budget_tuples = ctx->chunk_budget / (3 * sizeof(float));
+    const uint64_t first_chunk = std::min<uint64_t>(n_pixels, std::max<uint64_t>(1, budget_tuples / spp)) * spp;
+    int trial = -1;
+    StageCaps caps{};
+    if (grh::trace_kernel_launches(ctx->kernel_mode, rs->S, first_chunk) == 3) {
+        if (T.best < 0) grh::tune_harvest(T);
+        if (T.best >= 0) {
+            caps = grh::kStageCapCandidates[T.best];
+        } else if (T.staged_calls++ >= 1) {  // the scene's first call carries one-time costs
+            for (int c = 0; c < StageCapTune::kCandidates && trial < 0; ++c)
+                if (!T.issued[c]) trial = c;
+            if (trial >= 0) {
+                auto &tr = T.trial[trial];
+                if (cudaEventCreate(&tr.start) != cudaSuccess || cudaEventCreate(&tr.stop) != cudaSuccess) {
+                    cudaGetLastError();
+                    trial = -1;  // untimed: stay on the built-in pair
+                } else {
+                    tr.candidate = trial;
+                    tr.tuples = n_pixels * spp;
+                    T.issued[trial] = true;
+                    caps = grh::kStageCapCandidates[trial];
+                    cudaEventRecord(tr.start, s);
+                }
+            }
+        }
+    }
+    gr_status st = grh::render_into(ctx, &shape, rs->S, resident_buffers(rs), sample_offset, spp, film_dev, s, caps);
+    if (trial >= 0) cudaEventRecord(rs->tune.trial[trial].stop, s);
+    return st;
+}
+
+gr_status gr_scene_stage_caps(gr_ctx *ctx, uint64_t id, uint32_t *cap_first, uint32_t *cap_second) {
+    if (!ctx || !cap_first || !cap_second) return fail(GR_EINVAL, "NULL argument");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    auto it = ctx->scenes.find(id);
+    if (it == ctx->scenes.end()) return fail(GR_ENOTFOUND, "unknown scene id %llu", (unsigned long long)id);
+    StageCapTune &T = it->second->tune;
+    if (T.best < 0) grh::tune_harvest(T);
+    *cap_first = T.best < 0 ? 0u : grh::kStageCapCandidates[T.best].first;
+    *cap_second = T.best < 0 ? 0u : grh::kStageCapCandidates[T.best].second;
+    return GR_OK;
 }
 
 gr_status gr_render_resident_static(gr_ctx *ctx, uint64_t id, uint32_t sample_offset, uint32_t spp, float *film_dev,

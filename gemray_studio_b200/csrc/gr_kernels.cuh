@@ -50,7 +50,7 @@ template <bool EXTRAS>
 __global__ void __launch_bounds__(TRACE_THREADS, GR_TRACE_MIN_BLOCKS) k_trace_stage1(SceneConst S, SceneBuffers B,
                                                                                      LaunchRange R,
                                                                                      float *__restrict__ xyz,
-                                                                                     ParkOut out) {
+                                                                                     ParkOut out, uint32_t bounce_cap) {
     extern __shared__ float4 s_planes[];
     const Planes PL = stage_plane_set(s_planes, B.planes, S.n_planes);
     const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -61,7 +61,7 @@ __global__ void __launch_bounds__(TRACE_THREADS, GR_TRACE_MIN_BLOCKS) k_trace_st
         tuple_coords(R, t, pixel, sample);
         path_init<1, EXTRAS>(P, S, B, pixel, sample, (uint32_t)t);
     }
-    if (run_or_park<EXTRAS>(P, S, PL, active, GR_STAGE_CAP, out) || !active) return;
+    if (run_or_park<EXTRAS>(P, S, PL, active, bounce_cap, out) || !active) return;
     const V3 c = path_finish<1>(P, S, B);
     xyz[3 * t + 0] = c.x;
     xyz[3 * t + 1] = c.y;

@@ -589,6 +589,15 @@ gr_status gr_denoise_tonemap_device(gr_ctx *ctx, const float *film, uint32_t sam
 #define GR_AUTO_STAGED_MIN_TUPLES (1u << 19)
 gr_status gr_set_kernel(gr_ctx *ctx, uint32_t kernel);
 
+/* Bounce caps of a resident scene's staged renders (stage 1, stage 2).  Every pair gives
+ * the same films; the fastest depends on the stone (measured on B200: 12 / 20 on the
+ * c2 brilliant, 8 / 16 on the c3 emerald, 3.9% faster there).  From the scene's second
+ * staged gr_render_resident call on, one call with each candidate pair is timed with
+ * device events and the pair with the least time per tuple is kept for the scene.
+ * Writes 0 / 0 while the choice is still open.  (gr_accumulate and batched launches use
+ * 12 / 20.) */
+gr_status gr_scene_stage_caps(gr_ctx *ctx, uint64_t scene_id, uint32_t *cap_first, uint32_t *cap_second);
+
 /* Per-launch timing: while enabled, every trace and film-fold launch is bracketed by
  * CUDA events on its own stream.  gr_timing_read waits for them, returns the summed
  * kernel milliseconds and launch counts since the last read (or enable), and resets. */

@@ -211,6 +211,42 @@ def test_auto_kernel_picks_by_launch_size(engine_lib):
         assert np.array_equal(films[abi.GR_KERNEL_STAGED].view(np.uint32), ref)
 
 
+def test_stage_cap_trials_keep_films_identical(engine_lib):
+    """A resident scene's staged renders time one call with each candidate stage-cap
+    pair and keep the faster (gr_scene_stage_caps): every call's film, trial or not,
+    is bit-identical to the plain kernel's."""
+    import torch
+
+    from gemray_studio_b200 import GpuFrameRenderer
+    sc = srb_scene("Sapphire", width=128, height=128, max_bounces=24)
+    n_px = sc.width * sc.height
+    spp = abi.GR_AUTO_STAGED_MIN_TUPLES // n_px  # staged launches
+    plain = GpuFrameRenderer(kernel=abi.GR_KERNEL_PLAIN)
+    r = GpuFrameRenderer()
+    try:
+        sid = C.c_uint64()
+        assert r.lib.gr_scene_upload(r.ctx, C.byref(sc.c_scene()), C.byref(sid)) == abi.GR_OK
+        c1, c2 = C.c_uint32(), C.c_uint32()
+        for k in range(4):
+            film = torch.zeros((n_px, 3), dtype=torch.float32, device="cuda")
+            torch.cuda.synchronize()
+            assert r.lib.gr_render_resident(r.ctx, sid.value, 7 + k * spp, spp, C.c_void_p(film.data_ptr()),
+                                            None) == abi.GR_OK
+            r.synchronize()
+            ref = np.zeros((n_px, 3), np.float32)
+            plain.accumulate(sc, 7 + k * spp, spp, ref)
+            assert np.array_equal(film.cpu().numpy().view(np.uint32), ref.view(np.uint32)), k
+            assert r.lib.gr_scene_stage_caps(r.ctx, sid.value, C.byref(c1), C.byref(c2)) == abi.GR_OK
+            if k == 0:
+                assert (c1.value, c2.value) == (0, 0)  # the first call carries one-time costs: no trial yet
+            del film
+        assert (c1.value, c2.value) in ((12, 20), (8, 16))
+        r.lib.gr_scene_release(r.ctx, sid.value)
+    finally:
+        r.close()
+        plain.close()
+
+
 def test_staged_kernels_bit_identical_when_park_buffers_overflow(engine_lib):
     """A light-trapping stone (n = 3.5): ~16% of paths outlive the first stage cap and
     ~11% the second, more than the park buffers hold (1/8 and 1/32 of a launch's

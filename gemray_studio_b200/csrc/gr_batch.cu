@@ -138,6 +138,7 @@ gr_status make_plan(gr_ctx *ctx, const grh::BatchItem *items, uint32_t n_items, 
             g.warp_begin = cur.warps;
             g.scene = slot;
             g.kahan = (rs->S.flags & GR_FLAG_KAHAN_FILM) ? 1u : 0u;
+            g.stage_cap = grh::scene_stage_cap(*rs);
             g.cont = items[i].cont;
             g.comp = items[i].comp;
             if (g.cont && g.kahan && !g.comp) return fail(GR_EINVAL, "item %u: continue mode with Kahan needs comp", i);

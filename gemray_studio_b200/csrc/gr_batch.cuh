@@ -28,6 +28,7 @@ struct BatchSegment {
     uint32_t kahan;
     uint32_t cont;         // fold_pixel continue mode
     uint32_t park_cap;     // park slots of this segment (paths alive after the stage cap)
+    uint32_t stage_cap;    // stage-1 bounce cap: the scene's chosen one (StageCapTune)
     uint64_t park_off;     // first park slot of this segment in the launch's park buffer
     uint64_t park_block_begin;  // first continuation block of the segment
 };
@@ -52,7 +53,7 @@ __device__ __forceinline__ void load_slot(SceneSlot &dst_slot, const SceneSlot *
 }
 
 // Stage 1 of a batched launch (the staged scheme of the single-scene kernels): paths
-// run up to GR_STAGE_CAP bounces; survivors are parked in their segment's park region
+// run up to their segment's stage cap; survivors are parked in their segment's park region
 // (`park`, slot counters `counts` per segment of the launch) for k_trace_batch_cont.
 // EXTRAS: the variant for launches holding a scene with frosted facets, scattering or
 // a biaxial material.
@@ -81,7 +82,7 @@ __global__ void __launch_bounds__(TRACE_THREADS, GR_TRACE_MIN_BLOCKS)
         path_init<1, EXTRAS>(P, S, B, pixel, sample, (uint32_t)t);
     }
     const ParkOut out{park + G.park_off, G.park_cap, counts + s_seg};
-    if (run_or_park<EXTRAS>(P, S, PL, active, GR_STAGE_CAP, out) || !active) return;
+    if (run_or_park<EXTRAS>(P, S, PL, active, G.stage_cap, out) || !active) return;
     const V3 c = path_finish<1>(P, S, B);
     float *xyz = G.xyz;
     xyz[3 * t + 0] = c.x;

@@ -151,6 +151,9 @@ gr_status launch_trace(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuffers
 // The kernel a launch of n_tuples tuples runs in `mode` (AUTO resolved by size), and
 // how many kernel launches that trace makes.
 int resolve_kernel(int mode, uint64_t n_tuples);
+// The stage-1 bounce cap a resident scene's staged launches use (its chosen pair's
+// first cap, the built-in one while the choice is open).
+uint32_t scene_stage_cap(const ResidentScene &rs);
 int trace_kernel_launches(int mode, const SceneConst &S, uint64_t n_tuples);
 gr_status launch_fold(const float *xyz, uint32_t n_pixels, uint32_t spp, uint32_t first_pixel, float *film,
                       uint32_t kahan, cudaStream_t stream);

@@ -604,6 +604,10 @@ void tune_harvest(StageCapTune &T) {
         if (T.ms_per_mtuple[c] < T.ms_per_mtuple[T.best]) T.best = c;
 }
 
+uint32_t scene_stage_cap(const ResidentScene &rs) {
+    return rs.tune.best >= 0 ? kStageCapCandidates[rs.tune.best].first : (uint32_t)GR_STAGE_CAP;
+}
+
 void tune_release(StageCapTune &T) {
     for (auto &tr : T.trial) {
         if (tr.start) cudaEventDestroy(tr.start);

@@ -241,6 +241,16 @@ def test_stage_cap_trials_keep_films_identical(engine_lib):
                 assert (c1.value, c2.value) == (0, 0)  # the first call carries one-time costs: no trial yet
             del film
         assert (c1.value, c2.value) in ((12, 20), (8, 16))
+        # a batched launch runs the segment with the scene's chosen first cap
+        film = torch.zeros((n_px, 3), dtype=torch.float32, device="cuda")
+        items = (abi.gr_batch_item * 1)(abi.gr_batch_item(sid.value, film.data_ptr(), 7, spp))
+        torch.cuda.synchronize()
+        assert r.lib.gr_render_batch(r.ctx, items, 1, 0, None) == abi.GR_OK
+        r.synchronize()
+        ref = np.zeros((n_px, 3), np.float32)
+        plain.accumulate(sc, 7, spp, ref)
+        assert np.array_equal(film.cpu().numpy().view(np.uint32), ref.view(np.uint32))
+        del film
         r.lib.gr_scene_release(r.ctx, sid.value)
     finally:
         r.close()

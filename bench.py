@@ -429,7 +429,8 @@ def run_engine(args):
 
     # e2e through the C-ABI call with host buffers (upload + readback in the timed region)
     host_acc = np.zeros((n_px, 3), np.float32)
-    r.accumulate(sc, base, spp, host_acc)  # warm
+    for i in range(args.warmup):  # warm (the stone's stage-cap trials run here, untimed)
+        r.accumulate(sc, base + i * spp, spp, host_acc)
     barrier(world)
     e_evs = []
     for i in range(args.steps):

@@ -90,6 +90,10 @@ struct gr_ctx {
     // launch stream); read back by gr_timing_read.
     bool timing = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> trace_ev, fold_ev;
+    // gr_accumulate's stage-cap choices, keyed by the stone (planes, finishes, material,
+    // depth, flags: what sets the path lengths); cleared past kMaxAccumTunes stones
+    std::map<uint64_t, StageCapTune> accum_tune;
+    static constexpr size_t kMaxAccumTunes = 64;
     size_t trace_used = 0, fold_used = 0;
     uint64_t trace_launches = 0, fold_launches = 0;
     // gr_render_batch: scene-slot + segment tables, captured launch sequences, and a
@@ -154,6 +158,17 @@ int resolve_kernel(int mode, uint64_t n_tuples);
 // The stage-1 bounce cap a resident scene's staged launches use (its chosen pair's
 // first cap, the built-in one while the choice is open).
 uint32_t scene_stage_cap(const ResidentScene &rs);
+// A staged call's caps under tuning state T: the chosen pair, or a device-timed trial
+// of the next unmeasured candidate (trial >= 0; tune_end records its end).  The
+// scene's first staged call runs untimed (it carries one-time costs).
+StageCaps tune_begin(StageCapTune &T, int kernel_mode, const SceneConst &S, uint64_t n_pixels, uint32_t spp,
+                     uint64_t chunk_budget, cudaStream_t s, int &trial);
+void tune_end(StageCapTune &T, int trial, cudaStream_t s);
+void tune_release(StageCapTune &T);
+// gr_accumulate's tuning state for the scene's stone (created on first use).
+StageCapTune &accum_tune(gr_ctx *ctx, const gr_scene *sc);
+// The gr_accumulate tuning key of a scene (its stone, not its view).
+uint64_t stone_key(const gr_scene *sc);
 int trace_kernel_launches(int mode, const SceneConst &S, uint64_t n_tuples);
 gr_status launch_fold(const float *xyz, uint32_t n_pixels, uint32_t spp, uint32_t first_pixel, float *film,
                       uint32_t kahan, cudaStream_t stream);

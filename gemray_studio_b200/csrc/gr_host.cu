@@ -608,12 +608,68 @@ uint32_t scene_stage_cap(const ResidentScene &rs) {
     return rs.tune.best >= 0 ? kStageCapCandidates[rs.tune.best].first : (uint32_t)GR_STAGE_CAP;
 }
 
+StageCaps tune_begin(StageCapTune &T, int kernel_mode, const SceneConst &S, uint64_t n_pixels, uint32_t spp,
+                     uint64_t chunk_budget, cudaStream_t s, int &trial) {
+    trial = -1;
+    const uint64_t budget_tuples = chunk_budget / (3 * sizeof(float));
+    const uint64_t first_chunk = std::min<uint64_t>(n_pixels, std::max<uint64_t>(1, budget_tuples / spp)) * spp;
+    if (trace_kernel_launches(kernel_mode, S, first_chunk) != 3) return StageCaps{};  // not staged
+    if (T.best < 0) tune_harvest(T);
+    if (T.best >= 0) return kStageCapCandidates[T.best];
+    if (T.staged_calls++ == 0) return StageCaps{};
+    for (int c = 0; c < StageCapTune::kCandidates && trial < 0; ++c)
+        if (!T.issued[c]) trial = c;
+    if (trial < 0) return StageCaps{};  // every trial issued, not all finished yet
+    auto &tr = T.trial[trial];
+    if ((!tr.start && cudaEventCreate(&tr.start) != cudaSuccess) || (!tr.stop && cudaEventCreate(&tr.stop) != cudaSuccess)) {
+        cudaGetLastError();
+        trial = -1;  // untimed: stay on the built-in pair
+        return StageCaps{};
+    }
+    tr.candidate = trial;
+    tr.tuples = n_pixels * spp;
+    T.issued[trial] = true;
+    cudaEventRecord(tr.start, s);
+    return kStageCapCandidates[trial];
+}
+
+void tune_end(StageCapTune &T, int trial, cudaStream_t s) {
+    if (trial >= 0) cudaEventRecord(T.trial[trial].stop, s);
+}
+
+uint64_t stone_key(const gr_scene *sc) {
+    uint64_t h = 1469598103934665603ull;  // FNV-1a, 64 bit
+    auto mix = [&h](const void *p, size_t n) {
+        const unsigned char *b = (const unsigned char *)p;
+        for (size_t i = 0; i < n; ++i) h = (h ^ b[i]) * 1099511628211ull;
+    };
+    mix(&sc->n_planes, sizeof(sc->n_planes));
+    mix(&sc->max_bounces, sizeof(sc->max_bounces));
+    mix(&sc->flags, sizeof(sc->flags));
+    if (sc->planes) mix(sc->planes, (size_t)sc->n_planes * sizeof(gr_plane));
+    if (sc->finishes) mix(sc->finishes, (size_t)sc->n_planes * sizeof(uint32_t));
+    if (sc->material) mix(sc->material, sizeof(gr_material));
+    if (sc->material_ext) mix(sc->material_ext, sizeof(gr_material_ext));
+    return h;
+}
+
 void tune_release(StageCapTune &T) {
     for (auto &tr : T.trial) {
         if (tr.start) cudaEventDestroy(tr.start);
         if (tr.stop) cudaEventDestroy(tr.stop);
         tr.start = tr.stop = nullptr;
     }
+}
+
+StageCapTune &accum_tune(gr_ctx *ctx, const gr_scene *sc) {
+    const uint64_t key = stone_key(sc);
+    auto it = ctx->accum_tune.find(key);
+    if (it != ctx->accum_tune.end()) return it->second;
+    if (ctx->accum_tune.size() >= gr_ctx::kMaxAccumTunes) {
+        for (auto &kv : ctx->accum_tune) tune_release(kv.second);
+        ctx->accum_tune.clear();
+    }
+    return ctx->accum_tune[key];
 }
 }  // namespace grh
 
@@ -708,6 +764,8 @@ gr_status gr_destroy(gr_ctx *ctx) {
         if (ctx->wf_done_host) cudaFreeHost(ctx->wf_done_host);
         for (auto &p : ctx->trace_ev) { cudaEventDestroy(p.first); cudaEventDestroy(p.second); }
         for (auto &p : ctx->fold_ev) { cudaEventDestroy(p.first); cudaEventDestroy(p.second); }
+        for (auto &kv : ctx->accum_tune) grh::tune_release(kv.second);
+        ctx->accum_tune.clear();
         for (auto &kv : ctx->scenes) {
             grh::tune_release(kv.second->tune);
             kv.second->planes.release();
@@ -740,7 +798,11 @@ gr_status gr_accumulate(gr_ctx *ctx, const gr_scene *sc, uint32_t sample_offset,
     st = ctx->film.reserve(fbytes);
     if (st != GR_OK) return st;
     GR_CUDA(cudaMemcpyAsync(ctx->film.ptr, accum, fbytes, cudaMemcpyHostToDevice, ctx->stream));
-    st = grh::render_into(ctx, sc, S, B, sample_offset, spp, (float *)ctx->film.ptr, ctx->stream);
+    StageCapTune &T = grh::accum_tune(ctx, sc);
+    int trial = -1;
+    const StageCaps caps = grh::tune_begin(T, ctx->kernel_mode, S, n_pixels, spp, ctx->chunk_budget, ctx->stream, trial);
+    st = grh::render_into(ctx, sc, S, B, sample_offset, spp, (float *)ctx->film.ptr, ctx->stream, caps);
+    grh::tune_end(T, trial, ctx->stream);
     if (st != GR_OK) {
         cudaStreamSynchronize(ctx->stream);
         return st;
@@ -775,7 +837,11 @@ gr_status gr_accumulate_device(gr_ctx *ctx, const gr_scene *sc, uint32_t sample_
         cudaStreamWaitEvent(s, ev, 0);
         cudaEventDestroy(ev);
     }
-    st = grh::render_into(ctx, sc, S, B, sample_offset, spp, accum_dev, s);
+    StageCapTune &T = grh::accum_tune(ctx, sc);
+    int trial = -1;
+    const StageCaps caps = grh::tune_begin(T, ctx->kernel_mode, S, n_pixels, spp, ctx->chunk_budget, s, trial);
+    st = grh::render_into(ctx, sc, S, B, sample_offset, spp, accum_dev, s, caps);
+    grh::tune_end(T, trial, s);
     if (st != GR_OK) return st;
     if (s != ctx->stream) {
         // Later uploads on the context stream must wait for this work.
@@ -945,36 +1011,11 @@ gr_status gr_render_resident(gr_ctx *ctx, uint64_t id, uint32_t sample_offset, u
     std::memset(&shape, 0, sizeof(shape));
     shape.width = rs->S.width;
     shape.height = rs->S.height;
-    // stage caps: the chosen pair, or a timed trial of the next unmeasured candidate
-    StageCapTune &T = rs->tune;
-    const uint64_t budget_tuples = ctx->chunk_budget / (3 * sizeof(float));
-    const uint64_t first_chunk = std::min<uint64_t>(n_pixels, std::max<uint64_t>(1, budget_tuples / spp)) * spp;
     int trial = -1;
-    StageCaps caps{};
-    if (grh::trace_kernel_launches(ctx->kernel_mode, rs->S, first_chunk) == 3) {
-        if (T.best < 0) grh::tune_harvest(T);
-        if (T.best >= 0) {
-            caps = grh::kStageCapCandidates[T.best];
-        } else if (T.staged_calls++ >= 1) {  // the scene's first call carries one-time costs
-            for (int c = 0; c < StageCapTune::kCandidates && trial < 0; ++c)
-                if (!T.issued[c]) trial = c;
-            if (trial >= 0) {
-                auto &tr = T.trial[trial];
-                if (cudaEventCreate(&tr.start) != cudaSuccess || cudaEventCreate(&tr.stop) != cudaSuccess) {
-                    cudaGetLastError();
-                    trial = -1;  // untimed: stay on the built-in pair
-                } else {
-                    tr.candidate = trial;
-                    tr.tuples = n_pixels * spp;
-                    T.issued[trial] = true;
-                    caps = grh::kStageCapCandidates[trial];
-                    cudaEventRecord(tr.start, s);
-                }
-            }
-        }
-    }
+    const StageCaps caps =
+        grh::tune_begin(rs->tune, ctx->kernel_mode, rs->S, n_pixels, spp, ctx->chunk_budget, s, trial);
     gr_status st = grh::render_into(ctx, &shape, rs->S, resident_buffers(rs), sample_offset, spp, film_dev, s, caps);
-    if (trial >= 0) cudaEventRecord(rs->tune.trial[trial].stop, s);
+    grh::tune_end(rs->tune, trial, s);
     return st;
 }
 

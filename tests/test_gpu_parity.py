@@ -252,6 +252,14 @@ def test_stage_cap_trials_keep_films_identical(engine_lib):
         assert np.array_equal(film.cpu().numpy().view(np.uint32), ref.view(np.uint32))
         del film
         r.lib.gr_scene_release(r.ctx, sid.value)
+        # gr_accumulate tunes per stone the same way: trial calls included, every film
+        # is the plain kernel's
+        for k in range(4):
+            got = np.zeros((n_px, 3), np.float32)
+            r.accumulate(sc, 11 + k * spp, spp, got)
+            ref = np.zeros((n_px, 3), np.float32)
+            plain.accumulate(sc, 11 + k * spp, spp, ref)
+            assert np.array_equal(got.view(np.uint32), ref.view(np.uint32)), k
     finally:
         r.close()
         plain.close()

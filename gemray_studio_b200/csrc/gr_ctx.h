@@ -42,7 +42,7 @@ struct StageCapTune {
     int best = -1;              // chosen candidate, -1 while measuring
     uint32_t staged_calls = 0;  // staged calls seen
     bool issued[kCandidates] = {};
-    float ms_per_mtuple[kCandidates] = {};
+    float ms_per_mtuple[kCandidates] = {3.0e38f, 3.0e38f};  // unmeasured: never chosen over a measured one
     struct Trial {
         cudaEvent_t start = nullptr, stop = nullptr;
         int candidate = 0;

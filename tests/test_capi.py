@@ -30,6 +30,26 @@ def test_header_compiles_with_static_asserts():
     assert r.returncode == 0, r.stderr
 
 
+def header_int_constants() -> dict[str, int]:
+    """Every `#define GR_* <integer expression>` of the header, evaluated."""
+    out = {}
+    for name, expr in re.findall(r"^#define\s+(GR_\w+)\s+(.+?)\s*(?:/\*.*)?$", HEADER.read_text(), flags=re.M):
+        py = re.sub(r"(?<=[0-9a-fA-F])[uU][lL]*\b", "", expr)
+        if not re.fullmatch(r"[0-9a-fA-Fx()<>| +\-*]+", py):
+            continue
+        out[name] = eval(py, {"__builtins__": {}})
+    return out
+
+
+def test_python_constants_match_header():
+    consts = header_int_constants()
+    assert "GR_KERNEL_AUTO" in consts and consts["GR_AUTO_STAGED_MIN_TUPLES"] == 1 << 19
+    shared = [n for n in consts if hasattr(abi, n)]
+    assert len(shared) >= 10
+    for n in shared:
+        assert getattr(abi, n) == consts[n], n
+
+
 def test_library_exports_every_declared_symbol(engine_lib):
     names = declared_functions()
     assert len(names) >= 15

@@ -158,6 +158,8 @@ int resolve_kernel(int mode, uint64_t n_tuples);
 // The stage-1 bounce cap a resident scene's staged launches use (its chosen pair's
 // first cap, the built-in one while the choice is open).
 uint32_t scene_stage_cap(const ResidentScene &rs);
+// Both caps of the scene's chosen pair ({0, 0}, the built-in pair, while open).
+StageCaps scene_stage_caps(const ResidentScene &rs);
 // A staged call's caps under tuning state T: the chosen pair, or a device-timed trial
 // of the next unmeasured candidate (trial >= 0; tune_end records its end).  The
 // scene's first staged call runs untimed (it carries one-time costs).

@@ -608,6 +608,10 @@ uint32_t scene_stage_cap(const ResidentScene &rs) {
     return rs.tune.best >= 0 ? kStageCapCandidates[rs.tune.best].first : (uint32_t)GR_STAGE_CAP;
 }
 
+StageCaps scene_stage_caps(const ResidentScene &rs) {
+    return rs.tune.best >= 0 ? kStageCapCandidates[rs.tune.best] : StageCaps{};
+}
+
 StageCaps tune_begin(StageCapTune &T, int kernel_mode, const SceneConst &S, uint64_t n_pixels, uint32_t spp,
                      uint64_t chunk_budget, cudaStream_t s, int &trial) {
     trial = -1;

@@ -96,6 +96,7 @@ struct FrameStream {
     ResidentScene *rs = nullptr;
     SceneConst S;
     grd::SceneBuffers B;
+    StageCaps caps;  // the scene's stage caps as chosen when the stream opened
     uint32_t first = 0, samples = 0;
     double target_ms = 100.0;
     uint32_t first_batch = 1, fixed_batch = 0;
@@ -149,7 +150,7 @@ gr_status trace_subbatch(FrameStream *fs, uint32_t bfirst, uint32_t n) {
         R.spp = n;
         R.n_tuples = np * n;
         st = grh::launch_trace(fs->ctx, fs->S, fs->B, R, (float *)fs->scratch.ptr, fs->main, GR_KERNEL_AUTO,
-                               &fs->park);
+                               &fs->park, fs->caps);
         if (st != GR_OK) return st;
         st = grh::launch_fold((const float *)fs->scratch.ptr, (uint32_t)np, n, (uint32_t)p0, (float *)fs->batch.ptr,
                               (fs->S.flags & GR_FLAG_KAHAN_FILM) ? 1u : 0u, fs->main);
@@ -320,6 +321,7 @@ gr_status gr_stream_open(gr_ctx *ctx, uint64_t scene_id, uint32_t first_sample, 
         fs->rs = it->second;
         fs->S = fs->rs->S;
         fs->B = resident_buffers(fs->rs);
+        fs->caps = grh::scene_stage_caps(*fs->rs);
         fs->rs->users++;
     }
     fs->n_pixels = (uint64_t)fs->S.width * fs->S.height;

@@ -597,8 +597,8 @@ gr_status gr_set_kernel(gr_ctx *ctx, uint32_t kernel);
  * Writes 0 / 0 while the choice is still open.  Batched launches (gr_render_batch, the
  * request loop) run each scene with its chosen first cap (their continuation stage is
  * uncapped); gr_accumulate and gr_accumulate_device choose the same way per stone
- * (planes, finishes, material, depth and flags; not the view), frame streams use
- * 12 / 20. */
+ * (planes, finishes, material, depth and flags; not the view); a frame stream uses
+ * its scene's pair as chosen when the stream opened. */
 gr_status gr_scene_stage_caps(gr_ctx *ctx, uint64_t scene_id, uint32_t *cap_first, uint32_t *cap_second);
 
 /* Per-launch timing: while enabled, every trace and film-fold launch is bracketed by

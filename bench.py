@@ -41,6 +41,7 @@ from pathlib import Path
 
 ROOT = Path(__file__).resolve().parent
 HBM_FALLBACK_GBS = 6650.0  # B200 copy bandwidth, used when the per-device measurement is absent
+KERNELS = ("auto", "staged", "plain", "regen", "wavefront")  # GR_KERNEL_<NAME>
 sys.path.insert(0, str(ROOT))
 
 import numpy as np  # noqa: E402
@@ -247,23 +248,35 @@ def run_reference(args):
     }), flush=True)
 
 
-def traffic_per_launch(tuples_per_launch: float):
-    """DRAM bytes (read + write) of one transport launch (the staged kernels' three
-    stages): the per-tuple traffic of the committed ncu capture
-    (profiles/k_trace_staged_traffic.json) times the tuples one launch processes, or
-    None without a capture."""
-    p = ROOT / "profiles" / "k_trace_staged_traffic.json"
+TRANSPORT_LABELS = {"staged": "k_trace_stage1 + k_trace_stage2 x2 (staged transport)", "plain": "k_trace_plain",
+                    "regen": "k_trace_regen", "wavefront": "k_wf_* (wavefront engine)"}
+
+
+def transport_kernel(kernel_arg: str, trace_launches: int, fold_launches: int) -> str:
+    """Which transport ran: regen / wavefront as asked; otherwise staged when every
+    chunk took the three staged launches, plain when one."""
+    if kernel_arg in ("regen", "wavefront"):
+        return kernel_arg
+    return "staged" if trace_launches >= 3 * max(1, fold_launches) else "plain"
+
+
+def traffic_per_launch(tuples_per_launch: float, kernel: str = "staged"):
+    """DRAM bytes (read + write) of one transport launch: the per-tuple traffic of the
+    committed ncu capture of that transport (profiles/k_trace_<kernel>_traffic.json;
+    the staged figure covers its three stages) times the tuples one launch processes,
+    or None without a capture."""
+    p = ROOT / "profiles" / f"k_trace_{kernel}_traffic.json"
     if not p.exists():
         return None
     per_tuple = json.loads(p.read_text())["dram_bytes_per_tuple"]
     return per_tuple * tuples_per_launch
 
 
-def hbm_view(tuples_per_launch: float, ms_per_launch: float):
+def hbm_view(tuples_per_launch: float, ms_per_launch: float, kernel: str = "staged"):
     """The transport kernel against the measured HBM copy bandwidth: its DRAM traffic
     per launch (from the committed ncu capture) over its event-timed duration.  Shows
     how far the kernel is from being memory-bound."""
-    t = traffic_per_launch(tuples_per_launch)
+    t = traffic_per_launch(tuples_per_launch, kernel)
     p = ROOT / "MEASURED_PEAKS.json"
     if t is None or ms_per_launch <= 0:
         return None
@@ -369,7 +382,7 @@ def run_engine(args):
     build.build()
     torch.cuda.set_device(local)
     sc, w = make_scene(args.workload)
-    r = GpuFrameRenderer(device=local)
+    r = GpuFrameRenderer(device=local, kernel=getattr(abi, "GR_KERNEL_" + args.kernel.upper()))
     lib, ctx = r.lib, r.ctx
     stream_ptr = lib.gr_stream(ctx)
     stream = torch.cuda.ExternalStream(stream_ptr)
@@ -459,6 +472,7 @@ def run_engine(args):
     dnv = denoise_view(r, sc, film, (args.warmup + args.steps) * spp, stream) if world == 1 else None
 
     trace_ms_per_launch = tr.value / max(1, ntr.value)
+    transport = transport_kernel(args.kernel, ntr.value, nfo.value)
     frames = args.steps
     flops_per_frame = model.flops_per_sample * samples_per_step
     achieved = flops_per_frame * frames / (tr.value * 1e-3) / 1e12
@@ -470,14 +484,15 @@ def run_engine(args):
             "metric": "path-samples/s", "value": value, "unit": "path-samples/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms_max / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": workload_config(args.workload, w, f"sample-range shards x{world}" if world > 1 else "single GPU"),
+            "config": {**workload_config(args.workload, w, f"sample-range shards x{world}" if world > 1 else "single GPU"),
+                       "kernel": args.kernel},
             "e2e": {"value": e2e_value, "unit": "path-samples/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
-            "roofline": {"bound": "fp32", "kernel": "k_trace_stage1 + k_trace_stage2 x2 (staged transport)", "achieved": achieved, "peak": fp32_peak,
+            "roofline": {"bound": "fp32", "kernel": TRANSPORT_LABELS[transport], "achieved": achieved, "peak": fp32_peak,
                          "unit": "TFLOP/s", "frac": achieved / fp32_peak,
-                         "traffic": traffic_per_launch(samples_per_step / max(1, ntr.value / frames)),
+                         "traffic": traffic_per_launch(samples_per_step / max(1, ntr.value / frames), transport),
                          "hbm_view": hbm_view(samples_per_step / max(1, ntr.value / frames),
-                                              tr.value / max(1, ntr.value)),
+                                              tr.value / max(1, ntr.value), transport),
                          "peak_source": "measured on this device by gr_probe_fp32_peak (8 independent FFMA chains)",
                          "flops_per_sample": model.flops_per_sample,
                          "sfu_ops_per_sample": model.sfu / max(1, model.paths),
@@ -738,6 +753,8 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernel", default="auto", choices=KERNELS,
+                    help="c1/c2/c3: transport kernel (auto: staged from 2^19 tuples per launch, plain below)")
     ap.add_argument("--scale", type=float, default=1.0, help="c4: film side scale")
     ap.add_argument("--rate", type=float, default=40.0, help="c5: arrivals per second")
     ap.add_argument("--duration", type=float, default=10.0, help="c5: seconds of arrivals")

@@ -9,10 +9,12 @@ namespace grd {
 // Staged kernels.  Within a warp path lengths differ widely (on the c2 brilliant the
 // warp's longest path averages ~2.6x the mean), so a warp spends most of its bounce
 // iterations on a few long paths with the other lanes idle.  Stage 1 runs every path
-// for at most GR_STAGE_CAP bounces; a path still alive then is parked -- its record
+// for at most a first cap of bounces; a path still alive then is parked -- its record
 // copied to a park buffer in warp-aggregated slots -- and a continuation stage
-// resumes the parked paths, now packed densely, one per thread, again up to a cap
-// (GR_STAGE_CAP2) with its own park buffer for a final, uncapped stage.  A path whose
+// resumes the parked paths, now packed densely, one per thread, again up to a second
+// cap with its own park buffer for a final, uncapped stage.  The caps are kernel
+// arguments: GR_STAGE_CAP / GR_STAGE_CAP2 by default, or the pair a resident scene
+// chose by timing (StageCapTune, gr_host.cu).  A path whose
 // slot would overflow a park buffer simply continues in place.  Each path runs the
 // same functions in the same order as in the plain kernel, so every XYZ is
 // bit-identical; only the schedule differs.

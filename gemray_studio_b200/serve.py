@@ -8,7 +8,9 @@ The library's worker thread admits requests by device-memory budget and advances
 running renders together, one slice per tick, in shared batched launches.  Slices
 continue each pixel's running sum, so a film is bit-identical to rendering the whole
 sample range alone in one call, however it was sliced and whatever else ran.  Metric
-sweeps (brilliance / fire / scintillation over a list of poses) share the same queue.
+sweeps (brilliance / fire / scintillation over a list of poses) use the same request
+ids and calls; they hold no film, skip admission and run on a second worker thread
+beside the renders.
 """
 from __future__ import annotations
 

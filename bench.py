@@ -46,34 +46,40 @@ sys.path.insert(0, str(ROOT))
 
 import numpy as np  # noqa: E402
 
+from gemray_studio_b200.workloads import CONFIGS  # noqa: E402
+
 WORKLOADS = {
-    "c1": dict(width=256, height=256, spp=64, max_bounces=32, env="uniform", stone="rb57"),
-    "c2": dict(width=1920, height=1080, spp=256, max_bounces=32, env="latlong", stone="rb57"),
-    "c3": dict(width=1024, height=1024, spp=1024, max_bounces=64, env="studio", stone="em49"),
-    # c2's scene at 480x270, 64 spp: the small case the ncu captures run on
-    "c2s": dict(width=480, height=270, spp=64, max_bounces=32, env="latlong", stone="rb57"),
+    **CONFIGS,
     # batched and served forms (run_batch / run_serve; their scenes come from workloads.py)
     "c4": dict(width=0, height=0, spp=0, max_bounces=32, env="latlong", stone="random"),
     "c5": dict(width=0, height=0, spp=0, max_bounces=32, env="latlong", stone="random"),
 }
 
 
-def make_scene(name: str):
-    from gemray_studio_b200 import abi, scene as S
-    w = WORKLOADS[name]
-    planes = S.round_brilliant_57() if w["stone"] == "rb57" else S.emerald_cut_49()
-    env_mode = {"uniform": abi.GR_ENV_UNIFORM, "latlong": abi.GR_ENV_LATLONG, "studio": abi.GR_ENV_STUDIO}[w["env"]]
-    latlong = S.gaussian_blob_latlong(2048, 1024, 12, seed=0) if w["env"] == "latlong" else None
-    ext = None
-    if w["stone"] == "rb57":
-        mat = S.builtin_material("Diamond")
-    else:  # the emerald's uniaxial, dichroic material with a wavelength-dependent birefringence
-        from gemray_studio_b200 import workloads as W
-        mat, ext = W.birefringent_emerald_material()
-    sc = S.Scene(width=w["width"], height=w["height"], planes=planes, material=mat, cam=S.camera(0.35, 0.28, 5.0, 18.0),
-                 max_bounces=w["max_bounces"], env_mode=env_mode, latlong=latlong, uniform_rgb=(1.0, 1.0, 1.0),
-                 ext=ext)
-    return sc, w
+def make_scene(name: str, builders: str = "engine"):
+    """The workload's scene.  builders="oracle" takes Camera::new and the built-in
+    material from the oracle (the reference arm loads no product library)."""
+    from gemray_studio_b200 import workloads as W
+    if builders == "oracle":
+        import ctypes as C
+
+        from gemray_studio_b200 import abi
+        sys.path.insert(0, str(ROOT / "tests"))
+        import oracle_lib
+        L = oracle_lib.lib()
+
+        def camera(yaw, pitch, dist, fov):
+            cam = abi.gr_camera()
+            L.gro_camera_new(yaw, pitch, dist, fov, C.byref(cam))
+            return cam
+
+        def material(name):
+            m = abi.gr_material()
+            assert L.gro_builtin_material(name.encode(), C.byref(m)) == 0
+            return m
+
+        return W.config_scene(name, camera=camera, builtin_material=material)
+    return W.config_scene(name)
 
 
 def workload_config(name: str, w: dict, parallelism: str) -> dict:
@@ -208,7 +214,7 @@ def run_reference(args):
     world, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
     if rank != 0:
         return
-    sc, w = make_scene(args.workload)
+    sc, w = make_scene(args.workload, builders="oracle")
     sys.path.insert(0, str(ROOT / "tests"))
     import oracle_lib
     oracle_lib.build_oracle()

@@ -59,6 +59,18 @@ GR_AUTO_STAGED_MIN_TUPLES = 1 << 19
 GR_STATIC_SCRATCH_BYTES = 16 << 20
 GR_STATIC_SCRATCH_TUPLES = GR_STATIC_SCRATCH_BYTES // 12
 
+# gr_trace_events: termination reasons and per-bounce events
+GR_TERM_ESCAPED, GR_TERM_ROULETTE, GR_TERM_HIT_CAP = 0, 2, 3
+GR_SEQ_TIR, GR_SEQ_REFLECT, GR_SEQ_REFRACT, GR_SEQ_SCATTER, GR_SEQ_NONE = 0, 1, 2, 3, 0xFF
+
+# gr_case_bank: per-function case banks (layouts in include/gemray_cuda.h)
+BANK_NAMES = ["camera_ray", "cmf", "blackbody", "dispersion", "absorption", "pleochroic", "fresnel_reflection",
+              "fresnel_transmission", "frame_rotation", "tir_retardation", "signed_psi", "tir_phase_delta",
+              "eigen_uniaxial", "walk_off", "extraordinary_index", "theta_c", "studio", "rgb_spectral", "exp_poly",
+              "hg_sample", "cosine_hemisphere", "e_field", "von_kries", "wavelengths"]
+GR_BANK = {n: i for i, n in enumerate(BANK_NAMES)}
+GR_BANK_COUNT = len(BANK_NAMES)
+
 
 class gr_plane(C.Structure):
     _fields_ = [("normal", C.c_float * 3), ("d", C.c_float)]
@@ -225,6 +237,15 @@ EXPORTS = [
     ("gr_event_counts", C.c_int, [_ctx_p, C.POINTER(gr_scene), C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                   C.POINTER(C.c_uint64), C.c_uint32]),
     ("gr_probe_fp32_peak", C.c_int, [_ctx_p, C.POINTER(C.c_double)]),
+    ("gr_trace_events", C.c_int, [_ctx_p, C.POINTER(gr_scene), C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                  C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_int32),
+                                  C.POINTER(C.c_float), C.POINTER(C.c_uint8)]),
+    ("gr_case_bank_arity", C.c_int, [C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    ("gr_case_bank", C.c_int, [_ctx_p, C.c_uint32, C.POINTER(gr_scene), C.POINTER(C.c_float), C.c_uint32,
+                               C.POINTER(C.c_float)]),
+    ("gr_device_code_version", C.c_int, [_ctx_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    ("gr_intersect_rays", C.c_int, [_ctx_p, C.c_void_p, C.c_uint32, C.POINTER(C.c_float), C.c_uint32,
+                                    C.POINTER(C.c_float), C.POINTER(C.c_int32)]),
     ("gr_optical_metrics", C.c_int, [_ctx_p, C.c_void_p, C.c_uint32, C.POINTER(gr_material), C.POINTER(gr_pose),
                                      C.c_uint32, C.c_uint32, C.POINTER(gr_metrics_out)]),
     ("gr_angular_profile", C.c_int, [_ctx_p, C.c_void_p, C.c_uint32, C.POINTER(gr_material), C.c_float, C.c_float,

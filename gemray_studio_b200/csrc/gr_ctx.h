@@ -146,6 +146,11 @@ namespace grd {
 struct LaunchRange;
 }
 namespace grh {
+// Scene checks and encoding (gr_host.cu): validate, encode the constants, and upload
+// the scene's arrays into the context's buffers (prepare does all three).
+gr_status validate_scene(const gr_scene *sc);
+void encode_scene(const gr_scene *sc, SceneConst &S);
+gr_status prepare(gr_ctx *ctx, const gr_scene *sc, SceneConst &S, grd::SceneBuffers &B);
 // Tuples [0, R.n_tuples) of one chunk traced into xyz on `stream` with kernel `mode`
 // (gr_host.cu), and the ordered per-pixel fold of n_pixels pixels into film.
 // STAGED mode parks paths in `park` (the context's buffer when NULL).

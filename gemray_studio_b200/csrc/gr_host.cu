@@ -1065,9 +1065,11 @@ gr_status gr_render_resident_static(gr_ctx *ctx, uint64_t id, uint32_t sample_of
         R.n_tuples = np * spp;
         gr_status st = grh::launch_trace(ctx, rs->S, B, R, scratch, s, GR_KERNEL_PLAIN);
         if (st != GR_OK) return st;
+        ctx->trace_launches += 1;
         st = grh::launch_fold(scratch, (uint32_t)np, spp, (uint32_t)first, film_dev,
                               (rs->S.flags & GR_FLAG_KAHAN_FILM) ? 1u : 0u, s);
         if (st != GR_OK) return st;
+        ctx->fold_launches += 1;
     }
     return GR_OK;
 }

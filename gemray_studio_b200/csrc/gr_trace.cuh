@@ -93,20 +93,54 @@ struct NoCounters {};
 template <class CT> __device__ __forceinline__ void tally(CT &, int, uint32_t = 1) {}
 template <> __device__ __forceinline__ void tally<Counters>(Counters &ct, int i, uint32_t v) { ct.c[i] += v; }
 
+// Per-tuple event-sequence recorder of the instrumented variant (gr_trace_events): the
+// facet, hit distance and event of each bounce b < kmax, and how the path ended.  The
+// other hook types record nothing, so their instantiations carry no recording code.
+struct EventRec {
+    int32_t *facets;
+    float *ts;
+    uint8_t *events;
+    uint32_t *bounces, *term;
+    uint32_t kmax;
+    uint64_t t;
+};
+template <class CT> __device__ __forceinline__ void note_hit(CT &, uint32_t, int, float) {}
+template <class CT> __device__ __forceinline__ void note_event(CT &, uint32_t, uint32_t) {}
+template <class CT> __device__ __forceinline__ void note_end(CT &, uint32_t, uint32_t) {}
+template <> __device__ __forceinline__ void note_hit<EventRec>(EventRec &r, uint32_t b, int f, float t) {
+    if (b < r.kmax) {
+        r.facets[r.t * r.kmax + b] = f;
+        r.ts[r.t * r.kmax + b] = t;
+    }
+}
+template <> __device__ __forceinline__ void note_event<EventRec>(EventRec &r, uint32_t b, uint32_t ev) {
+    if (b < r.kmax) r.events[r.t * r.kmax + b] = (uint8_t)ev;
+}
+template <> __device__ __forceinline__ void note_end<EventRec>(EventRec &r, uint32_t b, uint32_t term) {
+    r.bounces[r.t] = b;
+    r.term[r.t] = term;
+}
+
 // Build the path of tuple (pixel, sample): sampler draws (sampling.rs:232-271),
 // camera ray (camera.rs:95-114), per-sample wavelength cache (refraction.rs:127-174).
 // X: the extension instantiation (biaxial materials keep their beta-ray coefficient,
 // or the ordinary one when the material has no third band set, where uniaxial ones
 // keep n_e - n_o, which no biaxial step reads).
+// Camera::generate_ray (camera.rs:95-114): the primary direction through pixel (x, y)
+// with jitter (jx, jy).
+__device__ __forceinline__ V3 camera_dir(const SceneConst &S, float x, float y, float jx, float jy) {
+    float aspect = S.width_f / S.height_f;
+    float u = ((x + jx) / S.width_f - 0.5f) * 2.0f * aspect * S.fov_tan;
+    float v = (0.5f - (y + jy) / S.height_f) * 2.0f * S.fov_tan;
+    return normalize(add(add(ld3(S.cam_f), mul(ld3(S.cam_r), u)), mul(ld3(S.cam_u), v)));
+}
+
 template <int U = 1, bool X = false>
 __device__ __forceinline__ void path_init(Path &P, const SceneConst &S, const SceneBuffers &B, uint32_t pixel,
                                           uint32_t sample, uint32_t tuple) {
     Draws dr = sample_draws(pixel, sample);
     uint32_t x = pixel % S.width, y = pixel / S.width;
-    float aspect = S.width_f / S.height_f;
-    float u = (((float)x + dr.jx) / S.width_f - 0.5f) * 2.0f * aspect * S.fov_tan;
-    float v = (0.5f - ((float)y + dr.jy) / S.height_f) * 2.0f * S.fov_tan;
-    V3 dir = normalize(add(add(ld3(S.cam_f), mul(ld3(S.cam_r), u)), mul(ld3(S.cam_u), v)));
+    V3 dir = camera_dir(S, (float)x, (float)y, dr.jx, dr.jy);
     P.o_hero = make_float4(S.cam_o[0], S.cam_o[1], S.cam_o[2], dr.hero);
     P.d_seed = make_float4(dir.x, dir.y, dir.z, __uint_as_float(dr.seed));
     P.prev_tuple = make_float4(0.f, 0.f, 0.f, __uint_as_float(tuple));
@@ -416,20 +450,26 @@ __device__ __forceinline__ void absorption_eigenmodes(const Path &P, const Scene
 }
 // effective_pleochroic_alpha (optics/birefringence.rs:272-286) of channel k against the
 // tensor the wavelength cache built for it (uniaxial, or biaxial with a beta band set).
+// effective_pleochroic_alpha for the uniaxial tensor (a_o, a_o, a_e) of the scene frame.
+__device__ __forceinline__ float pleochroic_alpha(const SceneConst &S, float a_o, float a_e, const Stokes &st, V3 e_hat,
+                                                  V3 ea, V3 eb) {
+    const float p = clampf(dop(st), 0.0f, 1.0f);
+    const float a_pol = quad_form(S, a_o, a_e, e_hat);
+    const float a_unp = midpoint(quad_form(S, a_o, a_e, ea), quad_form(S, a_o, a_e, eb));
+    return fmaf(p, a_pol - a_unp, a_unp);
+}
 template <bool X>
 __device__ __forceinline__ float channel_alpha(const Path &P, const SceneConst &S, int k, const Stokes &st, V3 e_hat,
                                                V3 ea, V3 eb) {
     const float a_o = arr(P.a_o4, k), a_e = arr(P.a_e4, k);
-    const float p = clampf(dop(st), 0.0f, 1.0f);
     if (X && S.biaxial) {
+        const float p = clampf(dop(st), 0.0f, 1.0f);
         const float a_b = arr(P.ne_d4, k);
         const float a_pol = quad_form3(S, a_o, a_b, a_e, e_hat);
         const float a_unp = midpoint(quad_form3(S, a_o, a_b, a_e, ea), quad_form3(S, a_o, a_b, a_e, eb));
         return fmaf(p, a_pol - a_unp, a_unp);
     }
-    const float a_pol = quad_form(S, a_o, a_e, e_hat);
-    const float a_unp = midpoint(quad_form(S, a_o, a_e, ea), quad_form(S, a_o, a_e, eb));
-    return fmaf(p, a_pol - a_unp, a_unp);
+    return pleochroic_alpha(S, a_o, a_e, st, e_hat, ea, eb);
 }
 
 template <int U, bool X = false>
@@ -452,7 +492,8 @@ __device__ __forceinline__ void segment_alphas(const Path &P, const SceneConst &
 
 // Roulette and the bounce count after a step that does not go through step_post
 // (apply_russian_roulette, transport.rs:204-220, then the loop's next bounce).
-__device__ __forceinline__ void advance_bounce(Path &P, const SceneConst &S) {
+template <class CT>
+__device__ __forceinline__ void advance_bounce(Path &P, const SceneConst &S, CT &ct) {
     uint32_t bits = state_bits(P);
     const uint32_t bounce = bits >> BOUNCE_SHIFT;
     if (bounce > 4) {
@@ -461,6 +502,7 @@ __device__ __forceinline__ void advance_bounce(Path &P, const SceneConst &S) {
         for (int k = 0; k < NCH; ++k) mx = fmaxf(mx, fmaxf(P.st[k].x, 0.0f));
         const float q = clampf(mx, 0.05f, 1.0f);
         if (rng_draw(p_seed(P), bounce, RUSSIAN_ROULETTE_STREAM) > q) {
+            note_end(ct, bounce, GR_TERM_ROULETTE);
             set_state_bits(P, bits & ~F_ALIVE);
             return;
         }
@@ -483,7 +525,7 @@ __device__ __forceinline__ void advance_bounce(Path &P, const SceneConst &S) {
 // event happened (the path moved to the event point with a new direction, and the
 // bounce is complete); false when the segment was crossed, its extinction applied.
 template <int U, class CT>
-__device__ __noinline__ bool scatter_step(Path &P, const SceneConst &S, float t_hit, CT &) {
+__device__ __noinline__ bool scatter_step(Path &P, const SceneConst &S, float t_hit, CT &ct) {
     const uint32_t bounce = p_bounce(P);
     const uint32_t seed = p_seed(P);
     const V3 kk = xyz(P.k_state);
@@ -512,7 +554,8 @@ __device__ __noinline__ bool scatter_step(Path &P, const SceneConst &S, float t_
         set_xyz(P.d_seed, nd);
         set_xyz(P.k_state, nd);
         set_xyz(P.prev_tuple, v3(0.f, 0.f, 0.f));  // depolarized: no previous plane of incidence
-        advance_bounce(P, S);
+        note_event(ct, bounce, GR_SEQ_SCATTER);
+        advance_bounce(P, S, ct);
         return true;
     }
     float sv[NCH];
@@ -559,6 +602,40 @@ static __device__ __noinline__ void biaxial_fast_entry(const Path &P, const Scen
     }
 }
 
+// signed_frame_rotation_psi (raytracer/absorption.rs:44-54)
+__device__ __forceinline__ float signed_psi(V3 prev, V3 cur, V3 kk) {
+    float cos_psi = clampf(dot(prev, cur), -1.0f, 1.0f);
+    float sin_psi = dot(cross(prev, cur), normalize_or_zero(kk));
+    return m_atan2(sin_psi, cos_psi);
+}
+
+// theta_c_for_bounce (refraction.rs:235-273): on entry the refracted wave normal's
+// angle to the c-axis after a two-step fixed point (refraction.rs:248-269), otherwise
+// the ray's own.
+template <int U>
+__device__ __forceinline__ float theta_c(V3 kk, V3 normal, float cos_i, float one_m_c2, float n_o_hero, float n_e_hero,
+                                         V3 c_axis, bool entry) {
+    float theta;
+    if (entry) {
+        float n_guess = n_o_hero;
+        theta = 0.0f;
+#pragma unroll U
+        for (int it = 0; it < 2; ++it) {
+            float eta = 1.0f / n_guess;
+            float s2 = eta * eta * one_m_c2;
+            if (s2 > 1.0f) break;
+            float ctg = sqrtf(fmaxf(1.0f - s2, 0.0f));
+            V3 wd = normalize(add(smul(eta, kk), smul(fmaf(eta, cos_i, -ctg), normal)));
+            theta = m_acos(fabsf(clampf(dot(wd, c_axis), -1.0f, 1.0f)));
+            float2 sc = m_sincos(theta);
+            n_guess = eff_e_index(n_o_hero, n_e_hero, sc.x, sc.y);
+        }
+    } else {
+        theta = m_acos(fabsf(clampf(dot(kk, c_axis), -1.0f, 1.0f)));
+    }
+    return theta;
+}
+
 // One intersection and everything of the bounce up to the hero's event decision
 // (transport.rs:781-895, raytracer/absorption.rs:71-141, refraction.rs:428-547,
 // 1036-1060).  Returns EV_DONE on an escape (F_ESCAPED set, F_ALIVE cleared).
@@ -577,9 +654,11 @@ __device__ __forceinline__ uint32_t step_hit(Path &P, const SceneConst &S, const
     if (!intersect<R>(PL, o, d, t_hit, fidx)) {
         // accumulate_miss_radiance (transport.rs:67-90) runs in path_finish
         tally(ct, C_ESCAPES);
+        note_end(ct, bounce, GR_TERM_ESCAPED);
         set_state_bits(P, (bits | F_ESCAPED) & ~F_ALIVE);
         return EV_DONE;
     }
+    note_hit(ct, bounce, fidx, t_hit);
     bool extinguished = false;  // the segment's extinction was applied by the scattering step
     if (X && inside && S.sigma_s > 0.0f) {
         // try_scatter_step / maybe_scatter_or_extinguish (raytracer/scattering.rs:132-315):
@@ -594,9 +673,7 @@ __device__ __forceinline__ uint32_t step_hit(Path &P, const SceneConst &S, const
     V3 cur_plane = normalize_or_zero(cross(kk, normal));
     const V3 prev = xyz(P.prev_tuple);
     if (dot(cur_plane, cur_plane) > 1e-6f && dot(prev, prev) > 1e-6f) {
-        float cos_psi = clampf(dot(prev, cur_plane), -1.0f, 1.0f);
-        float sin_psi = dot(cross(prev, cur_plane), normalize_or_zero(kk));
-        float psi = m_atan2(sin_psi, cos_psi);
+        float psi = signed_psi(prev, cur_plane, kk);
         float2 sc = m_sincos(2.0f * psi);
 #pragma unroll ROT_UNROLL
         for (int k = 0; k < NCH; ++k) {
@@ -642,26 +719,7 @@ __device__ __forceinline__ uint32_t step_hit(Path &P, const SceneConst &S, const
     } else if (aniso) {
         tally(ct, C_ANISO_BOUNCES);
         float n_e_hero = n_o_hero + arr(P.ne_d4, 0);
-        V3 c_axis = ld3(S.c_axis);
-        float theta;
-        if (!inside) {
-            // theta_c_for_bounce entry fixed point (refraction.rs:248-269)
-            float n_guess = n_o_hero;
-            theta = 0.0f;
-#pragma unroll U
-            for (int it = 0; it < 2; ++it) {
-                float eta = 1.0f / n_guess;
-                float s2 = eta * eta * one_m_c2;
-                if (s2 > 1.0f) break;
-                float ctg = sqrtf(fmaxf(1.0f - s2, 0.0f));
-                V3 wd = normalize(add(smul(eta, kk), smul(fmaf(eta, cos_i, -ctg), normal)));
-                theta = m_acos(fabsf(clampf(dot(wd, c_axis), -1.0f, 1.0f)));
-                float2 sc = m_sincos(theta);
-                n_guess = eff_e_index(n_o_hero, n_e_hero, sc.x, sc.y);
-            }
-        } else {
-            theta = m_acos(fabsf(clampf(dot(kk, c_axis), -1.0f, 1.0f)));
-        }
+        const float theta = theta_c<U>(kk, normal, cos_i, one_m_c2, n_o_hero, n_e_hero, ld3(S.c_axis), !inside);
         float2 sc = m_sincos(theta);
         const bool use_o = inside && !(bits & F_IS_E);
 #pragma unroll U
@@ -738,6 +796,7 @@ __device__ __forceinline__ void step_post(Path &P, const SceneConst &S, V3 hp, V
         float q = clampf(mx, 0.05f, 1.0f);
         if (rng_draw(seed, bounce, RUSSIAN_ROULETTE_STREAM) > q) {
             tally(ct, C_ROULETTE_KILLS);
+            note_end(ct, bounce, GR_TERM_ROULETTE);
             set_state_bits(P, bits & ~F_ALIVE);
             return;
         }
@@ -767,6 +826,7 @@ __device__ __noinline__ void frosted_bounce(Path &P, const SceneConst &S, V3 hp,
     V3 nd;
     bool new_inside = inside, has_update = false, use_e = false;
     if (sin2_t > 1.0f) {
+        note_event(ct, bounce, GR_SEQ_TIR);
         nd = cosine_weighted_hemisphere(u1, u2, normal);
 #pragma unroll
         for (int k = 0; k < NCH; ++k) P.st[k] = make_float4(fmaxf(P.st[k].x, 0.0f), 0.0f, 0.0f, 0.0f);
@@ -776,6 +836,7 @@ __device__ __noinline__ void frosted_bounce(Path &P, const SceneConst &S, V3 hp,
         const float r_p = fmaf(n1, -c_t, n2 * cos_i) / fmaf(n1, c_t, n2 * cos_i);
         const float ru = clampf(0.5f * fmaf(r_p, r_p, r_s * r_s), 1e-4f, 1.0f - 1e-4f);
         if (rng_draw(seed, bounce, FRESNEL_BRANCH_STREAM) < ru) {
+            note_event(ct, bounce, GR_SEQ_REFLECT);
             nd = cosine_weighted_hemisphere(u1, u2, normal);
 #pragma unroll
             for (int k = 0; k < NCH; ++k) {
@@ -783,6 +844,7 @@ __device__ __noinline__ void frosted_bounce(Path &P, const SceneConst &S, V3 hp,
                 arr(P.pdf4, k) = arr(P.pdf4, k) * ru;
             }
         } else {
+            note_event(ct, bounce, GR_SEQ_REFRACT);
             nd = cosine_weighted_hemisphere(u1, u2, neg(normal));
             const bool entering_aniso = !inside && S.anisotropic;
             use_e = entering_aniso ? rng_draw(seed, bounce, BIREFRINGENT_SPLIT_STREAM) < 0.5f : (bits & F_IS_E) != 0;
@@ -811,6 +873,7 @@ __device__ __forceinline__ void step_reflect(Path &P, const SceneConst &S, const
     const float one_m_c2 = fmaf(cos_i, -cos_i, 1.0f);
     const float sin_i = sqrtf(fmaxf(one_m_c2, 0.0f));
     if (hero_tir) tally(ct, C_TIR); else tally(ct, C_REFLECT);
+    note_event(ct, bits >> BOUNCE_SHIFT, hero_tir ? GR_SEQ_TIR : GR_SEQ_REFLECT);
     // A TIR event applies each channel's matrix unscaled: the reflect branch's
     // `.scale(1 / r_unpol)` with factor 1.0 (x * 1.0f == x exactly).
     const float inv = hero_tir ? 1.0f : 1.0f / E.n_ru.w;
@@ -859,6 +922,7 @@ __device__ __forceinline__ void step_refract(Path &P, const SceneConst &S, const
     const float cos_i = E.hp_cos.w, ru = E.n_ru.w;
     const float one_m_c2 = fmaf(cos_i, -cos_i, 1.0f);
     tally(ct, C_REFRACT);
+    note_event(ct, bounce, GR_SEQ_REFRACT);
     const float n_med0 = arr(E.n_med4, 0);
     const float n1 = inside ? n_med0 : 1.0f;
     const float n2 = inside ? 1.0f : n_med0;

@@ -91,6 +91,44 @@ def birefringent_emerald_material(lambda_dependent: bool = True, seed: int = 0,
     return m, ext
 
 
+# The single-scene benchmark configurations: c1 (CPU-runnable), c2 (the headline
+# frame), c3 (the birefringent dichroic emerald) and c2s (c2's scene at 480x270, 64 spp,
+# the small case of the profiler captures).
+CONFIGS = {
+    "c1": dict(width=256, height=256, spp=64, max_bounces=32, env="uniform", stone="rb57"),
+    "c2": dict(width=1920, height=1080, spp=256, max_bounces=32, env="latlong", stone="rb57"),
+    "c3": dict(width=1024, height=1024, spp=1024, max_bounces=64, env="studio", stone="em49"),
+    "c2s": dict(width=480, height=270, spp=64, max_bounces=32, env="latlong", stone="rb57"),
+}
+
+
+def config_scene(name: str, camera=None, builtin_material=None, lambda_dependent: bool = True):
+    """The scene of benchmark configuration `name` and its sizes (CONFIGS[name]).
+
+    c1/c2: the 57-facet round brilliant (table 57%, crown 34.5 deg, pavilion 40.75 deg,
+    16 girdle planes), Diamond, camera Camera::new(0.35, 0.28, 5.0, 18.0); c1 in a
+    uniform white environment, c2 in the seeded 2048x1024 lat-long map of 12 Gaussian
+    lights.  c3: the 49-plane step-cut emerald with birefringent_emerald_material()
+    (lambda_dependent=False: the reference model's constant Delta n) in the studio rig.
+    `camera` / `builtin_material` replace the scene builders (Camera::new and the
+    built-in material table) -- the engine library's by default."""
+    camera = camera or S.camera
+    builtin_material = builtin_material or S.builtin_material
+    w = CONFIGS[name]
+    planes = S.round_brilliant_57() if w["stone"] == "rb57" else S.emerald_cut_49()
+    env_mode = {"uniform": abi.GR_ENV_UNIFORM, "latlong": abi.GR_ENV_LATLONG, "studio": abi.GR_ENV_STUDIO}[w["env"]]
+    latlong = S.gaussian_blob_latlong(2048, 1024, 12, seed=0) if w["env"] == "latlong" else None
+    ext = None
+    if w["stone"] == "rb57":
+        mat = builtin_material("Diamond")
+    else:
+        mat, ext = birefringent_emerald_material(lambda_dependent=lambda_dependent)
+    sc = S.Scene(width=w["width"], height=w["height"], planes=planes, material=mat, cam=camera(0.35, 0.28, 5.0, 18.0),
+                 max_bounces=w["max_bounces"], env_mode=env_mode, latlong=latlong, uniform_rgb=(1.0, 1.0, 1.0),
+                 ext=ext)
+    return sc, dict(w)
+
+
 def material_tables() -> list[tuple[str, abi.gr_material]]:
     return [("crown glass", _crown_glass())] + [(n, S.builtin_material(n)) for n in
                                                 ("Quartz", "Spinel", "Sapphire", "Zircon", "Diamond")]

@@ -299,6 +299,79 @@ gr_status gr_event_counts(gr_ctx *ctx, const gr_scene *scene, uint32_t first_pix
  * denominator of the transport kernels. */
 gr_status gr_probe_fp32_peak(gr_ctx *ctx, double *tflops);
 
+/* Per-tuple event sequence of the transport -- the device side of the reference's
+ * instrumented trace (trace_spectral_ray_with_finish_instrumented,
+ * optics/raytracer/transport.rs:512-537, whose log the facet-sequence check of
+ * renderer/gpu/polyhedron_check.rs compares per hit).  For each tuple of samples
+ * [sample_offset, +spp) of pixels [first_pixel, +n_pixels), in (pixel, sample) order:
+ *   bounces[t]       the bounce index the path ended at (max_bounces at the cap);
+ *   termination[t]   GR_TERM_*;
+ *   facets[t*kmax+b] the facet hit at bounce b, t_hits[t*kmax+b] its distance, and
+ *   events[t*kmax+b] the GR_SEQ_* event taken there, for b < min(kmax, recorded),
+ *                    recorded = bounces + (termination == GR_TERM_ROULETTE); slots past
+ *                    that hold -1 / 0 / 0xFF.
+ * Host arrays.  The plain kernel with recording hooks runs the same functions in the
+ * same order as every other transport kernel, so its sequences are theirs. */
+#define GR_TERM_ESCAPED 0u
+#define GR_TERM_ROULETTE 2u
+#define GR_TERM_HIT_CAP 3u
+#define GR_SEQ_TIR 0u
+#define GR_SEQ_REFLECT 1u
+#define GR_SEQ_REFRACT 2u
+#define GR_SEQ_SCATTER 3u
+#define GR_SEQ_NONE 0xFFu
+gr_status gr_trace_events(gr_ctx *ctx, const gr_scene *scene, uint32_t first_pixel, uint32_t n_pixels,
+                          uint32_t sample_offset, uint32_t spp, uint32_t kmax, uint32_t *bounces,
+                          uint32_t *termination, int32_t *facets, float *t_hits, uint8_t *events);
+
+/* Per-function case banks: the device functions the transport kernels inline, run one
+ * case per thread over caller inputs -- the counterpart of the reference's Tier-2
+ * per-function checks (renderer/gpu/transport_check/mod.rs:38-75, camera_check.rs,
+ * environment_check.rs), which hold each function to a ULP budget.  `in` holds n rows
+ * of n_in floats, `out` receives n rows of n_out floats (gr_case_bank_arity).  Banks
+ * that read scene state take it from `scene` (camera and frame size, material,
+ * environment); the others ignore it (NULL allowed).  Host arrays. */
+#define GR_BANK_CAMERA_RAY 0u           /* x, y, jitter_x, jitter_y -> dir[3]; scene camera + frame */
+#define GR_BANK_CMF 1u                  /* lambda -> xyz[3] (cie_1931_cmf_x8 lane) */
+#define GR_BANK_BLACKBODY 2u            /* lambda -> blackbody_spectrum at scene env temp_k */
+#define GR_BANK_DISPERSION 3u           /* lambda -> n (scene material dispersion) */
+#define GR_BANK_ABSORPTION 4u           /* lambda -> alpha_o, alpha_e (bands or extension table) */
+#define GR_BANK_PLEOCHROIC 5u           /* stokes[4], s_axis[3], k[3], a_o, a_e -> alpha (scene c-axis) */
+#define GR_BANK_FRESNEL_REFLECTION 6u   /* r_s, r_p, stokes[4] -> stokes[4] */
+#define GR_BANK_FRESNEL_TRANSMISSION 7u /* n1, n2, cos_i, cos_t, t_s, t_p, stokes[4] -> stokes[4] */
+#define GR_BANK_FRAME_ROTATION 8u       /* psi, stokes[4] -> stokes[4] */
+#define GR_BANK_TIR_RETARDATION 9u      /* delta, stokes[4] -> stokes[4] */
+#define GR_BANK_SIGNED_PSI 10u          /* prev[3], cur[3], k[3] -> psi */
+#define GR_BANK_TIR_PHASE_DELTA 11u     /* n1, cos_i, sin_i -> delta */
+#define GR_BANK_EIGEN_UNIAXIAL 12u      /* k[3], c[3] -> ordinary[3], extraordinary[3] */
+#define GR_BANK_WALK_OFF 13u            /* k[3], c[3], n_o, n_e -> extraordinary Poynting dir[3] */
+#define GR_BANK_EXTRAORDINARY_INDEX 14u /* n_o, n_e, theta -> n_eff */
+#define GR_BANK_THETA_C 15u             /* k[3], normal[3], n_o, n_e, entry -> theta (scene c-axis) */
+#define GR_BANK_STUDIO 16u              /* dir[3], lambda -> radiance (scene studio environment) */
+#define GR_BANK_RGB_SPECTRAL 17u        /* r, g, b, lambda -> rgb_to_spectral_radiance */
+#define GR_BANK_EXP_POLY 18u            /* x -> simd::exp_f32x8 lane */
+#define GR_BANK_HG_SAMPLE 19u           /* u1, u2, g, fwd[3] -> dir[3] */
+#define GR_BANK_COSINE_HEMISPHERE 20u   /* u1, u2, n[3] -> dir[3] */
+#define GR_BANK_E_FIELD 21u             /* stokes[4], s_axis[3], k[3] -> electric_field_direction[3] */
+#define GR_BANK_VON_KRIES 22u           /* xyz[3] -> white-balanced xyz[3] (scene environment) */
+#define GR_BANK_WAVELENGTHS 23u         /* hero_rand -> lambda[8] (wrapped_hero_wavelengths) */
+#define GR_BANK_COUNT 24u
+gr_status gr_case_bank_arity(uint32_t bank, uint32_t *n_in, uint32_t *n_out);
+gr_status gr_case_bank(gr_ctx *ctx, uint32_t bank, const gr_scene *scene, const float *in, uint32_t n, float *out);
+
+/* The compute capability the library's device code was built for, as the CUDA runtime
+ * reports it for a kernel of this library on the context's device
+ * (cudaFuncGetAttributes): binary_version 100 for the sm_100a cubin, ptx_version 0
+ * when no PTX is embedded. */
+gr_status gr_device_code_version(gr_ctx *ctx, uint32_t *binary_version, uint32_t *ptx_version);
+
+/* The transport's convex clip (the paired shared-memory plane scan of every transport
+ * kernel) for n rays, rays[6*i..] = origin[3], dir[3]: t[i] and facet[i] (-1 on a
+ * miss) -- the device side of renderer/gpu/polyhedron_check.rs's case bank for
+ * intersect_polyhedron (optics/raytracer/intersect.rs:93-132).  Host arrays. */
+gr_status gr_intersect_rays(gr_ctx *ctx, const gr_plane *planes, uint32_t n_planes, const float *rays, uint32_t n,
+                            float *t, int32_t *facet);
+
 /* ---- optical metrics ------------------------------------------------------------ */
 
 /* = GemOpticalMetrics (color/metrics.rs:33-39). */
@@ -448,7 +521,7 @@ gr_status gr_request_release(gr_ctx *ctx, uint64_t request_id);
  * The per-tuple XYZ scratch is a fixed file-scope device array of
  * GR_STATIC_SCRATCH_BYTES (one per device per process) instead of the context's
  * growable buffer; the call makes no cudaMalloc / cudaFree and no library call that
- * allocates, always runs the PLAIN kernel and records no timing events.  The frame is
+ * allocates and always runs the PLAIN kernel.  The frame is
  * traced in chunks of floor(GR_STATIC_SCRATCH_TUPLES / spp) pixels, each folded into
  * the film before the next is traced (stream order), so results are identical to
  * gr_render_resident.  spp > GR_STATIC_SCRATCH_TUPLES (one pixel's samples do not fit)
@@ -460,7 +533,10 @@ gr_status gr_request_release(gr_ctx *ctx, uint64_t request_id);
  *
  * Set-up: the first call on each device looks up the array's address once
  * (cudaGetSymbolAddress, which may load the module); make that first call before any
- * stream capture begins.  Races: the scratch is shared by every context on the
+ * stream capture begins.  A cudaDeviceReset in the process unloads the module and
+ * leaves the cached address stale: after a reset, do not call this entry point again
+ * in that process.  The call adds its launches to the counts gr_timing_read reports
+ * (no timing events).  Races: the scratch is shared by every context on the
  * device, so calls whose device work may overlap (other contexts, or different
  * streams not ordered with each other) race on it; the caller must serialise them. */
 #define GR_STATIC_SCRATCH_BYTES (16u << 20)

@@ -266,18 +266,24 @@ static inline gr_camera camera_new(float yaw, float pitch, float distance, float
     return c;
 }
 
+// camera.rs:95-114 in precision R (the estimator always takes the FP32 ray; the FP64
+// form is the camera case bank's reference).
+template <class R>
+static inline Ray<R> generate_ray_t(const gr_camera &cam, R sx, R sy, R w, R h, R jx, R jy) {
+    R aspect = w / h;
+    R u = ((sx + jx) / w - R(0.5f)) * R(2) * aspect * R(cam.fov_tan);
+    R v = (R(0.5f) - (sy + jy) / h) * R(2) * R(cam.fov_tan);
+    V3<R> f = v3f<R>(cam.forward), r = v3f<R>(cam.right), up = v3f<R>(cam.up);
+    V3<R> dir = (f + r * u + up * v).normalize();
+    Ray<R> ray;
+    ray.origin = v3f<R>(cam.origin);
+    ray.dir = dir;
+    return ray;
+}
 // camera.rs:95-114 (always FP32: the camera ray is an input of the estimator).
 static inline Ray<float> generate_ray(const gr_camera &cam, float sx, float sy, float w, float h,
                                       float jx, float jy) {
-    float aspect = w / h;
-    float u = ((sx + jx) / w - 0.5f) * 2.0f * aspect * cam.fov_tan;
-    float v = (0.5f - (sy + jy) / h) * 2.0f * cam.fov_tan;
-    V3<float> f = v3f<float>(cam.forward), r = v3f<float>(cam.right), up = v3f<float>(cam.up);
-    V3<float> dir = (f + r * u + up * v).normalize();
-    Ray<float> ray;
-    ray.origin = v3f<float>(cam.origin);
-    ray.dir = dir;
-    return ray;
+    return generate_ray_t<float>(cam, sx, sy, w, h, jx, jy);
 }
 
 // ---------------------------------------------------------------------------------
@@ -938,7 +944,7 @@ template <class R> static inline V3<R> integrate_channels_to_xyz(const R rad[8],
 // The transport loop -- transport.rs:684-940 and refraction.rs
 // ---------------------------------------------------------------------------------
 enum Termination : uint32_t { TERM_ESCAPED = 0, TERM_SCATTER_ABSORBED = 1, TERM_RUSSIAN_ROULETTE = 2, TERM_HIT_CAP = 3 };
-enum EventKind : uint32_t { EV_TIR = 0, EV_REFLECT = 1, EV_REFRACT = 2 };
+enum EventKind : uint32_t { EV_TIR = 0, EV_REFLECT = 1, EV_REFRACT = 2, EV_SCATTER = 3 };
 
 // Per-scene environment state prepared once (white balance, studio rig, map).
 template <class R> struct EnvCtx {
@@ -1066,6 +1072,40 @@ static inline WaveCache<R> build_cache(const MaterialCtx<R> &mc, const R lam[8])
     return wc;
 }
 
+// signed_frame_rotation_psi (raytracer/absorption.rs:44-54): the signed angle from the
+// previous plane-of-incidence normal to the current one about the wave normal.
+template <class R> static inline R signed_frame_rotation_psi(const V3<R> &prev, const V3<R> &cur, const V3<R> &k) {
+    R cos_psi = clampr(prev.dot(cur), R(-1), R(1));
+    R sin_psi = prev.cross(cur).dot(k.normalize_or_zero());
+    return M<R>::atan2(sin_psi, cos_psi);
+}
+
+// theta_c_for_bounce (refraction.rs:235-273): the angle between the c-axis and the
+// wave normal the extraordinary index is taken at -- on entry (outside, uniaxial) the
+// refracted wave normal after a two-step fixed point, otherwise the ray's own.
+template <class R>
+static inline R theta_c_for_bounce(const V3<R> &k_hat, const V3<R> &normal, R cos_i, R n_o_seed, R n_e_seed,
+                                   const V3<R> &c_axis, bool entry) {
+    R theta;
+    if (entry) {
+        R n_guess = n_o_seed;
+        theta = R(0);
+        for (int it = 0; it < 2; ++it) {
+            R eta = R(1) / n_guess;
+            R s2 = eta * eta * M<R>::fma(cos_i, -cos_i, R(1));
+            if (s2 > R(1)) break;
+            R ct = M<R>::sqrt(rmax(R(1) - s2, R(0)));
+            V3<R> wd = (eta * k_hat + M<R>::fma(eta, cos_i, -ct) * normal).normalize();
+            R ctw = std::fabs(clampr(wd.dot(c_axis), R(-1), R(1)));
+            theta = M<R>::acos(ctw);
+            n_guess = effective_extraordinary_index(n_o_seed, n_e_seed, theta);
+        }
+    } else {
+        theta = M<R>::acos(std::fabs(clampr(k_hat.dot(c_axis), R(-1), R(1))));
+    }
+    return theta;
+}
+
 // refraction.rs:46-50
 template <class R> static inline R tir_phase_delta(R n1k, R cos_i, R sin_i) {
     R num = cos_i * M<R>::sqrt(rmax(M<R>::fma(n1k * n1k * sin_i, sin_i, R(-1)), R(0)));
@@ -1087,25 +1127,8 @@ static inline Geo<R> bounce_geometry(const MaterialCtx<R> &mc, const WaveCache<R
     g.cos_i = clampr((-k_hat).dot(normal), R(0), R(1));
     g.sin_i = M<R>::sqrt(rmax(M<R>::fma(g.cos_i, -g.cos_i, R(1)), R(0)));
     R n_o_seed = wc.n_o[0];
-    // theta_c_for_bounce (refraction.rs:235-273)
-    R theta;
-    if (!inside && mc.anisotropic && !mc.biaxial) {
-        R n_e_seed = n_o_seed + wc.n_e_delta[0];
-        R n_guess = n_o_seed;
-        theta = R(0);
-        for (int it = 0; it < 2; ++it) {
-            R eta = R(1) / n_guess;
-            R s2 = eta * eta * M<R>::fma(g.cos_i, -g.cos_i, R(1));
-            if (s2 > R(1)) break;
-            R ct = M<R>::sqrt(rmax(R(1) - s2, R(0)));
-            V3<R> wd = (eta * k_hat + M<R>::fma(eta, g.cos_i, -ct) * normal).normalize();
-            R ctw = std::fabs(clampr(wd.dot(mc.c_axis), R(-1), R(1)));
-            theta = M<R>::acos(ctw);
-            n_guess = effective_extraordinary_index(n_o_seed, n_e_seed, theta);
-        }
-    } else {
-        theta = M<R>::acos(std::fabs(clampr(k_hat.dot(mc.c_axis), R(-1), R(1))));
-    }
+    const R theta = theta_c_for_bounce(k_hat, normal, g.cos_i, n_o_seed, n_o_seed + wc.n_e_delta[0], mc.c_axis,
+                                       !inside && mc.anisotropic && !mc.biaxial);
     R n_eff[8];
     for (int k = 0; k < 8; ++k) {
         R n_o_k = wc.n_o[k];
@@ -1233,6 +1256,7 @@ struct EventLog {
     uint32_t n_scatter;   // Henyey-Greenstein volume events
     int32_t facets[64];
     uint8_t events[64];
+    float ts[64];  // hit distance of each logged bounce (the tie rule's t)
 };
 
 struct TraceOpts {
@@ -1272,7 +1296,7 @@ static inline V3<R> trace_spectral_ray(const Ray<float> &initial, const gr_plane
             if (log) { log->bounces = bounce; log->termination = TERM_ESCAPED; log->n_escape++; }
             break;
         }
-        if (log && bounce < 64) log->facets[bounce] = hit.facet;
+        if (log && bounce < 64) { log->facets[bounce] = hit.facet; log->ts[bounce] = (float)hit.t; }
         // try_scatter_step (raytracer/scattering.rs:246-315, maybe_scatter_or_extinguish
         // :132-212): a Henyey-Greenstein event somewhere along this interior segment,
         // drawn before the facet is processed; on no event, the segment's extinction
@@ -1308,7 +1332,7 @@ static inline V3<R> trace_spectral_ray(const Ray<float> &initial, const gr_plane
                 ray.dir = new_dir;
                 cur_k = new_dir;
                 have_prev = false;  // depolarized: no previous plane of incidence
-                if (log) log->n_scatter++;
+                if (log) { log->n_scatter++; if (bounce < 64) log->events[bounce] = EV_SCATTER; }
                 if (bounce > 4) {   // apply_russian_roulette (transport.rs:204-220)
                     R mx = R(0);
                     for (int k = 0; k < 8; ++k) mx = rmax(mx, st[k].intensity());
@@ -1336,9 +1360,7 @@ static inline V3<R> trace_spectral_ray(const Ray<float> &initial, const gr_plane
         // rotate_stokes_to_plane_of_incidence (raytracer/absorption.rs:71-89)
         V3<R> cur_plane = cur_k.cross(normal).normalize_or_zero();
         if (have_prev && cur_plane.length_squared() > R(1e-6f) && prev_plane.length_squared() > R(1e-6f)) {
-            R cos_psi = clampr(prev_plane.dot(cur_plane), R(-1), R(1));
-            R sin_psi = prev_plane.cross(cur_plane).dot(cur_k.normalize_or_zero());
-            R psi = M<R>::atan2(sin_psi, cos_psi);
+            R psi = signed_frame_rotation_psi(prev_plane, cur_plane, cur_k);
             Mat4<R> rot = frame_rotation(psi);
             for (int k = 0; k < 8; ++k) st[k] = apply_matrix(st[k], rot);
         }

@@ -574,6 +574,221 @@ void gro_rng_records(const uint32_t *pixels, const uint32_t *samples, uint32_t n
     }
 }
 
+// Material cache of one wavelength (build_ray_wavelength_cache, refraction.rs:127-174,
+// with the extension's tabulated absorption and Cauchy n_e): out = n_o, n_e,
+// alpha_o, alpha_e.  precision 32 or 64.
+int gro_material_channel(const gr_material *m, const gr_material_ext *ext, float lambda_nm, int precision,
+                         double out[4]) {
+    if (!m || !out) return GR_EINVAL;
+    if (precision == 64) {
+        MaterialCtx<double> mc = make_material<double>(m, ext);
+        double lam[8];
+        for (double &l : lam) l = (double)lambda_nm;
+        WaveCache<double> wc = build_cache(mc, lam);
+        out[0] = wc.n_o[0]; out[1] = wc.n_o[0] + wc.n_e_delta[0];
+        out[2] = wc.tensor[0].alpha.x; out[3] = wc.tensor[0].alpha.z;
+    } else {
+        MaterialCtx<float> mc = make_material<float>(m, ext);
+        float lam[8];
+        for (float &l : lam) l = lambda_nm;
+        WaveCache<float> wc = build_cache(mc, lam);
+        out[0] = wc.n_o[0]; out[1] = wc.n_o[0] + wc.n_e_delta[0];
+        out[2] = wc.tensor[0].alpha.x; out[3] = wc.tensor[0].alpha.z;
+    }
+    return GR_OK;
+}
+
+// Per-sample event sequences of the FP32 tracer (the instrumented trace,
+// transport.rs:512-537): the layout of gr_trace_events -- per tuple the final bounce
+// index and termination, and per logged bounce (b < min(kmax, 64)) the facet, its
+// hit distance and the event; unrecorded slots -1 / 0 / 0xFF.
+int gro_trace_events(const gr_scene *sc, uint32_t first_pixel, uint32_t n_pixels, uint32_t sample_offset,
+                     uint32_t spp, uint32_t kmax, uint32_t *bounces, uint32_t *term, int32_t *facets, float *t_hits,
+                     uint8_t *events, int threads) {
+    if (!sc || !bounces || !term || (kmax && (!facets || !t_hits || !events))) return GR_EINVAL;
+    if (!material_supported(sc->material, sc->finishes, sc->n_planes)) return GR_DECLINED_MATERIAL;
+    MaterialCtx<float> mc = make_material<float>(sc->material, sc->material_ext);
+    EnvCtx<float> env = make_env<float>(sc->env);
+    if (threads <= 0) threads = (int)std::thread::hardware_concurrency();
+    if (threads <= 0) threads = 1;
+    std::atomic<uint32_t> next(0);
+    auto worker = [&]() {
+        std::vector<EventLog> logs(spp);
+        for (;;) {
+            uint32_t i = next.fetch_add(1);
+            if (i >= n_pixels) break;
+            double s[3];
+            trace_pixel_samples<float>(*sc, mc, env, first_pixel + i, sample_offset, spp, nullptr, s, logs.data());
+            for (uint32_t k = 0; k < spp; ++k) {
+                const size_t o = (size_t)i * spp + k;
+                const EventLog &lg = logs[k];
+                bounces[o] = lg.bounces;
+                term[o] = lg.termination;
+                const uint32_t rec = lg.bounces + (lg.termination == TERM_RUSSIAN_ROULETTE ? 1u : 0u);
+                for (uint32_t b = 0; b < kmax; ++b) {
+                    const bool have = b < rec && b < 64;
+                    facets[o * kmax + b] = have ? lg.facets[b] : -1;
+                    t_hits[o * kmax + b] = have ? lg.ts[b] : 0.0f;
+                    events[o * kmax + b] = have ? lg.events[b] : (uint8_t)0xFF;
+                }
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; ++t) pool.emplace_back(worker);
+    for (auto &t : pool) t.join();
+    return GR_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// One case of a per-function bank (the layouts of GR_BANK_* in gemray_cuda.h) in
+// precision R, each through the oracle's restatement of the reference function.
+template <class R>
+void bank_case(uint32_t bank, const gr_scene *sc, const float *x, double *y) {
+    auto v = [&](int i) { return V3<R>(R(x[i]), R(x[i + 1]), R(x[i + 2])); };
+    auto st = [&](int i) { return Stokes<R>{R(x[i]), R(x[i + 1]), R(x[i + 2]), R(x[i + 3])}; };
+    auto put3 = [&](const V3<R> &a, int o) { y[o] = a.x; y[o + 1] = a.y; y[o + 2] = a.z; };
+    auto put4 = [&](const Stokes<R> &a) { y[0] = a.i; y[1] = a.q; y[2] = a.u; y[3] = a.v; };
+    switch (bank) {
+    case GR_BANK_CAMERA_RAY: {
+        Ray<R> r = generate_ray_t<R>(sc->camera, R(x[0]), R(x[1]), R((float)sc->width), R((float)sc->height), R(x[2]),
+                                     R(x[3]));
+        put3(r.dir, 0);
+        break;
+    }
+    case GR_BANK_CMF: {
+        R lam[8], c[8][3];
+        for (R &l : lam) l = R(x[0]);
+        cmf_x8(lam, c);
+        y[0] = c[0][0]; y[1] = c[0][1]; y[2] = c[0][2];
+        break;
+    }
+    case GR_BANK_BLACKBODY: y[0] = blackbody_spectrum(R(x[0]), R(sc->env.temp_k)); break;
+    case GR_BANK_DISPERSION: y[0] = dispersion_evaluate(sc->material->dispersion, R(x[0])); break;
+    case GR_BANK_ABSORPTION: {
+        const gr_material *m = sc->material;
+        const gr_material_ext *e = sc->material_ext;
+        if (e && e->n_absorption > 0) {
+            y[0] = table_lookup(e->alpha_o_table, e->n_absorption, e->absorption_nm_first, e->absorption_nm_step, R(x[0]));
+            y[1] = table_lookup(e->alpha_e_table, e->n_absorption, e->absorption_nm_first, e->absorption_nm_step, R(x[0]));
+        } else {
+            y[0] = spectral_absorption(m->o_ray_bands, m->o_ray_band_count, R(x[0]));
+            y[1] = spectral_absorption(m->e_ray_bands, m->e_ray_band_count, R(x[0]));
+        }
+        break;
+    }
+    case GR_BANK_PLEOCHROIC: {
+        const MaterialCtx<R> mc = make_material<R>(sc->material, sc->material_ext);
+        const Stokes<R> s = st(0);
+        const V3<R> k = v(7);
+        const Tensor3<R> t = tensor_uniaxial(R(x[10]), R(x[11]), mc.c_axis);
+        const V3<R> e_hat = electric_field_direction(s, v(4), k);
+        const V3<R> ea = ordinary_eigen_polarization(k, mc.c_axis), eb = extraordinary_eigen_polarization(k, mc.c_axis);
+        y[0] = effective_pleochroic_alpha(t, e_hat, ea, eb, s.degree_of_polarization());
+        break;
+    }
+    case GR_BANK_FRESNEL_REFLECTION: put4(apply_matrix(st(2), fresnel_reflection(R(x[0]), R(x[1])))); break;
+    case GR_BANK_FRESNEL_TRANSMISSION:
+        put4(apply_matrix(st(6), fresnel_transmission(R(x[0]), R(x[1]), R(x[2]), R(x[3]), R(x[4]), R(x[5]))));
+        break;
+    case GR_BANK_FRAME_ROTATION: put4(apply_matrix(st(1), frame_rotation(R(x[0])))); break;
+    case GR_BANK_TIR_RETARDATION: put4(apply_matrix(st(1), tir_retardation(R(x[0])))); break;
+    case GR_BANK_SIGNED_PSI: y[0] = signed_frame_rotation_psi(v(0), v(3), v(6)); break;
+    case GR_BANK_TIR_PHASE_DELTA: y[0] = tir_phase_delta(R(x[0]), R(x[1]), R(x[2])); break;
+    case GR_BANK_EIGEN_UNIAXIAL:
+        put3(ordinary_eigen_polarization(v(0), v(3)), 0);
+        put3(extraordinary_eigen_polarization(v(0), v(3)), 3);
+        break;
+    case GR_BANK_WALK_OFF: put3(extraordinary_poynting_dir(v(0), v(3), R(x[6]), R(x[7])), 0); break;
+    case GR_BANK_EXTRAORDINARY_INDEX: y[0] = effective_extraordinary_index(R(x[0]), R(x[1]), R(x[2])); break;
+    case GR_BANK_THETA_C: {
+        const MaterialCtx<R> mc = make_material<R>(sc->material, sc->material_ext);
+        const V3<R> k = v(0), n = v(3);
+        const R cos_i = clampr((-k).dot(n), R(0), R(1));
+        y[0] = theta_c_for_bounce(k, n, cos_i, R(x[6]), R(x[7]), mc.c_axis, x[8] != 0.0f);
+        break;
+    }
+    case GR_BANK_STUDIO: {
+        const StudioRig<R> rig = studio_rig_new(R(sc->env.light_yaw), R(sc->env.light_pitch));
+        y[0] = studio_radiance(v(0), R(x[3]), R(sc->env.temp_k), R(sc->env.spot_mult), R(sc->env.exposure), rig);
+        break;
+    }
+    case GR_BANK_RGB_SPECTRAL: y[0] = rgb_to_spectral(R(x[0]), R(x[1]), R(x[2]), R(x[3])); break;
+    case GR_BANK_EXP_POLY: y[0] = M<R>::exp_poly(R(x[0])); break;
+    case GR_BANK_HG_SAMPLE: put3(sample_hg_direction(R(x[0]), R(x[1]), R(x[2]), v(3)), 0); break;
+    case GR_BANK_COSINE_HEMISPHERE: put3(cosine_weighted_hemisphere(R(x[0]), R(x[1]), v(2)), 0); break;
+    case GR_BANK_E_FIELD: put3(electric_field_direction(st(0), v(4), v(7)), 0); break;
+    case GR_BANK_VON_KRIES: {
+        const EnvCtx<R> env = make_env<R>(sc->env);
+        put3(apply_von_kries(v(0), env.white_balance), 0);
+        break;
+    }
+    case GR_BANK_WAVELENGTHS: {
+        R lam[8];
+        wrapped_hero_wavelengths<R>(x[0], lam);
+        for (int k = 0; k < 8; ++k) y[k] = lam[k];
+        break;
+    }
+    default: break;
+    }
+}
+
+const uint32_t kBankArity[GR_BANK_COUNT][2] = {
+    {4, 3}, {1, 3}, {1, 1}, {1, 1}, {1, 2}, {12, 1}, {6, 4}, {10, 4}, {5, 4}, {5, 4}, {9, 1}, {3, 1},
+    {6, 6}, {8, 3}, {3, 1}, {9, 1}, {4, 1}, {4, 1}, {1, 1}, {6, 3}, {5, 3}, {10, 3}, {3, 3}, {1, 8},
+};
+
+}  // namespace
+
+extern "C" {
+
+// Case bank `bank` over n input rows in precision 32 (the reference's f32 arithmetic)
+// or 64 (the FP64 oracle); out receives n rows of the bank's outputs as doubles.
+int gro_case_bank(uint32_t bank, int precision, const gr_scene *sc, const float *in, uint32_t n, double *out) {
+    if (bank >= GR_BANK_COUNT || !in || !out) return GR_EINVAL;
+    const uint32_t ni = kBankArity[bank][0], no = kBankArity[bank][1];
+    for (uint32_t i = 0; i < n; ++i) {
+        if (precision == 64) bank_case<double>(bank, sc, in + (size_t)i * ni, out + (size_t)i * no);
+        else bank_case<float>(bank, sc, in + (size_t)i * ni, out + (size_t)i * no);
+    }
+    return GR_OK;
+}
+
+int gro_case_bank_arity(uint32_t bank, uint32_t *n_in, uint32_t *n_out) {
+    if (bank >= GR_BANK_COUNT) return GR_EINVAL;
+    *n_in = kBankArity[bank][0];
+    *n_out = kBankArity[bank][1];
+    return GR_OK;
+}
+
+// intersect_polyhedron (intersect.rs:93-132) for n rays (origin[3], dir[3] each) in
+// precision 32 or 64: t (rounded to f32) and the facet, -1 on a miss.
+int gro_intersect_rays(const gr_plane *planes, uint32_t n_planes, const float *rays, uint32_t n, int precision,
+                       float *t, int32_t *facet) {
+    for (uint32_t i = 0; i < n; ++i) {
+        const float *r = rays + 6 * (size_t)i;
+        if (precision == 64) {
+            Ray<double> ray;
+            ray.origin = V3<double>(r[0], r[1], r[2]);
+            ray.dir = V3<double>(r[3], r[4], r[5]);
+            const Hit<double> h = intersect_polyhedron(ray, planes, n_planes);
+            t[i] = h.hit ? (float)h.t : 0.0f;
+            facet[i] = h.hit ? h.facet : -1;
+        } else {
+            Ray<float> ray;
+            ray.origin = V3<float>(r[0], r[1], r[2]);
+            ray.dir = V3<float>(r[3], r[4], r[5]);
+            const Hit<float> h = intersect_polyhedron(ray, planes, n_planes);
+            t[i] = h.hit ? h.t : 0.0f;
+            facet[i] = h.hit ? h.facet : -1;
+        }
+    }
+    return GR_OK;
+}
+
 // evaluate_gem_optical_metrics (color/metrics.rs:1082-1237): out = brilliance %,
 // fire index, scintillation %, windowing %, extinction %.
 void gro_metrics(const gr_plane *planes, uint32_t n, const gr_material *m, float cam_yaw, float cam_pitch,

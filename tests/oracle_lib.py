@@ -114,6 +114,17 @@ def lib():
     L.gro_metrics.argtypes = [C.POINTER(abi.gr_plane), U, C.POINTER(abi.gr_material), F, F, F, F, fp]
     L.gro_tonemap.restype = None
     L.gro_tonemap.argtypes = [fp, F, U, C.POINTER(C.c_uint8)]
+    L.gro_material_channel.restype = C.c_int
+    L.gro_material_channel.argtypes = [C.POINTER(abi.gr_material), C.POINTER(abi.gr_material_ext), F, C.c_int,
+                                       C.POINTER(C.c_double)]
+    L.gro_trace_events.restype = C.c_int
+    L.gro_trace_events.argtypes = [sc, U, U, U, U, U, up, up, C.POINTER(C.c_int32), fp, C.POINTER(C.c_uint8), C.c_int]
+    L.gro_case_bank.restype = C.c_int
+    L.gro_case_bank.argtypes = [U, C.c_int, sc, fp, U, C.POINTER(C.c_double)]
+    L.gro_case_bank_arity.restype = C.c_int
+    L.gro_case_bank_arity.argtypes = [U, up, up]
+    L.gro_intersect_rays.restype = C.c_int
+    L.gro_intersect_rays.argtypes = [C.c_void_p, U, fp, U, C.c_int, fp, C.POINTER(C.c_int32)]
     L.gro_rng_records.restype = None
     L.gro_rng_records.argtypes = [up, up, U, up]
     _lib = L

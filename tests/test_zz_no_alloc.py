@@ -1,10 +1,18 @@
 """gr_render_resident_static (fixed device scratch, no allocation) against gr_render_resident.
 
+Some callers cannot allocate device memory inside a render call: a serving loop that
+commits its memory up front (a caching allocator holding the device), where a mid-frame
+cudaMalloc can fail and a cudaFree would synchronise the whole device.  The static
+entry point traces into a file-scope device array instead.
+
 Named so that it is collected last: it must pass alone and after every other test.
-Two consecutive calls (sample ranges [0, spp) and [spp, 2*spp)) into the same film
-must give a film bit-identical to the same two calls through gr_render_resident (same
-kernels, each pixel's samples folded in the same order; only the chunking differs),
-and the second call must leave the device's free memory unchanged.
+Each case uses a fresh context and runs the static calls BEFORE any gr_render_resident
+call on it, so nothing the resident path grew can hide an allocation: a one-pixel warm
+call looks up the array (and loads the kernels), then the device's free memory must be
+the same before the first real static call and after each of two consecutive calls
+(sample ranges [0, spp) and [spp, 2*spp)).  The resident comparison runs afterwards:
+the films must be bit-identical (same kernels, each pixel's samples folded in the same
+order; only the chunking differs).
 """
 from __future__ import annotations
 
@@ -33,14 +41,22 @@ def _upload(lib, ctx, sc):
     return sid.value
 
 
-def _two_calls(lib, ctx, fn, sid, spp, film, mem=None):
+def _call(lib, ctx, fn, sid, offset, spp, film):
+    st = fn(ctx, sid, offset, spp, C.c_void_p(film.data_ptr()), None)
+    assert st == abi.GR_OK, lib.gr_last_error_string()
+    assert lib.gr_synchronize(ctx) == abi.GR_OK
+
+
+def _warm_static(lib, ctx):
+    """One real static call on a 1-pixel scene: the scratch address lookup and the
+    first launches of the plain trace and fold kernels happen here."""
     import torch
-    for k in range(2):
-        st = fn(ctx, sid, k * spp, spp, C.c_void_p(film.data_ptr()), None)
-        assert st == abi.GR_OK, lib.gr_last_error_string()
-        assert lib.gr_synchronize(ctx) == abi.GR_OK
-        if mem is not None:
-            mem.append(torch.cuda.mem_get_info()[0])
+    tiny = srb_scene("Diamond", width=1, height=1, max_bounces=2)
+    sid = _upload(lib, ctx, tiny)
+    film = torch.zeros((1, 3), dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    _call(lib, ctx, lib.gr_render_resident_static, sid, 0, 1, film)
+    return sid, film
 
 
 @pytest.mark.parametrize("case", ["latlong_multichunk", "studio_onechunk"])
@@ -56,21 +72,51 @@ def test_static_scratch_matches_resident_on_two_calls(engine_lib, ctx, case):
     else:
         sc = srb_scene("Sapphire", width=40, height=30, max_bounces=24)
         spp = 64
+    warm_sid, warm_film = _warm_static(lib, ctx)
     sid = _upload(lib, ctx, sc)
     n = sc.width * sc.height
     seed = torch.rand((n, 3), dtype=torch.float32, generator=torch.Generator().manual_seed(5))
-    ref = seed.clone().cuda()
     got = seed.clone().cuda()
+    ref = seed.clone().cuda()
     torch.cuda.synchronize()
-    _two_calls(lib, ctx, lib.gr_render_resident, sid, spp, ref)
-    mem = []
-    _two_calls(lib, ctx, lib.gr_render_resident_static, sid, spp, got, mem)
+    free = [torch.cuda.mem_get_info()[0]]
+    for k in range(2):
+        _call(lib, ctx, lib.gr_render_resident_static, sid, k * spp, spp, got)
+        free.append(torch.cuda.mem_get_info()[0])
+    assert free[0] == free[1] == free[2], free  # no call allocated device memory
+    for k in range(2):
+        _call(lib, ctx, lib.gr_render_resident, sid, k * spp, spp, ref)
     a = ref.cpu().numpy()
     b = got.cpu().numpy()
     assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
     assert not np.array_equal(a, seed.numpy())  # the calls added light
-    assert mem[0] == mem[1], mem                # the second call allocated nothing
     assert lib.gr_scene_release(ctx, sid) == abi.GR_OK
+    assert lib.gr_scene_release(ctx, warm_sid) == abi.GR_OK
+    del warm_film
+
+
+def test_static_scratch_exact_fill(engine_lib, ctx):
+    """spp = GR_STATIC_SCRATCH_TUPLES, the largest accepted: one pixel per chunk fills
+    16,777,212 of the array's 16,777,216 bytes.  Two pixels, two chunks; the film is the
+    resident path's bit for bit."""
+    import torch
+    lib = engine_lib
+    spp = abi.GR_STATIC_SCRATCH_TUPLES
+    sc = srb_scene("Diamond", width=2, height=1, max_bounces=3)
+    warm_sid, warm_film = _warm_static(lib, ctx)
+    sid = _upload(lib, ctx, sc)
+    got = torch.zeros((2, 3), dtype=torch.float32, device="cuda")
+    ref = torch.zeros((2, 3), dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    before = torch.cuda.mem_get_info()[0]
+    _call(lib, ctx, lib.gr_render_resident_static, sid, 0, spp, got)
+    assert torch.cuda.mem_get_info()[0] == before
+    _call(lib, ctx, lib.gr_render_resident, sid, 0, spp, ref)
+    assert np.array_equal(got.cpu().numpy().view(np.uint32), ref.cpu().numpy().view(np.uint32))
+    assert got.sum().item() > 0
+    assert lib.gr_scene_release(ctx, sid) == abi.GR_OK
+    assert lib.gr_scene_release(ctx, warm_sid) == abi.GR_OK
+    del warm_film
 
 
 def test_static_scratch_rejects_oversize_spp(engine_lib, ctx):
@@ -85,6 +131,7 @@ def test_static_scratch_rejects_oversize_spp(engine_lib, ctx):
     assert b"static scratch" in lib.gr_last_error_string()
     assert lib.gr_synchronize(ctx) == abi.GR_OK
     assert torch.equal(film.cpu(), torch.ones((16, 3)))
-    # the largest accepted spp is the scratch capacity (one pixel per chunk); spp 0 is a no-op
+    # spp 0 is a no-op
     assert lib.gr_render_resident_static(ctx, sid, 0, 0, C.c_void_p(film.data_ptr()), None) == abi.GR_OK
+    assert torch.equal(film.cpu(), torch.ones((16, 3)))
     assert lib.gr_scene_release(ctx, sid) == abi.GR_OK

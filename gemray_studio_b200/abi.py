@@ -231,6 +231,8 @@ EXPORTS = [
     ("gr_accumulate_device", C.c_int, [_ctx_p, C.POINTER(gr_scene), C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]),
     ("gr_trace_samples", C.c_int, [_ctx_p, C.POINTER(gr_scene), C.c_uint32, C.c_uint32, C.c_uint32,
                                    C.c_uint32, C.POINTER(C.c_float)]),
+    ("gr_accumulate_stokes", C.c_int, [_ctx_p, C.POINTER(gr_scene), C.c_uint32, C.c_uint32, C.POINTER(C.c_float),
+                                       C.POINTER(C.c_float)]),
     ("gr_tonemap", C.c_int, [_ctx_p, C.POINTER(C.c_float), C.c_float, C.c_uint32, C.POINTER(C.c_uint8)]),
     ("gr_rng_records", C.c_int, [_ctx_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.c_uint32,
                                  C.POINTER(gr_rng_record)]),

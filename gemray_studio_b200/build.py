@@ -18,8 +18,10 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 OUT = PKG / "libgemray_cuda.so"
-SOURCES = ["gr_host.cu", "gr_batch.cu", "gr_serve.cu", "gr_stream.cu", "gr_denoise.cu", "gr_tonemap.cu", "gr_metrics.cu", "gr_static.cu", "gr_verify.cu", "gr_scene_builders.cpp"]
-HEADERS = ["gr_device.cuh", "gr_stage.cuh", "gr_trace.cuh", "gr_launch.cuh", "gr_kernels.cuh", "gr_batch.cuh", "gr_wavefront.cuh",
+SOURCES = ["gr_host.cu", "gr_batch.cu", "gr_serve.cu", "gr_stream.cu", "gr_denoise.cu", "gr_tonemap.cu", "gr_metrics.cu", "gr_static.cu", "gr_verify.cu", "gr_stokes.cu", "gr_single_clear.cu",
+           "gr_single_general.cu", "gr_scene_builders.cpp"]
+HEADERS = ["gr_device.cuh", "gr_stage.cuh", "gr_trace.cuh", "gr_launch.cuh", "gr_kernels.cuh", "gr_transport.cuh",
+           "gr_single.cuh", "gr_batch.cuh", "gr_wavefront.cuh",
            "gr_ctx.h", "gr_host.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # Compile-time engine options (see csrc/gr_device.cuh).
@@ -53,18 +55,34 @@ def needs_build() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False, defines: tuple[str, ...] = DEFINES, out: Path | None = None) -> Path:
+    """Compile every translation unit to an object in parallel (one nvcc per source,
+    objects under _build/), then link the shared library."""
+    from concurrent.futures import ThreadPoolExecutor
     target = Path(out) if out is not None else OUT
     if out is None and not force and not needs_build():
         return OUT
+    objdir = ROOT / "_build" / (target.stem + "".join(f"_{d}" for d in defines).replace("=", "-"))
+    objdir.mkdir(parents=True, exist_ok=True)
+    base = [nvcc(), *flags(verbose), *[f"-D{d}" for d in defines]]
+
+    def compile_one(src: str):
+        obj = objdir / (src.rsplit(".", 1)[0] + ".o")
+        return src, subprocess.run([*base, "-c", "-o", str(obj), str(CSRC / src)], capture_output=True, text=True), obj
+
+    jobs = max(1, min(len(SOURCES), os.cpu_count() or 1))
+    with ThreadPoolExecutor(jobs) as ex:
+        results = list(ex.map(compile_one, SOURCES))
+    for src, r, _ in results:
+        if verbose or r.returncode != 0:
+            sys.stderr.write(f"--- {src}\n" + r.stdout + r.stderr)
+        if r.returncode != 0:
+            raise RuntimeError(f"nvcc failed compiling {src}")
     tmp = target.with_suffix(".so.tmp")
-    cmd = [nvcc(), *flags(verbose), *[f"-D{d}" for d in defines], "-shared", "-o", str(tmp),
-           *[str(CSRC / s) for s in SOURCES]]
-    r = subprocess.run(cmd, capture_output=True, text=True)
+    r = subprocess.run([nvcc(), *ARCH, "-shared", "-o", str(tmp), *[str(o) for _, _, o in results]],
+                       capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
-        raise RuntimeError("nvcc failed building libgemray_cuda.so")
-    if verbose:
-        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("nvcc failed linking libgemray_cuda.so")
     os.replace(tmp, target)
     return target
 

@@ -144,6 +144,7 @@ void streams_shutdown(gr_ctx *ctx);
 
 namespace grd {
 struct LaunchRange;
+struct Path;
 }
 namespace grh {
 // Scene checks and encoding (gr_host.cu): validate, encode the constants, and upload
@@ -157,6 +158,23 @@ gr_status prepare(gr_ctx *ctx, const gr_scene *sc, SceneConst &S, grd::SceneBuff
 gr_status launch_trace(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuffers &B, const grd::LaunchRange &R,
                        float *xyz, cudaStream_t stream, int mode, grh::DeviceBuffer *park = nullptr,
                        StageCaps caps = StageCaps{});
+// The compile-time scene class of a single-scene launch (gr_trace.cuh K_*): clear
+// isotropic stones (K_ISO | K_CLEAR) and the rest, each with its environment kind;
+// -1 for scenes the extension variant handles (frosted, scattering, biaxial).
+int scene_class(const SceneConst &S);
+// Park buffers and caps of a staged single-scene launch (prepared by launch_trace).
+struct StagedLaunch {
+    grd::Path *park1, *park2;
+    unsigned int *counts;
+    uint64_t cap1, cap2;
+    uint32_t cap_first, cap_second;
+};
+// The plain kernel (st == NULL) or the three staged launches of scene class K
+// (gr_single_clear.cu / gr_single_general.cu).
+gr_status launch_single_clear(int K, const SceneConst &S, const grd::SceneBuffers &B, const grd::LaunchRange &R,
+                              float *xyz, cudaStream_t stream, const StagedLaunch *st);
+gr_status launch_single_general(int K, const SceneConst &S, const grd::SceneBuffers &B, const grd::LaunchRange &R,
+                                float *xyz, cudaStream_t stream, const StagedLaunch *st);
 // The kernel a launch of n_tuples tuples runs in `mode` (AUTO resolved by size), and
 // how many kernel launches that trace makes.
 int resolve_kernel(int mode, uint64_t n_tuples);

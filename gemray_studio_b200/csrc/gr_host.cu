@@ -431,6 +431,12 @@ int trace_kernel_launches(int mode, const SceneConst &S, uint64_t n_tuples) {
 }
 
 // Trace tuples [0, R.n_tuples) of one chunk into xyz (device).
+int scene_class(const SceneConst &S) {
+    if (grd::needs_extras(S)) return -1;
+    const bool iso = !S.anisotropic && !S.biaxial, clear = !S.absorbing;
+    return ((iso && clear) ? (grd::K_ISO | grd::K_CLEAR) : 0) | grd::k_env(S.env_mode);
+}
+
 gr_status launch_trace(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuffers &B, const grd::LaunchRange &R,
                        float *xyz, cudaStream_t stream, int mode, grh::DeviceBuffer *park_buf, StageCaps caps) {
     if (caps.first == 0) caps = StageCaps{GR_STAGE_CAP, GR_STAGE_CAP2};
@@ -449,15 +455,17 @@ gr_status launch_trace(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuffers
         GR_CUDA(cudaGetLastError());
         return GR_OK;
     }
+    const int K = scene_class(S);
+    const bool clear = K >= 0 && (K & grd::K_CLEAR);
     if (mode == GR_KERNEL_PLAIN || S.max_bounces == 0) {
-        if (extras)
+        if (extras) {
             grd::k_trace_plain<grd::NoCounters, false, true><<<(unsigned)plain_blocks, grd::TRACE_THREADS, smem, stream>>>(
                 S, B, R, xyz, nullptr);
-        else
-            grd::k_trace_plain<grd::NoCounters><<<(unsigned)plain_blocks, grd::TRACE_THREADS, smem, stream>>>(S, B, R, xyz,
-                                                                                                           nullptr);
-        GR_CUDA(cudaGetLastError());
-        return GR_OK;
+            GR_CUDA(cudaGetLastError());
+            return GR_OK;
+        }
+        return clear ? launch_single_clear(K, S, B, R, xyz, stream, nullptr)
+                     : launch_single_general(K, S, B, R, xyz, stream, nullptr);
     }
     if (mode == GR_KERNEL_STAGED) {
         // park buffers: stage 1 parks up to 1/8 of the launch's paths (at most 4 GiB),
@@ -474,12 +482,17 @@ gr_status launch_trace(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuffers
         grd::Path *park1 = (grd::Path *)((char *)pk.ptr + 256);
         grd::Path *park2 = park1 + cap1;
         GR_CUDA(cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned int), stream));
+        if (!extras) {
+            const StagedLaunch sl{park1, park2, counts, cap1, cap2, caps.first, caps.second};
+            return clear ? launch_single_clear(K, S, B, R, xyz, stream, &sl)
+                         : launch_single_general(K, S, B, R, xyz, stream, &sl);
+        }
         const grd::ParkOut out1{park1, (uint32_t)cap1, counts};
         const grd::ParkOut out2{park2, (uint32_t)cap2, counts + 1};
         const grd::ParkOut none{nullptr, 0, nullptr};
         const unsigned b2 = (unsigned)((cap1 + grd::TRACE_THREADS - 1) / grd::TRACE_THREADS);
         const unsigned b3 = (unsigned)((cap2 + grd::TRACE_THREADS - 1) / grd::TRACE_THREADS);
-        if (extras) {
+        {
             grd::k_trace_stage1<true><<<(unsigned)plain_blocks, grd::TRACE_THREADS, smem, stream>>>(S, B, R, xyz, out1,
                                                                                                   caps.first);
             grd::k_trace_stage2<true><<<b2, grd::TRACE_THREADS, smem, stream>>>(S, B, park1, (uint32_t)cap1, counts,
@@ -487,14 +500,6 @@ gr_status launch_trace(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuffers
             if (cap2)
                 grd::k_trace_stage2<true><<<b3, grd::TRACE_THREADS, smem, stream>>>(S, B, park2, (uint32_t)cap2,
                                                                                     counts + 1, 0xFFFFFFFFu, none, xyz);
-        } else {
-            grd::k_trace_stage1<false><<<(unsigned)plain_blocks, grd::TRACE_THREADS, smem, stream>>>(S, B, R, xyz, out1,
-                                                                                                   caps.first);
-            grd::k_trace_stage2<false><<<b2, grd::TRACE_THREADS, smem, stream>>>(S, B, park1, (uint32_t)cap1, counts,
-                                                                                 caps.second, out2, xyz);
-            if (cap2)
-                grd::k_trace_stage2<false><<<b3, grd::TRACE_THREADS, smem, stream>>>(S, B, park2, (uint32_t)cap2,
-                                                                                     counts + 1, 0xFFFFFFFFu, none, xyz);
         }
         GR_CUDA(cudaGetLastError());
         return GR_OK;

@@ -40,7 +40,7 @@ struct ParkOut {
 // and a slot is free; returns true when parked.  A path that cannot be parked is run
 // to its end.  Every lane of the warp must call this (the slot ballot), `active`
 // false for lanes without a path.
-template <bool EXTRAS>
+template <bool EXTRAS, int K = K_ANY>
 __device__ __forceinline__ bool run_or_park(Path &P, const SceneConst &S, const Planes &PL, bool active, uint32_t cap,
                                             const ParkOut &out) {
     NoCounters nc;
@@ -49,9 +49,9 @@ __device__ __forceinline__ bool run_or_park(Path &P, const SceneConst &S, const 
         if (active) {
             while ((state_bits(P) & F_ALIVE) && p_bounce(P) < cap) {
                 Event E;
-                const uint32_t ev = step_hit<GR_STEP_UNROLL, NoCounters, false, EXTRAS>(P, S, PL, E, nc);
-                if (ev == EV_REFLECT) step_reflect<GR_STEP_UNROLL, NoCounters, EXTRAS>(P, S, E, nc);
-                else if (ev == EV_REFRACT) step_refract<GR_STEP_UNROLL, NoCounters, EXTRAS>(P, S, E, nc);
+                const uint32_t ev = step_hit<GR_STEP_UNROLL, NoCounters, false, EXTRAS, K>(P, S, PL, E, nc);
+                if (ev == EV_REFLECT) step_reflect<GR_STEP_UNROLL, NoCounters, EXTRAS, K>(P, S, E, nc);
+                else if (ev == EV_REFRACT) step_refract<GR_STEP_UNROLL, NoCounters, EXTRAS, K>(P, S, E, nc);
             }
         }
         if (round == 1 || out.cap == 0) break;

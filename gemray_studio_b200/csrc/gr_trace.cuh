@@ -64,6 +64,26 @@ constexpr uint32_t F_ALIVE = 1u << 4;
 constexpr uint32_t F_TIR = 1u << 5;  // the pending event is a hero TIR
 constexpr uint32_t BOUNCE_SHIFT = 8;
 
+// Scene class known at compile time (template parameter K of the single-scene kernels):
+// the run-time material and environment checks it settles are folded away, so a clear
+// isotropic stone's kernel carries none of the birefringence, walk-off, absorption or
+// other-environment code.  K = K_ANY keeps every check at run time (batched launches,
+// the wavefront and regeneration schedules, the instrumented variants).
+constexpr int K_ANY = 0;
+constexpr int K_ISO = 1;        // S.anisotropic == 0 (and not biaxial)
+constexpr int K_CLEAR = 2;      // S.absorbing == 0: no absorption data at all
+constexpr int K_ENV_SHIFT = 2;  // bits 2-3: 0 = the environment kind at run time, else GR_ENV_* + 1
+__host__ __device__ constexpr int k_env(uint32_t env) { return (int)(env + 1) << K_ENV_SHIFT; }
+template <int K> __device__ __forceinline__ bool aniso_k(const SceneConst &S) {
+    return (K & K_ISO) ? false : (S.anisotropic != 0);
+}
+template <int K> __device__ __forceinline__ bool absorbing_k(uint32_t bits) {
+    return (K & K_CLEAR) ? false : ((bits & F_ABSORBING) != 0);
+}
+template <int K> __device__ __forceinline__ uint32_t env_k(const SceneConst &S) {
+    return (K >> K_ENV_SHIFT) ? (uint32_t)((K >> K_ENV_SHIFT) - 1) : S.env_mode;
+}
+
 // EV_HANDLED: the bounce was completed inside step_hit (a frosted facet or a volume
 // scattering event); the path continues with the next intersection if still alive.
 enum EventKind : uint32_t { EV_DONE = 0, EV_REFLECT = 1, EV_REFRACT = 2, EV_HANDLED = 3 };
@@ -135,7 +155,7 @@ __device__ __forceinline__ V3 camera_dir(const SceneConst &S, float x, float y, 
     return normalize(add(add(ld3(S.cam_f), mul(ld3(S.cam_r), u)), mul(ld3(S.cam_u), v)));
 }
 
-template <int U = 1, bool X = false>
+template <int U = 1, bool X = false, int K = K_ANY>
 __device__ __forceinline__ void path_init(Path &P, const SceneConst &S, const SceneBuffers &B, uint32_t pixel,
                                           uint32_t sample, uint32_t tuple) {
     Draws dr = sample_draws(pixel, sample);
@@ -152,7 +172,9 @@ __device__ __forceinline__ void path_init(Path &P, const SceneConst &S, const Sc
         float lam = lambda_k(dr.hero, k);
         float n_o = dispersion(S, lam);
         arr(P.n_o4, k) = n_o;
-        if (S.has_cauchy_e) {
+        if (K & K_ISO) {
+            // no birefringence: n_e - n_o is never read
+        } else if (S.has_cauchy_e) {
             float lum = lam * 1e-3f;
             float l2 = lum * lum, l4 = l2 * l2;
             float n_e = S.cauchy_e[0] + S.cauchy_e[1] / l2 + S.cauchy_e[2] / l4;
@@ -161,7 +183,7 @@ __device__ __forceinline__ void path_init(Path &P, const SceneConst &S, const Sc
             arr(P.ne_d4, k) = S.bire;
         }
         float ao = 0.0f, ae = 0.0f;
-        if (S.absorbing) {
+        if (!(K & K_CLEAR) && S.absorbing) {
             if (S.ext_n > 0) {
                 ao = table_lookup(B.ext_alpha_o, S.ext_n, S.ext_first, S.ext_step, lam);
                 ae = table_lookup(B.ext_alpha_e, S.ext_n, S.ext_first, S.ext_step, lam);
@@ -170,8 +192,10 @@ __device__ __forceinline__ void path_init(Path &P, const SceneConst &S, const Sc
                 ae = band_sum(S.e_bands, S.n_e_bands, lam);
             }
         }
-        arr(P.a_o4, k) = ao;
-        arr(P.a_e4, k) = ae;
+        if (!(K & K_CLEAR)) {  // a clear stone's kernel never reads them
+            arr(P.a_o4, k) = ao;
+            arr(P.a_e4, k) = ae;
+        }
         any = any || (ao != 0.0f) || (ae != 0.0f);
         if (X && S.biaxial) {
             const float ab = (S.absorbing && S.has_beta) ? band_sum(S.b_bands, S.n_b_bands, lam) : ao;
@@ -642,7 +666,7 @@ __device__ __forceinline__ float theta_c(V3 kk, V3 normal, float cos_i, float on
 // X: the instantiation that handles frosted facets, volume scattering and biaxial
 // materials (scenes without any of them run the X = false code, which has none of
 // those branches).
-template <int U, class CT, bool R = false, bool X = false>
+template <int U, class CT, bool R = false, bool X = false, int K = K_ANY>
 __device__ __forceinline__ uint32_t step_hit(Path &P, const SceneConst &S, const Planes &PL, Event &E, CT &ct) {
     const uint32_t bits = state_bits(P);
     const uint32_t bounce = bits >> BOUNCE_SHIFT;
@@ -688,7 +712,7 @@ __device__ __forceinline__ uint32_t step_hit(Path &P, const SceneConst &S, const
     // apply_interior_segment (transport.rs:586-605) -> apply_absorption (absorption.rs:115-141)
     if (inside) {
         normal = neg(normal);
-        if ((bits & F_ABSORBING) && !extinguished) {
+        if (absorbing_k<K>(bits) && !extinguished) {
             tally(ct, C_ABSORB);
             V3 ea, eb;
             absorption_eigenmodes<X>(P, S, kk, ea, eb);
@@ -709,7 +733,7 @@ __device__ __forceinline__ uint32_t step_hit(Path &P, const SceneConst &S, const
     }
 
     // compute_bounce_refraction_geometry (refraction.rs:428-547), uniaxial branch
-    const bool aniso = S.anisotropic != 0;
+    const bool aniso = aniso_k<K>(S);
     float cos_i = clampf(dot(neg(kk), normal), 0.0f, 1.0f);
     float one_m_c2 = fmaf(cos_i, -cos_i, 1.0f);
     float n_o_hero = arr(P.n_o4, 0);
@@ -773,7 +797,7 @@ __device__ __forceinline__ uint32_t step_hit(Path &P, const SceneConst &S, const
 
 // Direction / state update after an event, internal mode coupling and Russian
 // roulette (transport.rs:177-193,204-220,343-353,919-928).
-template <class CT>
+template <class CT, int K = K_ANY>
 __device__ __forceinline__ void step_post(Path &P, const SceneConst &S, V3 hp, V3 new_k, V3 new_s, bool new_inside,
                                           bool has_update, bool update_val, CT &ct) {
     uint32_t bits = state_bits(P);
@@ -786,7 +810,7 @@ __device__ __forceinline__ void step_post(Path &P, const SceneConst &S, V3 hp, V
     bits = new_inside ? (bits | F_INSIDE) : (bits & ~F_INSIDE);
     if (has_update) bits = update_val ? (bits | F_IS_E) : (bits & ~F_IS_E);
     const uint32_t seed = p_seed(P);
-    if (S.anisotropic && was_internal_reflection)
+    if (aniso_k<K>(S) && was_internal_reflection)
         bits = rng_draw(seed, bounce, MODE_COUPLING_STREAM) < 0.5f ? (bits | F_IS_E) : (bits & ~F_IS_E);
     if (bounce > 4) {
         tally(ct, C_ROULETTE);
@@ -863,7 +887,7 @@ __device__ __noinline__ void frosted_bounce(Path &P, const SceneConst &S, V3 hp,
 
 // apply_tir_bounce (refraction.rs:599-637) and apply_partial_reflect_bounce
 // (refraction.rs:650-690) in one channel loop.
-template <int U, class CT, bool X = false>
+template <int U, class CT, bool X = false, int K = K_ANY>
 __device__ __forceinline__ void step_reflect(Path &P, const SceneConst &S, const Event &E, CT &ct) {
     const uint32_t bits = state_bits(P);
     const bool inside = (bits & F_INSIDE) != 0;
@@ -904,20 +928,20 @@ __device__ __forceinline__ void step_reflect(Path &P, const SceneConst &S, const
     V3 new_s = new_k;
     if (X && S.biaxial) {
         if (inside && S.anisotropic) new_s = mode_poynting_dir(S, make_ind(S, arr(P.n_o4, 0)), new_k, (bits & F_IS_E) != 0);
-    } else if (inside && S.anisotropic && (bits & F_IS_E)) {
+    } else if (inside && aniso_k<K>(S) && (bits & F_IS_E)) {
         float n_o_hero = arr(P.n_o4, 0);
         new_s = extraordinary_poynting_dir(new_k, ld3(S.c_axis), n_o_hero, n_o_hero + arr(P.ne_d4, 0));
     }
-    step_post(P, S, hp, new_k, new_s, inside, false, false, ct);
+    step_post<CT, K>(P, S, hp, new_k, new_s, inside, false, false, ct);
 }
 
 // apply_refract_bounce (refraction.rs:748-867) + apply_refract_channel (:883-1011)
-template <int U, class CT, bool X = false>
+template <int U, class CT, bool X = false, int K = K_ANY>
 __device__ __forceinline__ void step_refract(Path &P, const SceneConst &S, const Event &E, CT &ct) {
     const uint32_t bits = state_bits(P);
     const uint32_t bounce = bits >> BOUNCE_SHIFT;
     const bool inside = (bits & F_INSIDE) != 0;
-    const bool aniso = S.anisotropic != 0;
+    const bool aniso = aniso_k<K>(S);
     const V3 hp = xyz(E.hp_cos), normal = xyz(E.n_ru), kk = xyz(P.k_state);
     const float cos_i = E.hp_cos.w, ru = E.n_ru.w;
     const float one_m_c2 = fmaf(cos_i, -cos_i, 1.0f);
@@ -982,13 +1006,19 @@ __device__ __forceinline__ void step_refract(Path &P, const SceneConst &S, const
         }
         P.st[k] = make_float4(s.i, s.q, s.u, s.v);
     }
-    step_post(P, S, hp, refr, final_dir, !inside, entering_aniso, use_e, ct);
+    step_post<CT, K>(P, S, hp, refr, final_dir, !inside, entering_aniso, use_e, ct);
 }
 
 // Escape radiance, spectral MIS and CIE integration (transport.rs:67-90,931-939,
-// raytracer/color.rs:122-164) for a finished path.
-template <int U = 1>
-__device__ __forceinline__ V3 path_finish(const Path &P, const SceneConst &S, const SceneBuffers &B) {
+// raytracer/color.rs:122-164) for a finished path.  STOKES: also the luminance-weighted
+// Stokes vector of the escaping light, iquv = sum_k ybar(lambda_k) * (S_k * env_k * w)
+// * norm in channel order (I with the intensity clamp of the XYZ sum, so iquv.x equals
+// the XYZ sum's Y before white balance bit for bit; Q, U, V in the frame of the last
+// plane of incidence).
+template <int U = 1, bool STOKES = false, int K = K_ANY>
+__device__ __forceinline__ V3 path_finish(const Path &P, const SceneConst &S, const SceneBuffers &B,
+                                          float4 *iquv = nullptr) {
+    const uint32_t env_mode = env_k<K>(S);
     float sum = -0.0f;
 #pragma unroll
     for (int k = 0; k < NCH; ++k) sum = sum + arr(P.pdf4, k);
@@ -1000,41 +1030,55 @@ __device__ __forceinline__ V3 path_finish(const Path &P, const SceneConst &S, co
     float rgb[3] = {0.0f, 0.0f, 0.0f};
     V3 dn = v3(0.f, 0.f, 0.f);
     if (escaped) {
-        if (S.env_mode == GR_ENV_STUDIO) {
+        if (env_mode == GR_ENV_STUDIO) {
             dn = normalize(dir);
-        } else if (S.env_mode == GR_ENV_UNIFORM) {
+        } else if (env_mode == GR_ENV_UNIFORM) {
             rgb[0] = S.uni_rgb[0]; rgb[1] = S.uni_rgb[1]; rgb[2] = S.uni_rgb[2];
         } else {
             latlong_rgb(S, B.map, dir, rgb);
         }
     }
     V3 acc = v3(0.f, 0.f, 0.f);
+    float4 sk = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 #pragma unroll U
     for (int k = 0; k < NCH; ++k) {
         const float lam = lambda_k(hero, k);
-        float rad = 0.0f;
+        float rad = 0.0f, q = 0.0f, u = 0.0f, v = 0.0f;
         if (escaped) {
-            float env = S.env_mode == GR_ENV_STUDIO ? studio_radiance(S, dn, lam)
+            float env = env_mode == GR_ENV_STUDIO ? studio_radiance(S, dn, lam)
                                                      : rgb_to_spectral(rgb[0], rgb[1], rgb[2], lam);
             rad = fmaf(fmaxf(P.st[k].x, 0.0f), env, 0.0f);
+            if (STOKES) {
+                q = P.st[k].y * env;
+                u = P.st[k].z * env;
+                v = P.st[k].w * env;
+            }
         }
         float wr = rad * w;
-        acc = add(acc, mul(cmf(lam), wr * norm));
+        const V3 c = cmf(lam);
+        acc = add(acc, mul(c, wr * norm));
+        if (STOKES) {
+            sk.x = sk.x + c.y * (wr * norm);
+            sk.y = sk.y + c.y * ((q * w) * norm);
+            sk.z = sk.z + c.y * ((u * w) * norm);
+            sk.w = sk.w + c.y * ((v * w) * norm);
+        }
     }
+    if (STOKES) *iquv = sk;
     return von_kries(acc, S.wb);
 }
 
 // One whole path in the calling thread (the plain kernel's body).
-template <class CT, bool R = false, bool X = false>
+template <class CT, bool R = false, bool X = false, int K = K_ANY>
 __device__ __forceinline__ V3 trace_path(Path &P, const SceneConst &S, const SceneBuffers &B, const Planes &PL,
                                          CT &ct) {
     while (state_bits(P) & F_ALIVE) {
         Event E;
-        uint32_t ev = step_hit<1, CT, R, X>(P, S, PL, E, ct);
-        if (ev == EV_REFLECT) step_reflect<1, CT, X>(P, S, E, ct);
-        else if (ev == EV_REFRACT) step_refract<1, CT, X>(P, S, E, ct);
+        uint32_t ev = step_hit<1, CT, R, X, K>(P, S, PL, E, ct);
+        if (ev == EV_REFLECT) step_reflect<1, CT, X, K>(P, S, E, ct);
+        else if (ev == EV_REFRACT) step_refract<1, CT, X, K>(P, S, E, ct);
     }
-    return path_finish<1>(P, S, B);
+    return path_finish<1, false, K>(P, S, B);
 }
 
 }  // namespace grd

@@ -250,6 +250,19 @@ gr_status gr_trace_samples(gr_ctx *ctx, const gr_scene *scene, uint32_t first_pi
                            uint32_t n_pixels, uint32_t sample_offset, uint32_t spp,
                            float *xyz_out);
 
+/* gr_accumulate plus a Stokes film (no counterpart in the reference, whose film is XYZ
+ * only, renderer/gpu/frame.rs:799-814; the transport's per-channel StokesVector state,
+ * optics/polarization.rs:4-66, is otherwise dropped when a path ends).  accum_xyz
+ * (W*H*3) receives exactly what gr_accumulate adds; accum_stokes (W*H*4, host) receives
+ * each pixel's sample-order sum of the luminance-weighted Stokes vector of the light
+ * that escapes:  (I, Q, U, V) = sum_k ybar(lambda_k) * w * norm * env_k * S_k  over the
+ * 8 hero channels, with the XYZ sum's spectral-MIS weight w, normaliser and intensity
+ * clamp, so I equals that sum's Y before white balance.  Q, U, V are in the frame of
+ * the last plane of incidence; every per-sample vector has sqrt(Q^2+U^2+V^2) <= I up to
+ * rounding.  Plain kernel; not with GR_FLAG_FP64_RESOLVE. */
+gr_status gr_accumulate_stokes(gr_ctx *ctx, const gr_scene *scene, uint32_t sample_offset, uint32_t spp,
+                               float *accum_xyz, float *accum_stokes);
+
 /* Device-side tone map: rgba[i] = ColorSpace::Srgb.encode(xyz[i] * scale, ACES)
  * (renderer/tonemap.rs:52-108, color/space.rs:290-334).  Host arrays. */
 gr_status gr_tonemap(gr_ctx *ctx, const float *xyz, float scale, uint32_t n_px,

@@ -924,6 +924,24 @@ template <class R> static inline V3<R> compute_illuminant_white_balance(R temp_k
                  ls.z > R(1e-6f) ? lt.z / ls.z : R(1));
 }
 
+// Extension (no reference counterpart): the luminance-weighted Stokes vector of the
+// escaping light, sum_k ybar(lambda_k) * ((S_k * env_k) * w) * norm in channel order,
+// with the XYZ integral's weight w, normaliser and intensity clamp (stokes_env[k] =
+// (fma(I_k clamped, env_k, 0), Q_k * env_k, U_k * env_k, V_k * env_k)), so its I is the
+// XYZ integral's Y.
+template <class R> static inline void integrate_channels_to_stokes(const R stokes_env[8][4], const R lam[8],
+                                                                    const R pdf[8], R out[4]) {
+    R sum = R(-0.0);
+    for (int k = 0; k < 8; ++k) sum = sum + pdf[k];
+    R w = sum <= R(1e-12f) ? R(1) : R(8) * pdf[0] / sum;
+    const R norm = R((400.0f / 8.0f) / 106.856f);
+    R c[8][3];
+    cmf_x8(lam, c);
+    for (int j = 0; j < 4; ++j) out[j] = R(0);
+    for (int k = 0; k < 8; ++k)
+        for (int j = 0; j < 4; ++j) out[j] = out[j] + c[k][1] * ((stokes_env[k][j] * w) * norm);
+}
+
 // color.rs:122-131 and 147-164
 template <class R> static inline V3<R> integrate_channels_to_xyz(const R rad[8], const R lam[8], const R pdf[8]) {
     R sum = R(-0.0);
@@ -1269,12 +1287,15 @@ template <class R>
 static inline V3<R> trace_spectral_ray(const Ray<float> &initial, const gr_plane *planes, uint32_t n_planes,
                                        const MaterialCtx<R> &mc, const EnvCtx<R> &env, uint32_t max_bounces,
                                        uint32_t rng_seed, float hero_rand, EventLog *log,
-                                       const uint32_t *finishes = nullptr) {
+                                       const uint32_t *finishes = nullptr, R *stokes_out = nullptr) {
     R lam[8];
     wrapped_hero_wavelengths<R>(hero_rand, lam);
     Stokes<R> st[8];
-    R rad[8], pdf[8];
-    for (int k = 0; k < 8; ++k) { st[k] = Stokes<R>{R(1), R(0), R(0), R(0)}; rad[k] = R(0); pdf[k] = R(1); }
+    R rad[8], pdf[8], stokes_env[8][4];
+    for (int k = 0; k < 8; ++k) {
+        st[k] = Stokes<R>{R(1), R(0), R(0), R(0)}; rad[k] = R(0); pdf[k] = R(1);
+        for (int j = 0; j < 4; ++j) stokes_env[k][j] = R(0);
+    }
     Ray<R> ray;
     ray.origin = V3<R>(initial.origin.x, initial.origin.y, initial.origin.z);
     ray.dir = V3<R>(initial.dir.x, initial.dir.y, initial.dir.z);
@@ -1292,6 +1313,10 @@ static inline V3<R> trace_spectral_ray(const Ray<float> &initial, const gr_plane
             for (int k = 0; k < 8; ++k) {
                 R e = env_channel(env, ray.dir, lam[k]);
                 rad[k] = M<R>::fma(st[k].intensity(), e, rad[k]);
+                stokes_env[k][0] = rad[k];
+                stokes_env[k][1] = st[k].q * e;
+                stokes_env[k][2] = st[k].u * e;
+                stokes_env[k][3] = st[k].v * e;
             }
             if (log) { log->bounces = bounce; log->termination = TERM_ESCAPED; log->n_escape++; }
             break;
@@ -1559,6 +1584,7 @@ static inline V3<R> trace_spectral_ray(const Ray<float> &initial, const gr_plane
         }
     }
     V3<R> xyz = integrate_channels_to_xyz(rad, lam, pdf);
+    if (stokes_out) integrate_channels_to_stokes(stokes_env, lam, pdf, stokes_out);
     return apply_von_kries(xyz, env.white_balance);
 }
 

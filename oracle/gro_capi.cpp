@@ -524,6 +524,90 @@ int gro_trace_samples(const gr_scene *sc, uint32_t first_pixel, uint32_t n_pixel
     return GR_OK;
 }
 
+}  // extern "C"
+
+// Per-sample XYZ and luminance-weighted Stokes vector (I, Q, U, V) of the FP32 tracer
+// (the Stokes film's oracle), (pixel, sample) order: xyz n*3, iquv n*4; and the films:
+// accum_xyz (W*H*3) and accum_iquv (W*H*4) += each pixel's sample-order sums.
+template <class R>
+static void stokes_pixel(const gr_scene &sc, const MaterialCtx<R> &mc, const EnvCtx<R> &env, uint32_t pixel,
+                         uint32_t sample_offset, uint32_t spp, float *xyz, float *iquv, float sum_x[3], float sum_s[4]) {
+    const uint32_t x = pixel % sc.width, y = pixel / sc.width;
+    const PixelRotations rot = pixel_rotations(pixel);
+    for (int c = 0; c < 3; ++c) sum_x[c] = 0.0f;
+    for (int c = 0; c < 4; ++c) sum_s[c] = 0.0f;
+    for (uint32_t s = 0; s < spp; ++s) {
+        const SampleDraws d = sample_draws(pixel, sample_offset + s, rot);
+        const Ray<float> ray = generate_ray(sc.camera, (float)x, (float)y, (float)sc.width, (float)sc.height, d.jitter_x,
+                                            d.jitter_y);
+        R so[4];
+        const V3<R> v = trace_spectral_ray<R>(ray, sc.planes, sc.n_planes, mc, env, sc.max_bounces, d.seed, d.hero_rand,
+                                              nullptr, sc.finishes, so);
+        const float fx[3] = {(float)v.x, (float)v.y, (float)v.z};
+        for (int c = 0; c < 3; ++c) {
+            if (xyz) xyz[3 * s + c] = fx[c];
+            sum_x[c] = sum_x[c] + fx[c];
+        }
+        for (int c = 0; c < 4; ++c) {
+            if (iquv) iquv[4 * s + c] = (float)so[c];
+            sum_s[c] = sum_s[c] + (float)so[c];
+        }
+    }
+}
+
+extern "C" int gro_trace_samples_stokes(const gr_scene *sc, uint32_t first_pixel, uint32_t n_pixels,
+                                        uint32_t sample_offset, uint32_t spp, float *xyz_out, float *iquv_out,
+                                        int threads) {
+    if (!material_supported(sc->material, sc->finishes, sc->n_planes)) return GR_DECLINED_MATERIAL;
+    MaterialCtx<float> mc = make_material<float>(sc->material, sc->material_ext);
+    EnvCtx<float> env = make_env<float>(sc->env);
+    if (threads <= 0) threads = (int)std::thread::hardware_concurrency();
+    if (threads <= 0) threads = 1;
+    std::atomic<uint32_t> next(0);
+    auto worker = [&]() {
+        for (;;) {
+            const uint32_t i = next.fetch_add(1);
+            if (i >= n_pixels) break;
+            float sx[3], ss[4];
+            stokes_pixel<float>(*sc, mc, env, first_pixel + i, sample_offset, spp, xyz_out + (size_t)i * spp * 3,
+                                iquv_out + (size_t)i * spp * 4, sx, ss);
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; ++t) pool.emplace_back(worker);
+    for (auto &t : pool) t.join();
+    return GR_OK;
+}
+
+extern "C" int gro_accumulate_stokes(const gr_scene *sc, uint32_t sample_offset, uint32_t spp, float *accum_xyz,
+                                     float *accum_iquv, int threads) {
+    if (!sc || !accum_xyz || !accum_iquv) return GR_EINVAL;
+    if (spp == 0 || sc->width == 0 || sc->height == 0) return GR_OK;
+    if (!material_supported(sc->material, sc->finishes, sc->n_planes)) return GR_DECLINED_MATERIAL;
+    MaterialCtx<float> mc = make_material<float>(sc->material, sc->material_ext);
+    EnvCtx<float> env = make_env<float>(sc->env);
+    if (threads <= 0) threads = (int)std::thread::hardware_concurrency();
+    if (threads <= 0) threads = 1;
+    const uint32_t n = sc->width * sc->height;
+    std::atomic<uint32_t> next(0);
+    auto worker = [&]() {
+        for (;;) {
+            const uint32_t p = next.fetch_add(1);
+            if (p >= n) break;
+            float sx[3], ss[4];
+            stokes_pixel<float>(*sc, mc, env, p, sample_offset, spp, nullptr, nullptr, sx, ss);
+            for (int c = 0; c < 3; ++c) accum_xyz[3 * (size_t)p + c] = accum_xyz[3 * (size_t)p + c] + sx[c];
+            for (int c = 0; c < 4; ++c) accum_iquv[4 * (size_t)p + c] = accum_iquv[4 * (size_t)p + c] + ss[c];
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; ++t) pool.emplace_back(worker);
+    for (auto &t : pool) t.join();
+    return GR_OK;
+}
+
+extern "C" {
+
 // Per-sample XYZ of the FP64 twin (values rounded to f32), for per-sample agreement
 // checks against the f32 engine.
 int gro_trace_samples_f64(const gr_scene *sc, uint32_t first_pixel, uint32_t n_pixels, uint32_t sample_offset,

@@ -125,6 +125,10 @@ def lib():
     L.gro_case_bank_arity.argtypes = [U, up, up]
     L.gro_intersect_rays.restype = C.c_int
     L.gro_intersect_rays.argtypes = [C.c_void_p, U, fp, U, C.c_int, fp, C.POINTER(C.c_int32)]
+    L.gro_trace_samples_stokes.restype = C.c_int
+    L.gro_trace_samples_stokes.argtypes = [sc, U, U, U, U, fp, fp, C.c_int]
+    L.gro_accumulate_stokes.restype = C.c_int
+    L.gro_accumulate_stokes.argtypes = [sc, U, U, fp, fp, C.c_int]
     L.gro_rng_records.restype = None
     L.gro_rng_records.argtypes = [up, up, U, up]
     _lib = L

@@ -55,6 +55,7 @@ GR_KERNEL_WAVEFRONT = 1
 GR_KERNEL_REGEN = 2
 GR_KERNEL_STAGED = 3
 GR_KERNEL_AUTO = 4
+GR_KERNEL_SORTED = 5
 GR_AUTO_STAGED_MIN_TUPLES = 1 << 19
 GR_STATIC_SCRATCH_BYTES = 16 << 20
 GR_STATIC_SCRATCH_TUPLES = GR_STATIC_SCRATCH_BYTES // 12

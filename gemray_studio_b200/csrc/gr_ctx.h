@@ -171,8 +171,10 @@ struct StagedLaunch {
 };
 // The plain kernel (st == NULL) or the three staged launches of scene class K
 // (gr_single_clear.cu / gr_single_general.cu).
+// sorted_work != NULL: the block-sorted kernel (gr_sorted.cuh) instead, its tuple counter.
 gr_status launch_single_clear(int K, const SceneConst &S, const grd::SceneBuffers &B, const grd::LaunchRange &R,
-                              float *xyz, cudaStream_t stream, const StagedLaunch *st);
+                              float *xyz, cudaStream_t stream, const StagedLaunch *st,
+                              unsigned int *sorted_work = nullptr, int sm_count = 0);
 gr_status launch_single_general(int K, const SceneConst &S, const grd::SceneBuffers &B, const grd::LaunchRange &R,
                                 float *xyz, cudaStream_t stream, const StagedLaunch *st);
 // The kernel a launch of n_tuples tuples runs in `mode` (AUTO resolved by size), and

@@ -424,24 +424,36 @@ int resolve_kernel(int mode, uint64_t n_tuples) {
     return n_tuples < GR_AUTO_STAGED_MIN_TUPLES ? GR_KERNEL_PLAIN : GR_KERNEL_STAGED;
 }
 
-int trace_kernel_launches(int mode, const SceneConst &S, uint64_t n_tuples) {
-    const bool staged = resolve_kernel(mode, n_tuples) == GR_KERNEL_STAGED && S.max_bounces > 0 &&
-                        !(S.flags & GR_FLAG_FP64_RESOLVE);
-    return staged ? 3 : 1;  // stages 1, 2 and 3
-}
-
-// Trace tuples [0, R.n_tuples) of one chunk into xyz (device).
 int scene_class(const SceneConst &S) {
     if (grd::needs_extras(S)) return -1;
     const bool iso = !S.anisotropic && !S.biaxial, clear = !S.absorbing;
     return ((iso && clear) ? (grd::K_ISO | grd::K_CLEAR) : 0) | grd::k_env(S.env_mode);
 }
 
+// The kernel a single-scene launch of this scene runs: GR_KERNEL_SORTED only for clear
+// isotropic stones (its slots hold that class's record; other scenes take AUTO's choice).
+static int scene_kernel(int mode, const SceneConst &S, uint64_t n_tuples) {
+    if (mode == GR_KERNEL_SORTED) {
+        const int K = scene_class(S);
+        const bool ok = K >= 0 && (K & grd::K_CLEAR) && S.max_bounces > 0 && !(S.flags & GR_FLAG_FP64_RESOLVE);
+        if (!ok) mode = GR_KERNEL_AUTO;
+    }
+    return resolve_kernel(mode, n_tuples);
+}
+
+int trace_kernel_launches(int mode, const SceneConst &S, uint64_t n_tuples) {
+    const int k = scene_kernel(mode, S, n_tuples);
+    const bool staged = k == GR_KERNEL_STAGED && S.max_bounces > 0 && !(S.flags & GR_FLAG_FP64_RESOLVE);
+    return staged ? 3 : 1;  // stages 1, 2 and 3
+}
+
+// Trace tuples [0, R.n_tuples) of one chunk into xyz (device).
+
 gr_status launch_trace(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuffers &B, const grd::LaunchRange &R,
                        float *xyz, cudaStream_t stream, int mode, grh::DeviceBuffer *park_buf, StageCaps caps) {
     if (caps.first == 0) caps = StageCaps{GR_STAGE_CAP, GR_STAGE_CAP2};
     if (R.n_tuples == 0) return GR_OK;
-    mode = resolve_kernel(mode, R.n_tuples);
+    mode = scene_kernel(mode, S, R.n_tuples);
     size_t smem = grd::planes_smem_bytes(S.n_planes);
     const bool extras = grd::needs_extras(S);
     const uint64_t plain_blocks = (R.n_tuples + grd::TRACE_THREADS - 1) / grd::TRACE_THREADS;
@@ -466,6 +478,14 @@ gr_status launch_trace(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuffers
         }
         return clear ? launch_single_clear(K, S, B, R, xyz, stream, nullptr)
                      : launch_single_general(K, S, B, R, xyz, stream, nullptr);
+    }
+    if (mode == GR_KERNEL_SORTED) {
+        // the tuple counter of the sorted blocks sits in the park buffer's header, so a
+        // frame stream (own park buffer and stream) never shares it with the context
+        grh::DeviceBuffer &pk = park_buf ? *park_buf : ctx->park;
+        gr_status st = pk.reserve(256);
+        if (st != GR_OK) return st;
+        return launch_single_clear(K, S, B, R, xyz, stream, nullptr, (unsigned int *)pk.ptr + 2, ctx->sm_count);
     }
     if (mode == GR_KERNEL_STAGED) {
         // park buffers: stage 1 parks up to 1/8 of the launch's paths (at most 4 GiB),
@@ -1230,7 +1250,7 @@ gr_status gr_angular_profile(gr_ctx *ctx, const gr_plane *planes, uint32_t n_pla
 gr_status gr_set_kernel(gr_ctx *ctx, uint32_t kernel) {
     if (!ctx) return fail(GR_EINVAL, "ctx is NULL");
     if (kernel != GR_KERNEL_PLAIN && kernel != GR_KERNEL_WAVEFRONT && kernel != GR_KERNEL_REGEN &&
-        kernel != GR_KERNEL_STAGED && kernel != GR_KERNEL_AUTO)
+        kernel != GR_KERNEL_STAGED && kernel != GR_KERNEL_AUTO && kernel != GR_KERNEL_SORTED)
         return fail(GR_EINVAL, "unknown kernel %u", kernel);
     std::lock_guard<std::mutex> lk(ctx->mu);
     ctx->kernel_mode = (int)kernel;

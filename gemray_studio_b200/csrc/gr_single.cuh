@@ -4,6 +4,7 @@
 #pragma once
 
 #include "gr_ctx.h"
+#include "gr_sorted.cuh"
 #include "gr_transport.cuh"
 
 namespace grh {
@@ -29,6 +30,27 @@ gr_status launch_single_k(const SceneConst &S, const grd::SceneBuffers &B, const
             grd::k_trace_stage2<false, K><<<b3, grd::TRACE_THREADS, smem, stream>>>(S, B, st->park2, (uint32_t)st->cap2,
                                                                                    st->counts + 1, 0xFFFFFFFFu, none, xyz);
     }
+    GR_CUDA(cudaGetLastError());
+    return GR_OK;
+}
+
+// The block-sorted kernel (gr_sorted.cuh) over a launch's tuples: one block per
+// resident slot set (blocks per SM from the occupancy calculator, at most one block per
+// SORT_THREADS tuples); `work` is a zeroed counter the blocks claim tuples from.
+template <int K>
+gr_status launch_sorted_k(const SceneConst &S, const grd::SceneBuffers &B, const grd::LaunchRange &R, float *xyz,
+                          cudaStream_t stream, unsigned int *work, int sm_count) {
+    const size_t smem = grd::sorted_smem_bytes(S.n_planes);
+    if (smem > 48 * 1024) GR_CUDA(cudaFuncSetAttribute(grd::k_trace_sorted<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                       (int)smem));
+    int per_sm = 0;
+    GR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grd::k_trace_sorted<K>, grd::SORT_THREADS, smem));
+    if (per_sm < 1) return fail(GR_EINVAL, "the sorted kernel does not fit an SM with %u planes", S.n_planes);
+    uint64_t blocks = (uint64_t)per_sm * (uint64_t)(sm_count > 0 ? sm_count : 1);
+    const uint64_t need = (R.n_tuples + grd::SORT_THREADS - 1) / grd::SORT_THREADS;
+    if (blocks > need) blocks = need;
+    GR_CUDA(cudaMemsetAsync(work, 0, sizeof(unsigned int), stream));
+    grd::k_trace_sorted<K><<<(unsigned)blocks, grd::SORT_THREADS, smem, stream>>>(S, B, R, xyz, work);
     GR_CUDA(cudaGetLastError());
     return GR_OK;
 }

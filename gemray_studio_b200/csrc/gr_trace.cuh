@@ -18,6 +18,8 @@
 // local memory, in the wavefront pool in global memory -- the same code serves both.
 #pragma once
 
+#include <cstddef>
+
 #include "gr_device.cuh"
 
 namespace grd {
@@ -48,6 +50,7 @@ struct __align__(16) Path {
     float4 a_e4[2];     // extraordinary absorption coefficient per channel
 };
 static_assert(sizeof(Path) == 352, "path record size");
+static_assert(offsetof(Path, ne_d4) == 256, "the tables a clear isotropic stone never touches come last");
 
 // Event scratch between step_hit and the event stage (64 B).
 struct __align__(16) Event {
@@ -90,6 +93,17 @@ enum EventKind : uint32_t { EV_DONE = 0, EV_REFLECT = 1, EV_REFRACT = 2, EV_HAND
 
 __device__ __forceinline__ float &arr(float4 (&a)[2], int k) { return reinterpret_cast<float *>(a)[k]; }
 __device__ __forceinline__ float arr(const float4 (&a)[2], int k) { return reinterpret_cast<const float *>(a)[k]; }
+// Bytes of Path an isotropic stone's kernels touch: the per-channel tables after n_o4
+// (n_e - n_o and the absorption coefficients) are neither written nor read for K_ISO |
+// K_CLEAR, and an isotropic stone's Event carries no medium indices (they are n_o4):
+// the shared-memory slots of the sorted kernel hold only these leading bytes.
+constexpr size_t PATH_CLEAR_BYTES = 256;
+constexpr size_t EVENT_ISO_BYTES = 32;
+// The medium index of channel k at the pending event: the ordinary index of an
+// isotropic stone, else what step_hit left in the event record.
+template <int K> __device__ __forceinline__ float n_med(const Path &P, const Event &E, int k) {
+    return (K & K_ISO) ? arr(P.n_o4, k) : arr(E.n_med4, k);
+}
 __device__ __forceinline__ V3 xyz(const float4 &v) { return v3(v.x, v.y, v.z); }
 __device__ __forceinline__ void set_xyz(float4 &v, V3 a) { v.x = a.x; v.y = a.y; v.z = a.z; }
 __device__ __forceinline__ uint32_t state_bits(const Path &P) { return __float_as_uint(P.k_state.w); }
@@ -751,11 +765,11 @@ __device__ __forceinline__ uint32_t step_hit(Path &P, const SceneConst &S, const
             float n_o = arr(P.n_o4, k);
             arr(E.n_med4, k) = use_o ? n_o : eff_e_index(n_o, n_o + arr(P.ne_d4, k), sc.x, sc.y);
         }
-    } else {
+    } else if (!(K & K_ISO)) {
         E.n_med4[0] = P.n_o4[0];
         E.n_med4[1] = P.n_o4[1];
     }
-    const float n_med0 = arr(E.n_med4, 0);
+    const float n_med0 = n_med<K>(P, E, 0);
     const float n1 = inside ? n_med0 : 1.0f;
     const float n2 = inside ? 1.0f : n_med0;
     const float eta0 = n1 / n2;
@@ -903,7 +917,7 @@ __device__ __forceinline__ void step_reflect(Path &P, const SceneConst &S, const
     const float inv = hero_tir ? 1.0f : 1.0f / E.n_ru.w;
 #pragma unroll U
     for (int k = 0; k < NCH; ++k) {
-        const float nm = arr(E.n_med4, k);
+        const float nm = n_med<K>(P, E, k);
         const float n1k = inside ? nm : 1.0f, n2k = inside ? 1.0f : nm;
         const float etak = n1k / n2k;
         const float s2k = etak * etak * one_m_c2;
@@ -947,11 +961,11 @@ __device__ __forceinline__ void step_refract(Path &P, const SceneConst &S, const
     const float one_m_c2 = fmaf(cos_i, -cos_i, 1.0f);
     tally(ct, C_REFRACT);
     note_event(ct, bounce, GR_SEQ_REFRACT);
-    const float n_med0 = arr(E.n_med4, 0);
+    const float n_med0 = n_med<K>(P, E, 0);
     const float n1 = inside ? n_med0 : 1.0f;
     const float n2 = inside ? 1.0f : n_med0;
     const float n_o_hero = arr(P.n_o4, 0);
-    const float n_e_hero = n_o_hero + arr(P.ne_d4, 0);
+    const float n_e_hero = (K & K_ISO) ? n_o_hero : n_o_hero + arr(P.ne_d4, 0);
     const bool entering_aniso = !inside && aniso;
     bool use_e = (bits & F_IS_E) != 0;
     if (entering_aniso) use_e = rng_draw(p_seed(P), bounce, BIREFRINGENT_SPLIT_STREAM) < 0.5f;
@@ -974,8 +988,8 @@ __device__ __forceinline__ void step_refract(Path &P, const SceneConst &S, const
 #pragma unroll U
     for (int k = 0; k < NCH; ++k) {
         const float n_o_k = arr(P.n_o4, k);
-        const float n1k = inside ? arr(E.n_med4, k) : 1.0f;
-        const float n2k = ordinary_entry ? n_o_k : (inside ? 1.0f : arr(E.n_med4, k));
+        const float n1k = inside ? n_med<K>(P, E, k) : 1.0f;
+        const float n2k = ordinary_entry ? n_o_k : (inside ? 1.0f : n_med<K>(P, E, k));
         const float ratio = n1k / n2k;
         const float s2k = (ratio * ratio) * one_m_c2;
         float4 s4 = P.st[k];

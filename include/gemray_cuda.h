@@ -675,6 +675,12 @@ gr_status gr_denoise_tonemap_device(gr_ctx *ctx, const float *film, uint32_t sam
 #define GR_KERNEL_REGEN 2u
 #define GR_KERNEL_STAGED 3u
 #define GR_KERNEL_AUTO 4u
+/* SORTED: clear isotropic stones (no birefringence, no absorption, no frosted facets or
+ * scattering) only -- other scenes run AUTO's choice.  Each block keeps 128 paths in
+ * shared memory and advances them bounce by bounce, any thread taking any path: dead
+ * paths are finished and replaced by the launch's next tuples, and at every bounce the
+ * reflecting and the refracting paths go to separate warps. */
+#define GR_KERNEL_SORTED 5u
 #define GR_AUTO_STAGED_MIN_TUPLES (1u << 19)
 gr_status gr_set_kernel(gr_ctx *ctx, uint32_t kernel);
 

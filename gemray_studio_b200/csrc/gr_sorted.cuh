@@ -103,10 +103,11 @@ __global__ void __launch_bounds__(SORT_THREADS, GR_SORT_MIN_BLOCKS) k_trace_sort
     for (;;) {
         // refill: finish ended paths, start the next tuples in their slots and in empty ones
         const uint32_t n_free = compact2(sh, sh.state[tid] != SLOT_LIVE, false).x;
-        if (tid == 0) sh.base = supply && n_free ? atomicAdd(work, n_free) : 0xFFFFFFFFu;
+        const uint32_t claim = supply ? n_free : 0u;  // no free slot: claim nothing, keep the supply
+        if (tid == 0 && claim) sh.base = atomicAdd(work, claim);
         __syncthreads();
         const uint32_t base = sh.base;
-        if (base == 0xFFFFFFFFu || base + n_free >= R.n_tuples) supply = false;
+        if (claim && (uint64_t)base + claim >= R.n_tuples) supply = false;
         if (tid < n_free) {
             const uint32_t slot = sh.list_a[tid];
             Path &P = slot_path(slots, slot);
@@ -118,7 +119,7 @@ __global__ void __launch_bounds__(SORT_THREADS, GR_SORT_MIN_BLOCKS) k_trace_sort
                 xyz[3 * t + 2] = c.z;
             }
             const uint64_t t = (uint64_t)base + tid;
-            if (base != 0xFFFFFFFFu && t < R.n_tuples) {
+            if (claim && t < R.n_tuples) {
                 uint32_t pixel, sample;
                 tuple_coords(R, t, pixel, sample);
                 path_init<1, false, K>(P, S, B, pixel, sample, (uint32_t)t);

@@ -744,7 +744,11 @@ gr_status gr_create(gr_ctx **out, const gr_create_opts *opts) {
     ctx->device = dev;
     if (opts && opts->chunk_budget_bytes) ctx->chunk_budget = opts->chunk_budget_bytes;
     if (opts && opts->serve_budget_bytes) ctx->serve_budget = opts->serve_budget_bytes;
-    e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+    // The context stream sits above the lowest stream priority, which the request loop's
+    // bulk lane takes (gr_serve.cu): blocks of work queued here are scheduled first.
+    int prio_lo = 0, prio_hi = 0;
+    cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+    e = cudaStreamCreateWithPriority(&ctx->stream, cudaStreamNonBlocking, (prio_lo + prio_hi) / 2);
     if (e != cudaSuccess) {
         delete ctx;
         return fail(GR_ECUDA, "cudaStreamCreate failed: %s", cudaGetErrorString(e));
@@ -1008,8 +1012,8 @@ gr_status gr_scene_release(gr_ctx *ctx, uint64_t id) {
     auto it = ctx->scenes.find(id);
     if (it == ctx->scenes.end()) return fail(GR_ENOTFOUND, "unknown scene id %llu", (unsigned long long)id);
     if (it->second->users)
-        return fail(GR_EBUSY, "scene %llu is rendered by %u open frame stream(s)", (unsigned long long)id,
-                    it->second->users);
+        return fail(GR_EBUSY, "scene %llu is in use by %u open frame stream(s) or bulk render(s)",
+                    (unsigned long long)id, it->second->users);
     GR_CUDA(cudaSetDevice(ctx->device));
     GR_CUDA(cudaStreamSynchronize(ctx->stream));
     ResidentScene *rs = it->second;

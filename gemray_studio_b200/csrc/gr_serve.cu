@@ -15,7 +15,16 @@
 //     slices;
 //   * metric requests (pose sweeps) skip admission (they hold no film): a second
 //     thread runs them in arrival order on its own high-priority stream, beside the
-//     tick in flight, so a sweep neither waits for a tick nor holds one up.
+//     tick in flight, so a sweep neither waits for a tick nor holds one up;
+//   * bulk lane -- a render larger than one tick (and without a slice_spp) is not
+//     sliced: a third thread renders its whole sample range with the single-scene
+//     kernels on a stream of the lowest priority, with scratch of its own, while the
+//     ticks of the smaller requests run on the context stream, whose priority is
+//     higher: the GPU's block scheduler gives their blocks the SMs that the bulk
+//     launch's blocks free, so a small request no longer waits behind a large one's
+//     slices, and a large one runs its samples at single-scene speed.  Bulk renders
+//     run one at a time in admission order; cancellation takes effect before one
+//     starts or between its launches, and leaves a zero film (no samples done).
 // Slices fold in continue mode (fold_pixel): each slice carries the pixel's running
 // sum on from the film (and the Kahan compensation from a side buffer), and a request
 // starts on a zero film, so its film is one sequential per-pixel sum over all of its
@@ -34,6 +43,7 @@
 #include <vector>
 
 #include "gr_ctx.h"
+#include "gr_launch.cuh"
 
 using grh::fail;
 
@@ -79,6 +89,7 @@ struct Request {
     StreamBuffer film, comp;
     uint32_t issued = 0, done = 0, in_flight = 0;  // samples per pixel
     bool cancel = false;
+    bool bulk = false;  // rendered whole by the bulk lane, not in ticks
     Clock::time_point t_submit, t_admit, t_done;
 };
 
@@ -104,6 +115,10 @@ constexpr size_t kTicksInFlight = 1;
 // admissions map no memory until the live films pass it (~2,800 films of 384^2
 // pixels with Kahan compensation); growing the pool was measured at up to ~0.5 s.
 constexpr uint64_t kFilmPoolReserve = 4ull << 30;
+// Renders of more path-samples than one tick carries go to the bulk lane.
+constexpr uint64_t kBulkTuples = kTickTuples;
+// Per-tuple XYZ scratch of one bulk launch (chunks of whole pixels).
+constexpr size_t kBulkChunkBytes = 512ull << 20;
 
 struct Tick {
     cudaEvent_t ev = nullptr;
@@ -119,6 +134,10 @@ double ms_between(Clock::time_point a, Clock::time_point b) {
 struct ServeState {
     std::mutex mu;
     cudaStream_t metrics_stream = nullptr;  // metric sweeps, beside the ticks
+    cudaStream_t bulk_stream = nullptr;     // bulk renders, lowest priority
+    std::condition_variable cv_bulk;
+    std::deque<uint64_t> bulk_queue;        // admitted bulk renders, admission order
+    grh::DeviceBuffer bulk_xyz, bulk_park;  // the bulk lane's own scratch
     cudaMemPool_t film_pool = nullptr;      // request films (null: the device's default pool)
     std::condition_variable cv_work, cv_done, cv_metrics;
     std::unordered_map<uint64_t, Request *> reqs;
@@ -128,7 +147,7 @@ struct ServeState {
     uint64_t next_id = 1;
     uint64_t film_bytes = 0;      // films of admitted requests
     bool stop = false;
-    std::thread worker, metrics_worker;
+    std::thread worker, metrics_worker, bulk_worker;
 };
 
 namespace {
@@ -169,7 +188,95 @@ void admit(gr_ctx *ctx, ServeState &sv, uint64_t resident_bytes) {
         sv.film_bytes += q->film_bytes;
         q->state = GR_REQ_RUNNING;
         q->t_admit = Clock::now();
-        sv.running.push_back(q->id);
+        if (sv.bulk_stream && q->r.slice_spp == 0 && (uint64_t)q->r.spp * q->n_px > kBulkTuples) {
+            q->bulk = true;
+            sv.bulk_queue.push_back(q->id);
+            sv.cv_bulk.notify_one();
+        } else {
+            sv.running.push_back(q->id);
+        }
+    }
+}
+
+// The bulk lane: one admitted render at a time, its whole sample range traced chunk by
+// chunk with the single-scene kernels (the scene's chosen stage caps; never the sorted
+// kernel, whose blocks stay resident until its launch ends, nor the wavefront engine,
+// which uses the context's own pool) and each chunk's pixels folded in add mode onto the
+// zero film -- the film of one gr_render_resident call over the range, which is what
+// the sliced path produces too.  The scene is marked in use meanwhile, so it cannot be
+// released under the launches.
+void bulk_main(gr_ctx *ctx, ServeState *sv) {
+    cudaSetDevice(ctx->device);
+    for (;;) {
+        Request *q;
+        {
+            std::unique_lock<std::mutex> lk(sv->mu);
+            sv->cv_bulk.wait(lk, [&] { return sv->stop || !sv->bulk_queue.empty(); });
+            if (sv->bulk_queue.empty()) return;  // stopping, nothing left
+            q = sv->reqs[sv->bulk_queue.front()];
+            sv->bulk_queue.pop_front();
+            if (q->cancel) {
+                finish(*sv, q, GR_REQ_CANCELLED);
+                continue;
+            }
+            q->issued = q->in_flight = q->r.spp;
+        }
+        SceneConst S;
+        grd::SceneBuffers B;
+        StageCaps caps;
+        int mode = GR_KERNEL_AUTO;
+        ResidentScene *rs = nullptr;
+        {
+            std::lock_guard<std::mutex> lk(ctx->mu);
+            auto it = ctx->scenes.find(q->r.scene_id);
+            if (it != ctx->scenes.end()) {
+                rs = it->second;
+                rs->users++;
+                S = rs->S;
+                B = resident_buffers(rs);
+                caps = grh::scene_stage_caps(*rs);
+            }
+            if (ctx->kernel_mode != GR_KERNEL_SORTED && ctx->kernel_mode != GR_KERNEL_WAVEFRONT) mode = ctx->kernel_mode;
+        }
+        gr_status st = rs ? GR_OK : GR_ENOTFOUND;
+        const uint32_t spp = q->r.spp;
+        const uint64_t n_px = q->n_px;
+        const uint64_t chunk_px = std::max<uint64_t>(1, std::min<uint64_t>(n_px, kBulkChunkBytes / 12 / spp));
+        if (st == GR_OK) st = sv->bulk_xyz.reserve((size_t)chunk_px * spp * 12);
+        for (uint64_t first = 0; st == GR_OK && first < n_px; first += chunk_px) {
+            if (q->cancel) break;  // between launches
+            grd::LaunchRange R;
+            R.first_pixel = (uint32_t)first;
+            R.n_pixels = (uint32_t)std::min<uint64_t>(chunk_px, n_px - first);
+            R.sample_offset = q->r.sample_offset;
+            R.spp = spp;
+            R.n_tuples = (uint64_t)R.n_pixels * spp;
+            st = grh::launch_trace(ctx, S, B, R, (float *)sv->bulk_xyz.ptr, sv->bulk_stream, mode, &sv->bulk_park, caps);
+            if (st == GR_OK)
+                st = grh::launch_fold((const float *)sv->bulk_xyz.ptr, R.n_pixels, spp, R.first_pixel,
+                                      (float *)q->film.ptr, (S.flags & GR_FLAG_KAHAN_FILM) ? 1u : 0u, sv->bulk_stream);
+        }
+        if (st == GR_OK && q->cancel) {
+            // cancelled between launches: no partial pixels -- the film is zero again, as
+            // its samples_done (0) says
+            const size_t fb = (size_t)n_px * 3 * sizeof(float);
+            if (cudaMemsetAsync(q->film.ptr, 0, fb, sv->bulk_stream) != cudaSuccess) st = GR_ECUDA;
+        }
+        if (cudaStreamSynchronize(sv->bulk_stream) != cudaSuccess && st == GR_OK) st = GR_ECUDA;
+        if (rs) {
+            std::lock_guard<std::mutex> lk(ctx->mu);
+            rs->users--;
+        }
+        std::lock_guard<std::mutex> lk(sv->mu);
+        q->in_flight = 0;
+        if (st != GR_OK) {
+            finish(*sv, q, GR_REQ_FAILED, st);
+        } else if (q->cancel) {
+            finish(*sv, q, GR_REQ_CANCELLED);  // a cancelled bulk render keeps no samples (zero film)
+        } else {
+            q->done = spp;
+            finish(*sv, q, GR_REQ_DONE);
+        }
     }
 }
 
@@ -358,6 +465,7 @@ ServeState *serve_state(gr_ctx *ctx) {
         int lo = 0, hi = 0;  // the numerically lowest priority is the highest
         cudaDeviceGetStreamPriorityRange(&lo, &hi);
         cudaStreamCreateWithPriority(&ctx->serve->metrics_stream, cudaStreamNonBlocking, hi);
+        if (lo != hi) cudaStreamCreateWithPriority(&ctx->serve->bulk_stream, cudaStreamNonBlocking, lo);
         cudaMemPoolProps props{};
         props.allocType = cudaMemAllocationTypePinned;
         props.location.type = cudaMemLocationTypeDevice;
@@ -375,6 +483,7 @@ ServeState *serve_state(gr_ctx *ctx) {
         cudaGetLastError();  // a pool that could not be set up leaves films on the default pool
         ctx->serve->worker = std::thread(worker_main, ctx, ctx->serve);
         ctx->serve->metrics_worker = std::thread(metrics_main, ctx, ctx->serve);
+        if (ctx->serve->bulk_stream) ctx->serve->bulk_worker = std::thread(bulk_main, ctx, ctx->serve);
     }
     return ctx->serve;
 }
@@ -406,8 +515,10 @@ void serve_shutdown(gr_ctx *ctx) {
     }
     sv->cv_work.notify_all();
     sv->cv_metrics.notify_all();
+    sv->cv_bulk.notify_all();
     if (sv->worker.joinable()) sv->worker.join();
     if (sv->metrics_worker.joinable()) sv->metrics_worker.join();
+    if (sv->bulk_worker.joinable()) sv->bulk_worker.join();
     cudaSetDevice(ctx->device);
     for (auto &kv : sv->reqs) {
         kv.second->film.release(ctx->stream);
@@ -417,6 +528,9 @@ void serve_shutdown(gr_ctx *ctx) {
     cudaStreamSynchronize(ctx->stream);  // stream-ordered frees above complete
     if (sv->film_pool) cudaMemPoolDestroy(sv->film_pool);
     if (sv->metrics_stream) cudaStreamDestroy(sv->metrics_stream);
+    if (sv->bulk_stream) cudaStreamDestroy(sv->bulk_stream);
+    sv->bulk_xyz.release();
+    sv->bulk_park.release();
     delete sv;
     ctx->serve = nullptr;
 }

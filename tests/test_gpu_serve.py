@@ -158,3 +158,45 @@ def test_admission_by_memory_budget(engine_lib):
     finally:
         srv.close()
         r.close()
+
+
+def test_large_requests_render_whole_beside_small_ones(engine_lib):
+    """Renders of more path-samples than one tick carries (~8.4 M, no slice_spp) go to
+    the bulk lane: rendered whole with the single-scene kernels on a low-priority stream
+    while the small requests' ticks run beside them.  Every film -- bulk (a Kahan scene
+    among them) or ticked -- is bit-identical to one gr_render_resident call over its
+    range on a zero film; a bulk render cancelled before it starts ends with no samples
+    and a zero film."""
+    srv = RenderServer()
+    try:
+        small = _scenes()
+        rng = np.random.default_rng(4)
+        big = [S.Scene(width=128, height=128, planes=S.round_brilliant_57(), material=S.builtin_material("Diamond"),
+                       cam=S.camera(0.35, 0.28, 5.0, 18.0), max_bounces=32, env_mode=abi.GR_ENV_LATLONG,
+                       latlong=S.gaussian_blob_latlong(256, 128, seed=2)),
+               S.Scene(width=96, height=96, planes=S.random_polyhedron(rng), material=S.builtin_material("Zircon"),
+                       cam=S.camera(0.3, 0.4, 4.0, 30.0), max_bounces=24, env_mode=abi.GR_ENV_STUDIO,
+                       flags=abi.GR_FLAG_KAHAN_FILM)]
+        big_ids = [srv.upload(sc) for sc in big]
+        small_ids = [srv.upload(sc) for sc in small]
+        jobs = [(big_ids[0], (128, 128), 5, 600), (big_ids[1], (96, 96), 0, 1000)]
+        assert all(w * h * spp > (8 << 20) for _, (w, h), _, spp in jobs)
+        rids = [srv.submit_render(sid, off, spp) for sid, _, off, spp in jobs]
+        cancelled = srv.submit_render(big_ids[0], 0, 600)
+        srv.cancel(cancelled)
+        shapes = [(48, 40), (32, 32), (24, 30)]
+        srids = [srv.submit_render(small_ids[k], 3 * k, 24 + 8 * k) for k in range(3)]
+        for r in rids + srids:
+            assert srv.wait(r).state == "done"
+        st = srv.wait(cancelled)
+        assert st.state == "cancelled" and st.samples_done == 0
+        assert not srv.film(cancelled).any()
+        for r, (sid, shape, off, spp) in zip(rids, jobs):
+            assert np.array_equal(srv.film(r).view(np.uint32), _resident(srv, sid, shape, off, spp).view(np.uint32))
+        for k, r in enumerate(srids):
+            ref = _resident(srv, small_ids[k], shapes[k], 3 * k, 24 + 8 * k)
+            assert np.array_equal(srv.film(r).view(np.uint32), ref.view(np.uint32))
+        for r in rids + srids + [cancelled]:
+            srv.release(r)
+    finally:
+        srv.close()

@@ -744,8 +744,9 @@ gr_status gr_create(gr_ctx **out, const gr_create_opts *opts) {
     ctx->device = dev;
     if (opts && opts->chunk_budget_bytes) ctx->chunk_budget = opts->chunk_budget_bytes;
     if (opts && opts->serve_budget_bytes) ctx->serve_budget = opts->serve_budget_bytes;
-    // The context stream sits above the lowest stream priority, which the request loop's
-    // bulk lane takes (gr_serve.cu): blocks of work queued here are scheduled first.
+    // The context stream sits between the stream priorities: the request loop's bulk
+    // lane (gr_serve.cu) takes the highest, so its blocks are scheduled before the
+    // ticks queued here.
     int prio_lo = 0, prio_hi = 0;
     cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
     e = cudaStreamCreateWithPriority(&ctx->stream, cudaStreamNonBlocking, (prio_lo + prio_hi) / 2);

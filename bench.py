@@ -45,7 +45,7 @@ from pathlib import Path
 
 ROOT = Path(__file__).resolve().parent
 HBM_FALLBACK_GBS = 6650.0  # B200 copy bandwidth, used when the per-device measurement is absent
-KERNELS = ("auto", "staged", "plain", "sorted", "regen", "wavefront")  # GR_KERNEL_<NAME>
+KERNELS = ("auto", "staged", "plain", "sorted")  # GR_KERNEL_<NAME>
 sys.path.insert(0, str(ROOT))
 
 import numpy as np  # noqa: E402
@@ -259,14 +259,13 @@ def run_reference(args):
 
 
 TRANSPORT_LABELS = {"staged": "k_trace_stage1 + k_trace_stage2 x2 (staged transport)", "plain": "k_trace_plain",
-                    "sorted": "k_trace_sorted (block-sorted transport)",
-                    "regen": "k_trace_regen", "wavefront": "k_wf_* (wavefront engine)"}
+                    "sorted": "k_trace_sorted (block-sorted transport)"}
 
 
 def transport_kernel(kernel_arg: str, trace_launches: int, fold_launches: int) -> str:
-    """Which transport ran: regen / wavefront as asked; otherwise staged when every
-    chunk took the three staged launches, plain when one."""
-    if kernel_arg in ("regen", "wavefront", "sorted"):
+    """Which transport ran: sorted as asked; otherwise staged when every chunk took the
+    three staged launches, plain when one."""
+    if kernel_arg == "sorted":
         return kernel_arg
     return "staged" if trace_launches >= 3 * max(1, fold_launches) else "plain"
 

@@ -80,12 +80,8 @@ struct gr_ctx {
     int sm_count = 0;
     grh::DeviceBuffer xyz, film, planes, map, ext, counter, rgba, metrics;
     int kernel_mode = GR_KERNEL_AUTO;
-    // wavefront engine pool (gr_wavefront.cuh)
-    uint32_t wave_cap = 1u << 18;
-    grh::DeviceBuffer wf_pool, wf_events, wf_queues, wf_cnt;
     // staged kernels' park buffer (count word, then parked path records)
     grh::DeviceBuffer park;
-    uint32_t *wf_done_host = nullptr;
     // Optional per-launch timing of the trace and fold kernels (CUDA events on the
     // launch stream); read back by gr_timing_read.
     bool timing = false;

@@ -23,7 +23,6 @@
 #include "gr_ctx.h"
 #include "gr_host.h"
 #include "gr_kernels.cuh"
-#include "gr_wavefront.cuh"
 
 using grd::SceneConst;
 
@@ -360,64 +359,6 @@ gr_status upload_scene(gr_ctx *ctx, const gr_scene *sc, const SceneConst &S, grd
     return GR_OK;
 }
 
-// Wavefront engine over tuples [0, R.n_tuples) of one chunk (gr_wavefront.cuh).
-gr_status launch_wavefront(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuffers &B, const grd::LaunchRange &R,
-                           float *xyz, cudaStream_t stream) {
-    uint64_t cap64 = R.n_tuples < (uint64_t)ctx->wave_cap ? R.n_tuples : (uint64_t)ctx->wave_cap;
-    uint32_t cap = (uint32_t)((cap64 + 31) & ~31ull);
-    gr_status st;
-    if ((st = ctx->wf_pool.reserve((size_t)cap * sizeof(grd::Path))) != GR_OK) return st;
-    if ((st = ctx->wf_events.reserve((size_t)cap * sizeof(grd::Event))) != GR_OK) return st;
-    if ((st = ctx->wf_queues.reserve((size_t)cap * 6 * sizeof(uint32_t))) != GR_OK) return st;
-    if ((st = ctx->wf_cnt.reserve(grd::W_NCOUNT * sizeof(uint32_t) + 2 * sizeof(unsigned long long))) != GR_OK) return st;
-    if (!ctx->wf_done_host) {
-        void *h = nullptr;
-        GR_CUDA(cudaHostAlloc(&h, sizeof(uint32_t), cudaHostAllocDefault));
-        ctx->wf_done_host = (uint32_t *)h;
-    }
-    grd::WaveBuffers W;
-    W.pool = (grd::Path *)ctx->wf_pool.ptr;
-    W.events = (grd::Event *)ctx->wf_events.ptr;
-    uint32_t *q = (uint32_t *)ctx->wf_queues.ptr;
-    W.q_active0 = q;
-    W.q_active1 = q + cap;
-    W.q_reflect = q + 2 * (size_t)cap;
-    W.q_refract = q + 3 * (size_t)cap;
-    W.q_finish = q + 4 * (size_t)cap;
-    W.q_free = q + 5 * (size_t)cap;
-    W.cnt = (uint32_t *)ctx->wf_cnt.ptr;
-    W.tuples = (unsigned long long *)((char *)ctx->wf_cnt.ptr + grd::W_NCOUNT * sizeof(uint32_t));
-    W.cap = cap;
-    const unsigned T = 256;
-    uint64_t want = (cap + T - 1) / T;
-    const unsigned grid = (unsigned)(want < (uint64_t)ctx->sm_count * 8 ? want : (uint64_t)ctx->sm_count * 8);
-    const size_t smem = grd::planes_smem_bytes(S.n_planes);
-    grd::k_wf_reset<<<grid, T, 0, stream>>>(W);
-    const int BATCH = 4;
-    uint32_t it = 0;
-    for (uint64_t guard = 0;; ++guard) {
-        for (int j = 0; j < BATCH; ++j, ++it) {
-            const uint32_t cur = it & 1u;
-            grd::k_wf_regen_prep<<<1, 1, 0, stream>>>(W, R.n_tuples);
-            grd::k_wf_regen<<<grid, T, 0, stream>>>(S, B, R, W, cur);
-            grd::k_wf_extend<<<grid, T, smem, stream>>>(S, B, W, cur);
-            grd::k_wf_event<false><<<grid, T, 0, stream>>>(S, W, cur ^ 1u);
-            grd::k_wf_event<true><<<grid, T, 0, stream>>>(S, W, cur ^ 1u);
-            grd::k_wf_finish<<<grid, T, 0, stream>>>(S, B, W, xyz);
-            grd::k_wf_bookkeep<<<1, 1, 0, stream>>>(W, cur, R.n_tuples);
-        }
-        GR_CUDA(cudaGetLastError());
-        GR_CUDA(cudaMemcpyAsync(ctx->wf_done_host, W.cnt + grd::W_DONE, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
-        GR_CUDA(cudaStreamSynchronize(stream));
-        if (*ctx->wf_done_host) break;
-        // Every path ends within max_bounces iterations of its start and a new batch
-        // of tuples starts every iteration, so this bound is never reached by a
-        // correct engine; it turns a logic error into an error return, not a hang.
-        if (guard > (R.n_tuples / 32 + 4) * ((uint64_t)S.max_bounces + 2))
-            return fail(GR_ETIMEOUT, "wavefront did not drain");
-    }
-    return GR_OK;
-}
 
 int resolve_kernel(int mode, uint64_t n_tuples) {
     if (mode != GR_KERNEL_AUTO) return mode;
@@ -524,14 +465,7 @@ gr_status launch_trace(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuffers
         GR_CUDA(cudaGetLastError());
         return GR_OK;
     }
-    if (mode == GR_KERNEL_REGEN) {
-        const uint64_t warps = (R.n_tuples + grd::REGEN_TUPLES - 1) / grd::REGEN_TUPLES;
-        const uint64_t blocks = (warps * 32 + grd::TRACE_THREADS - 1) / grd::TRACE_THREADS;
-        grd::k_trace_regen<<<(unsigned)blocks, grd::TRACE_THREADS, smem, stream>>>(S, B, R, xyz);
-        GR_CUDA(cudaGetLastError());
-        return GR_OK;
-    }
-    return launch_wavefront(ctx, S, B, R, xyz, stream);
+    return fail(GR_EINVAL, "unknown kernel mode %d", mode);
 }
 
 gr_status launch_fold(const float *xyz, uint32_t n_pixels, uint32_t spp, uint32_t first_pixel, float *film,
@@ -791,11 +725,6 @@ gr_status gr_destroy(gr_ctx *ctx) {
         ctx->batch_graphs.clear();
         ctx->batch_tables.release();
         ctx->batch_park.release();
-        ctx->wf_pool.release();
-        ctx->wf_events.release();
-        ctx->wf_queues.release();
-        ctx->wf_cnt.release();
-        if (ctx->wf_done_host) cudaFreeHost(ctx->wf_done_host);
         for (auto &p : ctx->trace_ev) { cudaEventDestroy(p.first); cudaEventDestroy(p.second); }
         for (auto &p : ctx->fold_ev) { cudaEventDestroy(p.first); cudaEventDestroy(p.second); }
         for (auto &kv : ctx->accum_tune) grh::tune_release(kv.second);
@@ -1258,7 +1187,8 @@ gr_status gr_set_kernel(gr_ctx *ctx, uint32_t kernel) {
         kernel != GR_KERNEL_STAGED && kernel != GR_KERNEL_AUTO && kernel != GR_KERNEL_SORTED)
         return fail(GR_EINVAL, "unknown kernel %u", kernel);
     std::lock_guard<std::mutex> lk(ctx->mu);
-    ctx->kernel_mode = (int)kernel;
+    // the retired wavefront and regeneration schedules run AUTO's choice
+    ctx->kernel_mode = (kernel == GR_KERNEL_WAVEFRONT || kernel == GR_KERNEL_REGEN) ? (int)GR_KERNEL_AUTO : (int)kernel;
     return GR_OK;
 }
 

@@ -202,8 +202,8 @@ void admit(gr_ctx *ctx, ServeState &sv, uint64_t resident_bytes) {
 
 // The bulk lane: one admitted render at a time, its whole sample range traced chunk by
 // chunk with the single-scene kernels (the scene's chosen stage caps; never the sorted
-// kernel, whose blocks stay resident until its launch ends, nor the wavefront engine,
-// which uses the context's own pool) and each chunk's pixels folded in add mode onto the
+// kernel, whose blocks stay resident until its launch ends) and each chunk's pixels
+// folded in add mode onto the
 // zero film -- the film of one gr_render_resident call over the range, which is what
 // the sliced path produces too.  The scene is marked in use meanwhile, so it cannot be
 // released under the launches.
@@ -238,7 +238,7 @@ void bulk_main(gr_ctx *ctx, ServeState *sv) {
                 B = resident_buffers(rs);
                 caps = grh::scene_stage_caps(*rs);
             }
-            if (ctx->kernel_mode != GR_KERNEL_SORTED && ctx->kernel_mode != GR_KERNEL_WAVEFRONT) mode = ctx->kernel_mode;
+            if (ctx->kernel_mode != GR_KERNEL_SORTED) mode = ctx->kernel_mode;
         }
         gr_status st = rs ? GR_OK : GR_ENOTFOUND;
         const uint32_t spp = q->r.spp;

@@ -11,11 +11,12 @@
 //   step_refract the refract channel updates (chromatic termination, walk-off)
 //   path_finish  escape radiance, spectral MIS, CIE integration, white balance
 //
-// The plain kernel runs the stages back to back in one thread.  The wavefront engine
-// (gr_wavefront.cuh) keeps records in a device pool and runs each stage as its own
-// kernel over a compacted queue, so warps execute one event type at a time.
-// `Path` is a record of float4 rows: in the plain kernel it lives in the thread's
-// local memory, in the wavefront pool in global memory -- the same code serves both.
+// The plain and staged kernels run the stages back to back in one thread; the sorted
+// kernel (gr_sorted.cuh) keeps records in shared-memory slots and lets any thread of
+// the block run any slot's next stage, grouped by event kind.  `Path` is a record of
+// float4 rows: in the plain kernel it lives in the thread's local memory, in the
+// sorted kernel in shared memory, in the staged kernels' park buffers in global
+// memory -- the same code serves all of them.
 #pragma once
 
 #include <cstddef>
@@ -71,7 +72,7 @@ constexpr uint32_t BOUNCE_SHIFT = 8;
 // the run-time material and environment checks it settles are folded away, so a clear
 // isotropic stone's kernel carries none of the birefringence, walk-off, absorption or
 // other-environment code.  K = K_ANY keeps every check at run time (batched launches,
-// the wavefront and regeneration schedules, the instrumented variants).
+// the instrumented variants).
 constexpr int K_ANY = 0;
 constexpr int K_ISO = 1;        // S.anisotropic == 0 (and not biaxial)
 constexpr int K_CLEAR = 2;      // S.absorbing == 0: no absorption data at all

@@ -658,11 +658,10 @@ gr_status gr_denoise_tonemap_device(gr_ctx *ctx, const float *film, uint32_t sam
 /* ---- engine controls ---------------------------------------------------------- */
 
 /* Transport kernel selection for single-scene renders.  PLAIN: one thread per
- * (pixel, sample) tuple, the reference kernel's launch shape.  WAVEFRONT: a device pool of path
- * records advanced by per-stage kernels over compacted event queues (about 3x slower
- * on B200: each bounce moves ~1 KB of record traffic).  REGEN: path regeneration,
- * each warp owns a run of consecutive tuples and lanes whose path has ended start the
- * next ones while the rest of the warp keeps bouncing.  STAGED: PLAIN's launch shape
+ * (pixel, sample) tuple, the reference kernel's launch shape.  WAVEFRONT and REGEN are
+ * retired schedules (a global-queue wavefront engine, ~0.3x, and per-warp path
+ * regeneration, 0.91x of STAGED on B200): both values are accepted and run AUTO's
+ * choice.  STAGED: PLAIN's launch shape
  * with paths capped at 12 bounces; the ones still alive are parked and resumed, packed
  * densely, by a second kernel (capped at 20, then a third), so warps stop waiting on
  * a few long paths (+24-28% from 4 M tuples per launch up, e.g. the c2 frame).  AUTO

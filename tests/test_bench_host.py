@@ -16,15 +16,15 @@ def test_transport_resolution_from_launch_counts():
     assert bench.transport_kernel("staged", 3, 1) == "staged"
     assert bench.transport_kernel("auto", 4, 4) == "plain"     # small launches under AUTO
     assert bench.transport_kernel("plain", 9, 9) == "plain"
-    assert bench.transport_kernel("regen", 9, 9) == "regen"
-    assert set(bench.TRANSPORT_LABELS) >= {"staged", "plain", "regen", "wavefront"}
+    assert bench.transport_kernel("sorted", 9, 9) == "sorted"
+    assert set(bench.TRANSPORT_LABELS) >= {"staged", "plain", "sorted"}
 
 
 def test_traffic_scales_the_committed_per_tuple_figures():
     for kernel in ("staged", "plain"):
         per_tuple = json.loads((ROOT / "profiles" / f"k_trace_{kernel}_traffic.json").read_text())["dram_bytes_per_tuple"]
         assert bench.traffic_per_launch(2e6, kernel) == per_tuple * 2e6
-    assert bench.traffic_per_launch(2e6, "wavefront") is None   # no capture committed
+    assert bench.traffic_per_launch(2e6, "sorted") is None   # no capture committed
 
 
 def test_hbm_view_names_its_peak():

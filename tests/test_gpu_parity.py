@@ -106,8 +106,8 @@ def test_film_is_deterministic_across_kernels_and_chunks(engine_lib):
     from gemray_studio_b200 import GpuFrameRenderer
     sc = srb_scene("Sapphire", width=40, height=30, max_bounces=24)
     outs = []
-    for kernel, budget in ((abi.GR_KERNEL_WAVEFRONT, 0), (abi.GR_KERNEL_PLAIN, 0), (abi.GR_KERNEL_WAVEFRONT, 4096 * 12),
-                           (abi.GR_KERNEL_PLAIN, 1000 * 12), (abi.GR_KERNEL_REGEN, 0), (abi.GR_KERNEL_REGEN, 777 * 12),
+    for kernel, budget in ((abi.GR_KERNEL_SORTED, 0), (abi.GR_KERNEL_PLAIN, 0), (abi.GR_KERNEL_SORTED, 4096 * 12),
+                           (abi.GR_KERNEL_PLAIN, 1000 * 12), (abi.GR_KERNEL_REGEN, 0), (abi.GR_KERNEL_WAVEFRONT, 777 * 12),
                            (abi.GR_KERNEL_STAGED, 0), (abi.GR_KERNEL_STAGED, 999 * 12)):
         r = GpuFrameRenderer(chunk_budget_bytes=budget, kernel=kernel)
         for _ in range(2):

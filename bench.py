@@ -751,6 +751,8 @@ def serve_measure(rate: float, duration: float, serve_side=(128, 384), serve_spp
                         if not q.is_metrics)
     lat = np.array([s.latency_ms for s in stats])
     is_m = np.array([q.is_metrics for q in reqs])
+    size = np.array([0 if q.is_metrics else stones[q.stone].scene.width * stones[q.stone].scene.height * q.spp
+                     for q in reqs])
     # serial unbatched server: each request alone, in arrival order, one at a time
     lib, ctx = srv.lib, srv.ctx
     stream = torch.cuda.ExternalStream(lib.gr_stream(ctx))
@@ -803,12 +805,19 @@ def serve_measure(rate: float, duration: float, serve_side=(128, 384), serve_spp
         return {"p50": float(np.percentile(x, 50)), "p99": float(np.percentile(x, 99)), "max": float(x.max())} \
             if x.size else None
 
+    classes = {}
+    for name, lo, hi in (("renders <= 2M samples", 1, 2 << 20), ("renders 2M-8M", (2 << 20) + 1, 8 << 20),
+                         ("renders > 8M", (8 << 20) + 1, 1 << 62)):
+        sel = (size >= lo) & (size <= hi)
+        classes[name] = {"n": int(sel.sum()), "served": pct(lat[sel]), "serial_replay": pct(lat_rep[sel])}
+
     out = {
         "workload": f"c5: Poisson arrivals {rate}/s for {duration} s ({len(reqs)} requests, {int(is_m.sum())} "
                     f"metric-only 64-tilt sweeps) over 32 random stones, films {serve_side[0]}-{serve_side[1]} px "
                     f"square, spp {serve_spp[0]}-{serve_spp[1]}",
         "value": render_tuples / (t_end - t0), "unit": "path-samples/s", "render_path_samples": render_tuples,
         "latency_ms": pct(lat), "latency_ms_renders": pct(lat[~is_m]), "latency_ms_metrics": pct(lat[is_m]),
+        "latency_ms_by_size": classes,
         "serial_replay": {"value": render_tuples / rep_span, **pct(lat_rep),
                           "how": "the same arrival schedule replayed in real time through a serial server: each "
                                  "request rendered alone with gr_render_resident in arrival order"},
@@ -835,7 +844,7 @@ def run_serve(args):
         "warmup": 1, "ms_per_step": args.duration * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": m["workload"], "render_path_samples": m["render_path_samples"]},
-        **{k: m[k] for k in ("latency_ms", "latency_ms_renders", "latency_ms_metrics", "serial_replay",
+        **{k: m[k] for k in ("latency_ms", "latency_ms_renders", "latency_ms_metrics", "latency_ms_by_size", "serial_replay",
                              "serial_model", "wall_clock", "matched_error", "clocks")},
     }), flush=True)
 

@@ -117,8 +117,16 @@ constexpr size_t kTicksInFlight = 1;
 // admissions map no memory until the live films pass it (~2,800 films of 384^2
 // pixels with Kahan compensation); growing the pool was measured at up to ~0.5 s.
 constexpr uint64_t kFilmPoolReserve = 4ull << 30;
-// Renders of more path-samples than one tick carries go to the bulk lane.
-constexpr uint64_t kBulkTuples = kTickTuples;
+// Renders of more than this many path-samples go to the bulk lane.
+#ifndef GR_SERVE_BULK_MTUPLES
+#define GR_SERVE_BULK_MTUPLES GR_SERVE_TICK_MTUPLES
+#endif
+constexpr uint64_t kBulkTuples = (uint64_t)GR_SERVE_BULK_MTUPLES << 20;
+// 1: the bulk lane's stream takes the highest priority (the ticks fill in around it);
+// 0: the lowest (the ticks go first).
+#ifndef GR_SERVE_BULK_HIGH
+#define GR_SERVE_BULK_HIGH 1
+#endif
 // Per-tuple XYZ scratch of one bulk launch (chunks of whole pixels).
 constexpr size_t kBulkChunkBytes = 512ull << 20;
 
@@ -467,7 +475,8 @@ ServeState *serve_state(gr_ctx *ctx) {
         int lo = 0, hi = 0;  // the numerically lowest priority is the highest
         cudaDeviceGetStreamPriorityRange(&lo, &hi);
         cudaStreamCreateWithPriority(&ctx->serve->metrics_stream, cudaStreamNonBlocking, hi);
-        if (lo != hi) cudaStreamCreateWithPriority(&ctx->serve->bulk_stream, cudaStreamNonBlocking, hi);
+        if (lo != hi)
+            cudaStreamCreateWithPriority(&ctx->serve->bulk_stream, cudaStreamNonBlocking, GR_SERVE_BULK_HIGH ? hi : lo);
         cudaMemPoolProps props{};
         props.allocType = cudaMemAllocationTypePinned;
         props.location.type = cudaMemLocationTypeDevice;

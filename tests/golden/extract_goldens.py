@@ -98,4 +98,6 @@ def main(root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: extract_goldens.py <gemray-studio checkout root>")
+    main(sys.argv[1])

@@ -423,6 +423,18 @@ def run_engine(args):
                                     C.c_void_p(stream_ptr))
         assert st == abi.GR_OK, lib.gr_last_error_string()
 
+    # untimed tuning calls: the scene's schedule tuner times its six candidate schedules
+    # (stage caps x blocks per SM) on whole calls, after one call that carries the
+    # one-time costs; then the warm-up proper
+    tune_calls = 0
+    tc1, tc2, tcb = C.c_uint32(), C.c_uint32(), C.c_uint32()
+    while args.kernel in ("auto", "staged") and tune_calls < 12:
+        assert lib.gr_scene_schedule(ctx, sid.value, C.byref(tc1), C.byref(tc2), C.byref(tcb)) == abi.GR_OK
+        if tc1.value:
+            break
+        step(args.warmup + args.steps + tune_calls)
+        torch.cuda.synchronize()
+        tune_calls += 1
     for i in range(args.warmup):
         step(i)
     torch.cuda.synchronize()
@@ -442,8 +454,8 @@ def run_engine(args):
         torch.cuda.synchronize()
         barrier(world)
     step_ms = sum(a.elapsed_time(b) for a, b in evs)
-    cap1, cap2 = C.c_uint32(), C.c_uint32()  # the scene's stage caps (chosen during the warm-up calls)
-    assert lib.gr_scene_stage_caps(ctx, sid.value, C.byref(cap1), C.byref(cap2)) == abi.GR_OK
+    cap1, cap2, blocks = C.c_uint32(), C.c_uint32(), C.c_uint32()  # the scene's schedule (chosen while tuning)
+    assert lib.gr_scene_schedule(ctx, sid.value, C.byref(cap1), C.byref(cap2), C.byref(blocks)) == abi.GR_OK
     tr, fo, ntr, nfo = C.c_double(), C.c_double(), C.c_uint64(), C.c_uint64()
     lib.gr_timing_read(ctx, C.byref(tr), C.byref(fo), C.byref(ntr), C.byref(nfo))
     lib.gr_timing_enable(ctx, 0)
@@ -456,7 +468,7 @@ def run_engine(args):
     d2h = n_px * 12
     if world == 1:
         host_acc = np.zeros((n_px, 3), np.float32)
-        for i in range(args.warmup):  # warm (the stone's stage-cap trials run here, untimed)
+        for i in range(max(args.warmup, 9)):  # warm (the stone's schedule trials run here, untimed)
             r.accumulate(sc, base + i * spp, spp, host_acc)
         e_evs = []
         for i in range(args.steps):
@@ -486,7 +498,7 @@ def run_engine(args):
                 if rank == 0:
                     host_film.copy_(film_e, non_blocking=True)
 
-        for i in range(args.warmup):
+        for i in range(max(args.warmup, 9)):  # the stone's schedule trials run here, untimed
             e2e_step(i)
         torch.cuda.synchronize()
         barrier(world)
@@ -543,7 +555,8 @@ def run_engine(args):
                          "sfu_ops_per_sample": model.sfu / max(1, model.paths),
                          "kernel_ms_per_step": tr.value / frames, "fold_ms_per_step": fo.value / frames,
                          "launches_per_step": (ntr.value + nfo.value) / frames,
-                         "stage_caps": [cap1.value, cap2.value]},
+                         "stage_caps": [cap1.value, cap2.value], "blocks_per_sm": blocks.value,
+                         "tuning_calls": tune_calls},
             "events_per_sample": {k: v / max(1, tallies["paths"]) for k, v in tallies.items() if k != "paths"},
             "metrics_16_tilts": {"ms": metrics_ms, "how": "gr_optical_metrics, one device batch, host wall clock",
                                  "brilliance_pct": [round(float(v), 3) for v in mvals[:, 0]],
@@ -619,8 +632,8 @@ def batch_measure(scale: float, steps: int, warmup: int, n_stones: int = 64) -> 
                                                     for k, st in enumerate(stones)])
         assert lib.gr_render_batch(ctx, items, len(stones), abi.GR_BATCH_GRAPH, None) == abi.GR_OK
 
-    def timed(fn, base):
-        for i in range(warmup):
+    def timed(fn, base, tune=0):
+        for i in range(max(warmup, tune)):
             fn(base + i)
         torch.cuda.synchronize()
         evs = []
@@ -636,7 +649,7 @@ def batch_measure(scale: float, steps: int, warmup: int, n_stones: int = 64) -> 
 
     lib.gr_timing_enable(ctx, 1)
     with ClockSampler(0) as clocks:
-        ms_serial = timed(serial, 0)
+        ms_serial = timed(serial, 0, tune=8)  # each stone's schedule trials run in these untimed calls
         ms_batch = timed(batched, 1000)
         # the same serial renders with the plain one-thread-per-tuple kernel
         assert lib.gr_set_kernel(ctx, abi.GR_KERNEL_PLAIN) == abi.GR_OK

@@ -294,6 +294,8 @@ EXPORTS = [
                                  C.POINTER(C.c_uint64)]),
     ("gr_set_kernel", C.c_int, [_ctx_p, C.c_uint32]),
     ("gr_scene_stage_caps", C.c_int, [_ctx_p, C.c_uint64, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    ("gr_scene_schedule", C.c_int, [_ctx_p, C.c_uint64, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                    C.POINTER(C.c_uint32)]),
     ("gr_synchronize", C.c_int, [_ctx_p]),
     ("gr_stream", C.c_void_p, [_ctx_p]),
     ("gr_camera_new", C.c_int, [C.c_float, C.c_float, C.c_float, C.c_float, C.POINTER(gr_camera)]),

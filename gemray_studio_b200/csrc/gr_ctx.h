@@ -27,22 +27,31 @@ gr_status fail(gr_status st, const char *fmt, ...);
         if (e_ != cudaSuccess) return grh::fail(GR_ECUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
     } while (0)
 
-// Bounce caps of the staged kernels' first two stages; {0, 0} = the built-in pair.
+// Bounce caps of the staged kernels' first two stages ({0, 0} = the built-in pair) and
+// the resident blocks per SM their register allocation targets (0 = the built-in
+// GR_TRACE_MIN_BLOCKS): a staged schedule.
 struct StageCaps {
     uint32_t first = 0, second = 0;
+    uint32_t blocks = 0;
 };
+// Blocks-per-SM targets the staged single-scene kernels are built for: [0] is the
+// built-in one.  Measured on B200 (c2 / c3 frames): 10 blocks (48 registers) 2.3%
+// faster than 9 (56) on both, 7 and 8 slower.
+constexpr uint32_t kScheduleBlocks[2] = {GR_TRACE_MIN_BLOCKS, 10};
 
-// The stage caps a resident scene's staged renders use.  Every cap pair gives the same
-// films, but the fastest depends on the stone's path lengths, so from the scene's
-// second staged gr_render_resident call on, one call with each candidate pair is timed
-// on the device (the whole call: its chunks cover different parts of the image) and
-// the pair with the least time per tuple is kept (gr_host.cu, kStageCapCandidates).
+// The staged schedule (stage caps and blocks per SM) a stone's staged renders use.
+// Every schedule gives the same films, but the fastest depends on the stone's path
+// lengths and register pressure, so from the stone's second staged call on, one call
+// with each candidate schedule is timed on the device (the whole call: its chunks cover
+// different parts of the image) and the schedule with the least time per tuple is kept
+// (gr_host.cu, kScheduleCandidates).
 struct StageCapTune {
-    static constexpr int kCandidates = 2;
+    static constexpr int kCandidates = 6;
     int best = -1;              // chosen candidate, -1 while measuring
     uint32_t staged_calls = 0;  // staged calls seen
     bool issued[kCandidates] = {};
-    float ms_per_mtuple[kCandidates] = {3.0e38f, 3.0e38f};  // unmeasured: never chosen over a measured one
+    float ms_per_mtuple[kCandidates] = {3.0e38f, 3.0e38f, 3.0e38f, 3.0e38f, 3.0e38f,
+                                        3.0e38f};  // unmeasured: never chosen over a measured one
     struct Trial {
         cudaEvent_t start = nullptr, stop = nullptr;
         int candidate = 0;
@@ -164,6 +173,7 @@ struct StagedLaunch {
     unsigned int *counts;
     uint64_t cap1, cap2;
     uint32_t cap_first, cap_second;
+    uint32_t blocks;  // kScheduleBlocks entry, 0 = the built-in one
 };
 // The plain kernel (st == NULL) or the three staged launches of scene class K
 // (gr_single_clear.cu / gr_single_general.cu).

@@ -444,7 +444,7 @@ gr_status launch_trace(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuffers
         grd::Path *park2 = park1 + cap1;
         GR_CUDA(cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned int), stream));
         if (!extras) {
-            const StagedLaunch sl{park1, park2, counts, cap1, cap2, caps.first, caps.second};
+            const StagedLaunch sl{park1, park2, counts, cap1, cap2, caps.first, caps.second, caps.blocks};
             return clear ? launch_single_clear(K, S, B, R, xyz, stream, &sl)
                          : launch_single_general(K, S, B, R, xyz, stream, &sl);
         }
@@ -539,10 +539,13 @@ gr_status prepare(gr_ctx *ctx, const gr_scene *sc, SceneConst &S, grd::SceneBuff
     return upload_scene(ctx, sc, S, B);
 }
 
-// Stage-cap pairs a resident scene chooses between (StageCapTune): the pair measured
-// best on the c2 brilliant (long, TIR-trapped diamond paths) and the one measured best
-// on the c3 emerald (n ~ 1.6, shorter paths; 3.9% faster there).
-constexpr StageCaps kStageCapCandidates[StageCapTune::kCandidates] = {{12, 20}, {8, 16}};
+// Staged schedules a stone chooses between (StageCapTune): the cap pair measured best on
+// the c2 brilliant (long, TIR-trapped diamond paths), the one measured best on the c3
+// emerald (n ~ 1.6, shorter paths; 3.9% faster there) and a longer pair for stones
+// whose paths run longer still, each at both blocks-per-SM targets.
+constexpr StageCaps kStageCapCandidates[StageCapTune::kCandidates] = {
+    {12, 20, kScheduleBlocks[0]}, {8, 16, kScheduleBlocks[0]}, {12, 20, kScheduleBlocks[1]},
+    {8, 16, kScheduleBlocks[1]},  {16, 28, kScheduleBlocks[0]}, {16, 28, kScheduleBlocks[1]}};
 
 // Reads the trials whose events have completed; chooses once every candidate has one.
 void tune_harvest(StageCapTune &T) {
@@ -991,6 +994,21 @@ gr_status gr_scene_stage_caps(gr_ctx *ctx, uint64_t id, uint32_t *cap_first, uin
     if (T.best < 0) grh::tune_harvest(T);
     *cap_first = T.best < 0 ? 0u : grh::kStageCapCandidates[T.best].first;
     *cap_second = T.best < 0 ? 0u : grh::kStageCapCandidates[T.best].second;
+    return GR_OK;
+}
+
+gr_status gr_scene_schedule(gr_ctx *ctx, uint64_t id, uint32_t *cap_first, uint32_t *cap_second,
+                            uint32_t *blocks_per_sm) {
+    if (!ctx || !cap_first || !cap_second || !blocks_per_sm) return fail(GR_EINVAL, "NULL argument");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    auto it = ctx->scenes.find(id);
+    if (it == ctx->scenes.end()) return fail(GR_ENOTFOUND, "unknown scene id %llu", (unsigned long long)id);
+    StageCapTune &T = it->second->tune;
+    if (T.best < 0) grh::tune_harvest(T);
+    const StageCaps c = T.best < 0 ? StageCaps{} : grh::kStageCapCandidates[T.best];
+    *cap_first = c.first;
+    *cap_second = c.second;
+    *blocks_per_sm = c.blocks;
     return GR_OK;
 }
 

@@ -47,12 +47,6 @@ __device__ __forceinline__ void tuple_coords(const LaunchRange &R, uint64_t t, u
     sample = R.sample_offset + s;  // u32 wrapping add, as the reference's wrapping_add
 }
 
-// 9 resident blocks of 128 threads per SM caps the kernel at 56 registers; measured
-// on B200 this beats the unconstrained 64-72 registers by 2-5% (more warps to hide
-// the latency of the scalar physics code outweighs a few spilled values).
-#ifndef GR_TRACE_MIN_BLOCKS
-#define GR_TRACE_MIN_BLOCKS 9
-#endif
 
 // One warp folds pixel `px` (local to its xyz block) into film pixel `film_pixel`.
 // Add mode (cont == 0): the samples are summed in order from zero and the sum is

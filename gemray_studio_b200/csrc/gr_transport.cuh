@@ -15,8 +15,8 @@ namespace grd {
 // GR_FLAG_FP64_RESOLVE variant (FP64 re-solve of ambiguous exits and TIR decisions);
 // EXTRAS the variant for scenes with frosted facets, volume scattering or a biaxial
 // material.
-template <class CT, bool RESOLVE = false, bool EXTRAS = false, int K = K_ANY>
-__global__ void __launch_bounds__(TRACE_THREADS, GR_TRACE_MIN_BLOCKS) k_trace_plain(SceneConst S, SceneBuffers B, LaunchRange R,
+template <class CT, bool RESOLVE = false, bool EXTRAS = false, int K = K_ANY, int MB = GR_TRACE_MIN_BLOCKS>
+__global__ void __launch_bounds__(TRACE_THREADS, MB) k_trace_plain(SceneConst S, SceneBuffers B, LaunchRange R,
                                                                float *__restrict__ xyz,
                                                                unsigned long long *__restrict__ tallies) {
     extern __shared__ float4 s_planes[];
@@ -48,8 +48,10 @@ __global__ void __launch_bounds__(TRACE_THREADS, GR_TRACE_MIN_BLOCKS) k_trace_pl
 }
 
 // Staged kernels (the scheme and run_or_park are in gr_stage.cuh).
-template <bool EXTRAS, int K = K_ANY>
-__global__ void __launch_bounds__(TRACE_THREADS, GR_TRACE_MIN_BLOCKS) k_trace_stage1(SceneConst S, SceneBuffers B,
+// MB: resident blocks per SM the register allocation targets (the schedule tuner's
+// warps-per-SM dimension).
+template <bool EXTRAS, int K = K_ANY, int MB = GR_TRACE_MIN_BLOCKS>
+__global__ void __launch_bounds__(TRACE_THREADS, MB) k_trace_stage1(SceneConst S, SceneBuffers B,
                                                                                      LaunchRange R,
                                                                                      float *__restrict__ xyz,
                                                                                      ParkOut out, uint32_t bounce_cap) {
@@ -72,8 +74,8 @@ __global__ void __launch_bounds__(TRACE_THREADS, GR_TRACE_MIN_BLOCKS) k_trace_st
 
 // Continuation: parked paths [0, min(*count_in, cap_in)) resumed one per thread, up to
 // `bounce_cap`, survivors parked in `out` (out.cap 0: run to the end).
-template <bool EXTRAS, int K = K_ANY>
-__global__ void __launch_bounds__(TRACE_THREADS, GR_TRACE_MIN_BLOCKS) k_trace_stage2(
+template <bool EXTRAS, int K = K_ANY, int MB = GR_TRACE_MIN_BLOCKS>
+__global__ void __launch_bounds__(TRACE_THREADS, MB) k_trace_stage2(
     SceneConst S, SceneBuffers B, const Path *__restrict__ park_in, uint32_t cap_in,
     const unsigned int *__restrict__ count_in, uint32_t bounce_cap, ParkOut out, float *__restrict__ xyz) {
     const uint32_t n = min((uint32_t)*count_in, cap_in);

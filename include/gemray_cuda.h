@@ -683,17 +683,22 @@ gr_status gr_denoise_tonemap_device(gr_ctx *ctx, const float *film, uint32_t sam
 #define GR_AUTO_STAGED_MIN_TUPLES (1u << 19)
 gr_status gr_set_kernel(gr_ctx *ctx, uint32_t kernel);
 
-/* Bounce caps of a resident scene's staged renders (stage 1, stage 2).  Every pair gives
- * the same films; the fastest depends on the stone (measured on B200: 12 / 20 on the
- * c2 brilliant, 8 / 16 on the c3 emerald, 3.9% faster there).  From the scene's second
- * staged gr_render_resident call on, one call with each candidate pair is timed with
- * device events and the pair with the least time per tuple is kept for the scene.
- * Writes 0 / 0 while the choice is still open.  Batched launches (gr_render_batch, the
- * request loop) run each scene with its chosen first cap (their continuation stage is
- * uncapped); gr_accumulate and gr_accumulate_device choose the same way per stone
- * (planes, finishes, material, depth and flags; not the view); a frame stream uses
- * its scene's pair as chosen when the stream opened. */
+/* The staged schedule of a resident scene's renders: bounce caps of stages 1 and 2 and
+ * the resident blocks per SM the kernels' register allocation targets.  Every schedule
+ * gives the same films; the fastest depends on the stone (measured on B200: caps 12 / 20
+ * on the c2 brilliant, 8 / 16 on the c3 emerald, 3.9% faster there; 10 blocks per SM
+ * 2.3% faster than 9 on both).  From the scene's second staged gr_render_resident call
+ * on, one call with each of six candidate schedules (caps 12 / 20, 8 / 16, 16 / 28, each
+ * at 9 and 10 blocks per SM) is timed with device events and the schedule with the
+ * least time per tuple is kept for the scene.  Writes zeros while the choice is still
+ * open.  Batched launches (gr_render_batch, the request loop) run each scene with its
+ * chosen first cap (their continuation stage is uncapped); gr_accumulate and
+ * gr_accumulate_device choose the same way per stone (planes, finishes, material,
+ * depth and flags; not the view); a frame stream uses its scene's schedule as chosen
+ * when the stream opened.  gr_scene_stage_caps reports the caps alone. */
 gr_status gr_scene_stage_caps(gr_ctx *ctx, uint64_t scene_id, uint32_t *cap_first, uint32_t *cap_second);
+gr_status gr_scene_schedule(gr_ctx *ctx, uint64_t scene_id, uint32_t *cap_first, uint32_t *cap_second,
+                            uint32_t *blocks_per_sm);
 
 /* Per-launch timing: while enabled, every trace and film-fold launch is bracketed by
  * CUDA events on its own stream.  gr_timing_read waits for them, returns the summed

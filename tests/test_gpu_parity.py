@@ -212,9 +212,9 @@ def test_auto_kernel_picks_by_launch_size(engine_lib):
 
 
 def test_stage_cap_trials_keep_films_identical(engine_lib):
-    """A resident scene's staged renders time one call with each candidate stage-cap
-    pair and keep the faster (gr_scene_stage_caps): every call's film, trial or not,
-    is bit-identical to the plain kernel's."""
+    """A resident scene's staged renders time one call with each of the six candidate
+    schedules (stage caps x blocks per SM) and keep the fastest (gr_scene_schedule):
+    every call's film, trial or not, is bit-identical to the plain kernel's."""
     import torch
 
     from gemray_studio_b200 import GpuFrameRenderer
@@ -226,8 +226,8 @@ def test_stage_cap_trials_keep_films_identical(engine_lib):
     try:
         sid = C.c_uint64()
         assert r.lib.gr_scene_upload(r.ctx, C.byref(sc.c_scene()), C.byref(sid)) == abi.GR_OK
-        c1, c2 = C.c_uint32(), C.c_uint32()
-        for k in range(4):
+        c1, c2, cb = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        for k in range(8):
             film = torch.zeros((n_px, 3), dtype=torch.float32, device="cuda")
             torch.cuda.synchronize()
             assert r.lib.gr_render_resident(r.ctx, sid.value, 7 + k * spp, spp, C.c_void_p(film.data_ptr()),
@@ -236,11 +236,14 @@ def test_stage_cap_trials_keep_films_identical(engine_lib):
             ref = np.zeros((n_px, 3), np.float32)
             plain.accumulate(sc, 7 + k * spp, spp, ref)
             assert np.array_equal(film.cpu().numpy().view(np.uint32), ref.view(np.uint32)), k
-            assert r.lib.gr_scene_stage_caps(r.ctx, sid.value, C.byref(c1), C.byref(c2)) == abi.GR_OK
+            assert r.lib.gr_scene_schedule(r.ctx, sid.value, C.byref(c1), C.byref(c2), C.byref(cb)) == abi.GR_OK
             if k == 0:
-                assert (c1.value, c2.value) == (0, 0)  # the first call carries one-time costs: no trial yet
+                assert (c1.value, c2.value, cb.value) == (0, 0, 0)  # the first call carries one-time costs
             del film
-        assert (c1.value, c2.value) in ((12, 20), (8, 16))
+        assert (c1.value, c2.value) in ((12, 20), (8, 16), (16, 28)) and cb.value in (9, 10)
+        s1, s2 = C.c_uint32(), C.c_uint32()
+        assert r.lib.gr_scene_stage_caps(r.ctx, sid.value, C.byref(s1), C.byref(s2)) == abi.GR_OK
+        assert (s1.value, s2.value) == (c1.value, c2.value)
         # a batched launch runs the segment with the scene's chosen first cap
         film = torch.zeros((n_px, 3), dtype=torch.float32, device="cuda")
         items = (abi.gr_batch_item * 1)(abi.gr_batch_item(sid.value, film.data_ptr(), 7, spp))
@@ -254,7 +257,7 @@ def test_stage_cap_trials_keep_films_identical(engine_lib):
         r.lib.gr_scene_release(r.ctx, sid.value)
         # gr_accumulate tunes per stone the same way: trial calls included, every film
         # is the plain kernel's
-        for k in range(4):
+        for k in range(8):
             got = np.zeros((n_px, 3), np.float32)
             r.accumulate(sc, 11 + k * spp, spp, got)
             ref = np.zeros((n_px, 3), np.float32)

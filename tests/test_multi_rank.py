@@ -1,7 +1,8 @@
 """Multi-rank sharding by absolute sample range, on CPU with gloo (world size 2).
 
 Each rank renders its slice of the sample range with the oracle standing in for the
-per-GPU engine and the films are summed with one all-reduce.  The result must equal,
+per-GPU engine and the films are summed with one all-reduce (and, as the sharded
+frame's end-to-end step does, with one reduce onto rank 0).  The result must equal,
 bit for bit, the single-process composition of the same slices (each slice folded
 from zero in sample order, the partial films added in rank order), and match one
 render of the whole range to f32 summation accuracy.
@@ -63,6 +64,11 @@ def _worker(rank: int, world: int, port: int, out_dir: str):
         film, rng = render_sharded(render, 5, 37, film, dst=None)
         np.save(os.path.join(out_dir, f"film{rank}.npy"), film.numpy())
         np.save(os.path.join(out_dir, f"range{rank}.npy"), np.array(rng))
+        # the sharded frame's reduction onto one rank (the multi-GPU e2e step's collective)
+        onto0 = torch.zeros_like(film)
+        onto0, _ = render_sharded(render, 5, 37, onto0, dst=0)
+        if rank == 0:
+            np.save(os.path.join(out_dir, "onto0.npy"), onto0.numpy())
     finally:
         dist.destroy_process_group()
 
@@ -83,5 +89,7 @@ def test_two_gloo_ranks_compose_like_one_process(oracle, tmp_path):
     for p in parts:
         composed = composed + p
     assert np.array_equal(films[0].view(np.uint32), composed.view(np.uint32))
+    onto0 = np.load(tmp_path / "onto0.npy")
+    assert np.array_equal(onto0.view(np.uint32), composed.view(np.uint32))   # reduce onto rank 0
     _, whole = oracle_accumulate(oracle, sc, 5, 37)
     assert np.allclose(films[0], whole, rtol=1e-5, atol=1e-6)

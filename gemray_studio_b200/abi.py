@@ -130,6 +130,10 @@ class gr_batch_item(C.Structure):
 
 
 GR_BATCH_GRAPH = 0x1
+GR_SCHEDULE_SET = 2
+# staged schedules a stone chooses between: cap pairs x blocks per SM
+SCHEDULE_CAP_PAIRS = ((12, 20), (8, 16), (16, 28))
+SCHEDULE_BLOCKS = (9, 10, 12, 16)
 
 
 GR_REQ_RENDER, GR_REQ_METRICS = 0, 1
@@ -296,6 +300,10 @@ EXPORTS = [
     ("gr_scene_stage_caps", C.c_int, [_ctx_p, C.c_uint64, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
     ("gr_scene_schedule", C.c_int, [_ctx_p, C.c_uint64, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
                                     C.POINTER(C.c_uint32)]),
+    ("gr_scene_set_schedule", C.c_int, [_ctx_p, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32]),
+    ("gr_tuning_save", C.c_int, [_ctx_p, C.c_char_p]),
+    ("gr_tuning_load", C.c_int, [_ctx_p, C.c_char_p, C.POINTER(C.c_uint32)]),
+    ("gr_tuning_count", C.c_int, [_ctx_p, C.POINTER(C.c_uint32)]),
     ("gr_synchronize", C.c_int, [_ctx_p]),
     ("gr_stream", C.c_void_p, [_ctx_p]),
     ("gr_camera_new", C.c_int, [C.c_float, C.c_float, C.c_float, C.c_float, C.POINTER(gr_camera)]),

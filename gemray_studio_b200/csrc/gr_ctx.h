@@ -29,39 +29,76 @@ gr_status fail(gr_status st, const char *fmt, ...);
 
 // Bounce caps of the staged kernels' first two stages ({0, 0} = the built-in pair) and
 // the resident blocks per SM their register allocation targets (0 = the built-in
-// GR_TRACE_MIN_BLOCKS): a staged schedule.
+// kBuiltinScheduleBlocks): a staged schedule.
 struct StageCaps {
     uint32_t first = 0, second = 0;
     uint32_t blocks = 0;
 };
-// Blocks-per-SM targets the staged single-scene kernels are built for: [0] is the
-// built-in one.  Measured on B200 (c2 / c3 frames): 10 blocks (48 registers) 2.3%
-// faster than 9 (56) on both, 7 and 8 slower.
-constexpr uint32_t kScheduleBlocks[2] = {GR_TRACE_MIN_BLOCKS, 10};
+// Blocks-per-SM targets the staged single-scene kernels are built for: register
+// budgets of 56 / 48 / 40 / 32 per thread on 128-thread blocks (a target of 11 compiles
+// to the same 40 registers as 12, 13-15 to the same 32 as 16).  Measured on B200 with
+// the clear brilliant and the dichroic emerald (ms per frame, whole-frame rates):
+// 9 -> 10 -> 12 blocks +2.3% / +4.6% on both stones.
+constexpr int kScheduleBlockCount = 4;
+constexpr uint32_t kScheduleBlocks[kScheduleBlockCount] = {9, 10, 12, 16};
+// The blocks per SM of a staged launch whose schedule is still open.
+constexpr uint32_t kBuiltinScheduleBlocks = 12;
+// Stage-cap pairs a stone chooses between: the pair measured best on the c2 brilliant
+// (long, TIR-trapped diamond paths), the one measured best on the c3 emerald (n ~ 1.6,
+// shorter paths; 3.9% faster there) and a longer pair for longer paths still.
+constexpr int kCapPairCount = 3;
+constexpr uint32_t kCapPairs[kCapPairCount][2] = {{12, 20}, {8, 16}, {16, 28}};
+// Candidate schedules: cap pair p at blocks b is candidate p * kScheduleBlockCount + b.
+constexpr int kScheduleCandidates = kCapPairCount * kScheduleBlockCount;
+inline StageCaps schedule_candidate(int c) {
+    return StageCaps{kCapPairs[c / kScheduleBlockCount][0], kCapPairs[c / kScheduleBlockCount][1],
+                     kScheduleBlocks[c % kScheduleBlockCount]};
+}
+// The candidate index of a schedule, -1 if it is not one.
+inline int schedule_index(uint32_t first, uint32_t second, uint32_t blocks) {
+    for (int c = 0; c < kScheduleCandidates; ++c) {
+        const StageCaps k = schedule_candidate(c);
+        if (k.first == first && k.second == second && k.blocks == blocks) return c;
+    }
+    return -1;
+}
 
 // The staged schedule (stage caps and blocks per SM) a stone's staged renders use.
 // Every schedule gives the same films, but the fastest depends on the stone's path
-// lengths and register pressure, so from the stone's second staged call on, one call
-// with each candidate schedule is timed on the device (the whole call: its chunks cover
-// different parts of the image) and the schedule with the least time per tuple is kept
-// (gr_host.cu, kScheduleCandidates).
+// lengths and register pressure.  From the stone's second staged call on, calls are
+// timed on the device as trials (the whole call: its chunks cover different parts of
+// the image), in two rounds: the first cap pair at each blocks-per-SM target, then the
+// other pairs at the fastest target; the candidate with the least time per tuple is
+// kept.  A choice can also come from the context's tuning table (measured earlier for
+// the same stone on this device, gr_tuning_load) or be pinned (gr_scene_set_schedule).
 struct StageCapTune {
-    static constexpr int kCandidates = 6;
+    static constexpr int kTrials = kScheduleBlockCount + kCapPairCount - 1;
+    uint64_t key = 0;           // the stone (stone_key), for the context's tuning table
     int best = -1;              // chosen candidate, -1 while measuring
     uint32_t staged_calls = 0;  // staged calls seen
-    bool issued[kCandidates] = {};
-    float ms_per_mtuple[kCandidates] = {3.0e38f, 3.0e38f, 3.0e38f, 3.0e38f, 3.0e38f,
-                                        3.0e38f};  // unmeasured: never chosen over a measured one
+    int n_trials = 0;           // trials issued
+    float ms_per_mtuple[kScheduleCandidates];
     struct Trial {
         cudaEvent_t start = nullptr, stop = nullptr;
         int candidate = 0;
         uint64_t tuples = 0;
+        bool ended = false;  // stop recorded (tune_end): until then the trial is not read
         bool done = false;
-    } trial[kCandidates];
+    } trial[kTrials];
+    StageCapTune() {
+        for (float &m : ms_per_mtuple) m = 3.0e38f;  // unmeasured: never chosen over a measured one
+    }
+};
+
+// A schedule chosen for a stone on this context's device: the tuning table's entry.
+struct TunedSchedule {
+    int candidate = 0;
+    float ms_per_mtuple = 0.0f;
 };
 
 struct ResidentScene {
     SceneConst S;
+    uint64_t stone = 0;  // stone_key of the uploaded scene
     grh::DeviceBuffer planes, map, ext;
     uint64_t bytes = 0;
     uint32_t users = 0;  // open frame streams rendering this scene (gr_stream.cu)
@@ -99,6 +136,10 @@ struct gr_ctx {
     // depth, flags: what sets the path lengths); cleared past kMaxAccumTunes stones
     std::map<uint64_t, StageCapTune> accum_tune;
     static constexpr size_t kMaxAccumTunes = 64;
+    // Schedules chosen per stone on this device (measured here, or read from a tuning
+    // table by gr_tuning_load): a stone met again starts from its entry, without trials.
+    std::map<uint64_t, TunedSchedule> tuned;
+    std::string tuning_cache;  // GR_TUNING_CACHE at creation: loaded then, saved at gr_destroy
     size_t trace_used = 0, fold_used = 0;
     uint64_t trace_launches = 0, fold_launches = 0;
     // gr_render_batch: scene-slot + segment tables, captured launch sequences, and a
@@ -173,7 +214,7 @@ struct StagedLaunch {
     unsigned int *counts;
     uint64_t cap1, cap2;
     uint32_t cap_first, cap_second;
-    uint32_t blocks;  // kScheduleBlocks entry, 0 = the built-in one
+    uint32_t blocks;  // kScheduleBlocks entry, 0 = kBuiltinScheduleBlocks
 };
 // The plain kernel (st == NULL) or the three staged launches of scene class K
 // (gr_single_clear.cu / gr_single_general.cu).
@@ -189,20 +230,31 @@ int resolve_kernel(int mode, uint64_t n_tuples);
 // The stage-1 bounce cap a resident scene's staged launches use (its chosen pair's
 // first cap, the built-in one while the choice is open).
 uint32_t scene_stage_cap(const ResidentScene &rs);
-// Both caps of the scene's chosen pair ({0, 0}, the built-in pair, while open).
+// The scene's chosen schedule ({0, 0, 0}, the built-in one, while open).
 StageCaps scene_stage_caps(const ResidentScene &rs);
-// A staged call's caps under tuning state T: the chosen pair, or a device-timed trial
-// of the next unmeasured candidate (trial >= 0; tune_end records its end).  The
-// scene's first staged call runs untimed (it carries one-time costs).
-StageCaps tune_begin(StageCapTune &T, int kernel_mode, const SceneConst &S, uint64_t n_pixels, uint32_t spp,
-                     uint64_t chunk_budget, cudaStream_t s, int &trial);
+// A staged call's schedule under tuning state T: the chosen one, or a device-timed
+// trial of the next candidate (trial >= 0; tune_end records its end).  The stone's
+// first staged call runs untimed (it carries one-time costs).  A finished choice is
+// entered in ctx->tuned.  The caller holds ctx->mu.
+StageCaps tune_begin(gr_ctx *ctx, StageCapTune &T, const SceneConst &S, uint64_t n_pixels, uint32_t spp,
+                     cudaStream_t s, int &trial);
+// The caller holds ctx->mu (a trial is read only after its end is recorded).
 void tune_end(StageCapTune &T, int trial, cudaStream_t s);
+// Reads T's finished trials; chooses (and enters the choice in ctx->tuned) once all
+// are in.  The caller holds ctx->mu.
+void tune_harvest(gr_ctx *ctx, StageCapTune &T);
+// A fresh tuning state for stone `key`, starting from ctx->tuned's entry if any.
+void tune_init(gr_ctx *ctx, StageCapTune &T, uint64_t key);
 void tune_release(StageCapTune &T);
 // gr_accumulate's tuning state for the scene's stone (created on first use).
 StageCapTune &accum_tune(gr_ctx *ctx, const gr_scene *sc);
 // The gr_accumulate tuning key of a scene (its stone, not its view).
 uint64_t stone_key(const gr_scene *sc);
 int trace_kernel_launches(int mode, const SceneConst &S, uint64_t n_tuples);
+// Park slots of a staged launch's first stage (1/8 of its tuples, at least 1,024, at
+// most 4 GiB of records), and the park buffer bytes of both capped stages.
+uint64_t staged_park_slots(uint64_t n_tuples);
+size_t staged_park_bytes(uint64_t n_tuples);
 gr_status launch_fold(const float *xyz, uint32_t n_pixels, uint32_t spp, uint32_t first_pixel, float *film,
                       uint32_t kahan, cudaStream_t stream);
 }  // namespace grh

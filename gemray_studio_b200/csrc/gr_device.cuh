@@ -20,8 +20,8 @@
 // Resident 128-thread blocks per SM the transport kernels' register allocation targets
 // by default: 9 caps them at 56 registers, measured on B200 2-5% faster than the
 // unconstrained 64-72 (more warps to hide the scalar physics code's latency outweigh a
-// few spilled values); the staged single-scene kernels are also built for 10 blocks,
-// which their per-stone schedule tuner may choose.
+// few spilled values).  The staged single-scene kernels are built for 9, 10, 12 and 16
+// blocks (kScheduleBlocks), among which their per-stone schedule tuner chooses.
 #ifndef GR_TRACE_MIN_BLOCKS
 #define GR_TRACE_MIN_BLOCKS 9
 #endif

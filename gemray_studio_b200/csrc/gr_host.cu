@@ -13,11 +13,14 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
 #include <string>
 #include <vector>
+
+#include <unistd.h>
 
 #include "gemray_cuda.h"
 #include "gr_ctx.h"
@@ -388,6 +391,19 @@ int trace_kernel_launches(int mode, const SceneConst &S, uint64_t n_tuples) {
     return staged ? 3 : 1;  // stages 1, 2 and 3
 }
 
+uint64_t staged_park_slots(uint64_t n_tuples) {
+    uint64_t cap1 = (n_tuples + 7) / 8;
+    const uint64_t max_cap = (4ull << 30) / sizeof(grd::Path);
+    if (cap1 > max_cap) cap1 = max_cap;
+    if (cap1 < 1024) cap1 = 1024;
+    return cap1;
+}
+
+size_t staged_park_bytes(uint64_t n_tuples) {
+    const uint64_t cap1 = staged_park_slots(n_tuples);
+    return (size_t)(cap1 + (cap1 + 3) / 4) * sizeof(grd::Path) + 256;
+}
+
 // Trace tuples [0, R.n_tuples) of one chunk into xyz (device).
 
 gr_status launch_trace(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuffers &B, const grd::LaunchRange &R,
@@ -431,10 +447,7 @@ gr_status launch_trace(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuffers
     if (mode == GR_KERNEL_STAGED) {
         // park buffers: stage 1 parks up to 1/8 of the launch's paths (at most 4 GiB),
         // stage 2 up to 1/4 of that; overflowing paths finish where they are
-        uint64_t cap1 = (R.n_tuples + 7) / 8;
-        const uint64_t max_cap = (4ull << 30) / sizeof(grd::Path);
-        if (cap1 > max_cap) cap1 = max_cap;
-        if (cap1 < 1024) cap1 = 1024;
+        const uint64_t cap1 = staged_park_slots(R.n_tuples);
         const uint64_t cap2 = caps.second == 0xFFFFFFFFu ? 0 : (cap1 + 3) / 4;
         grh::DeviceBuffer &pk = park_buf ? *park_buf : ctx->park;
         gr_status st = pk.reserve((size_t)(cap1 + cap2) * sizeof(grd::Path) + 256);
@@ -539,19 +552,25 @@ gr_status prepare(gr_ctx *ctx, const gr_scene *sc, SceneConst &S, grd::SceneBuff
     return upload_scene(ctx, sc, S, B);
 }
 
-// Staged schedules a stone chooses between (StageCapTune): the cap pair measured best on
-// the c2 brilliant (long, TIR-trapped diamond paths), the one measured best on the c3
-// emerald (n ~ 1.6, shorter paths; 3.9% faster there) and a longer pair for stones
-// whose paths run longer still, each at both blocks-per-SM targets.
-constexpr StageCaps kStageCapCandidates[StageCapTune::kCandidates] = {
-    {12, 20, kScheduleBlocks[0]}, {8, 16, kScheduleBlocks[0]}, {12, 20, kScheduleBlocks[1]},
-    {8, 16, kScheduleBlocks[1]},  {16, 28, kScheduleBlocks[0]}, {16, 28, kScheduleBlocks[1]}};
+// The candidate a trial times: trials [0, kScheduleBlockCount) the first cap pair at
+// each blocks-per-SM target, then the other pairs at the fastest of those targets (-1
+// while that target is not known yet).
+int trial_candidate(const StageCapTune &T, int n) {
+    if (n < kScheduleBlockCount) return n;
+    int fast = 0;
+    for (int b = 0; b < kScheduleBlockCount; ++b) {
+        if (!T.trial[b].done) return -1;
+        if (T.ms_per_mtuple[b] < T.ms_per_mtuple[fast]) fast = b;
+    }
+    return (n - kScheduleBlockCount + 1) * kScheduleBlockCount + fast;
+}
 
-// Reads the trials whose events have completed; chooses once every candidate has one.
-void tune_harvest(StageCapTune &T) {
-    bool all = true;
-    for (auto &tr : T.trial) {
-        if (tr.start && !tr.done && cudaEventQuery(tr.stop) == cudaSuccess) {
+void tune_harvest(gr_ctx *ctx, StageCapTune &T) {
+    if (T.best >= 0) return;
+    bool all = T.n_trials == StageCapTune::kTrials;
+    for (int i = 0; i < T.n_trials; ++i) {
+        auto &tr = T.trial[i];
+        if (tr.ended && !tr.done && cudaEventQuery(tr.stop) == cudaSuccess) {
             float ms = 0.0f;
             if (cudaEventElapsedTime(&ms, tr.start, tr.stop) == cudaSuccess && tr.tuples)
                 T.ms_per_mtuple[tr.candidate] = ms / (float)((double)tr.tuples * 1e-6);
@@ -561,46 +580,57 @@ void tune_harvest(StageCapTune &T) {
     }
     cudaGetLastError();  // a query of an unfinished event is not an error to keep
     if (!all) return;
-    T.best = 0;
-    for (int c = 1; c < StageCapTune::kCandidates; ++c)
-        if (T.ms_per_mtuple[c] < T.ms_per_mtuple[T.best]) T.best = c;
+    int best = 0;
+    for (int c = 1; c < kScheduleCandidates; ++c)
+        if (T.ms_per_mtuple[c] < T.ms_per_mtuple[best]) best = c;
+    T.best = best;
+    if (T.key) ctx->tuned[T.key] = TunedSchedule{best, T.ms_per_mtuple[best]};
+}
+
+void tune_init(gr_ctx *ctx, StageCapTune &T, uint64_t key) {
+    tune_release(T);
+    T = StageCapTune{};
+    T.key = key;
+    auto it = ctx->tuned.find(key);
+    if (key && it != ctx->tuned.end()) T.best = it->second.candidate;
 }
 
 uint32_t scene_stage_cap(const ResidentScene &rs) {
-    return rs.tune.best >= 0 ? kStageCapCandidates[rs.tune.best].first : (uint32_t)GR_STAGE_CAP;
+    return rs.tune.best >= 0 ? schedule_candidate(rs.tune.best).first : (uint32_t)GR_STAGE_CAP;
 }
 
 StageCaps scene_stage_caps(const ResidentScene &rs) {
-    return rs.tune.best >= 0 ? kStageCapCandidates[rs.tune.best] : StageCaps{};
+    return rs.tune.best >= 0 ? schedule_candidate(rs.tune.best) : StageCaps{};
 }
 
-StageCaps tune_begin(StageCapTune &T, int kernel_mode, const SceneConst &S, uint64_t n_pixels, uint32_t spp,
-                     uint64_t chunk_budget, cudaStream_t s, int &trial) {
+StageCaps tune_begin(gr_ctx *ctx, StageCapTune &T, const SceneConst &S, uint64_t n_pixels, uint32_t spp,
+                     cudaStream_t s, int &trial) {
     trial = -1;
-    const uint64_t budget_tuples = chunk_budget / (3 * sizeof(float));
+    const uint64_t budget_tuples = ctx->chunk_budget / (3 * sizeof(float));
     const uint64_t first_chunk = std::min<uint64_t>(n_pixels, std::max<uint64_t>(1, budget_tuples / spp)) * spp;
-    if (trace_kernel_launches(kernel_mode, S, first_chunk) != 3) return StageCaps{};  // not staged
-    if (T.best < 0) tune_harvest(T);
-    if (T.best >= 0) return kStageCapCandidates[T.best];
-    if (T.staged_calls++ == 0) return StageCaps{};
-    for (int c = 0; c < StageCapTune::kCandidates && trial < 0; ++c)
-        if (!T.issued[c]) trial = c;
-    if (trial < 0) return StageCaps{};  // every trial issued, not all finished yet
-    auto &tr = T.trial[trial];
+    if (trace_kernel_launches(ctx->kernel_mode, S, first_chunk) != 3) return StageCaps{};  // not staged
+    tune_harvest(ctx, T);
+    if (T.best >= 0) return schedule_candidate(T.best);
+    if (T.staged_calls++ == 0 || T.n_trials == StageCapTune::kTrials) return StageCaps{};
+    const int c = trial_candidate(T, T.n_trials);
+    if (c < 0) return StageCaps{};  // the second round waits for the first round's times
+    auto &tr = T.trial[T.n_trials];
     if ((!tr.start && cudaEventCreate(&tr.start) != cudaSuccess) || (!tr.stop && cudaEventCreate(&tr.stop) != cudaSuccess)) {
         cudaGetLastError();
-        trial = -1;  // untimed: stay on the built-in pair
-        return StageCaps{};
+        return StageCaps{};  // untimed: stay on the built-in schedule
     }
-    tr.candidate = trial;
+    tr.candidate = c;
     tr.tuples = n_pixels * spp;
-    T.issued[trial] = true;
+    tr.ended = tr.done = false;
+    trial = T.n_trials++;
     cudaEventRecord(tr.start, s);
-    return kStageCapCandidates[trial];
+    return schedule_candidate(c);
 }
 
 void tune_end(StageCapTune &T, int trial, cudaStream_t s) {
-    if (trial >= 0) cudaEventRecord(T.trial[trial].stop, s);
+    if (trial < 0) return;
+    cudaEventRecord(T.trial[trial].stop, s);
+    T.trial[trial].ended = true;
 }
 
 uint64_t stone_key(const gr_scene *sc) {
@@ -635,7 +665,9 @@ StageCapTune &accum_tune(gr_ctx *ctx, const gr_scene *sc) {
         for (auto &kv : ctx->accum_tune) tune_release(kv.second);
         ctx->accum_tune.clear();
     }
-    return ctx->accum_tune[key];
+    StageCapTune &T = ctx->accum_tune[key];
+    tune_init(ctx, T, key);
+    return T;
 }
 }  // namespace grh
 
@@ -660,6 +692,11 @@ extern "C" {
 uint32_t gr_abi_version(void) { return GR_ABI_VERSION; }
 
 const char *gr_last_error_string(void) { return grh::g_last_error.c_str(); }
+
+namespace {
+gr_status tuning_save_locked(gr_ctx *ctx, const char *path);
+gr_status tuning_load_locked(gr_ctx *ctx, const char *path, uint32_t *n_loaded);
+}  // namespace
 
 gr_status gr_create(gr_ctx **out, const gr_create_opts *opts) {
     if (!out) return fail(GR_EINVAL, "out is NULL");
@@ -695,6 +732,14 @@ gr_status gr_create(gr_ctx **out, const gr_create_opts *opts) {
     char buf[512];
     snprintf(buf, sizeof(buf), "%.256s (CUDA, sm_%d%d, %d SMs)", prop.name, prop.major, prop.minor, prop.multiProcessorCount);
     ctx->label = buf;
+    // GR_TUNING_CACHE: a per-device schedule table read now and written back (merged)
+    // by gr_destroy; a table for another device or schedule set is left to be replaced
+    const char *cache = getenv("GR_TUNING_CACHE");
+    if (cache && *cache) {
+        ctx->tuning_cache = cache;
+        tuning_load_locked(ctx, cache, nullptr);
+        grh::g_last_error.clear();
+    }
     *out = ctx;
     return GR_OK;
 }
@@ -730,6 +775,11 @@ gr_status gr_destroy(gr_ctx *ctx) {
         ctx->batch_park.release();
         for (auto &p : ctx->trace_ev) { cudaEventDestroy(p.first); cudaEventDestroy(p.second); }
         for (auto &p : ctx->fold_ev) { cudaEventDestroy(p.first); cudaEventDestroy(p.second); }
+        if (!ctx->tuning_cache.empty()) {
+            for (auto &kv : ctx->scenes) grh::tune_harvest(ctx, kv.second->tune);
+            for (auto &kv : ctx->accum_tune) grh::tune_harvest(ctx, kv.second);
+            if (!ctx->tuned.empty()) tuning_save_locked(ctx, ctx->tuning_cache.c_str());
+        }
         for (auto &kv : ctx->accum_tune) grh::tune_release(kv.second);
         ctx->accum_tune.clear();
         for (auto &kv : ctx->scenes) {
@@ -766,7 +816,7 @@ gr_status gr_accumulate(gr_ctx *ctx, const gr_scene *sc, uint32_t sample_offset,
     GR_CUDA(cudaMemcpyAsync(ctx->film.ptr, accum, fbytes, cudaMemcpyHostToDevice, ctx->stream));
     StageCapTune &T = grh::accum_tune(ctx, sc);
     int trial = -1;
-    const StageCaps caps = grh::tune_begin(T, ctx->kernel_mode, S, n_pixels, spp, ctx->chunk_budget, ctx->stream, trial);
+    const StageCaps caps = grh::tune_begin(ctx, T, S, n_pixels, spp, ctx->stream, trial);
     st = grh::render_into(ctx, sc, S, B, sample_offset, spp, (float *)ctx->film.ptr, ctx->stream, caps);
     grh::tune_end(T, trial, ctx->stream);
     if (st != GR_OK) {
@@ -805,7 +855,7 @@ gr_status gr_accumulate_device(gr_ctx *ctx, const gr_scene *sc, uint32_t sample_
     }
     StageCapTune &T = grh::accum_tune(ctx, sc);
     int trial = -1;
-    const StageCaps caps = grh::tune_begin(T, ctx->kernel_mode, S, n_pixels, spp, ctx->chunk_budget, s, trial);
+    const StageCaps caps = grh::tune_begin(ctx, T, S, n_pixels, spp, s, trial);
     st = grh::render_into(ctx, sc, S, B, sample_offset, spp, accum_dev, s, caps);
     grh::tune_end(T, trial, s);
     if (st != GR_OK) return st;
@@ -932,6 +982,8 @@ gr_status gr_scene_upload(gr_ctx *ctx, const gr_scene *sc, uint64_t *out_id) {
         return fail(GR_ECUDA, "scene upload failed: %s", cudaGetErrorString(e));
     }
     rs->bytes = total;
+    rs->stone = grh::stone_key(sc);
+    grh::tune_init(ctx, rs->tune, rs->stone);
     ctx->resident_bytes += total;
     uint64_t id = ctx->next_scene_id++;
     ctx->scenes[id] = rs;
@@ -979,7 +1031,7 @@ gr_status gr_render_resident(gr_ctx *ctx, uint64_t id, uint32_t sample_offset, u
     shape.height = rs->S.height;
     int trial = -1;
     const StageCaps caps =
-        grh::tune_begin(rs->tune, ctx->kernel_mode, rs->S, n_pixels, spp, ctx->chunk_budget, s, trial);
+        grh::tune_begin(ctx, rs->tune, rs->S, n_pixels, spp, s, trial);
     gr_status st = grh::render_into(ctx, &shape, rs->S, resident_buffers(rs), sample_offset, spp, film_dev, s, caps);
     grh::tune_end(rs->tune, trial, s);
     return st;
@@ -991,9 +1043,10 @@ gr_status gr_scene_stage_caps(gr_ctx *ctx, uint64_t id, uint32_t *cap_first, uin
     auto it = ctx->scenes.find(id);
     if (it == ctx->scenes.end()) return fail(GR_ENOTFOUND, "unknown scene id %llu", (unsigned long long)id);
     StageCapTune &T = it->second->tune;
-    if (T.best < 0) grh::tune_harvest(T);
-    *cap_first = T.best < 0 ? 0u : grh::kStageCapCandidates[T.best].first;
-    *cap_second = T.best < 0 ? 0u : grh::kStageCapCandidates[T.best].second;
+    grh::tune_harvest(ctx, T);
+    const StageCaps c = T.best < 0 ? StageCaps{} : schedule_candidate(T.best);
+    *cap_first = c.first;
+    *cap_second = c.second;
     return GR_OK;
 }
 
@@ -1004,11 +1057,137 @@ gr_status gr_scene_schedule(gr_ctx *ctx, uint64_t id, uint32_t *cap_first, uint3
     auto it = ctx->scenes.find(id);
     if (it == ctx->scenes.end()) return fail(GR_ENOTFOUND, "unknown scene id %llu", (unsigned long long)id);
     StageCapTune &T = it->second->tune;
-    if (T.best < 0) grh::tune_harvest(T);
-    const StageCaps c = T.best < 0 ? StageCaps{} : grh::kStageCapCandidates[T.best];
+    grh::tune_harvest(ctx, T);
+    const StageCaps c = T.best < 0 ? StageCaps{} : schedule_candidate(T.best);
     *cap_first = c.first;
     *cap_second = c.second;
     *blocks_per_sm = c.blocks;
+    return GR_OK;
+}
+
+gr_status gr_scene_set_schedule(gr_ctx *ctx, uint64_t id, uint32_t cap_first, uint32_t cap_second,
+                                uint32_t blocks_per_sm) {
+    if (!ctx) return fail(GR_EINVAL, "ctx is NULL");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    auto it = ctx->scenes.find(id);
+    if (it == ctx->scenes.end()) return fail(GR_ENOTFOUND, "unknown scene id %llu", (unsigned long long)id);
+    ResidentScene *rs = it->second;
+    if (cap_first == 0 && cap_second == 0 && blocks_per_sm == 0) {
+        // open again: forget the stone's entry and time the candidates afresh
+        ctx->tuned.erase(rs->stone);
+        grh::tune_init(ctx, rs->tune, rs->stone);
+        return GR_OK;
+    }
+    const int c = schedule_index(cap_first, cap_second, blocks_per_sm);
+    if (c < 0)
+        return fail(GR_EINVAL, "schedule (%u, %u, %u blocks/SM) is not a candidate", cap_first, cap_second,
+                    blocks_per_sm);
+    grh::tune_init(ctx, rs->tune, rs->stone);
+    rs->tune.best = c;
+    return GR_OK;
+}
+
+namespace {
+// The identity line of a tuning table: what its timings are valid for.
+std::string tuning_identity(const gr_ctx *ctx) {
+    char buf[640];
+    snprintf(buf, sizeof(buf), "gemray-schedules %d %s", GR_SCHEDULE_SET, ctx->label.c_str());
+    return buf;
+}
+
+// Reads a tuning table's entries into `out` (entries naming no candidate are skipped);
+// GR_EINVAL when it was written for another schedule set or device.
+gr_status read_table(const char *path, const std::string &id, std::map<uint64_t, TunedSchedule> &out, uint32_t *n) {
+    *n = 0;
+    FILE *f = fopen(path, "r");
+    if (!f) return fail(GR_ENOTFOUND, "cannot read %s", path);
+    char line[1024];
+    std::string head = fgets(line, sizeof(line), f) ? line : "";
+    while (!head.empty() && (head.back() == '\n' || head.back() == '\r')) head.pop_back();
+    if (head != id) {
+        fclose(f);
+        return fail(GR_EINVAL, "%s was not written for this schedule set and device (%s)", path, id.c_str());
+    }
+    while (fgets(line, sizeof(line), f)) {
+        unsigned long long key = 0;
+        unsigned first = 0, second = 0, blocks = 0;
+        float ms = 0.0f;
+        if (sscanf(line, "%llx %u %u %u %g", &key, &first, &second, &blocks, &ms) != 5 || key == 0) continue;
+        const int c = schedule_index(first, second, blocks);
+        if (c < 0) continue;
+        out[key] = TunedSchedule{c, ms};
+        ++*n;
+    }
+    fclose(f);
+    return GR_OK;
+}
+
+// Writes the context's entries, merged over those the file already holds for this
+// schedule set and device, through a temporary file renamed into place.
+gr_status tuning_save_locked(gr_ctx *ctx, const char *path) {
+    std::map<uint64_t, TunedSchedule> all;
+    uint32_t n = 0;
+    const std::string id = tuning_identity(ctx);
+    read_table(path, id, all, &n);  // a missing or foreign table is replaced
+    for (auto &kv : ctx->tuned) all[kv.first] = kv.second;
+    const std::string tmp = std::string(path) + ".tmp." + std::to_string((long long)getpid());
+    FILE *f = fopen(tmp.c_str(), "w");
+    if (!f) return fail(GR_EINVAL, "cannot write %s", tmp.c_str());
+    fprintf(f, "%s\n", id.c_str());
+    for (auto &kv : all) {
+        const StageCaps c = schedule_candidate(kv.second.candidate);
+        fprintf(f, "%016llx %u %u %u %.6g\n", (unsigned long long)kv.first, c.first, c.second, c.blocks,
+                (double)kv.second.ms_per_mtuple);
+    }
+    const bool ok = fflush(f) == 0;
+    fclose(f);
+    if (!ok || rename(tmp.c_str(), path) != 0) {
+        remove(tmp.c_str());
+        return fail(GR_EINVAL, "cannot write %s", path);
+    }
+    return GR_OK;
+}
+
+gr_status tuning_load_locked(gr_ctx *ctx, const char *path, uint32_t *n_loaded) {
+    uint32_t n = 0;
+    if (n_loaded) *n_loaded = 0;
+    const gr_status st = read_table(path, tuning_identity(ctx), ctx->tuned, &n);
+    if (st != GR_OK) return st;
+    // stones already resident or met by gr_accumulate, and still open, take their entry
+    for (auto &kv : ctx->scenes) {
+        StageCapTune &T = kv.second->tune;
+        auto t = ctx->tuned.find(T.key);
+        if (T.best < 0 && T.key && t != ctx->tuned.end()) T.best = t->second.candidate;
+    }
+    for (auto &kv : ctx->accum_tune) {
+        auto t = ctx->tuned.find(kv.first);
+        if (kv.second.best < 0 && t != ctx->tuned.end()) kv.second.best = t->second.candidate;
+    }
+    if (n_loaded) *n_loaded = n;
+    return GR_OK;
+}
+}  // namespace
+
+gr_status gr_tuning_save(gr_ctx *ctx, const char *path) {
+    if (!ctx || !path) return fail(GR_EINVAL, "ctx or path is NULL");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    for (auto &kv : ctx->scenes) grh::tune_harvest(ctx, kv.second->tune);
+    for (auto &kv : ctx->accum_tune) grh::tune_harvest(ctx, kv.second);
+    return tuning_save_locked(ctx, path);
+}
+
+gr_status gr_tuning_load(gr_ctx *ctx, const char *path, uint32_t *n_loaded) {
+    if (!ctx || !path) return fail(GR_EINVAL, "ctx or path is NULL");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    return tuning_load_locked(ctx, path, n_loaded);
+}
+
+gr_status gr_tuning_count(gr_ctx *ctx, uint32_t *n_entries) {
+    if (!ctx || !n_entries) return fail(GR_EINVAL, "NULL argument");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    for (auto &kv : ctx->scenes) grh::tune_harvest(ctx, kv.second->tune);
+    for (auto &kv : ctx->accum_tune) grh::tune_harvest(ctx, kv.second);
+    *n_entries = (uint32_t)ctx->tuned.size();
     return GR_OK;
 }
 

@@ -127,8 +127,8 @@ constexpr uint64_t kBulkTuples = (uint64_t)GR_SERVE_BULK_MTUPLES << 20;
 #ifndef GR_SERVE_BULK_HIGH
 #define GR_SERVE_BULK_HIGH 1
 #endif
-// Per-tuple XYZ scratch of one bulk launch (chunks of whole pixels).
-constexpr size_t kBulkChunkBytes = 512ull << 20;
+// Per-tuple XYZ scratch of one bulk launch (chunks of whole pixels: 22 M tuples).
+constexpr size_t kBulkChunkBytes = 256ull << 20;
 
 struct Tick {
     cudaEvent_t ev = nullptr;
@@ -235,6 +235,7 @@ void bulk_main(gr_ctx *ctx, ServeState *sv) {
         grd::SceneBuffers B;
         StageCaps caps;
         int mode = GR_KERNEL_AUTO;
+        int trial = -1;
         ResidentScene *rs = nullptr;
         {
             std::lock_guard<std::mutex> lk(ctx->mu);
@@ -244,9 +245,11 @@ void bulk_main(gr_ctx *ctx, ServeState *sv) {
                 rs->users++;
                 S = rs->S;
                 B = resident_buffers(rs);
-                caps = grh::scene_stage_caps(*rs);
             }
             if (ctx->kernel_mode != GR_KERNEL_SORTED) mode = ctx->kernel_mode;
+            // a bulk render is one gr_render_resident call: it takes part in the
+            // stone's schedule tuning (a trial is timed on the bulk stream)
+            if (rs) caps = grh::tune_begin(ctx, rs->tune, S, q->n_px, q->r.spp, sv->bulk_stream, trial);
         }
         gr_status st = rs ? GR_OK : GR_ENOTFOUND;
         const uint32_t spp = q->r.spp;
@@ -271,6 +274,10 @@ void bulk_main(gr_ctx *ctx, ServeState *sv) {
             // its samples_done (0) says
             const size_t fb = (size_t)n_px * 3 * sizeof(float);
             if (cudaMemsetAsync(q->film.ptr, 0, fb, sv->bulk_stream) != cudaSuccess) st = GR_ECUDA;
+        }
+        if (rs) {
+            std::lock_guard<std::mutex> lk(ctx->mu);
+            grh::tune_end(rs->tune, trial, sv->bulk_stream);
         }
         if (cudaStreamSynchronize(sv->bulk_stream) != cudaSuccess && st == GR_OK) st = GR_ECUDA;
         if (rs) {
@@ -492,6 +499,18 @@ ServeState *serve_state(gr_ctx *ctx) {
             ctx->serve->film_pool = pool;
         }
         cudaGetLastError();  // a pool that could not be set up leaves films on the default pool
+        // Scratch of a full tick and of a full bulk chunk, reserved now: growing a
+        // buffer later frees the old one, which waits for the whole device (every
+        // stream's work) and stalls the lanes behind it.
+        const uint64_t bulk_tuples = kBulkChunkBytes / 12;
+        ctx->xyz.reserve(std::max<size_t>(ctx->xyz.cap, 2 * kTickTuples * 3 * sizeof(float)));
+        ctx->batch_tables.reserve(std::max<size_t>(ctx->batch_tables.cap, (size_t)1 << 20));
+        ctx->batch_park.reserve(std::max<size_t>(ctx->batch_park.cap, 4096 + (kTickTuples / 16 + 32 * 1024) * sizeof(grd::Path)));
+        if (ctx->serve->bulk_stream) {
+            ctx->serve->bulk_xyz.reserve(kBulkChunkBytes);
+            ctx->serve->bulk_park.reserve(grh::staged_park_bytes(bulk_tuples));
+        }
+        cudaGetLastError();  // a reservation that failed is retried (grown) where it is used
         ctx->serve->worker = std::thread(worker_main, ctx, ctx->serve);
         ctx->serve->metrics_worker = std::thread(metrics_main, ctx, ctx->serve);
         if (ctx->serve->bulk_stream) ctx->serve->bulk_worker = std::thread(bulk_main, ctx, ctx->serve);

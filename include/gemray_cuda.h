@@ -684,21 +684,44 @@ gr_status gr_denoise_tonemap_device(gr_ctx *ctx, const float *film, uint32_t sam
 gr_status gr_set_kernel(gr_ctx *ctx, uint32_t kernel);
 
 /* The staged schedule of a resident scene's renders: bounce caps of stages 1 and 2 and
- * the resident blocks per SM the kernels' register allocation targets.  Every schedule
- * gives the same films; the fastest depends on the stone (measured on B200: caps 12 / 20
- * on the c2 brilliant, 8 / 16 on the c3 emerald, 3.9% faster there; 10 blocks per SM
- * 2.3% faster than 9 on both).  From the scene's second staged gr_render_resident call
- * on, one call with each of six candidate schedules (caps 12 / 20, 8 / 16, 16 / 28, each
- * at 9 and 10 blocks per SM) is timed with device events and the schedule with the
- * least time per tuple is kept for the scene.  Writes zeros while the choice is still
- * open.  Batched launches (gr_render_batch, the request loop) run each scene with its
- * chosen first cap (their continuation stage is uncapped); gr_accumulate and
- * gr_accumulate_device choose the same way per stone (planes, finishes, material,
- * depth and flags; not the view); a frame stream uses its scene's schedule as chosen
- * when the stream opened.  gr_scene_stage_caps reports the caps alone. */
+ * the resident blocks per SM the kernels' register allocation targets (9, 10, 12 or 16:
+ * 56, 48, 40 or 32 registers per thread).  Every schedule gives the same films; the
+ * fastest depends on the stone (measured on B200: caps 12 / 20 on the c2 brilliant,
+ * 8 / 16 on the c3 emerald, 3.9% faster there; 12 blocks per SM 4.6% faster than 9 on
+ * both).  From the scene's second staged gr_render_resident call on, calls are timed with
+ * device events as trials, in two rounds: caps 12 / 20 at each blocks-per-SM target, then
+ * caps 8 / 16 and 16 / 28 at the fastest target; the schedule with the least time per
+ * tuple is kept for the scene and entered in the context's tuning table.  Writes zeros
+ * while the choice is still open (the built-in schedule, caps 12 / 20 at 12 blocks per
+ * SM, runs meanwhile).  Batched launches (gr_render_batch, the request loop) run each
+ * scene with its chosen first cap (their continuation stage is uncapped); gr_accumulate
+ * and gr_accumulate_device choose the same way per stone (planes, finishes, material,
+ * depth and flags; not the view); a frame stream uses its scene's schedule as chosen when
+ * the stream opened.  Scenes that need the frosted / scattering / biaxial kernels run
+ * those at 9 blocks per SM whatever the schedule's target.  gr_scene_stage_caps reports
+ * the caps alone. */
 gr_status gr_scene_stage_caps(gr_ctx *ctx, uint64_t scene_id, uint32_t *cap_first, uint32_t *cap_second);
 gr_status gr_scene_schedule(gr_ctx *ctx, uint64_t scene_id, uint32_t *cap_first, uint32_t *cap_second,
                             uint32_t *blocks_per_sm);
+/* Pins a resident scene's schedule to one of the candidates (GR_EINVAL for any other
+ * triple); (0, 0, 0) forgets the stone's choice and times the candidates afresh. */
+gr_status gr_scene_set_schedule(gr_ctx *ctx, uint64_t scene_id, uint32_t cap_first, uint32_t cap_second,
+                                uint32_t blocks_per_sm);
+
+/* The context's tuning table: one schedule per stone (the scene key gr_accumulate uses),
+ * measured on this device or loaded.  A stone met again -- a new upload, a new
+ * gr_accumulate stone -- starts from its entry without trials.  gr_tuning_save writes it
+ * as text (a first line naming GR_SCHEDULE_SET and the device label, then one
+ * "key first second blocks ms_per_mtuple" line per stone), merged over the entries the
+ * file already holds for the same device, through a renamed temporary file.
+ * gr_tuning_load reads one (GR_EINVAL if it names another schedule set or device;
+ * GR_ENOTFOUND if it cannot be read) and gives open scenes their entries.  With the
+ * environment variable GR_TUNING_CACHE set to a path, gr_create loads that file and
+ * gr_destroy saves to it: a per-device schedule cache across processes. */
+#define GR_SCHEDULE_SET 2
+gr_status gr_tuning_save(gr_ctx *ctx, const char *path);
+gr_status gr_tuning_load(gr_ctx *ctx, const char *path, uint32_t *n_loaded);
+gr_status gr_tuning_count(gr_ctx *ctx, uint32_t *n_entries);
 
 /* Per-launch timing: while enabled, every trace and film-fold launch is bracketed by
  * CUDA events on its own stream.  gr_timing_read waits for them, returns the summed

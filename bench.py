@@ -511,6 +511,8 @@ def run_engine(args):
             e_evs.append((a, b))
         e2e_how = ("per rank: scene + film upload, gr_accumulate_device over its own sample range, NCCL reduce of "
                    "the W*H*3 films onto rank 0, film readback on rank 0")
+        torch.cuda.synchronize()
+        e2e_step = film_e = host_film = None  # before the context and its stream go
     torch.cuda.synchronize()
     barrier(world)
     e2e_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in e_evs), world)
@@ -698,7 +700,9 @@ def batch_measure(scale: float, steps: int, warmup: int, n_stones: int = 64) -> 
         "gpu_launches": int(ntr.value + nfo.value),
         "clocks": clocks.summary(),
     }
-    del host, films, flush  # torch tensors used on the context stream go before the context
+    # every torch tensor used on the context stream goes before the context (the loop
+    # variables too: a pinned host block records an event on its streams when freed)
+    host = films = flush = h = f = None
     torch.cuda.synchronize()
     r.close()
     return out

@@ -36,13 +36,15 @@ struct StageCaps {
 };
 // Blocks-per-SM targets the staged single-scene kernels are built for: register
 // budgets of 56 / 48 / 40 / 32 per thread on 128-thread blocks (a target of 11 compiles
-// to the same 40 registers as 12, 13-15 to the same 32 as 16).  Measured on B200 with
-// the clear brilliant and the dichroic emerald (ms per frame, whole-frame rates):
-// 9 -> 10 -> 12 blocks +2.3% / +4.6% on both stones.
+// to the same 40 registers as 12, 13-15 to the same 32 as 16).  Measured on B200, ms
+// per frame at 9 / 10 / 12 / 16 blocks: the c2 brilliant (caps 12 / 20) 554.8 / 542.7 /
+// 531.0 / 513.4, the c3 emerald (caps 8 / 16) 2019.6 / 1970.1 / 1937.1 / 1904.4 -- the
+// latency of the scalar physics code is hidden better by more warps than it costs in
+// spilled values.
 constexpr int kScheduleBlockCount = 4;
 constexpr uint32_t kScheduleBlocks[kScheduleBlockCount] = {9, 10, 12, 16};
 // The blocks per SM of a staged launch whose schedule is still open.
-constexpr uint32_t kBuiltinScheduleBlocks = 12;
+constexpr uint32_t kBuiltinScheduleBlocks = 16;
 // Stage-cap pairs a stone chooses between: the pair measured best on the c2 brilliant
 // (long, TIR-trapped diamond paths), the one measured best on the c3 emerald (n ~ 1.6,
 // shorter paths; 3.9% faster there) and a longer pair for longer paths still.

@@ -16,17 +16,19 @@
 //   * metric requests (pose sweeps) skip admission (they hold no film): a second
 //     thread runs them in arrival order on its own high-priority stream, beside the
 //     tick in flight, so a sweep neither waits for a tick nor holds one up;
-//   * bulk lane -- a render larger than one tick (and without a slice_spp) is not
-//     sliced: a third thread renders its whole sample range with the single-scene
-//     kernels on a stream of the highest priority, with scratch of its own.  The GPU's
-//     block scheduler gives its blocks the SMs first, so a large request runs at
-//     single-scene speed from the moment it is admitted (a tick in flight only lends
-//     it the SMs its short blocks free), while the ticks of the smaller requests fill
-//     the SMs around it on the context stream.  (With the priorities the other way
-//     round the ticks starved the large renders: measured on B200 at 80 req/s, p99
-//     92 ms and a maximum of 254 ms against a serial server's 34 ms.)  Bulk renders
-//     run one at a time in admission order; cancellation takes effect before one
-//     starts or between its launches, and leaves a zero film (no samples done).
+//   * render lanes -- a render without a slice size of its own (slice_spp == 0) is
+//     not cut into ticks: a lane thread renders its whole sample range with the
+//     single-scene kernels and the stone's tuned schedule (the kernels and schedule of
+//     gr_render_resident) on the lane's own stream, with scratch of its own.  Lanes
+//     are grouped by request size (path-samples <= GR_SERVE_SMALL_MTUPLES,
+//     <= GR_SERVE_BULK_MTUPLES, larger), each size class with its own FIFO queue and
+//     stream priority: by default the smaller classes take the higher priorities, so
+//     the GPU's block scheduler gives a small request the SMs that blocks of larger
+//     ones free (within a few hundred microseconds) and it no longer waits behind them,
+//     while the larger ones keep the rest of the device.  Several requests therefore
+//     run on the device at once, one per lane.  Cancellation takes effect before a
+//     lane starts a request or between its launches, and leaves a zero film.
+//     Sliced renders (slice_spp > 0, progressive rendering) go to the ticks.
 // Slices fold in continue mode (fold_pixel): each slice carries the pixel's running
 // sum on from the film (and the Kahan compensation from a side buffer), and a request
 // starts on a zero film, so its film is one sequential per-pixel sum over all of its
@@ -91,7 +93,8 @@ struct Request {
     StreamBuffer film, comp;
     uint32_t issued = 0, done = 0, in_flight = 0;  // samples per pixel
     bool cancel = false;
-    bool bulk = false;  // rendered whole by the bulk lane, not in ticks
+    int lane_class = -1;  // rendered whole by a lane of this size class; -1: in ticks
+    bool admitted = false;  // film_bytes counted in the serve budget
     Clock::time_point t_submit, t_admit, t_done;
 };
 
@@ -117,18 +120,27 @@ constexpr size_t kTicksInFlight = 1;
 // admissions map no memory until the live films pass it (~2,800 films of 384^2
 // pixels with Kahan compensation); growing the pool was measured at up to ~0.5 s.
 constexpr uint64_t kFilmPoolReserve = 4ull << 30;
-// Renders of more than this many path-samples go to the bulk lane.
+// Render lanes by size class: path-samples up to GR_SERVE_SMALL_MTUPLES M, up to
+// GR_SERVE_BULK_MTUPLES M, and larger; lanes per class; a lane's chunk (scratch) size.
+#ifndef GR_SERVE_SMALL_MTUPLES
+#define GR_SERVE_SMALL_MTUPLES 2
+#endif
 #ifndef GR_SERVE_BULK_MTUPLES
 #define GR_SERVE_BULK_MTUPLES GR_SERVE_TICK_MTUPLES
 #endif
-constexpr uint64_t kBulkTuples = (uint64_t)GR_SERVE_BULK_MTUPLES << 20;
-// 1: the bulk lane's stream takes the highest priority (the ticks fill in around it);
-// 0: the lowest (the ticks go first).
-#ifndef GR_SERVE_BULK_HIGH
-#define GR_SERVE_BULK_HIGH 1
+// Stream priorities of the classes: 0 = the smaller the request, the higher its
+// priority; 1 = the larger, the higher.
+#ifndef GR_SERVE_LANE_ORDER
+#define GR_SERVE_LANE_ORDER 0
 #endif
-// Per-tuple XYZ scratch of one bulk launch (chunks of whole pixels: 22 M tuples).
-constexpr size_t kBulkChunkBytes = 256ull << 20;
+constexpr int kLaneClasses = 3;
+constexpr uint32_t kLanesPerClass[kLaneClasses] = {2, 1, 1};
+constexpr uint64_t kClassTuples[kLaneClasses] = {(uint64_t)GR_SERVE_SMALL_MTUPLES << 20,
+                                                 (uint64_t)GR_SERVE_BULK_MTUPLES << 20, 22ull << 20};
+
+int lane_class(uint64_t tuples) {
+    return tuples <= kClassTuples[0] ? 0 : tuples <= kClassTuples[1] ? 1 : 2;
+}
 
 struct Tick {
     cudaEvent_t ev = nullptr;
@@ -144,10 +156,15 @@ double ms_between(Clock::time_point a, Clock::time_point b) {
 struct ServeState {
     std::mutex mu;
     cudaStream_t metrics_stream = nullptr;  // metric sweeps, beside the ticks
-    cudaStream_t bulk_stream = nullptr;     // bulk renders, highest priority
-    std::condition_variable cv_bulk;
-    std::deque<uint64_t> bulk_queue;        // admitted bulk renders, admission order
-    grh::DeviceBuffer bulk_xyz, bulk_park;  // the bulk lane's own scratch
+    struct Lane {
+        int cls = 0;
+        cudaStream_t stream = nullptr;
+        grh::DeviceBuffer xyz, park;  // a chunk's per-tuple XYZ and park records
+        std::thread th;
+    };
+    std::vector<Lane *> lanes;
+    std::condition_variable cv_lane;
+    std::deque<uint64_t> lane_queue[kLaneClasses];  // admitted lane renders per class, admission order
     cudaMemPool_t film_pool = nullptr;      // request films (null: the device's default pool)
     std::condition_variable cv_work, cv_done, cv_metrics;
     std::unordered_map<uint64_t, Request *> reqs;
@@ -157,7 +174,7 @@ struct ServeState {
     uint64_t next_id = 1;
     uint64_t film_bytes = 0;      // films of admitted requests
     bool stop = false;
-    std::thread worker, metrics_worker, bulk_worker;
+    std::thread worker, metrics_worker;
 };
 
 namespace {
@@ -185,6 +202,18 @@ void admit(gr_ctx *ctx, ServeState &sv, uint64_t resident_bytes) {
             continue;
         }
         if (resident_bytes + sv.film_bytes + q->film_bytes > ctx->serve_budget) break;  // wait for releases
+        if (!sv.lanes.empty() && q->r.slice_spp == 0) {
+            // a lane renders it whole; the lane takes the film on its own stream
+            sv.queue.pop_front();
+            sv.film_bytes += q->film_bytes;
+            q->admitted = true;
+            q->state = GR_REQ_RUNNING;
+            q->t_admit = Clock::now();
+            q->lane_class = lane_class((uint64_t)q->r.spp * q->n_px);
+            sv.lane_queue[q->lane_class].push_back(q->id);
+            sv.cv_lane.notify_all();
+            continue;
+        }
         const size_t fb = (size_t)q->n_px * 3 * sizeof(float);
         if (q->film.alloc(fb, ctx->stream, sv.film_pool) != cudaSuccess ||
             (q->kahan && q->comp.alloc(fb, ctx->stream, sv.film_pool) != cudaSuccess)) {
@@ -196,35 +225,33 @@ void admit(gr_ctx *ctx, ServeState &sv, uint64_t resident_bytes) {
         }
         sv.queue.pop_front();
         sv.film_bytes += q->film_bytes;
+        q->admitted = true;
         q->state = GR_REQ_RUNNING;
         q->t_admit = Clock::now();
-        if (sv.bulk_stream && q->r.slice_spp == 0 && (uint64_t)q->r.spp * q->n_px > kBulkTuples) {
-            q->bulk = true;
-            sv.bulk_queue.push_back(q->id);
-            sv.cv_bulk.notify_one();
-        } else {
-            sv.running.push_back(q->id);
-        }
+        sv.running.push_back(q->id);
     }
 }
 
-// The bulk lane: one admitted render at a time, its whole sample range traced chunk by
-// chunk with the single-scene kernels (the scene's chosen stage caps; never the sorted
+// A render lane: the admitted renders of its size class one at a time, each on a
+// zero film taken from the film pool on the lane's stream, its whole sample range
+// traced chunk by chunk with the single-scene kernels (the stone's tuned schedule,
+// which the lane's calls help choose like gr_render_resident calls; never the sorted
 // kernel, whose blocks stay resident until its launch ends) and each chunk's pixels
-// folded in add mode onto the
-// zero film -- the film of one gr_render_resident call over the range, which is what
-// the sliced path produces too.  The scene is marked in use meanwhile, so it cannot be
-// released under the launches.
-void bulk_main(gr_ctx *ctx, ServeState *sv) {
+// folded in add mode -- the film of one gr_render_resident call over the range, which
+// is what the sliced path produces too.  The scene is marked in use meanwhile, so it
+// cannot be released under the launches.
+void lane_main(gr_ctx *ctx, ServeState *sv, ServeState::Lane *lane) {
     cudaSetDevice(ctx->device);
+    const uint64_t chunk_tuples = kClassTuples[lane->cls];
     for (;;) {
         Request *q;
         {
             std::unique_lock<std::mutex> lk(sv->mu);
-            sv->cv_bulk.wait(lk, [&] { return sv->stop || !sv->bulk_queue.empty(); });
-            if (sv->bulk_queue.empty()) return;  // stopping, nothing left
-            q = sv->reqs[sv->bulk_queue.front()];
-            sv->bulk_queue.pop_front();
+            auto &queue = sv->lane_queue[lane->cls];
+            sv->cv_lane.wait(lk, [&] { return sv->stop || !queue.empty(); });
+            if (queue.empty()) return;  // stopping, nothing left
+            q = sv->reqs[queue.front()];
+            queue.pop_front();
             if (q->cancel) {
                 finish(*sv, q, GR_REQ_CANCELLED);
                 continue;
@@ -237,7 +264,14 @@ void bulk_main(gr_ctx *ctx, ServeState *sv) {
         int mode = GR_KERNEL_AUTO;
         int trial = -1;
         ResidentScene *rs = nullptr;
-        {
+        const uint32_t spp = q->r.spp;
+        const uint64_t n_px = q->n_px;
+        gr_status st = GR_OK;
+        if (q->film.alloc((size_t)n_px * 3 * sizeof(float), lane->stream, sv->film_pool) != cudaSuccess) {
+            cudaGetLastError();
+            st = GR_ENOMEM;
+        }
+        if (st == GR_OK) {
             std::lock_guard<std::mutex> lk(ctx->mu);
             auto it = ctx->scenes.find(q->r.scene_id);
             if (it != ctx->scenes.end()) {
@@ -245,17 +279,14 @@ void bulk_main(gr_ctx *ctx, ServeState *sv) {
                 rs->users++;
                 S = rs->S;
                 B = resident_buffers(rs);
+                if (ctx->kernel_mode != GR_KERNEL_SORTED) mode = ctx->kernel_mode;
+                caps = grh::tune_begin(ctx, rs->tune, S, n_px, spp, lane->stream, trial);
+            } else {
+                st = GR_ENOTFOUND;
             }
-            if (ctx->kernel_mode != GR_KERNEL_SORTED) mode = ctx->kernel_mode;
-            // a bulk render is one gr_render_resident call: it takes part in the
-            // stone's schedule tuning (a trial is timed on the bulk stream)
-            if (rs) caps = grh::tune_begin(ctx, rs->tune, S, q->n_px, q->r.spp, sv->bulk_stream, trial);
         }
-        gr_status st = rs ? GR_OK : GR_ENOTFOUND;
-        const uint32_t spp = q->r.spp;
-        const uint64_t n_px = q->n_px;
-        const uint64_t chunk_px = std::max<uint64_t>(1, std::min<uint64_t>(n_px, kBulkChunkBytes / 12 / spp));
-        if (st == GR_OK) st = sv->bulk_xyz.reserve((size_t)chunk_px * spp * 12);
+        const uint64_t chunk_px = std::max<uint64_t>(1, std::min<uint64_t>(n_px, chunk_tuples / spp));
+        if (st == GR_OK) st = lane->xyz.reserve((size_t)chunk_px * spp * 12);
         for (uint64_t first = 0; st == GR_OK && first < n_px; first += chunk_px) {
             if (q->cancel) break;  // between launches
             grd::LaunchRange R;
@@ -264,22 +295,22 @@ void bulk_main(gr_ctx *ctx, ServeState *sv) {
             R.sample_offset = q->r.sample_offset;
             R.spp = spp;
             R.n_tuples = (uint64_t)R.n_pixels * spp;
-            st = grh::launch_trace(ctx, S, B, R, (float *)sv->bulk_xyz.ptr, sv->bulk_stream, mode, &sv->bulk_park, caps);
+            st = grh::launch_trace(ctx, S, B, R, (float *)lane->xyz.ptr, lane->stream, mode, &lane->park, caps);
             if (st == GR_OK)
-                st = grh::launch_fold((const float *)sv->bulk_xyz.ptr, R.n_pixels, spp, R.first_pixel,
-                                      (float *)q->film.ptr, (S.flags & GR_FLAG_KAHAN_FILM) ? 1u : 0u, sv->bulk_stream);
+                st = grh::launch_fold((const float *)lane->xyz.ptr, R.n_pixels, spp, R.first_pixel,
+                                      (float *)q->film.ptr, (S.flags & GR_FLAG_KAHAN_FILM) ? 1u : 0u, lane->stream);
         }
         if (st == GR_OK && q->cancel) {
             // cancelled between launches: no partial pixels -- the film is zero again, as
             // its samples_done (0) says
             const size_t fb = (size_t)n_px * 3 * sizeof(float);
-            if (cudaMemsetAsync(q->film.ptr, 0, fb, sv->bulk_stream) != cudaSuccess) st = GR_ECUDA;
+            if (cudaMemsetAsync(q->film.ptr, 0, fb, lane->stream) != cudaSuccess) st = GR_ECUDA;
         }
         if (rs) {
             std::lock_guard<std::mutex> lk(ctx->mu);
-            grh::tune_end(rs->tune, trial, sv->bulk_stream);
+            grh::tune_end(rs->tune, trial, lane->stream);
         }
-        if (cudaStreamSynchronize(sv->bulk_stream) != cudaSuccess && st == GR_OK) st = GR_ECUDA;
+        if (cudaStreamSynchronize(lane->stream) != cudaSuccess && st == GR_OK) st = GR_ECUDA;
         if (rs) {
             std::lock_guard<std::mutex> lk(ctx->mu);
             rs->users--;
@@ -289,7 +320,7 @@ void bulk_main(gr_ctx *ctx, ServeState *sv) {
         if (st != GR_OK) {
             finish(*sv, q, GR_REQ_FAILED, st);
         } else if (q->cancel) {
-            finish(*sv, q, GR_REQ_CANCELLED);  // a cancelled bulk render keeps no samples (zero film)
+            finish(*sv, q, GR_REQ_CANCELLED);  // a cancelled lane render keeps no samples (zero film)
         } else {
             q->done = spp;
             finish(*sv, q, GR_REQ_DONE);
@@ -482,8 +513,6 @@ ServeState *serve_state(gr_ctx *ctx) {
         int lo = 0, hi = 0;  // the numerically lowest priority is the highest
         cudaDeviceGetStreamPriorityRange(&lo, &hi);
         cudaStreamCreateWithPriority(&ctx->serve->metrics_stream, cudaStreamNonBlocking, hi);
-        if (lo != hi)
-            cudaStreamCreateWithPriority(&ctx->serve->bulk_stream, cudaStreamNonBlocking, GR_SERVE_BULK_HIGH ? hi : lo);
         cudaMemPoolProps props{};
         props.allocType = cudaMemAllocationTypePinned;
         props.location.type = cudaMemLocationTypeDevice;
@@ -499,21 +528,33 @@ ServeState *serve_state(gr_ctx *ctx) {
             ctx->serve->film_pool = pool;
         }
         cudaGetLastError();  // a pool that could not be set up leaves films on the default pool
-        // Scratch of a full tick and of a full bulk chunk, reserved now: growing a
+        // Scratch of a full tick and of each lane's full chunk, reserved now: growing a
         // buffer later frees the old one, which waits for the whole device (every
         // stream's work) and stalls the lanes behind it.
-        const uint64_t bulk_tuples = kBulkChunkBytes / 12;
         ctx->xyz.reserve(std::max<size_t>(ctx->xyz.cap, 2 * kTickTuples * 3 * sizeof(float)));
         ctx->batch_tables.reserve(std::max<size_t>(ctx->batch_tables.cap, (size_t)1 << 20));
         ctx->batch_park.reserve(std::max<size_t>(ctx->batch_park.cap, 4096 + (kTickTuples / 16 + 32 * 1024) * sizeof(grd::Path)));
-        if (ctx->serve->bulk_stream) {
-            ctx->serve->bulk_xyz.reserve(kBulkChunkBytes);
-            ctx->serve->bulk_park.reserve(grh::staged_park_bytes(bulk_tuples));
+        // render lanes, their priorities below the metric sweeps' (the highest): by
+        // default the smallest class next, the largest last
+        for (int c = 0; c < kLaneClasses; ++c) {
+            const int rank = GR_SERVE_LANE_ORDER ? kLaneClasses - 1 - c : c;
+            const int prio = std::min(lo, hi + 1 + rank);  // numerically larger = lower priority
+            for (uint32_t k = 0; k < kLanesPerClass[c]; ++k) {
+                auto *L = new ServeState::Lane();
+                L->cls = c;
+                if (cudaStreamCreateWithPriority(&L->stream, cudaStreamNonBlocking, prio) != cudaSuccess) {
+                    delete L;
+                    continue;
+                }
+                L->xyz.reserve((size_t)kClassTuples[c] * 12);
+                L->park.reserve(grh::staged_park_bytes(kClassTuples[c]));
+                ctx->serve->lanes.push_back(L);
+            }
         }
         cudaGetLastError();  // a reservation that failed is retried (grown) where it is used
         ctx->serve->worker = std::thread(worker_main, ctx, ctx->serve);
         ctx->serve->metrics_worker = std::thread(metrics_main, ctx, ctx->serve);
-        if (ctx->serve->bulk_stream) ctx->serve->bulk_worker = std::thread(bulk_main, ctx, ctx->serve);
+        for (auto *L : ctx->serve->lanes) L->th = std::thread(lane_main, ctx, ctx->serve, L);
     }
     return ctx->serve;
 }
@@ -545,10 +586,11 @@ void serve_shutdown(gr_ctx *ctx) {
     }
     sv->cv_work.notify_all();
     sv->cv_metrics.notify_all();
-    sv->cv_bulk.notify_all();
+    sv->cv_lane.notify_all();
     if (sv->worker.joinable()) sv->worker.join();
     if (sv->metrics_worker.joinable()) sv->metrics_worker.join();
-    if (sv->bulk_worker.joinable()) sv->bulk_worker.join();
+    for (auto *L : sv->lanes)
+        if (L->th.joinable()) L->th.join();
     cudaSetDevice(ctx->device);
     for (auto &kv : sv->reqs) {
         kv.second->film.release(ctx->stream);
@@ -558,9 +600,14 @@ void serve_shutdown(gr_ctx *ctx) {
     cudaStreamSynchronize(ctx->stream);  // stream-ordered frees above complete
     if (sv->film_pool) cudaMemPoolDestroy(sv->film_pool);
     if (sv->metrics_stream) cudaStreamDestroy(sv->metrics_stream);
-    if (sv->bulk_stream) cudaStreamDestroy(sv->bulk_stream);
-    sv->bulk_xyz.release();
-    sv->bulk_park.release();
+    for (auto *L : sv->lanes) {
+        cudaStreamSynchronize(L->stream);
+        cudaStreamDestroy(L->stream);
+        L->xyz.release();
+        L->park.release();
+        delete L;
+    }
+    sv->lanes.clear();
     delete sv;
     ctx->serve = nullptr;
 }
@@ -720,7 +767,7 @@ gr_status gr_request_release(gr_ctx *ctx, uint64_t id) {
         if (!q) return fail(GR_ENOTFOUND, "unknown request id %llu", (unsigned long long)id);
         if (q->state == GR_REQ_QUEUED || q->state == GR_REQ_RUNNING)
             return fail(GR_EBUSY, "request %llu is still active (cancel it first)", (unsigned long long)id);
-        if (q->film.ptr) sv->film_bytes -= q->film_bytes;
+        if (q->admitted) sv->film_bytes -= q->film_bytes;
         sv->reqs.erase(id);
     }
     std::lock_guard<std::mutex> lk(ctx->mu);

@@ -473,10 +473,11 @@ gr_status gr_render_batch(gr_ctx *ctx, const gr_batch_item *items, uint32_t n_it
  * sweep.  Pointers are copied at submit. */
 typedef struct gr_request {
     uint32_t kind;
-    uint32_t slice_spp;      /* render: at most this many samples per pixel per tick, 0 = no cap (a tick
-                                carries ~8.4 M path-samples, filled from the running renders in arrival
-                                order).  Progress, interleaving and cancellation happen between slices;
-                                the film does not depend on the slicing */
+    uint32_t slice_spp;      /* render: > 0: at most this many samples per pixel per tick (a tick
+                                carries ~8.4 M path-samples in one batched launch, filled from the
+                                running sliced renders in arrival order); progress and cancellation
+                                happen between slices.  0: rendered whole by a render lane of its
+                                size class (see gr_submit).  The film does not depend on either */
     uint64_t scene_id;       /* render: resident scene */
     uint32_t sample_offset;  /* render: first absolute sample */
     uint32_t spp;            /* render: samples per pixel */
@@ -509,16 +510,23 @@ typedef struct gr_request_status {
  * which renders one dispatch at a time; the worker's render loop is
  * apps/gemray-worker/src/render_core/mod.rs).  A worker thread admits requests in
  * arrival order while their film (W*H*3 f32) fits the context's serve budget next to
- * the resident scenes and unreleased films, and advances every running render by one
- * slice per tick in a shared batched launch; metric requests hold no film and run on
- * a second worker thread in arrival order, beside the renders.  Slices continue each pixel's running
- * sum, so a film is bit-identical to one gr_render_resident call over the same sample
- * range on a zero film -- for any slicing, alone or in any mix. */
+ * the resident scenes and unreleased films.  A render with slice_spp == 0 goes to a
+ * render lane of its size class (up to 2 M path-samples: two lanes; up to 8 M: one;
+ * larger: one), which renders it whole with the single-scene kernels and the stone's
+ * tuned schedule on the lane's own stream -- the smaller the class, the higher the
+ * stream priority, so small requests do not wait behind large ones; the lanes run at
+ * once.  A sliced render (slice_spp > 0) advances by one slice per tick in a shared
+ * batched launch.  Metric requests hold no film and run on another worker thread in
+ * arrival order at the highest stream priority, beside the renders.  Slices continue
+ * each pixel's running sum, so a film is bit-identical to one gr_render_resident call
+ * over the same sample range on a zero film -- lane or ticks, for any slicing, alone
+ * or in any mix. */
 gr_status gr_submit(gr_ctx *ctx, const gr_request *request, uint64_t *request_id);
 gr_status gr_poll(gr_ctx *ctx, uint64_t request_id, gr_request_status *status);
 /* Blocks until the request has finished or timeout_ms passed (GR_ETIMEOUT). */
 gr_status gr_wait(gr_ctx *ctx, uint64_t request_id, uint32_t timeout_ms, gr_request_status *status);
-/* Stops a request between slices; its film keeps the slices already folded. */
+/* Stops a request between slices (a sliced render's film keeps the slices already
+ * folded) or, in a lane, before it starts or between its launches (the film is zero). */
 gr_status gr_cancel(gr_ctx *ctx, uint64_t request_id);
 /* Copies a finished (or cancelled) render's film, W*H*3 f32, to host memory. */
 gr_status gr_request_film(gr_ctx *ctx, uint64_t request_id, float *xyz_host);
@@ -687,12 +695,12 @@ gr_status gr_set_kernel(gr_ctx *ctx, uint32_t kernel);
  * the resident blocks per SM the kernels' register allocation targets (9, 10, 12 or 16:
  * 56, 48, 40 or 32 registers per thread).  Every schedule gives the same films; the
  * fastest depends on the stone (measured on B200: caps 12 / 20 on the c2 brilliant,
- * 8 / 16 on the c3 emerald, 3.9% faster there; 12 blocks per SM 4.6% faster than 9 on
+ * 8 / 16 on the c3 emerald, 3.8% faster there; 16 blocks per SM 6-8% faster than 9 on
  * both).  From the scene's second staged gr_render_resident call on, calls are timed with
  * device events as trials, in two rounds: caps 12 / 20 at each blocks-per-SM target, then
  * caps 8 / 16 and 16 / 28 at the fastest target; the schedule with the least time per
  * tuple is kept for the scene and entered in the context's tuning table.  Writes zeros
- * while the choice is still open (the built-in schedule, caps 12 / 20 at 12 blocks per
+ * while the choice is still open (the built-in schedule, caps 12 / 20 at 16 blocks per
  * SM, runs meanwhile).  Batched launches (gr_render_batch, the request loop) run each
  * scene with its chosen first cap (their continuation stage is uncapped); gr_accumulate
  * and gr_accumulate_device choose the same way per stone (planes, finishes, material,

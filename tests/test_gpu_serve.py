@@ -160,13 +160,13 @@ def test_admission_by_memory_budget(engine_lib):
         r.close()
 
 
-def test_large_requests_render_whole_beside_small_ones(engine_lib):
-    """Renders of more path-samples than one tick carries (~8.4 M, no slice_spp) go to
-    the bulk lane: rendered whole with the single-scene kernels on a low-priority stream
-    while the small requests' ticks run beside them.  Every film -- bulk (a Kahan scene
-    among them) or ticked -- is bit-identical to one gr_render_resident call over its
-    range on a zero film; a bulk render cancelled before it starts ends with no samples
-    and a zero film."""
+def test_lanes_render_every_size_class_beside_ticks(engine_lib):
+    """Renders without a slice_spp go to the render lanes by size (<= 2 M path-samples,
+    <= 8 M, larger), each rendered whole with the single-scene kernels on its lane's
+    stream, several at once; sliced renders go to the ticks beside them.  Every film --
+    each lane class (a Kahan scene among them) and ticked -- is bit-identical to one
+    gr_render_resident call over its range on a zero film; a lane render cancelled
+    before it starts ends with no samples and a zero film."""
     srv = RenderServer()
     try:
         small = _scenes()
@@ -179,14 +179,18 @@ def test_large_requests_render_whole_beside_small_ones(engine_lib):
                        flags=abi.GR_FLAG_KAHAN_FILM)]
         big_ids = [srv.upload(sc) for sc in big]
         small_ids = [srv.upload(sc) for sc in small]
-        jobs = [(big_ids[0], (128, 128), 5, 600), (big_ids[1], (96, 96), 0, 1000)]
-        assert all(w * h * spp > (8 << 20) for _, (w, h), _, spp in jobs)
+        jobs = [(big_ids[0], (128, 128), 5, 600), (big_ids[1], (96, 96), 0, 1000), (big_ids[0], (128, 128), 9, 200),
+                (big_ids[1], (96, 96), 3, 300)]
+        sizes = [w * h * spp for _, (w, h), _, spp in jobs]
+        assert sizes[0] > (8 << 20) and sizes[1] > (8 << 20) and (2 << 20) < sizes[2] <= (8 << 20)
+        assert (2 << 20) < sizes[3] <= (8 << 20)
         rids = [srv.submit_render(sid, off, spp) for sid, _, off, spp in jobs]
         cancelled = srv.submit_render(big_ids[0], 0, 600)
         srv.cancel(cancelled)
         shapes = [(48, 40), (32, 32), (24, 30)]
         srids = [srv.submit_render(small_ids[k], 3 * k, 24 + 8 * k) for k in range(3)]
-        for r in rids + srids:
+        sliced = srv.submit_render(small_ids[0], 50, 40, slice_spp=8)
+        for r in rids + srids + [sliced]:
             assert srv.wait(r).state == "done"
         st = srv.wait(cancelled)
         assert st.state == "cancelled" and st.samples_done == 0
@@ -196,6 +200,9 @@ def test_large_requests_render_whole_beside_small_ones(engine_lib):
         for k, r in enumerate(srids):
             ref = _resident(srv, small_ids[k], shapes[k], 3 * k, 24 + 8 * k)
             assert np.array_equal(srv.film(r).view(np.uint32), ref.view(np.uint32))
+        ref = _resident(srv, small_ids[0], shapes[0], 50, 40)
+        assert np.array_equal(srv.film(sliced).view(np.uint32), ref.view(np.uint32))
+        srv.release(sliced)
         for r in rids + srids + [cancelled]:
             srv.release(r)
     finally:

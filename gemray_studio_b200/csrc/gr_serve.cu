@@ -92,6 +92,7 @@ struct Request {
     bool kahan = false;
     StreamBuffer film, comp;
     uint32_t issued = 0, done = 0, in_flight = 0;  // samples per pixel
+    uint64_t px_done = 0;  // lane renders: pixels whose samples are all folded
     bool cancel = false;
     int lane_class = -1;  // rendered whole by a lane of this size class; -1: in ticks
     bool admitted = false;  // film_bytes counted in the serve budget
@@ -133,6 +134,19 @@ constexpr uint64_t kFilmPoolReserve = 4ull << 30;
 #ifndef GR_SERVE_LANE_ORDER
 #define GR_SERVE_LANE_ORDER 0
 #endif
+// Lane policy: 0 = size classes, each request rendered whole by a lane of its class;
+// 1 = one shared queue, shortest remaining work first: a lane renders one chunk of
+// GR_SERVE_CHUNK_MTUPLES path-samples of the request with the least work left, then
+// chooses again (GR_SERVE_SRPT_LANES lanes).
+#ifndef GR_SERVE_POLICY
+#define GR_SERVE_POLICY 0
+#endif
+#ifndef GR_SERVE_CHUNK_MTUPLES
+#define GR_SERVE_CHUNK_MTUPLES 4
+#endif
+#ifndef GR_SERVE_SRPT_LANES
+#define GR_SERVE_SRPT_LANES 1
+#endif
 constexpr int kLaneClasses = 3;
 constexpr uint32_t kLanesPerClass[kLaneClasses] = {2, 1, 1};
 constexpr uint64_t kClassTuples[kLaneClasses] = {(uint64_t)GR_SERVE_SMALL_MTUPLES << 20,
@@ -165,6 +179,7 @@ struct ServeState {
     std::vector<Lane *> lanes;
     std::condition_variable cv_lane;
     std::deque<uint64_t> lane_queue[kLaneClasses];  // admitted lane renders per class, admission order
+    std::vector<uint64_t> lane_pending;  // policy 1: renders with pixels left, none of them in a lane
     cudaMemPool_t film_pool = nullptr;      // request films (null: the device's default pool)
     std::condition_variable cv_work, cv_done, cv_metrics;
     std::unordered_map<uint64_t, Request *> reqs;
@@ -210,7 +225,10 @@ void admit(gr_ctx *ctx, ServeState &sv, uint64_t resident_bytes) {
             q->state = GR_REQ_RUNNING;
             q->t_admit = Clock::now();
             q->lane_class = lane_class((uint64_t)q->r.spp * q->n_px);
-            sv.lane_queue[q->lane_class].push_back(q->id);
+            if (GR_SERVE_POLICY == 1)
+                sv.lane_pending.push_back(q->id);
+            else
+                sv.lane_queue[q->lane_class].push_back(q->id);
             sv.cv_lane.notify_all();
             continue;
         }
@@ -232,99 +250,141 @@ void admit(gr_ctx *ctx, ServeState &sv, uint64_t resident_bytes) {
     }
 }
 
-// A render lane: the admitted renders of its size class one at a time, each on a
-// zero film taken from the film pool on the lane's stream, its whole sample range
-// traced chunk by chunk with the single-scene kernels (the stone's tuned schedule,
-// which the lane's calls help choose like gr_render_resident calls; never the sorted
-// kernel, whose blocks stay resident until its launch ends) and each chunk's pixels
-// folded in add mode -- the film of one gr_render_resident call over the range, which
-// is what the sliced path produces too.  The scene is marked in use meanwhile, so it
-// cannot be released under the launches.
+// One chunk of a lane render: pixels [first, first + count) of request q over its whole
+// sample range, traced with the single-scene kernels (the stone's tuned schedule,
+// which lane chunks help choose like gr_render_resident calls; never the sorted
+// kernel, whose blocks stay resident until its launch ends) and folded in add mode onto
+// its film, on the lane's stream; returns after the stream has drained.  The first
+// chunk takes the zero film from the loop's pool on the lane's stream.  The scene is
+// marked in use meanwhile, so it cannot be released under the launches.
+gr_status lane_chunk(gr_ctx *ctx, ServeState *sv, ServeState::Lane *lane, Request *q, uint64_t first, uint64_t count) {
+    const uint32_t spp = q->r.spp;
+    gr_status st = GR_OK;
+    if (!q->film.ptr && q->film.alloc((size_t)q->n_px * 3 * sizeof(float), lane->stream, sv->film_pool) != cudaSuccess) {
+        cudaGetLastError();
+        return GR_ENOMEM;
+    }
+    SceneConst S;
+    grd::SceneBuffers B;
+    StageCaps caps;
+    int mode = GR_KERNEL_AUTO;
+    int trial = -1;
+    ResidentScene *rs = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        auto it = ctx->scenes.find(q->r.scene_id);
+        if (it == ctx->scenes.end()) return GR_ENOTFOUND;
+        rs = it->second;
+        rs->users++;
+        S = rs->S;
+        B = resident_buffers(rs);
+        if (ctx->kernel_mode != GR_KERNEL_SORTED) mode = ctx->kernel_mode;
+        caps = grh::tune_begin(ctx, rs->tune, S, count, spp, lane->stream, trial);
+    }
+    const uint64_t step_px = std::max<uint64_t>(1, std::min<uint64_t>(count, kClassTuples[2] / spp));
+    st = lane->xyz.reserve((size_t)step_px * spp * 12);
+    for (uint64_t p = first; st == GR_OK && p < first + count; p += step_px) {
+        if (q->cancel) break;  // between launches
+        grd::LaunchRange R;
+        R.first_pixel = (uint32_t)p;
+        R.n_pixels = (uint32_t)std::min<uint64_t>(step_px, first + count - p);
+        R.sample_offset = q->r.sample_offset;
+        R.spp = spp;
+        R.n_tuples = (uint64_t)R.n_pixels * spp;
+        st = grh::launch_trace(ctx, S, B, R, (float *)lane->xyz.ptr, lane->stream, mode, &lane->park, caps);
+        if (st == GR_OK)
+            st = grh::launch_fold((const float *)lane->xyz.ptr, R.n_pixels, spp, R.first_pixel, (float *)q->film.ptr,
+                                  (S.flags & GR_FLAG_KAHAN_FILM) ? 1u : 0u, lane->stream);
+    }
+    {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        grh::tune_end(rs->tune, trial, lane->stream);
+    }
+    if (cudaStreamSynchronize(lane->stream) != cudaSuccess && st == GR_OK) st = GR_ECUDA;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    rs->users--;
+    return st;
+}
+
+// Ends a lane render (caller holds sv->mu).  A cancelled one keeps no samples: its film,
+// if it has one, is zeroed on the lane's stream first.
+void lane_finish(ServeState *sv, ServeState::Lane *lane, Request *q, gr_status st) {
+    q->in_flight = 0;
+    if (st != GR_OK) {
+        finish(*sv, q, GR_REQ_FAILED, st);
+    } else if (q->cancel) {
+        if (q->film.ptr) {
+            cudaMemsetAsync(q->film.ptr, 0, (size_t)q->n_px * 3 * sizeof(float), lane->stream);
+            cudaStreamSynchronize(lane->stream);
+        }
+        finish(*sv, q, GR_REQ_CANCELLED);
+    } else {
+        q->done = q->r.spp;
+        finish(*sv, q, GR_REQ_DONE);
+    }
+}
+
+// A render lane.  Policy 0: the admitted renders of the lane's size class, one at a
+// time, each rendered whole (in chunks of the class's size).  Policy 1: from the shared
+// pending list, the render with the least work left, one chunk of it, then choose again
+// -- a request that arrives during a long render waits at most one chunk.
 void lane_main(gr_ctx *ctx, ServeState *sv, ServeState::Lane *lane) {
     cudaSetDevice(ctx->device);
-    const uint64_t chunk_tuples = kClassTuples[lane->cls];
     for (;;) {
-        Request *q;
+        Request *q = nullptr;
+        uint64_t first = 0, count = 0;
         {
             std::unique_lock<std::mutex> lk(sv->mu);
-            auto &queue = sv->lane_queue[lane->cls];
-            sv->cv_lane.wait(lk, [&] { return sv->stop || !queue.empty(); });
-            if (queue.empty()) return;  // stopping, nothing left
-            q = sv->reqs[queue.front()];
-            queue.pop_front();
+            if (GR_SERVE_POLICY == 1) {
+                sv->cv_lane.wait(lk, [&] { return sv->stop || !sv->lane_pending.empty(); });
+                if (sv->lane_pending.empty()) return;  // stopping, nothing left
+                size_t pick = 0;
+                uint64_t least = UINT64_MAX;
+                for (size_t i = 0; i < sv->lane_pending.size(); ++i) {
+                    const Request *c = sv->reqs[sv->lane_pending[i]];
+                    const uint64_t left = (c->n_px - c->px_done) * c->r.spp;
+                    if (left < least) {
+                        least = left;
+                        pick = i;
+                    }
+                }
+                q = sv->reqs[sv->lane_pending[pick]];
+                sv->lane_pending.erase(sv->lane_pending.begin() + (ptrdiff_t)pick);
+                const uint64_t chunk_px = std::max<uint64_t>(1, ((uint64_t)GR_SERVE_CHUNK_MTUPLES << 20) / q->r.spp);
+                first = q->px_done;
+                count = std::min<uint64_t>(chunk_px, q->n_px - first);
+            } else {
+                auto &queue = sv->lane_queue[lane->cls];
+                sv->cv_lane.wait(lk, [&] { return sv->stop || !queue.empty(); });
+                if (queue.empty()) return;  // stopping, nothing left
+                q = sv->reqs[queue.front()];
+                queue.pop_front();
+                first = 0;
+                count = q->n_px;
+            }
             if (q->cancel) {
-                finish(*sv, q, GR_REQ_CANCELLED);
+                lane_finish(sv, lane, q, GR_OK);
                 continue;
             }
             q->issued = q->in_flight = q->r.spp;
         }
-        SceneConst S;
-        grd::SceneBuffers B;
-        StageCaps caps;
-        int mode = GR_KERNEL_AUTO;
-        int trial = -1;
-        ResidentScene *rs = nullptr;
-        const uint32_t spp = q->r.spp;
-        const uint64_t n_px = q->n_px;
         gr_status st = GR_OK;
-        if (q->film.alloc((size_t)n_px * 3 * sizeof(float), lane->stream, sv->film_pool) != cudaSuccess) {
-            cudaGetLastError();
-            st = GR_ENOMEM;
-        }
-        if (st == GR_OK) {
-            std::lock_guard<std::mutex> lk(ctx->mu);
-            auto it = ctx->scenes.find(q->r.scene_id);
-            if (it != ctx->scenes.end()) {
-                rs = it->second;
-                rs->users++;
-                S = rs->S;
-                B = resident_buffers(rs);
-                if (ctx->kernel_mode != GR_KERNEL_SORTED) mode = ctx->kernel_mode;
-                caps = grh::tune_begin(ctx, rs->tune, S, n_px, spp, lane->stream, trial);
-            } else {
-                st = GR_ENOTFOUND;
-            }
-        }
-        const uint64_t chunk_px = std::max<uint64_t>(1, std::min<uint64_t>(n_px, chunk_tuples / spp));
-        if (st == GR_OK) st = lane->xyz.reserve((size_t)chunk_px * spp * 12);
-        for (uint64_t first = 0; st == GR_OK && first < n_px; first += chunk_px) {
-            if (q->cancel) break;  // between launches
-            grd::LaunchRange R;
-            R.first_pixel = (uint32_t)first;
-            R.n_pixels = (uint32_t)std::min<uint64_t>(chunk_px, n_px - first);
-            R.sample_offset = q->r.sample_offset;
-            R.spp = spp;
-            R.n_tuples = (uint64_t)R.n_pixels * spp;
-            st = grh::launch_trace(ctx, S, B, R, (float *)lane->xyz.ptr, lane->stream, mode, &lane->park, caps);
-            if (st == GR_OK)
-                st = grh::launch_fold((const float *)lane->xyz.ptr, R.n_pixels, spp, R.first_pixel,
-                                      (float *)q->film.ptr, (S.flags & GR_FLAG_KAHAN_FILM) ? 1u : 0u, lane->stream);
-        }
-        if (st == GR_OK && q->cancel) {
-            // cancelled between launches: no partial pixels -- the film is zero again, as
-            // its samples_done (0) says
-            const size_t fb = (size_t)n_px * 3 * sizeof(float);
-            if (cudaMemsetAsync(q->film.ptr, 0, fb, lane->stream) != cudaSuccess) st = GR_ECUDA;
-        }
-        if (rs) {
-            std::lock_guard<std::mutex> lk(ctx->mu);
-            grh::tune_end(rs->tune, trial, lane->stream);
-        }
-        if (cudaStreamSynchronize(lane->stream) != cudaSuccess && st == GR_OK) st = GR_ECUDA;
-        if (rs) {
-            std::lock_guard<std::mutex> lk(ctx->mu);
-            rs->users--;
+        if (GR_SERVE_POLICY == 1) {
+            st = lane_chunk(ctx, sv, lane, q, first, count);
+        } else {
+            const uint64_t chunk_px = std::max<uint64_t>(1, kClassTuples[lane->cls] / q->r.spp);
+            for (uint64_t p = 0; st == GR_OK && p < q->n_px && !q->cancel; p += chunk_px)
+                st = lane_chunk(ctx, sv, lane, q, p, std::min<uint64_t>(chunk_px, q->n_px - p));
+            count = q->n_px - first;
         }
         std::lock_guard<std::mutex> lk(sv->mu);
-        q->in_flight = 0;
-        if (st != GR_OK) {
-            finish(*sv, q, GR_REQ_FAILED, st);
-        } else if (q->cancel) {
-            finish(*sv, q, GR_REQ_CANCELLED);  // a cancelled lane render keeps no samples (zero film)
-        } else {
-            q->done = spp;
-            finish(*sv, q, GR_REQ_DONE);
+        q->px_done = first + count;
+        if (st == GR_OK && !q->cancel && q->px_done < q->n_px) {
+            sv->lane_pending.push_back(q->id);  // policy 1: more chunks to come
+            sv->cv_lane.notify_all();
+            continue;
         }
+        lane_finish(sv, lane, q, st);
     }
 }
 
@@ -538,8 +598,9 @@ ServeState *serve_state(gr_ctx *ctx) {
         // default the smallest class next, the largest last
         for (int c = 0; c < kLaneClasses; ++c) {
             const int rank = GR_SERVE_LANE_ORDER ? kLaneClasses - 1 - c : c;
-            const int prio = std::min(lo, hi + 1 + rank);  // numerically larger = lower priority
-            for (uint32_t k = 0; k < kLanesPerClass[c]; ++k) {
+            const int prio = std::min(lo, hi + 1 + (GR_SERVE_POLICY == 1 ? 0 : rank));  // larger = lower priority
+            const uint32_t n_lanes = GR_SERVE_POLICY == 1 ? (c == 2 ? GR_SERVE_SRPT_LANES : 0) : kLanesPerClass[c];
+            for (uint32_t k = 0; k < n_lanes; ++k) {
                 auto *L = new ServeState::Lane();
                 L->cls = c;
                 if (cudaStreamCreateWithPriority(&L->stream, cudaStreamNonBlocking, prio) != cudaSuccess) {

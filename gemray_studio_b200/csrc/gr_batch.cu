@@ -289,13 +289,44 @@ gr_status batch_enqueue(gr_ctx *ctx, const BatchItem *items, uint32_t n_items, u
 
 }  // namespace grh
 
+// Items of at least this many path-samples render with the single-scene kernels (the
+// stone's tuned schedule) instead of in a shared launch: one launch of ~2 M tuples
+// already fills a B200 for many waves, and the specialised single-scene kernels at the
+// stone's blocks-per-SM target run such a launch faster than the general batched
+// kernels (measured on the c4 stones at full size: 577 M path-samples/s one stone at a
+// time against 526 M packed).
+#ifndef GR_BATCH_SOLO_MTUPLES
+#define GR_BATCH_SOLO_MTUPLES 2
+#endif
+
 extern "C" gr_status gr_render_batch(gr_ctx *ctx, const gr_batch_item *items, uint32_t n_items, uint32_t flags,
                                      void *stream) {
     if (!ctx) return fail(GR_EINVAL, "ctx is NULL");
     if (n_items && !items) return fail(GR_EINVAL, "items is NULL");
-    std::vector<grh::BatchItem> bi(n_items);
-    for (uint32_t i = 0; i < n_items; ++i) bi[i] = grh::BatchItem{items[i], nullptr, 0u};
     std::lock_guard<std::mutex> lk(ctx->mu);
     GR_CUDA(cudaSetDevice(ctx->device));
-    return grh::batch_enqueue(ctx, bi.data(), n_items, flags, (cudaStream_t)stream);
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    std::vector<grh::BatchItem> packed;
+    std::vector<std::pair<ResidentScene *, const gr_batch_item *>> solo;
+    for (uint32_t i = 0; i < n_items; ++i) {
+        const gr_batch_item &it = items[i];
+        auto f = ctx->scenes.find(it.scene_id);
+        if (f == ctx->scenes.end())
+            return fail(GR_ENOTFOUND, "item %u: unknown scene id %llu", i, (unsigned long long)it.scene_id);
+        ResidentScene *rs = f->second;
+        const uint64_t tuples = (uint64_t)rs->S.width * rs->S.height * it.spp;
+        if (tuples && !it.film_device) return fail(GR_EINVAL, "item %u: film is NULL", i);
+        if (rs->S.flags & GR_FLAG_FP64_RESOLVE)
+            return fail(GR_EINVAL, "item %u: GR_FLAG_FP64_RESOLVE scenes render through the single-scene calls", i);
+        if (tuples >= ((uint64_t)GR_BATCH_SOLO_MTUPLES << 20))
+            solo.emplace_back(rs, &it);
+        else
+            packed.push_back(grh::BatchItem{it, nullptr, 0u});
+    }
+    for (auto &p : solo) {
+        const gr_status st = grh::render_resident_locked(ctx, p.first, p.second->sample_offset, p.second->spp,
+                                                         p.second->film_device, s);
+        if (st != GR_OK) return st;
+    }
+    return grh::batch_enqueue(ctx, packed.data(), (uint32_t)packed.size(), flags, s);
 }

@@ -179,6 +179,10 @@ struct BatchItem {
     float *comp;
     uint32_t cont;
 };
+// gr_render_resident's body (the stone's tuned schedule, its trials included); the
+// caller holds ctx->mu and has made ctx->device current.
+gr_status render_resident_locked(gr_ctx *ctx, ResidentScene *rs, uint32_t sample_offset, uint32_t spp, float *film_dev,
+                                 cudaStream_t s);
 // gr_render_batch's body; the caller holds ctx->mu and has made ctx->device current.
 gr_status batch_enqueue(gr_ctx *ctx, const BatchItem *items, uint32_t n_items, uint32_t flags, cudaStream_t stream);
 }  // namespace grh

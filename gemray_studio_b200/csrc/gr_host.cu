@@ -1013,6 +1013,26 @@ gr_status gr_scene_release(gr_ctx *ctx, uint64_t id) {
 }
 
 
+}  // extern "C"
+
+namespace grh {
+gr_status render_resident_locked(gr_ctx *ctx, ResidentScene *rs, uint32_t sample_offset, uint32_t spp, float *film_dev,
+                                 cudaStream_t s) {
+    const uint64_t n_pixels = (uint64_t)rs->S.width * rs->S.height;
+    gr_scene shape;
+    std::memset(&shape, 0, sizeof(shape));
+    shape.width = rs->S.width;
+    shape.height = rs->S.height;
+    int trial = -1;
+    const StageCaps caps = tune_begin(ctx, rs->tune, rs->S, n_pixels, spp, s, trial);
+    gr_status st = render_into(ctx, &shape, rs->S, resident_buffers(rs), sample_offset, spp, film_dev, s, caps);
+    tune_end(rs->tune, trial, s);
+    return st;
+}
+}  // namespace grh
+
+extern "C" {
+
 gr_status gr_render_resident(gr_ctx *ctx, uint64_t id, uint32_t sample_offset, uint32_t spp, float *film_dev,
                              void *stream) {
     if (!ctx) return fail(GR_EINVAL, "ctx is NULL");
@@ -1025,16 +1045,7 @@ gr_status gr_render_resident(gr_ctx *ctx, uint64_t id, uint32_t sample_offset, u
     if (!film_dev) return fail(GR_EINVAL, "film is NULL");
     GR_CUDA(cudaSetDevice(ctx->device));
     cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
-    gr_scene shape;
-    std::memset(&shape, 0, sizeof(shape));
-    shape.width = rs->S.width;
-    shape.height = rs->S.height;
-    int trial = -1;
-    const StageCaps caps =
-        grh::tune_begin(ctx, rs->tune, rs->S, n_pixels, spp, s, trial);
-    gr_status st = grh::render_into(ctx, &shape, rs->S, resident_buffers(rs), sample_offset, spp, film_dev, s, caps);
-    grh::tune_end(rs->tune, trial, s);
-    return st;
+    return grh::render_resident_locked(ctx, rs, sample_offset, spp, film_dev, s);
 }
 
 gr_status gr_scene_stage_caps(gr_ctx *ctx, uint64_t id, uint32_t *cap_first, uint32_t *cap_second) {

@@ -454,12 +454,15 @@ typedef struct gr_batch_item {
  * batch shape (scenes, films, spp, frame sizes) recurs; sample offsets may change. */
 #define GR_BATCH_GRAPH 0x1u
 
-/* Renders all items in shared launches (no counterpart in the reference, whose
- * frame renderer takes one scene per dispatch, renderer/gpu/frame.rs:632-814): scenes
- * of any plane count, material and frame size are packed into launches of at most
- * the context's chunk budget of per-tuple scratch.  Each film is bit-identical to
- * gr_render_resident of its item alone.  Work is queued on `stream` (NULL = the
- * context stream) and the call returns without waiting for it. */
+/* Renders all items (no counterpart in the reference, whose frame renderer takes one
+ * scene per dispatch, renderer/gpu/frame.rs:632-814): items under 2 M path-samples --
+ * scenes of any plane count, material and frame size -- are packed into shared
+ * launches of at most the context's chunk budget of per-tuple scratch (GR_BATCH_GRAPH
+ * applies to these); larger items, which fill the device on their own, render with
+ * the single-scene kernels and their stone's tuned schedule, as gr_render_resident
+ * does, before them.  Each film is bit-identical to gr_render_resident of its item
+ * alone.  Work is queued on `stream` (NULL = the context stream) and the call returns
+ * without waiting for it. */
 gr_status gr_render_batch(gr_ctx *ctx, const gr_batch_item *items, uint32_t n_items, uint32_t flags, void *stream);
 
 /* ---- serving: render requests over resident scenes ------------------------------ */

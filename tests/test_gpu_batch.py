@@ -90,11 +90,32 @@ def test_batch_edge_cases(engine_lib, ctx):
     assert lib.gr_render_batch(ctx, items, 2, 0, None) == abi.GR_ENOTFOUND
     items[1] = abi.gr_batch_item(sid, None, 0, 4)
     assert lib.gr_render_batch(ctx, items, 2, 0, None) == abi.GR_EINVAL
-    # spp larger than the whole chunk budget: one pixel per launch
-    items = (abi.gr_batch_item * 1)(abi.gr_batch_item(sid, film.data_ptr(), 0, 10000))
-    ref = torch.zeros_like(film)
+    # spp larger than the whole chunk budget: one pixel per packed launch (a 12x12 frame
+    # stays under the 2 M path-samples from which an item renders on its own)
+    tiny = _scenes()[0]
+    tiny.width = tiny.height = 12
+    (tid,) = _upload(lib, ctx, [tiny])
+    tfilm = torch.zeros((144, 3), dtype=torch.float32, device="cuda")
+    items = (abi.gr_batch_item * 1)(abi.gr_batch_item(tid, tfilm.data_ptr(), 0, 10000))
+    ref = torch.zeros_like(tfilm)
     torch.cuda.synchronize()
     assert lib.gr_render_batch(ctx, items, 1, 0, None) == abi.GR_OK
-    assert lib.gr_render_resident(ctx, sid, 0, 10000, C.c_void_p(ref.data_ptr()), None) == abi.GR_OK
+    assert lib.gr_render_resident(ctx, tid, 0, 10000, C.c_void_p(ref.data_ptr()), None) == abi.GR_OK
     assert lib.gr_synchronize(ctx) == abi.GR_OK
-    assert torch.equal(film, ref)
+    assert torch.equal(tfilm, ref)
+    # an item of 2 M path-samples or more renders with the single-scene kernels, beside
+    # packed ones: every film is still gr_render_resident's
+    small = _scenes()[1]
+    (smid,) = _upload(lib, ctx, [small])
+    sfilm = torch.zeros((small.width * small.height, 3), dtype=torch.float32, device="cuda")
+    film.zero_()
+    items = (abi.gr_batch_item * 2)(abi.gr_batch_item(sid, film.data_ptr(), 7, 1200),
+                                    abi.gr_batch_item(smid, sfilm.data_ptr(), 3, 40))
+    assert sc.width * sc.height * 1200 >= (2 << 20)
+    ref, sref = torch.zeros_like(film), torch.zeros_like(sfilm)
+    torch.cuda.synchronize()
+    assert lib.gr_render_batch(ctx, items, 2, abi.GR_BATCH_GRAPH, None) == abi.GR_OK
+    assert lib.gr_render_resident(ctx, sid, 7, 1200, C.c_void_p(ref.data_ptr()), None) == abi.GR_OK
+    assert lib.gr_render_resident(ctx, smid, 3, 40, C.c_void_p(sref.data_ptr()), None) == abi.GR_OK
+    assert lib.gr_synchronize(ctx) == abi.GR_OK
+    assert torch.equal(film, ref) and torch.equal(sfilm, sref) and film.any()

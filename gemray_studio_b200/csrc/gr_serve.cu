@@ -137,7 +137,9 @@ constexpr uint64_t kFilmPoolReserve = 4ull << 30;
 // Lane policy: 0 = size classes, each request rendered whole by a lane of its class;
 // 1 = one shared queue, shortest remaining work first: a lane renders one chunk of
 // GR_SERVE_CHUNK_MTUPLES path-samples of the request with the least work left, then
-// chooses again (GR_SERVE_SRPT_LANES lanes).
+// chooses again (GR_SERVE_SRPT_LANES lanes at one priority); 2 = the same chunks taken
+// oldest request first by GR_SERVE_SRPT_LANES lanes of descending stream priority, so
+// the oldest renders run as if alone and younger ones fill the SMs they leave idle.
 #ifndef GR_SERVE_POLICY
 #define GR_SERVE_POLICY 0
 #endif
@@ -225,7 +227,7 @@ void admit(gr_ctx *ctx, ServeState &sv, uint64_t resident_bytes) {
             q->state = GR_REQ_RUNNING;
             q->t_admit = Clock::now();
             q->lane_class = lane_class((uint64_t)q->r.spp * q->n_px);
-            if (GR_SERVE_POLICY == 1)
+            if (GR_SERVE_POLICY != 0)
                 sv.lane_pending.push_back(q->id);
             else
                 sv.lane_queue[q->lane_class].push_back(q->id);
@@ -335,16 +337,16 @@ void lane_main(gr_ctx *ctx, ServeState *sv, ServeState::Lane *lane) {
         uint64_t first = 0, count = 0;
         {
             std::unique_lock<std::mutex> lk(sv->mu);
-            if (GR_SERVE_POLICY == 1) {
+            if (GR_SERVE_POLICY != 0) {
                 sv->cv_lane.wait(lk, [&] { return sv->stop || !sv->lane_pending.empty(); });
                 if (sv->lane_pending.empty()) return;  // stopping, nothing left
                 size_t pick = 0;
                 uint64_t least = UINT64_MAX;
                 for (size_t i = 0; i < sv->lane_pending.size(); ++i) {
                     const Request *c = sv->reqs[sv->lane_pending[i]];
-                    const uint64_t left = (c->n_px - c->px_done) * c->r.spp;
-                    if (left < least) {
-                        least = left;
+                    const uint64_t key = GR_SERVE_POLICY == 1 ? (c->n_px - c->px_done) * c->r.spp : c->id;
+                    if (key < least) {
+                        least = key;
                         pick = i;
                     }
                 }
@@ -369,7 +371,7 @@ void lane_main(gr_ctx *ctx, ServeState *sv, ServeState::Lane *lane) {
             q->issued = q->in_flight = q->r.spp;
         }
         gr_status st = GR_OK;
-        if (GR_SERVE_POLICY == 1) {
+        if (GR_SERVE_POLICY != 0) {
             st = lane_chunk(ctx, sv, lane, q, first, count);
         } else {
             const uint64_t chunk_px = std::max<uint64_t>(1, kClassTuples[lane->cls] / q->r.spp);
@@ -598,9 +600,10 @@ ServeState *serve_state(gr_ctx *ctx) {
         // default the smallest class next, the largest last
         for (int c = 0; c < kLaneClasses; ++c) {
             const int rank = GR_SERVE_LANE_ORDER ? kLaneClasses - 1 - c : c;
-            const int prio = std::min(lo, hi + 1 + (GR_SERVE_POLICY == 1 ? 0 : rank));  // larger = lower priority
-            const uint32_t n_lanes = GR_SERVE_POLICY == 1 ? (c == 2 ? GR_SERVE_SRPT_LANES : 0) : kLanesPerClass[c];
+            const uint32_t n_lanes = GR_SERVE_POLICY != 0 ? (c == 2 ? GR_SERVE_SRPT_LANES : 0) : kLanesPerClass[c];
             for (uint32_t k = 0; k < n_lanes; ++k) {
+                // numerically larger = lower priority
+                const int prio = std::min(lo, hi + 1 + (GR_SERVE_POLICY == 0 ? rank : GR_SERVE_POLICY == 2 ? (int)k : 0));
                 auto *L = new ServeState::Lane();
                 L->cls = c;
                 if (cudaStreamCreateWithPriority(&L->stream, cudaStreamNonBlocking, prio) != cudaSuccess) {

@@ -139,7 +139,11 @@ constexpr uint64_t kFilmPoolReserve = 4ull << 30;
 // GR_SERVE_CHUNK_MTUPLES path-samples of the request with the least work left, then
 // chooses again (GR_SERVE_SRPT_LANES lanes at one priority); 2 = the same chunks taken
 // oldest request first by GR_SERVE_SRPT_LANES lanes of descending stream priority, so
-// the oldest renders run as if alone and younger ones fill the SMs they leave idle.
+// the oldest renders run as if alone and younger ones fill the SMs they leave idle;
+// 3 = the chunks taken in order of submission time + remaining work (at
+// GR_SERVE_PS_PER_TUPLE picoseconds per path-sample): short requests pass long ones that
+// have not run long, and a long one that has waited or run for longer than the work
+// left in a newer request goes first.
 #ifndef GR_SERVE_POLICY
 #define GR_SERVE_POLICY 0
 #endif
@@ -148,6 +152,9 @@ constexpr uint64_t kFilmPoolReserve = 4ull << 30;
 #endif
 #ifndef GR_SERVE_SRPT_LANES
 #define GR_SERVE_SRPT_LANES 1
+#endif
+#ifndef GR_SERVE_PS_PER_TUPLE
+#define GR_SERVE_PS_PER_TUPLE 1400
 #endif
 constexpr int kLaneClasses = 3;
 constexpr uint32_t kLanesPerClass[kLaneClasses] = {2, 1, 1};
@@ -344,7 +351,13 @@ void lane_main(gr_ctx *ctx, ServeState *sv, ServeState::Lane *lane) {
                 uint64_t least = UINT64_MAX;
                 for (size_t i = 0; i < sv->lane_pending.size(); ++i) {
                     const Request *c = sv->reqs[sv->lane_pending[i]];
-                    const uint64_t key = GR_SERVE_POLICY == 1 ? (c->n_px - c->px_done) * c->r.spp : c->id;
+                    const uint64_t left = (c->n_px - c->px_done) * c->r.spp;
+                    const uint64_t key =
+                        GR_SERVE_POLICY == 1   ? left
+                        : GR_SERVE_POLICY == 2 ? c->id
+                                               : (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
+                                                     c->t_submit.time_since_epoch()).count() +
+                                                     left * GR_SERVE_PS_PER_TUPLE / 1000;
                     if (key < least) {
                         least = key;
                         pick = i;

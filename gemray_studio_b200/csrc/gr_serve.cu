@@ -92,7 +92,10 @@ struct Request {
     bool kahan = false;
     StreamBuffer film, comp;
     uint32_t issued = 0, done = 0, in_flight = 0;  // samples per pixel
-    uint64_t px_done = 0;  // lane renders: pixels whose samples are all folded
+    uint64_t px_done = 0;      // lane renders: pixels whose samples are all folded
+    uint64_t px_issued = 0;    // policy 1: pixels whose chunk has been queued
+    uint64_t px_inflight = 0;  // policy 1: pixels of queued chunks not yet retired
+    cudaEvent_t film_ev = nullptr;  // policy 1: the film's allocation and zeroing, for other lanes' streams
     bool cancel = false;
     int lane_class = -1;  // rendered whole by a lane of this size class; -1: in ticks
     bool admitted = false;  // film_bytes counted in the serve budget
@@ -135,27 +138,26 @@ constexpr uint64_t kFilmPoolReserve = 4ull << 30;
 #define GR_SERVE_LANE_ORDER 0
 #endif
 // Lane policy: 0 = size classes, each request rendered whole by a lane of its class;
-// 1 = one shared queue, shortest remaining work first: a lane renders one chunk of
-// GR_SERVE_CHUNK_MTUPLES path-samples of the request with the least work left, then
-// chooses again (GR_SERVE_SRPT_LANES lanes at one priority); 2 = the same chunks taken
-// oldest request first by GR_SERVE_SRPT_LANES lanes of descending stream priority, so
-// the oldest renders run as if alone and younger ones fill the SMs they leave idle;
-// 3 = the chunks taken in order of submission time + remaining work (at
-// GR_SERVE_PS_PER_TUPLE picoseconds per path-sample): short requests pass long ones that
-// have not run long, and a long one that has waited or run for longer than the work
-// left in a newer request goes first.
+// 1 = one shared queue of chunks: a lane renders GR_SERVE_CHUNK_MTUPLES path-samples
+// (whole pixels) of the request that comes first in the order "submission time +
+// remaining work at GR_SERVE_PS_PER_TUPLE picoseconds per path-sample", then chooses
+// again, with up to kChunksInFlight chunks queued on its stream so the device never
+// waits for the host between chunks.  The order lets a short request pass a long one
+// that has not waited or run long, and puts a long one that has ahead of newer short
+// ones (GR_SERVE_PS_PER_TUPLE 0: oldest first; very large: least remaining work first).
 #ifndef GR_SERVE_POLICY
 #define GR_SERVE_POLICY 0
 #endif
 #ifndef GR_SERVE_CHUNK_MTUPLES
 #define GR_SERVE_CHUNK_MTUPLES 4
 #endif
-#ifndef GR_SERVE_SRPT_LANES
-#define GR_SERVE_SRPT_LANES 1
+#ifndef GR_SERVE_CHUNK_LANES
+#define GR_SERVE_CHUNK_LANES 1
 #endif
 #ifndef GR_SERVE_PS_PER_TUPLE
 #define GR_SERVE_PS_PER_TUPLE 1400
 #endif
+constexpr size_t kChunksInFlight = 2;
 constexpr int kLaneClasses = 3;
 constexpr uint32_t kLanesPerClass[kLaneClasses] = {2, 1, 1};
 constexpr uint64_t kClassTuples[kLaneClasses] = {(uint64_t)GR_SERVE_SMALL_MTUPLES << 20,
@@ -188,7 +190,7 @@ struct ServeState {
     std::vector<Lane *> lanes;
     std::condition_variable cv_lane;
     std::deque<uint64_t> lane_queue[kLaneClasses];  // admitted lane renders per class, admission order
-    std::vector<uint64_t> lane_pending;  // policy 1: renders with pixels left, none of them in a lane
+    std::vector<uint64_t> lane_pending;  // policy 1: admitted lane renders not yet finished
     cudaMemPool_t film_pool = nullptr;      // request films (null: the device's default pool)
     std::condition_variable cv_work, cv_done, cv_metrics;
     std::unordered_map<uint64_t, Request *> reqs;
@@ -234,7 +236,7 @@ void admit(gr_ctx *ctx, ServeState &sv, uint64_t resident_bytes) {
             q->state = GR_REQ_RUNNING;
             q->t_admit = Clock::now();
             q->lane_class = lane_class((uint64_t)q->r.spp * q->n_px);
-            if (GR_SERVE_POLICY != 0)
+            if (GR_SERVE_POLICY == 1)
                 sv.lane_pending.push_back(q->id);
             else
                 sv.lane_queue[q->lane_class].push_back(q->id);
@@ -333,50 +335,182 @@ void lane_finish(ServeState *sv, ServeState::Lane *lane, Request *q, gr_status s
     }
 }
 
+// Policy 1: the pending render whose next chunk comes first (submission time + remaining
+// work), or -1 when none has pixels left to queue (caller holds sv->mu).
+int next_chunk_owner(ServeState &sv) {
+    int pick = -1;
+    uint64_t best = UINT64_MAX;
+    for (size_t i = 0; i < sv.lane_pending.size(); ++i) {
+        const Request *c = sv.reqs[sv.lane_pending[i]];
+        if (c->cancel || c->px_issued >= c->n_px) continue;
+        const uint64_t left = (c->n_px - c->px_issued) * c->r.spp;
+        const uint64_t key = (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
+                                 c->t_submit.time_since_epoch()).count() +
+                             left * (uint64_t)GR_SERVE_PS_PER_TUPLE / 1000;
+        if (key < best) {
+            best = key;
+            pick = (int)i;
+        }
+    }
+    return pick;
+}
+
+// Policy 1: a cancelled pending render with no chunk queued, or -1 (caller holds sv->mu).
+int idle_cancelled(ServeState &sv) {
+    for (size_t i = 0; i < sv.lane_pending.size(); ++i) {
+        const Request *c = sv.reqs[sv.lane_pending[i]];
+        if (c->cancel && c->px_inflight == 0) return (int)i;
+    }
+    return -1;
+}
+
+// Policy 1: queue one chunk of q on the lane's stream (no wait).  The first chunk takes
+// the film (zeroed, stream-ordered) and records film_ev, which later chunks on any
+// lane's stream wait for; the scene stays in use until the chunk retires (*rs_out).
+gr_status lane_launch(gr_ctx *ctx, ServeState::Lane *lane, Request *q, uint64_t first, uint64_t count,
+                      ResidentScene **rs_out) {
+    *rs_out = nullptr;
+    const uint32_t spp = q->r.spp;
+    if (q->film_ev) GR_CUDA(cudaStreamWaitEvent(lane->stream, q->film_ev, 0));
+    SceneConst S;
+    grd::SceneBuffers B;
+    StageCaps caps;
+    int mode = GR_KERNEL_AUTO;
+    int trial = -1;
+    ResidentScene *rs = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        auto it = ctx->scenes.find(q->r.scene_id);
+        if (it == ctx->scenes.end()) return GR_ENOTFOUND;
+        rs = it->second;
+        rs->users++;
+        *rs_out = rs;
+        S = rs->S;
+        B = resident_buffers(rs);
+        if (ctx->kernel_mode != GR_KERNEL_SORTED) mode = ctx->kernel_mode;
+        caps = grh::tune_begin(ctx, rs->tune, S, count, spp, lane->stream, trial);
+    }
+    gr_status st = lane->xyz.reserve((size_t)count * spp * 12);
+    grd::LaunchRange R;
+    R.first_pixel = (uint32_t)first;
+    R.n_pixels = (uint32_t)count;
+    R.sample_offset = q->r.sample_offset;
+    R.spp = spp;
+    R.n_tuples = (uint64_t)count * spp;
+    if (st == GR_OK) st = grh::launch_trace(ctx, S, B, R, (float *)lane->xyz.ptr, lane->stream, mode, &lane->park, caps);
+    if (st == GR_OK)
+        st = grh::launch_fold((const float *)lane->xyz.ptr, R.n_pixels, spp, R.first_pixel, (float *)q->film.ptr,
+                              (S.flags & GR_FLAG_KAHAN_FILM) ? 1u : 0u, lane->stream);
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    grh::tune_end(rs->tune, trial, lane->stream);
+    return st;
+}
+
 // A render lane.  Policy 0: the admitted renders of the lane's size class, one at a
-// time, each rendered whole (in chunks of the class's size).  Policy 1: from the shared
-// pending list, the render with the least work left, one chunk of it, then choose again
-// -- a request that arrives during a long render waits at most one chunk.
+// time, each rendered whole (in chunks of the class's size).  Policy 1: chunks of the
+// pending renders in the order of next_chunk_owner, up to kChunksInFlight queued on the
+// lane's stream; a request finishes when its last chunk retires (or, cancelled, when
+// its queued chunks have retired).
 void lane_main(gr_ctx *ctx, ServeState *sv, ServeState::Lane *lane) {
     cudaSetDevice(ctx->device);
-    for (;;) {
-        Request *q = nullptr;
-        uint64_t first = 0, count = 0;
-        {
-            std::unique_lock<std::mutex> lk(sv->mu);
-            if (GR_SERVE_POLICY != 0) {
-                sv->cv_lane.wait(lk, [&] { return sv->stop || !sv->lane_pending.empty(); });
-                if (sv->lane_pending.empty()) return;  // stopping, nothing left
-                size_t pick = 0;
-                uint64_t least = UINT64_MAX;
-                for (size_t i = 0; i < sv->lane_pending.size(); ++i) {
-                    const Request *c = sv->reqs[sv->lane_pending[i]];
-                    const uint64_t left = (c->n_px - c->px_done) * c->r.spp;
-                    const uint64_t key =
-                        GR_SERVE_POLICY == 1   ? left
-                        : GR_SERVE_POLICY == 2 ? c->id
-                                               : (uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(
-                                                     c->t_submit.time_since_epoch()).count() +
-                                                     left * GR_SERVE_PS_PER_TUPLE / 1000;
-                    if (key < least) {
-                        least = key;
-                        pick = i;
+    if (GR_SERVE_POLICY == 1) {
+        struct Flight {
+            Request *q;
+            uint64_t first, count;
+            ResidentScene *rs;
+            gr_status st;
+            cudaEvent_t ev;
+        };
+        std::deque<Flight> flight;
+        std::vector<cudaEvent_t> spare;
+        const uint64_t chunk_tuples = (uint64_t)GR_SERVE_CHUNK_MTUPLES << 20;
+        for (;;) {
+            Request *q = nullptr;
+            uint64_t first = 0, count = 0;
+            gr_status st = GR_OK;
+            {
+                std::unique_lock<std::mutex> lk(sv->mu);
+                if (flight.empty()) {
+                    sv->cv_lane.wait(lk, [&] {
+                        return sv->stop || next_chunk_owner(*sv) >= 0 || idle_cancelled(*sv) >= 0;
+                    });
+                    for (int c; (c = idle_cancelled(*sv)) >= 0;) {  // cancelled before (or between) chunks
+                        Request *r = sv->reqs[sv->lane_pending[c]];
+                        sv->lane_pending.erase(sv->lane_pending.begin() + c);
+                        lane_finish(sv, lane, r, r->error);
+                    }
+                    if (next_chunk_owner(*sv) < 0) {
+                        if (sv->stop) return;  // stopping, nothing left to queue
+                        continue;
                     }
                 }
-                q = sv->reqs[sv->lane_pending[pick]];
-                sv->lane_pending.erase(sv->lane_pending.begin() + (ptrdiff_t)pick);
-                const uint64_t chunk_px = std::max<uint64_t>(1, ((uint64_t)GR_SERVE_CHUNK_MTUPLES << 20) / q->r.spp);
-                first = q->px_done;
-                count = std::min<uint64_t>(chunk_px, q->n_px - first);
-            } else {
-                auto &queue = sv->lane_queue[lane->cls];
-                sv->cv_lane.wait(lk, [&] { return sv->stop || !queue.empty(); });
-                if (queue.empty()) return;  // stopping, nothing left
-                q = sv->reqs[queue.front()];
-                queue.pop_front();
-                first = 0;
-                count = q->n_px;
+                const int i = flight.size() < kChunksInFlight ? next_chunk_owner(*sv) : -1;
+                if (i >= 0) {
+                    q = sv->reqs[sv->lane_pending[i]];
+                    first = q->px_issued;
+                    count = std::min<uint64_t>(std::max<uint64_t>(1, chunk_tuples / q->r.spp), q->n_px - first);
+                    q->px_issued += count;
+                    q->px_inflight += count;
+                    q->issued = q->in_flight = q->r.spp;
+                    if (!q->film.ptr) {  // the first chunk: the zero film, then its event
+                        if (q->film.alloc((size_t)q->n_px * 3 * sizeof(float), lane->stream, sv->film_pool) !=
+                                cudaSuccess ||
+                            cudaEventCreateWithFlags(&q->film_ev, cudaEventDisableTiming) != cudaSuccess ||
+                            cudaEventRecord(q->film_ev, lane->stream) != cudaSuccess) {
+                            cudaGetLastError();
+                            st = GR_ENOMEM;
+                        }
+                    }
+                }
             }
+            if (q) {
+                Flight f{q, first, count, nullptr, st, nullptr};
+                if (f.st == GR_OK) f.st = lane_launch(ctx, lane, q, first, count, &f.rs);
+                if (!spare.empty()) {
+                    f.ev = spare.back();
+                    spare.pop_back();
+                } else if (cudaEventCreateWithFlags(&f.ev, cudaEventDisableTiming) != cudaSuccess) {
+                    f.ev = nullptr;
+                }
+                if (f.ev && cudaEventRecord(f.ev, lane->stream) != cudaSuccess && f.st == GR_OK) f.st = GR_ECUDA;
+                flight.push_back(f);
+                continue;  // fill the pipeline
+            }
+            // the pipeline is full, or nothing is left to queue: retire the oldest chunk
+            Flight f = flight.front();
+            flight.pop_front();
+            cudaError_t e = f.ev ? cudaEventSynchronize(f.ev) : cudaStreamSynchronize(lane->stream);
+            if (e != cudaSuccess && f.st == GR_OK) f.st = GR_ECUDA;
+            if (f.ev) spare.push_back(f.ev);
+            if (f.rs) {
+                std::lock_guard<std::mutex> lk(ctx->mu);
+                f.rs->users--;
+            }
+            std::lock_guard<std::mutex> lk(sv->mu);
+            Request *r = f.q;
+            r->px_inflight -= f.count;
+            if (f.st == GR_OK) r->px_done += f.count;
+            if (f.st != GR_OK && r->error == GR_OK) {
+                r->error = f.st;
+                r->cancel = true;  // queue no more of it
+            }
+            if (r->px_inflight == 0 && (r->cancel || r->px_done == r->n_px)) {
+                auto &pend = sv->lane_pending;
+                pend.erase(std::remove(pend.begin(), pend.end(), r->id), pend.end());
+                lane_finish(sv, lane, r, r->error);
+            }
+            sv->cv_lane.notify_all();
+        }
+    }
+    for (;;) {
+        Request *q = nullptr;
+        {
+            std::unique_lock<std::mutex> lk(sv->mu);
+            auto &queue = sv->lane_queue[lane->cls];
+            sv->cv_lane.wait(lk, [&] { return sv->stop || !queue.empty(); });
+            if (queue.empty()) return;  // stopping, nothing left
+            q = sv->reqs[queue.front()];
+            queue.pop_front();
             if (q->cancel) {
                 lane_finish(sv, lane, q, GR_OK);
                 continue;
@@ -384,21 +518,11 @@ void lane_main(gr_ctx *ctx, ServeState *sv, ServeState::Lane *lane) {
             q->issued = q->in_flight = q->r.spp;
         }
         gr_status st = GR_OK;
-        if (GR_SERVE_POLICY != 0) {
-            st = lane_chunk(ctx, sv, lane, q, first, count);
-        } else {
-            const uint64_t chunk_px = std::max<uint64_t>(1, kClassTuples[lane->cls] / q->r.spp);
-            for (uint64_t p = 0; st == GR_OK && p < q->n_px && !q->cancel; p += chunk_px)
-                st = lane_chunk(ctx, sv, lane, q, p, std::min<uint64_t>(chunk_px, q->n_px - p));
-            count = q->n_px - first;
-        }
+        const uint64_t chunk_px = std::max<uint64_t>(1, kClassTuples[lane->cls] / q->r.spp);
+        for (uint64_t p = 0; st == GR_OK && p < q->n_px && !q->cancel; p += chunk_px)
+            st = lane_chunk(ctx, sv, lane, q, p, std::min<uint64_t>(chunk_px, q->n_px - p));
         std::lock_guard<std::mutex> lk(sv->mu);
-        q->px_done = first + count;
-        if (st == GR_OK && !q->cancel && q->px_done < q->n_px) {
-            sv->lane_pending.push_back(q->id);  // policy 1: more chunks to come
-            sv->cv_lane.notify_all();
-            continue;
-        }
+        q->px_done = q->n_px;
         lane_finish(sv, lane, q, st);
     }
 }
@@ -613,10 +737,10 @@ ServeState *serve_state(gr_ctx *ctx) {
         // default the smallest class next, the largest last
         for (int c = 0; c < kLaneClasses; ++c) {
             const int rank = GR_SERVE_LANE_ORDER ? kLaneClasses - 1 - c : c;
-            const uint32_t n_lanes = GR_SERVE_POLICY != 0 ? (c == 2 ? GR_SERVE_SRPT_LANES : 0) : kLanesPerClass[c];
+            const uint32_t n_lanes = GR_SERVE_POLICY == 1 ? (c == 2 ? GR_SERVE_CHUNK_LANES : 0) : kLanesPerClass[c];
             for (uint32_t k = 0; k < n_lanes; ++k) {
                 // numerically larger = lower priority
-                const int prio = std::min(lo, hi + 1 + (GR_SERVE_POLICY == 0 ? rank : GR_SERVE_POLICY == 2 ? (int)k : 0));
+                const int prio = std::min(lo, hi + 1 + (GR_SERVE_POLICY == 0 ? rank : 0));
                 auto *L = new ServeState::Lane();
                 L->cls = c;
                 if (cudaStreamCreateWithPriority(&L->stream, cudaStreamNonBlocking, prio) != cudaSuccess) {
@@ -672,6 +796,7 @@ void serve_shutdown(gr_ctx *ctx) {
     for (auto &kv : sv->reqs) {
         kv.second->film.release(ctx->stream);
         kv.second->comp.release(ctx->stream);
+        if (kv.second->film_ev) cudaEventDestroy(kv.second->film_ev);
         delete kv.second;
     }
     cudaStreamSynchronize(ctx->stream);  // stream-ordered frees above complete
@@ -851,6 +976,7 @@ gr_status gr_request_release(gr_ctx *ctx, uint64_t id) {
     cudaSetDevice(ctx->device);
     q->film.release(ctx->stream);  // stream-ordered: after every tick that wrote it
     q->comp.release(ctx->stream);
+    if (q->film_ev) cudaEventDestroy(q->film_ev);
     delete q;
     return GR_OK;
 }

@@ -18,10 +18,11 @@ PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
 CSRC = PKG / "csrc"
 OUT = PKG / "libgemray_cuda.so"
-SOURCES = ["gr_host.cu", "gr_batch.cu", "gr_serve.cu", "gr_stream.cu", "gr_denoise.cu", "gr_tonemap.cu", "gr_metrics.cu", "gr_static.cu", "gr_verify.cu", "gr_stokes.cu", "gr_single_clear.cu",
+SOURCES = ["gr_host.cu", "gr_batch.cu", "gr_batch_classes.cu", "gr_serve.cu", "gr_stream.cu", "gr_denoise.cu",
+           "gr_tonemap.cu", "gr_metrics.cu", "gr_static.cu", "gr_verify.cu", "gr_stokes.cu", "gr_single_clear.cu",
            "gr_single_general.cu", "gr_scene_builders.cpp"]
 HEADERS = ["gr_device.cuh", "gr_stage.cuh", "gr_trace.cuh", "gr_launch.cuh", "gr_kernels.cuh", "gr_transport.cuh",
-           "gr_single.cuh", "gr_batch.cuh",
+           "gr_single.cuh", "gr_sorted.cuh", "gr_batch.cuh",
            "gr_ctx.h", "gr_host.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # Compile-time engine options (see csrc/gr_device.cuh).

@@ -1,8 +1,10 @@
 // gr_batch.cu -- gr_render_batch: many resident scenes in shared launches.
 //
 // The planner cuts every item (resident scene, film, sample range) into segments of
-// whole pixels and packs them, in item order, into launches of at most the context's
-// per-launch tuple budget (chunk_budget / 12 B of per-tuple XYZ scratch).  Each launch
+// whole pixels and packs them, grouped by scene class and in item order within a class,
+// into launches of at most the context's per-launch tuple budget (chunk_budget / 12 B
+// of per-tuple XYZ scratch); each launch runs the trace kernels specialised for its
+// class (gr_batch_classes.cu), as the single-scene renders do.  Each launch
 // is one k_trace_batch grid over all of its segments followed by one k_fold_batch
 // grid, so scenes with few pixels or few samples share the device with the others
 // instead of each paying a launch, a tail and a host round trip.  Per-tuple arithmetic
@@ -30,6 +32,17 @@
 
 using grh::fail;
 
+namespace grd {
+// The ordered per-pixel fold of a batched launch: one warp per pixel of each segment.
+__global__ void k_fold_batch(const BatchSegment *__restrict__ segs, uint32_t n_segs) {
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const BatchSegment &G = segs[find_segment<1>(segs, n_segs, warp)];
+    const uint64_t px = warp - G.warp_begin;
+    if (px >= G.R.n_pixels) return;  // the grid's last warps past the final segment
+    fold_pixel(G.xyz, px, G.R.spp, G.R.first_pixel + (uint32_t)px, G.film, G.kahan, G.cont, G.comp);
+}
+}  // namespace grd
+
 namespace {
 
 struct Launch {
@@ -38,6 +51,7 @@ struct Launch {
     uint32_t max_planes;
     bool extras;  // a segment's scene has frosted facets, scattering or a biaxial material
     uint64_t park_paths, park_blocks;  // park slots over the launch's segments, continuation blocks
+    int K;        // the scene class of every segment (scene_class), -1: the extension kernels
 };
 
 struct Plan {
@@ -80,7 +94,7 @@ void place_park(Plan &P, Launch &L) {
 // until the scratch is placed.
 gr_status make_plan(gr_ctx *ctx, const grh::BatchItem *items, uint32_t n_items, uint64_t budget, Plan &P) {
     std::unordered_map<uint64_t, uint32_t> slot_of;
-    Launch cur{0, 0, 0, 0, 0, false, 0, 0};
+    Launch cur{0, 0, 0, 0, 0, false, 0, 0, -1};
     uint64_t used = 0;
     auto close = [&]() {
         if (cur.seg_count) {
@@ -88,16 +102,28 @@ gr_status make_plan(gr_ctx *ctx, const grh::BatchItem *items, uint32_t n_items, 
             P.launches.push_back(cur);
         }
         P.max_tuples = std::max(P.max_tuples, used);
-        cur = Launch{(uint32_t)P.segs.size(), 0, 0, 0, 0, false, 0, 0};
+        cur = Launch{(uint32_t)P.segs.size(), 0, 0, 0, 0, false, 0, 0, -1};
         used = 0;
     };
+    // Items grouped by scene class (stable within a class), so each launch runs the
+    // kernels specialised for its class; unknown scenes fail in item order first.
+    std::vector<int> cls(n_items, -1);
     for (uint32_t i = 0; i < n_items; ++i) {
+        auto f = ctx->scenes.find(items[i].it.scene_id);
+        if (f == ctx->scenes.end())
+            return fail(GR_ENOTFOUND, "item %u: unknown scene id %llu", i, (unsigned long long)items[i].it.scene_id);
+        cls[i] = grh::scene_class(f->second->S);
+    }
+    std::vector<uint32_t> order(n_items);
+    for (uint32_t i = 0; i < n_items; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return cls[a] < cls[b]; });
+    for (uint32_t i : order) {
         const gr_batch_item &it = items[i].it;
-        auto f = ctx->scenes.find(it.scene_id);
-        if (f == ctx->scenes.end()) return fail(GR_ENOTFOUND, "item %u: unknown scene id %llu", i, (unsigned long long)it.scene_id);
-        ResidentScene *rs = f->second;
+        ResidentScene *rs = ctx->scenes.find(it.scene_id)->second;
         const uint64_t n_px = (uint64_t)rs->S.width * rs->S.height;
         if (it.spp == 0 || n_px == 0) continue;
+        if (cur.seg_count && cur.K != cls[i]) close();  // one class per launch
+        cur.K = cls[i];
         if (!it.film_device) return fail(GR_EINVAL, "item %u: film is NULL", i);
         if (rs->S.flags & GR_FLAG_FP64_RESOLVE)
             return fail(GR_EINVAL, "item %u: GR_FLAG_FP64_RESOLVE scenes render through the single-scene calls", i);
@@ -120,6 +146,7 @@ gr_status make_plan(gr_ctx *ctx, const grh::BatchItem *items, uint32_t n_items, 
             if (room == 0) {
                 if (used > 0) {
                     close();
+                    cur.K = cls[i];
                     continue;
                 }
                 room = 1;
@@ -175,15 +202,15 @@ gr_status launch_plan(const Plan &P, const grd::SceneSlot *slots, const grd::Bat
         const size_t smem = grd::planes_smem_bytes(L.max_planes);
         GR_CUDA(cudaMemsetAsync(counts, 0, (size_t)L.seg_count * sizeof(unsigned int), s));
         if (L.extras) {
-            grd::k_trace_batch<true><<<(unsigned)L.blocks, grd::TRACE_THREADS, smem, s>>>(slots, segs + L.seg_first,
-                                                                                          L.seg_count, park, counts);
-            grd::k_trace_batch_cont<true><<<(unsigned)L.park_blocks, grd::TRACE_THREADS, smem, s>>>(
-                slots, segs + L.seg_first, L.seg_count, park, counts);
+            grd::launch_batch_grids<true, grd::K_ANY, GR_TRACE_MIN_BLOCKS>(slots, segs + L.seg_first, L.seg_count, park,
+                                                                           counts, L.blocks, L.park_blocks, smem, s);
+        } else if (L.K >= 0) {
+            const gr_status st = grh::launch_batch_class(L.K, slots, segs + L.seg_first, L.seg_count, park, counts,
+                                                         L.blocks, L.park_blocks, smem, s);
+            if (st != GR_OK) return st;
         } else {
-            grd::k_trace_batch<false><<<(unsigned)L.blocks, grd::TRACE_THREADS, smem, s>>>(slots, segs + L.seg_first,
-                                                                                           L.seg_count, park, counts);
-            grd::k_trace_batch_cont<false><<<(unsigned)L.park_blocks, grd::TRACE_THREADS, smem, s>>>(
-                slots, segs + L.seg_first, L.seg_count, park, counts);
+            grd::launch_batch_grids<false, grd::K_ANY, GR_TRACE_MIN_BLOCKS>(slots, segs + L.seg_first, L.seg_count, park,
+                                                                            counts, L.blocks, L.park_blocks, smem, s);
         }
         const unsigned T = 256;
         grd::k_fold_batch<<<(unsigned)((L.warps * 32 + T - 1) / T), T, 0, s>>>(segs + L.seg_first, L.seg_count);
@@ -206,7 +233,9 @@ std::vector<uint64_t> graph_key(const Plan &P, const void *tables, const void *x
         k.push_back(((uint64_t)g.R.spp << 32) | g.scene);
         k.push_back((uint64_t)(uintptr_t)g.comp ^ g.cont);
     }
-    for (const Launch &L : P.launches) k.push_back(((uint64_t)L.seg_count << 32) | L.max_planes | ((uint64_t)L.extras << 31));
+    for (const Launch &L : P.launches)
+        k.push_back(((uint64_t)L.seg_count << 32) | L.max_planes | ((uint64_t)L.extras << 31) |
+                    ((uint64_t)(uint8_t)(L.K + 1) << 20));
     return k;
 }
 

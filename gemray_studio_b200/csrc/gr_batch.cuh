@@ -56,9 +56,10 @@ __device__ __forceinline__ void load_slot(SceneSlot &dst_slot, const SceneSlot *
 // run up to their segment's stage cap; survivors are parked in their segment's park region
 // (`park`, slot counters `counts` per segment of the launch) for k_trace_batch_cont.
 // EXTRAS: the variant for launches holding a scene with frosted facets, scattering or
-// a biaxial material.
-template <bool EXTRAS>
-__global__ void __launch_bounds__(TRACE_THREADS, GR_TRACE_MIN_BLOCKS)
+// a biaxial material.  K: the scene class every segment of the launch belongs to
+// (gr_trace.cuh K_*; K_ANY: checked at run time), MB: resident blocks per SM.
+template <bool EXTRAS, int K = K_ANY, int MB = GR_TRACE_MIN_BLOCKS>
+__global__ void __launch_bounds__(TRACE_THREADS, MB)
     k_trace_batch(const SceneSlot *__restrict__ slots, const BatchSegment *__restrict__ segs, uint32_t n_segs,
                   Path *__restrict__ park, unsigned int *__restrict__ counts) {
     __shared__ SceneSlot s_slot;
@@ -79,11 +80,11 @@ __global__ void __launch_bounds__(TRACE_THREADS, GR_TRACE_MIN_BLOCKS)
     if (active) {
         uint32_t pixel, sample;
         tuple_coords(R, t, pixel, sample);
-        path_init<1, EXTRAS>(P, S, B, pixel, sample, (uint32_t)t);
+        path_init<1, EXTRAS, K>(P, S, B, pixel, sample, (uint32_t)t);
     }
     const ParkOut out{park + G.park_off, G.park_cap, counts + s_seg};
-    if (run_or_park<EXTRAS>(P, S, PL, active, G.stage_cap, out) || !active) return;
-    const V3 c = path_finish<1>(P, S, B);
+    if (run_or_park<EXTRAS, K>(P, S, PL, active, G.stage_cap, out) || !active) return;
+    const V3 c = path_finish<1, false, K>(P, S, B);
     float *xyz = G.xyz;
     xyz[3 * t + 0] = c.x;
     xyz[3 * t + 1] = c.y;
@@ -92,8 +93,8 @@ __global__ void __launch_bounds__(TRACE_THREADS, GR_TRACE_MIN_BLOCKS)
 
 // Stage 2: each block resumes up to 128 parked paths of one segment (its scene in
 // shared memory, as in stage 1) and runs them to their end.
-template <bool EXTRAS>
-__global__ void __launch_bounds__(TRACE_THREADS, GR_TRACE_MIN_BLOCKS)
+template <bool EXTRAS, int K = K_ANY, int MB = GR_TRACE_MIN_BLOCKS>
+__global__ void __launch_bounds__(TRACE_THREADS, MB)
     k_trace_batch_cont(const SceneSlot *__restrict__ slots, const BatchSegment *__restrict__ segs, uint32_t n_segs,
                        const Path *__restrict__ park, const unsigned int *__restrict__ counts) {
     __shared__ SceneSlot s_slot;
@@ -114,7 +115,7 @@ __global__ void __launch_bounds__(TRACE_THREADS, GR_TRACE_MIN_BLOCKS)
     if (i >= n) return;
     Path P = park[G.park_off + i];
     NoCounters nc;
-    const V3 c = trace_path<NoCounters, false, EXTRAS>(P, S, B, PL, nc);
+    const V3 c = trace_path<NoCounters, false, EXTRAS, K>(P, S, B, PL, nc);
     const uint64_t t = p_tuple(P);
     float *xyz = G.xyz;
     xyz[3 * t + 0] = c.x;
@@ -122,12 +123,14 @@ __global__ void __launch_bounds__(TRACE_THREADS, GR_TRACE_MIN_BLOCKS)
     xyz[3 * t + 2] = c.z;
 }
 
-__global__ void k_fold_batch(const BatchSegment *__restrict__ segs, uint32_t n_segs) {
-    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const BatchSegment &G = segs[find_segment<1>(segs, n_segs, warp)];
-    const uint64_t px = warp - G.warp_begin;
-    if (px >= G.R.n_pixels) return;  // the grid's last warps past the final segment
-    fold_pixel(G.xyz, px, G.R.spp, G.R.first_pixel + (uint32_t)px, G.film, G.kahan, G.cont, G.comp);
+// One batched launch's two trace grids for scene class K at MB blocks per SM.
+template <bool EXTRAS, int K, int MB>
+void launch_batch_grids(const SceneSlot *slots, const BatchSegment *segs, uint32_t n_segs, Path *park,
+                        unsigned int *counts, uint64_t blocks, uint64_t park_blocks, size_t smem, cudaStream_t s) {
+    k_trace_batch<EXTRAS, K, MB><<<(unsigned)blocks, TRACE_THREADS, smem, s>>>(slots, segs, n_segs, park, counts);
+    k_trace_batch_cont<EXTRAS, K, MB><<<(unsigned)park_blocks, TRACE_THREADS, smem, s>>>(slots, segs, n_segs, park,
+                                                                                        counts);
 }
+
 
 }  // namespace grd

@@ -197,8 +197,15 @@ void streams_shutdown(gr_ctx *ctx);
 namespace grd {
 struct LaunchRange;
 struct Path;
+struct SceneSlot;
+struct BatchSegment;
 }
 namespace grh {
+// The two trace grids of a batched launch whose segments all have scene class K
+// (gr_batch_classes.cu); K is a clear-isotropic or general class with its environment.
+gr_status launch_batch_class(int K, const grd::SceneSlot *slots, const grd::BatchSegment *segs, uint32_t n_segs,
+                             grd::Path *park, unsigned int *counts, uint64_t blocks, uint64_t park_blocks, size_t smem,
+                             cudaStream_t s);
 // Scene checks and encoding (gr_host.cu): validate, encode the constants, and upload
 // the scene's arrays into the context's buffers (prepare does all three).
 gr_status validate_scene(const gr_scene *sc);

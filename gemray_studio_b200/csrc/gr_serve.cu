@@ -146,10 +146,10 @@ constexpr uint64_t kFilmPoolReserve = 4ull << 30;
 // that has not waited or run long, and puts a long one that has ahead of newer short
 // ones (GR_SERVE_PS_PER_TUPLE 0: oldest first; very large: least remaining work first).
 #ifndef GR_SERVE_POLICY
-#define GR_SERVE_POLICY 0
+#define GR_SERVE_POLICY 1
 #endif
 #ifndef GR_SERVE_CHUNK_MTUPLES
-#define GR_SERVE_CHUNK_MTUPLES 4
+#define GR_SERVE_CHUNK_MTUPLES 8
 #endif
 #ifndef GR_SERVE_CHUNK_LANES
 #define GR_SERVE_CHUNK_LANES 1

@@ -17,18 +17,19 @@
 //     thread runs them in arrival order on its own high-priority stream, beside the
 //     tick in flight, so a sweep neither waits for a tick nor holds one up;
 //   * render lanes -- a render without a slice size of its own (slice_spp == 0) is
-//     not cut into ticks: a lane thread renders its whole sample range with the
-//     single-scene kernels and the stone's tuned schedule (the kernels and schedule of
-//     gr_render_resident) on the lane's own stream, with scratch of its own.  Lanes
-//     are grouped by request size (path-samples <= GR_SERVE_SMALL_MTUPLES,
-//     <= GR_SERVE_BULK_MTUPLES, larger), each size class with its own FIFO queue and
-//     stream priority: by default the smaller classes take the higher priorities, so
-//     the GPU's block scheduler gives a small request the SMs that blocks of larger
-//     ones free (within a few hundred microseconds) and it no longer waits behind them,
-//     while the larger ones keep the rest of the device.  Several requests therefore
-//     run on the device at once, one per lane.  Cancellation takes effect before a
-//     lane starts a request or between its launches, and leaves a zero film.
-//     Sliced renders (slice_spp > 0, progressive rendering) go to the ticks.
+//     not cut into ticks but into chunks of whole pixels over its whole sample range
+//     (GR_SERVE_CHUNK_MTUPLES path-samples), rendered with the single-scene kernels
+//     and the stone's tuned schedule (the kernels and schedule of gr_render_resident)
+//     on a lane's own stream, with scratch of its own.  After each chunk the lane takes
+//     the next chunk of whichever admitted render comes first by submission time plus
+//     remaining work, two chunks queued at a time so the device never waits for the
+//     host: a short request passes a long one that has not waited or run long, so it
+//     waits at most about a chunk behind it, while a long one that has waited longer
+//     than a newer request's remaining work goes first.  Cancellation takes effect
+//     between chunks and leaves a zero film.  GR_SERVE_POLICY=0 selects size-class
+//     lanes instead (each request whole on a lane of its size class, smaller classes
+//     at higher stream priority, several requests on the device at once).  Sliced
+//     renders (slice_spp > 0, progressive rendering) go to the ticks.
 // Slices fold in continue mode (fold_pixel): each slice carries the pixel's running
 // sum on from the film (and the Kahan compensation from a side buffer), and a request
 // starts on a zero film, so its film is one sequential per-pixel sum over all of its

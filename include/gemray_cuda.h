@@ -479,8 +479,8 @@ typedef struct gr_request {
     uint32_t slice_spp;      /* render: > 0: at most this many samples per pixel per tick (a tick
                                 carries ~8.4 M path-samples in one batched launch, filled from the
                                 running sliced renders in arrival order); progress and cancellation
-                                happen between slices.  0: rendered whole by a render lane of its
-                                size class (see gr_submit).  The film does not depend on either */
+                                happen between slices.  0: rendered by the render lane in chunks
+                                (see gr_submit).  The film does not depend on either */
     uint64_t scene_id;       /* render: resident scene */
     uint32_t sample_offset;  /* render: first absolute sample */
     uint32_t spp;            /* render: samples per pixel */
@@ -513,13 +513,14 @@ typedef struct gr_request_status {
  * which renders one dispatch at a time; the worker's render loop is
  * apps/gemray-worker/src/render_core/mod.rs).  A worker thread admits requests in
  * arrival order while their film (W*H*3 f32) fits the context's serve budget next to
- * the resident scenes and unreleased films.  A render with slice_spp == 0 goes to a
- * render lane of its size class (up to 2 M path-samples: two lanes; up to 8 M: one;
- * larger: one), which renders it whole with the single-scene kernels and the stone's
- * tuned schedule on the lane's own stream -- the smaller the class, the higher the
- * stream priority, so small requests do not wait behind large ones; the lanes run at
- * once.  A sliced render (slice_spp > 0) advances by one slice per tick in a shared
- * batched launch.  Metric requests hold no film and run on another worker thread in
+ * the resident scenes and unreleased films.  A render with slice_spp == 0 goes to the
+ * render lane, which renders it in chunks of whole pixels (8 M path-samples) with the
+ * single-scene kernels and the stone's tuned schedule, choosing after every chunk the
+ * render that comes first by submission time plus remaining work: a small request
+ * waits about one chunk behind a large one instead of all of it, and a large one that
+ * has waited longer than a newer request's whole work goes first.  A sliced render
+ * (slice_spp > 0) advances by one slice per tick in a shared batched launch beside the
+ * lane.  Metric requests hold no film and run on another worker thread in
  * arrival order at the highest stream priority, beside the renders.  Slices continue
  * each pixel's running sum, so a film is bit-identical to one gr_render_resident call
  * over the same sample range on a zero film -- lane or ticks, for any slicing, alone
@@ -529,7 +530,7 @@ gr_status gr_poll(gr_ctx *ctx, uint64_t request_id, gr_request_status *status);
 /* Blocks until the request has finished or timeout_ms passed (GR_ETIMEOUT). */
 gr_status gr_wait(gr_ctx *ctx, uint64_t request_id, uint32_t timeout_ms, gr_request_status *status);
 /* Stops a request between slices (a sliced render's film keeps the slices already
- * folded) or, in a lane, before it starts or between its launches (the film is zero). */
+ * folded) or, in the lane, before it starts or between its chunks (the film is zero). */
 gr_status gr_cancel(gr_ctx *ctx, uint64_t request_id);
 /* Copies a finished (or cancelled) render's film, W*H*3 f32, to host memory. */
 gr_status gr_request_film(gr_ctx *ctx, uint64_t request_id, float *xyz_host);

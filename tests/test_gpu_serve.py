@@ -160,12 +160,12 @@ def test_admission_by_memory_budget(engine_lib):
         r.close()
 
 
-def test_lanes_render_every_size_class_beside_ticks(engine_lib):
-    """Renders without a slice_spp go to the render lanes by size (<= 2 M path-samples,
-    <= 8 M, larger), each rendered whole with the single-scene kernels on its lane's
-    stream, several at once; sliced renders go to the ticks beside them.  Every film --
-    each lane class (a Kahan scene among them) and ticked -- is bit-identical to one
-    gr_render_resident call over its range on a zero film; a lane render cancelled
+def test_lane_renders_every_size_beside_ticks(engine_lib):
+    """Renders without a slice_spp go to the render lane: requests of every size (up to
+    and over one 8 M path-sample chunk, a Kahan scene among them) rendered chunk by
+    chunk with the single-scene kernels, interleaved by submission time plus remaining
+    work; sliced renders go to the ticks beside them.  Every film is bit-identical to
+    one gr_render_resident call over its range on a zero film; a lane render cancelled
     before it starts ends with no samples and a zero film."""
     srv = RenderServer()
     try:

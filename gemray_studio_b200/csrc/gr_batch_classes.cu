@@ -5,9 +5,13 @@
 #include "gr_batch.cuh"
 #include "gr_ctx.h"
 
-// Resident blocks per SM of the class-specialised batched grids.
+// Resident blocks per SM of the class-specialised batched grids.  Measured on B200
+// with the c4 stones (batched path-samples/s at film scales 1/32 and 1/8): 9 blocks
+// 328 M / 428 M, 16 blocks 311 M / 405 M -- unlike the single-scene kernels, these
+// grids lose more to their spills (the scene constants come from shared memory) than
+// they gain from the extra warps.
 #ifndef GR_BATCH_MIN_BLOCKS
-#define GR_BATCH_MIN_BLOCKS 16
+#define GR_BATCH_MIN_BLOCKS 9
 #endif
 
 namespace grh {

@@ -158,7 +158,10 @@ constexpr uint64_t kFilmPoolReserve = 4ull << 30;
 #ifndef GR_SERVE_PS_PER_TUPLE
 #define GR_SERVE_PS_PER_TUPLE 1400
 #endif
-constexpr size_t kChunksInFlight = 2;
+#ifndef GR_SERVE_CHUNK_DEPTH
+#define GR_SERVE_CHUNK_DEPTH 2
+#endif
+constexpr size_t kChunksInFlight = GR_SERVE_CHUNK_DEPTH;
 constexpr int kLaneClasses = 3;
 constexpr uint32_t kLanesPerClass[kLaneClasses] = {2, 1, 1};
 constexpr uint64_t kClassTuples[kLaneClasses] = {(uint64_t)GR_SERVE_SMALL_MTUPLES << 20,

@@ -60,6 +60,25 @@ WORKLOADS = {
 }
 
 
+# The committed per-device schedule table (gemray_studio_b200/tuning_table.py writes it);
+# --no-tuning-table leaves every stone to its live trials.
+TUNING_TABLE = ROOT / "gemray_studio_b200" / "tuning" / "b200_schedules.txt"
+_use_tuning_table = True
+
+
+def load_tuning_table(lib, ctx) -> str:
+    """Loads the committed schedule table into the context when it was written for this
+    device and schedule set; returns where the stones' schedules come from."""
+    from gemray_studio_b200 import abi
+    if not _use_tuning_table or not TUNING_TABLE.exists():
+        return "trials"
+    n = C.c_uint32()
+    st = lib.gr_tuning_load(ctx, str(TUNING_TABLE).encode(), C.byref(n))
+    if st != abi.GR_OK:
+        return f"trials ({lib.gr_last_error_string().decode(errors='replace')})"
+    return f"{TUNING_TABLE.relative_to(ROOT)} ({n.value} stones), trials for the others"
+
+
 def make_scene(name: str, builders: str = "engine"):
     """The workload's scene.  builders="oracle" takes Camera::new and the built-in
     material from the oracle (the reference arm loads no product library)."""
@@ -394,6 +413,7 @@ def run_engine(args):
     sc, w = make_scene(args.workload)
     r = GpuFrameRenderer(device=local, kernel=getattr(abi, "GR_KERNEL_" + args.kernel.upper()))
     lib, ctx = r.lib, r.ctx
+    schedule_source = load_tuning_table(lib, ctx)
     stream_ptr = lib.gr_stream(ctx)
     stream = torch.cuda.ExternalStream(stream_ptr)
     spp = w["spp"]
@@ -558,7 +578,7 @@ def run_engine(args):
                          "kernel_ms_per_step": tr.value / frames, "fold_ms_per_step": fo.value / frames,
                          "launches_per_step": (ntr.value + nfo.value) / frames,
                          "stage_caps": [cap1.value, cap2.value], "blocks_per_sm": blocks.value,
-                         "tuning_calls": tune_calls},
+                         "tuning_calls": tune_calls, "schedule_source": schedule_source},
             "events_per_sample": {k: v / max(1, tallies["paths"]) for k, v in tallies.items() if k != "paths"},
             "metrics_16_tilts": {"ms": metrics_ms, "how": "gr_optical_metrics, one device batch, host wall clock",
                                  "brilliance_pct": [round(float(v), 3) for v in mvals[:, 0]],
@@ -611,6 +631,7 @@ def batch_measure(scale: float, steps: int, warmup: int, n_stones: int = 64) -> 
                              spp=(32, 512))
     r = GpuFrameRenderer()
     lib, ctx = r.lib, r.ctx
+    schedule_source = load_tuning_table(lib, ctx)
     stream_ptr = lib.gr_stream(ctx)
     stream = torch.cuda.ExternalStream(stream_ptr)
     ids = []
@@ -698,6 +719,7 @@ def batch_measure(scale: float, steps: int, warmup: int, n_stones: int = 64) -> 
         "e2e": {"value": tuples / (ms_e2e * 1e-3), "unit": "path-samples/s", "h2d_bytes_per_step": film_bytes,
                 "d2h_bytes_per_step": film_bytes},
         "gpu_launches": int(ntr.value + nfo.value),
+        "schedule_source": schedule_source,
         "clocks": clocks.summary(),
     }
     # every torch tensor used on the context stream goes before the context (the loop
@@ -720,7 +742,7 @@ def run_batch(args):
         "config": {"workload": m["workload"], "path_samples_per_step": m["path_samples_per_step"], "scale": args.scale,
                    "l2": "flushed between steps (256 MiB device write)"},
         **{k: m[k] for k in ("serial", "serial_plain_kernel", "batched_over_serial", "batched_over_plain_kernel",
-                             "matched_error", "e2e", "gpu_launches", "clocks")},
+                             "matched_error", "e2e", "gpu_launches", "schedule_source", "clocks")},
     }), flush=True)
 
 
@@ -738,6 +760,7 @@ def serve_measure(rate: float, duration: float, serve_side=(128, 384), serve_spp
     stones = W.random_stones(32, seed=0, side=(serve_side[0], serve_side[1]), spp=(16, 128))
     reqs = W.request_stream(stones, rate, duration, seed=1, spp=(serve_spp[0], serve_spp[1]))
     srv = RenderServer()
+    schedule_source = load_tuning_table(srv.lib, srv.ctx)
     ids = [srv.upload(st.scene) for st in stones]
     # warm the worker, both kinds of request and their kernels' modules (loaded lazily on
     # first launch), so the timed stream sees no one-time costs
@@ -857,6 +880,7 @@ def serve_measure(rate: float, duration: float, serve_side=(128, 384), serve_spp
         "wall_clock": "arrivals, latencies and throughput are host wall-clock (a request stream has no device-side "
                       "clock)",
         "matched_error": "each served film is bit-identical to one gr_render_resident call over its sample range",
+        "schedule_source": schedule_source,
         "clocks": clocks.summary(),
     }
     del films
@@ -876,7 +900,7 @@ def run_serve(args):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": m["workload"], "render_path_samples": m["render_path_samples"]},
         **{k: m[k] for k in ("latency_ms", "latency_ms_renders", "latency_ms_metrics", "latency_ms_by_size", "serial_replay",
-                             "serial_model", "wall_clock", "matched_error", "clocks")},
+                             "serial_model", "wall_clock", "matched_error", "schedule_source", "clocks")},
     }), flush=True)
 
 
@@ -941,7 +965,11 @@ def main():
     ap.add_argument("--duration", type=float, default=10.0, help="c5: seconds of arrivals")
     ap.add_argument("--serve-side", type=int, nargs=2, default=(128, 384), help="c5: film side range")
     ap.add_argument("--serve-spp", type=int, nargs=2, default=(16, 128), help="c5: spp range")
+    ap.add_argument("--no-tuning-table", action="store_true",
+                    help="choose every stone's staged schedule by live trials, not from the committed table")
     args = ap.parse_args()
+    global _use_tuning_table
+    _use_tuning_table = not args.no_tuning_table
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "c4":

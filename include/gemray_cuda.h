@@ -514,7 +514,7 @@ typedef struct gr_request_status {
  * apps/gemray-worker/src/render_core/mod.rs).  A worker thread admits requests in
  * arrival order while their film (W*H*3 f32) fits the context's serve budget next to
  * the resident scenes and unreleased films.  A render with slice_spp == 0 goes to the
- * render lane, which renders it in chunks of whole pixels (8 M path-samples) with the
+ * render lane, which renders it in chunks of whole pixels (16 M path-samples) with the
  * single-scene kernels and the stone's tuned schedule, choosing after every chunk the
  * render that comes first by submission time plus remaining work: a small request
  * waits about one chunk behind a large one instead of all of it, and a large one that

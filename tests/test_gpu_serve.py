@@ -161,8 +161,8 @@ def test_admission_by_memory_budget(engine_lib):
 
 
 def test_lane_renders_every_size_beside_ticks(engine_lib):
-    """Renders without a slice_spp go to the render lane: requests of every size (up to
-    and over one 8 M path-sample chunk, a Kahan scene among them) rendered chunk by
+    """Renders without a slice_spp go to the render lane: requests of every size (a Kahan
+    scene among them; the long render of the sweep test spans many chunks) rendered chunk by
     chunk with the single-scene kernels, interleaved by submission time plus remaining
     work; sliced renders go to the ticks beside them.  Every film is bit-identical to
     one gr_render_resident call over its range on a zero film; a lane render cancelled

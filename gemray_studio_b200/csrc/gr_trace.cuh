@@ -34,6 +34,13 @@ constexpr int NCH = 8;
 #ifndef GR_RR_UNROLL
 #define GR_RR_UNROLL 4  // measured on the c2 frame: 4 beats 8 / 2 / 1 by 1-3% (code layout)
 #endif
+// The rotation loop of the general (absorbing or birefringent) scene classes: measured
+// on the c3 emerald at 16 blocks per SM, unrolled by 2 / 4 / 8: 585.5 / 576.3 / 563.6 M
+// path-samples/s, while the clear brilliant wants 8 (1,032.6 against 1,017.2 at 4 and
+// 1,009.6 at 2).
+#ifndef GR_ROT_UNROLL_GENERAL
+#define GR_ROT_UNROLL_GENERAL 2
+#endif
 constexpr int ROT_UNROLL = GR_ROT_UNROLL;
 constexpr int RR_UNROLL = GR_RR_UNROLL;
 
@@ -78,6 +85,10 @@ constexpr int K_ISO = 1;        // S.anisotropic == 0 (and not biaxial)
 constexpr int K_CLEAR = 2;      // S.absorbing == 0: no absorption data at all
 constexpr int K_ENV_SHIFT = 2;  // bits 2-3: 0 = the environment kind at run time, else GR_ENV_* + 1
 __host__ __device__ constexpr int k_env(uint32_t env) { return (int)(env + 1) << K_ENV_SHIFT; }
+// The rotation loop's unroll factor in the kernels of scene class K.
+__host__ __device__ constexpr int rot_unroll(int K) {
+    return (K != K_ANY && !(K & K_CLEAR)) ? GR_ROT_UNROLL_GENERAL : GR_ROT_UNROLL;
+}
 template <int K> __device__ __forceinline__ bool aniso_k(const SceneConst &S) {
     return (K & K_ISO) ? false : (S.anisotropic != 0);
 }
@@ -714,7 +725,7 @@ __device__ __forceinline__ uint32_t step_hit(Path &P, const SceneConst &S, const
     if (dot(cur_plane, cur_plane) > 1e-6f && dot(prev, prev) > 1e-6f) {
         float psi = signed_psi(prev, cur_plane, kk);
         float2 sc = m_sincos(2.0f * psi);
-#pragma unroll ROT_UNROLL
+#pragma unroll (rot_unroll(K))
         for (int k = 0; k < NCH; ++k) {
             float4 s = P.st[k];
             Stokes r = apply_rotation(Stokes{s.x, s.y, s.z, s.w}, sc.y, sc.x);

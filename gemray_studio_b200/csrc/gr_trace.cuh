@@ -37,7 +37,8 @@ constexpr int NCH = 8;
 // The rotation loop of the general (absorbing or birefringent) scene classes: measured
 // on the c3 emerald at 16 blocks per SM, unrolled by 2 / 4 / 8: 585.5 / 576.3 / 563.6 M
 // path-samples/s, while the clear brilliant wants 8 (1,032.6 against 1,017.2 at 4 and
-// 1,009.6 at 2).
+// 1,009.6 at 2).  The c4 random stones, one at a time at full size, lose 2% at 2 (565
+// against 577 M path-samples/s): the best factor depends on the kernel's code layout.
 #ifndef GR_ROT_UNROLL_GENERAL
 #define GR_ROT_UNROLL_GENERAL 2
 #endif

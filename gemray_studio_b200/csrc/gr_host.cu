@@ -484,9 +484,9 @@ gr_status launch_trace(gr_ctx *ctx, const SceneConst &S, const grd::SceneBuffers
 gr_status launch_fold(const float *xyz, uint32_t n_pixels, uint32_t spp, uint32_t first_pixel, float *film,
                       uint32_t kahan, cudaStream_t stream) {
     if (n_pixels == 0) return GR_OK;
-    const unsigned threads = 256;
-    uint64_t blocks = ((uint64_t)n_pixels * 32 + threads - 1) / threads;
-    grd::k_film_fold<<<(unsigned)blocks, threads, 0, stream>>>(xyz, n_pixels, spp, first_pixel, film, kahan);
+    const uint64_t blocks = ((uint64_t)n_pixels + grd::FOLD_THREADS - 1) / grd::FOLD_THREADS;
+    grd::k_film_fold_tiled<<<(unsigned)blocks, grd::FOLD_THREADS, 0, stream>>>(xyz, n_pixels, spp, first_pixel, film,
+                                                                              kahan);
     GR_CUDA(cudaGetLastError());
     return GR_OK;
 }

@@ -148,6 +148,9 @@ struct gr_ctx {
     // ring of pinned host staging buffers for the table uploads (a pageable source
     // would make each upload wait for the previous batch to reach its copy)
     grh::DeviceBuffer batch_tables, batch_park;  // segment tables; staged park records + slot counters
+    // gr_accumulate's pinned readback buffer (grown, kept)
+    void *host_stage = nullptr;
+    size_t host_stage_cap = 0;
     static constexpr int kStageSlots = 4;
     void *stage_host[kStageSlots] = {};
     size_t stage_cap[kStageSlots] = {};

@@ -773,6 +773,8 @@ gr_status gr_destroy(gr_ctx *ctx) {
         ctx->batch_graphs.clear();
         ctx->batch_tables.release();
         ctx->batch_park.release();
+        if (ctx->host_stage) cudaFreeHost(ctx->host_stage);
+        ctx->host_stage = nullptr;
         for (auto &p : ctx->trace_ev) { cudaEventDestroy(p.first); cudaEventDestroy(p.second); }
         for (auto &p : ctx->fold_ev) { cudaEventDestroy(p.first); cudaEventDestroy(p.second); }
         if (!ctx->tuning_cache.empty()) {
@@ -823,11 +825,19 @@ gr_status gr_accumulate(gr_ctx *ctx, const gr_scene *sc, uint32_t sample_offset,
         cudaStreamSynchronize(ctx->stream);
         return st;
     }
-    // Copy into a staging vector first so a failure leaves accum untouched.
-    std::vector<float> tmp(n_pixels * 3);
-    GR_CUDA(cudaMemcpyAsync(tmp.data(), ctx->film.ptr, fbytes, cudaMemcpyDeviceToHost, ctx->stream));
+    // Copy into the context's pinned staging buffer first (a failure leaves accum
+    // untouched; a pinned target takes the copy at full link speed and is not
+    // allocated and zeroed per call), then into the caller's buffer.
+    if (ctx->host_stage_cap < fbytes) {
+        if (ctx->host_stage) cudaFreeHost(ctx->host_stage);
+        ctx->host_stage = nullptr;
+        ctx->host_stage_cap = 0;
+        GR_CUDA(cudaHostAlloc(&ctx->host_stage, fbytes, cudaHostAllocDefault));
+        ctx->host_stage_cap = fbytes;
+    }
+    GR_CUDA(cudaMemcpyAsync(ctx->host_stage, ctx->film.ptr, fbytes, cudaMemcpyDeviceToHost, ctx->stream));
     GR_CUDA(cudaStreamSynchronize(ctx->stream));
-    std::memcpy(accum, tmp.data(), fbytes);
+    std::memcpy(accum, ctx->host_stage, fbytes);
     return GR_OK;
 }
 

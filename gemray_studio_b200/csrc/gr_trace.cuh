@@ -35,12 +35,12 @@ constexpr int NCH = 8;
 #define GR_RR_UNROLL 4  // measured on the c2 frame: 4 beats 8 / 2 / 1 by 1-3% (code layout)
 #endif
 // The rotation loop of the general (absorbing or birefringent) scene classes: measured
-// on the c3 emerald at 16 blocks per SM, unrolled by 2 / 4 / 8: 585.5 / 576.3 / 563.6 M
-// path-samples/s, while the clear brilliant wants 8 (1,032.6 against 1,017.2 at 4 and
-// 1,009.6 at 2).  The c4 random stones, one at a time at full size, lose 2% at 2 (565
-// against 577 M path-samples/s): the best factor depends on the kernel's code layout.
+// at 16 blocks per SM, unrolled by 2 / 4 / 8, the c3 emerald 585.5 / 580.7 / 563.6 M
+// path-samples/s and the c4 random stones one at a time at full size 571 / 583 / 577 M;
+// the clear brilliant wants 8 (1,032.6 against 1,017.2 at 4 and 1,009.6 at 2).  The best
+// factor follows the kernel's code layout; 4 is the best for both general workloads.
 #ifndef GR_ROT_UNROLL_GENERAL
-#define GR_ROT_UNROLL_GENERAL 2
+#define GR_ROT_UNROLL_GENERAL 4
 #endif
 constexpr int ROT_UNROLL = GR_ROT_UNROLL;
 constexpr int RR_UNROLL = GR_RR_UNROLL;

@@ -7,7 +7,8 @@
 
 // Resident blocks per SM of the class-specialised batched grids.  Measured on B200
 // with the c4 stones (batched path-samples/s at film scales 1/32 and 1/8): 9 blocks
-// 328 M / 428 M, 16 blocks 311 M / 405 M -- unlike the single-scene kernels, these
+// 328 M / 428 M, 16 blocks 311 M / 405 M (another run: 9, 10, 12 blocks 350 / 350 /
+// 345 M and 448 / 447 / 443 M) -- unlike the single-scene kernels, these
 // grids lose more to their spills (the scene constants come from shared memory) than
 // they gain from the extra warps.
 #ifndef GR_BATCH_MIN_BLOCKS

@@ -875,6 +875,12 @@ gr_status gr_submit(gr_ctx *ctx, const gr_request *req, uint64_t *request_id) {
         }
         sv->reqs[q->id] = q;
         *request_id = q->id;
+        if (q->r.kind == GR_REQ_RENDER && q->state == GR_REQ_QUEUED) {
+            // admitted here when its film fits, so a lane render starts without waiting
+            // for a turn of the worker thread (which admits whatever stays queued)
+            cudaSetDevice(ctx->device);
+            admit(ctx, *sv, ctx->resident_bytes);
+        }
     }
     if (q->r.kind == GR_REQ_METRICS)
         sv->cv_metrics.notify_all();

@@ -454,7 +454,12 @@ void lane_main(gr_ctx *ctx, ServeState *sv, ServeState::Lane *lane) {
                 if (i >= 0) {
                     q = sv->reqs[sv->lane_pending[i]];
                     first = q->px_issued;
-                    count = std::min<uint64_t>(std::max<uint64_t>(1, chunk_tuples / q->r.spp), q->n_px - first);
+                    const uint64_t left = q->n_px - first;
+                    count = std::min<uint64_t>(std::max<uint64_t>(1, chunk_tuples / q->r.spp), left);
+                    // a remainder under half a chunk joins this one while the lane's
+                    // scratch holds both: a short last launch costs its own stage tails
+                    if (2 * (left - count) * q->r.spp <= chunk_tuples && left * q->r.spp <= kClassTuples[2])
+                        count = left;
                     q->px_issued += count;
                     q->px_inflight += count;
                     q->issued = q->in_flight = q->r.spp;

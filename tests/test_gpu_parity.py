@@ -381,6 +381,35 @@ def test_tuning_table_round_trip(engine_lib, tmp_path):
     assert open(path).read().splitlines() == lines
 
 
+def test_committed_table_covers_the_benchmark_stones(engine_lib):
+    """The committed B200 schedule table loads on this device and gives the benchmark
+    stones (the c1 / c2 brilliant, the c3 emerald, a c4 stone) their schedule at upload,
+    with no trial calls: the stone keys it was written with still match the scenes."""
+    from pathlib import Path
+
+    from gemray_studio_b200 import GpuFrameRenderer
+    from gemray_studio_b200 import workloads as W
+    table = Path(__file__).resolve().parents[1] / "gemray_studio_b200" / "tuning" / "b200_schedules.txt"
+    r = GpuFrameRenderer()
+    try:
+        n = C.c_uint32()
+        st = r.lib.gr_tuning_load(r.ctx, str(table).encode(), C.byref(n))
+        if st == abi.GR_EINVAL and "B200" not in r.lib.gr_device_label(r.ctx).decode():
+            pytest.skip("the committed table was written for a B200")
+        assert st == abi.GR_OK and n.value >= 3, r.lib.gr_last_error_string()
+        scenes = [W.config_scene("c1")[0], W.config_scene("c3")[0],
+                  W.random_stones(1, seed=0, side=(128, 1024), spp=(32, 512))[0].scene]
+        c1, c2, cb = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        for sc in scenes:
+            sid = C.c_uint64()
+            assert r.lib.gr_scene_upload(r.ctx, C.byref(sc.c_scene()), C.byref(sid)) == abi.GR_OK
+            assert r.lib.gr_scene_schedule(r.ctx, sid.value, C.byref(c1), C.byref(c2), C.byref(cb)) == abi.GR_OK
+            assert (c1.value, c2.value) in abi.SCHEDULE_CAP_PAIRS and cb.value in abi.SCHEDULE_BLOCKS
+            r.lib.gr_scene_release(r.ctx, sid.value)
+    finally:
+        r.close()
+
+
 def test_staged_kernels_bit_identical_when_park_buffers_overflow(engine_lib):
     """A light-trapping stone (n = 3.5): ~16% of paths outlive the first stage cap and
     ~11% the second, more than the park buffers hold (1/8 and 1/32 of a launch's

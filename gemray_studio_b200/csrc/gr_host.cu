@@ -645,7 +645,16 @@ uint64_t stone_key(const gr_scene *sc) {
     if (sc->planes) mix(sc->planes, (size_t)sc->n_planes * sizeof(gr_plane));
     if (sc->finishes) mix(sc->finishes, (size_t)sc->n_planes * sizeof(uint32_t));
     if (sc->material) mix(sc->material, sizeof(gr_material));
-    if (sc->material_ext) mix(sc->material_ext, sizeof(gr_material_ext));
+    if (const gr_material_ext *e = sc->material_ext) {
+        // its values and tables, not its table pointers (which differ between processes)
+        mix(&e->n_absorption, sizeof(e->n_absorption));
+        mix(&e->absorption_nm_first, sizeof(e->absorption_nm_first));
+        mix(&e->absorption_nm_step, sizeof(e->absorption_nm_step));
+        if (e->n_absorption && e->alpha_o_table) mix(e->alpha_o_table, (size_t)e->n_absorption * sizeof(float));
+        if (e->n_absorption && e->alpha_e_table) mix(e->alpha_e_table, (size_t)e->n_absorption * sizeof(float));
+        mix(&e->has_cauchy_e, sizeof(e->has_cauchy_e));
+        mix(e->cauchy_e, sizeof(e->cauchy_e));
+    }
     return h;
 }
 

@@ -135,7 +135,8 @@ struct gr_ctx {
     bool timing = false;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> trace_ev, fold_ev;
     // gr_accumulate's stage-cap choices, keyed by the stone (planes, finishes, material,
-    // depth, flags: what sets the path lengths); cleared past kMaxAccumTunes stones
+    // depth, flags -- what sets the path lengths -- and the environment kind, which
+    // selects the kernels); cleared past kMaxAccumTunes stones
     std::map<uint64_t, StageCapTune> accum_tune;
     static constexpr size_t kMaxAccumTunes = 64;
     // Schedules chosen per stone on this device (measured here, or read from a tuning

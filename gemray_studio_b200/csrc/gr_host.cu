@@ -642,6 +642,7 @@ uint64_t stone_key(const gr_scene *sc) {
     mix(&sc->n_planes, sizeof(sc->n_planes));
     mix(&sc->max_bounces, sizeof(sc->max_bounces));
     mix(&sc->flags, sizeof(sc->flags));
+    mix(&sc->env.mode, sizeof(sc->env.mode));  // the environment kind selects the kernels
     if (sc->planes) mix(sc->planes, (size_t)sc->n_planes * sizeof(gr_plane));
     if (sc->finishes) mix(sc->finishes, (size_t)sc->n_planes * sizeof(uint32_t));
     if (sc->material) mix(sc->material, sizeof(gr_material));

@@ -11,8 +11,8 @@ its timed frames start from the measured choices.
 
     python -m gemray_studio_b200.tuning_table [--out PATH]
 
-The table is keyed by stone (planes, finishes, material, depth, flags), not by view or
-film size.
+The table is keyed by stone (planes, finishes, material, depth, flags, environment
+kind), not by view or film size.
 """
 from __future__ import annotations
 

@@ -708,7 +708,7 @@ gr_status gr_set_kernel(gr_ctx *ctx, uint32_t kernel);
  * SM, runs meanwhile).  Batched launches (gr_render_batch, the request loop) run each
  * scene with its chosen first cap (their continuation stage is uncapped); gr_accumulate
  * and gr_accumulate_device choose the same way per stone (planes, finishes, material,
- * depth and flags; not the view); a frame stream uses its scene's schedule as chosen when
+ * depth, flags and environment kind; not the view); a frame stream uses its scene's schedule as chosen when
  * the stream opened.  Scenes that need the frosted / scattering / biaxial kernels run
  * those at 9 blocks per SM whatever the schedule's target.  gr_scene_stage_caps reports
  * the caps alone. */

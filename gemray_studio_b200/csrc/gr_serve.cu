@@ -932,6 +932,7 @@ gr_status gr_cancel(gr_ctx *ctx, uint64_t id) {
         q->cancel = true;
     }
     sv->cv_work.notify_all();
+    sv->cv_lane.notify_all();  // a lane render cancelled before its first chunk ends there
     return GR_OK;
 }
 

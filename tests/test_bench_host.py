@@ -1,6 +1,7 @@
 """bench.py's host-side bookkeeping, no GPU: which transport a run used (from its launch
-counts), the per-launch DRAM traffic taken from the committed captures, and the HBM
-view's labelled fallback peak."""
+counts), the per-launch DRAM traffic taken from the committed captures, the HBM view's
+labelled fallback peak, and where the stones' schedules come from (the committed table
+or live trials)."""
 from __future__ import annotations
 
 import json
@@ -31,3 +32,33 @@ def test_hbm_view_names_its_peak():
     v = bench.hbm_view(1e6, 10.0, "staged")
     assert v["unit"] == "GB/s" and v["peak"] > 0 and abs(v["frac"] - v["achieved"] / v["peak"]) < 1e-12
     assert "measured" in v["peak_source"] or "fallback" in v["peak_source"]
+
+
+class _FakeLib:
+    """Stands in for the engine library's tuning-table loader."""
+
+    def __init__(self, status: int, n: int = 0, error: bytes = b""):
+        self.status, self.n, self.error, self.paths = status, n, error, []
+
+    def gr_tuning_load(self, ctx, path, n_out):
+        self.paths.append(path)
+        n_out._obj.value = self.n
+        return self.status
+
+    def gr_last_error_string(self):
+        return self.error
+
+
+def test_schedule_source_names_the_committed_table_or_the_trials():
+    from gemray_studio_b200 import abi
+    ok = _FakeLib(abi.GR_OK, n=67)
+    assert bench.load_tuning_table(ok, None).startswith("gemray_studio_b200/tuning/b200_schedules.txt (67 stones)")
+    assert ok.paths == [str(bench.TUNING_TABLE).encode()]
+    foreign = _FakeLib(abi.GR_EINVAL, error=b"not written for this schedule set and device")
+    assert bench.load_tuning_table(foreign, None).startswith("trials (not written")
+    bench._use_tuning_table = False
+    try:
+        off = _FakeLib(abi.GR_OK, n=67)
+        assert bench.load_tuning_table(off, None) == "trials" and off.paths == []
+    finally:
+        bench._use_tuning_table = True
